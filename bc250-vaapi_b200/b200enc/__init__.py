@@ -1,0 +1,302 @@
+"""Python binding of libb200enc.so, the B200 compute-encoder hot path.
+
+The product is the C-ABI library (include/gpu_compute.h, include/b200enc.h);
+this module only loads it with ctypes and moves torch device tensors through
+it, for tests, benchmarks and Python callers. Every compute call goes to the
+CUDA library; there is no CPU or PyTorch fallback, and using the module
+without the built library or without a GPU raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.normpath(os.path.join(HERE, "..", "lib", "libb200enc.so"))
+
+# Every entry point include/*.h declares (checked by the CPU test suite).
+EXPORTS = [
+    # include/b200enc.h
+    "b200enc_me_full_search", "b200enc_p_frame", "b200enc_wavefront_scratch_bytes", "b200enc_i_frame",
+    "b200enc_deblock", "b200enc_wavefront_status", "b200enc_i_frame_launch", "b200enc_deblock_launch",
+    # include/gpu_compute.h
+    "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
+    "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",
+    "gpu_compute_map_surface", "gpu_compute_unmap_surface", "gpu_compute_upload_nv12",
+    "gpu_compute_download_nv12", "gpu_compute_copy_from_wc", "gpu_compute_wait_for_image_ready_host",
+    "gpu_compute_cpu_read_safe", "bc250_debug_dump_open", "gpu_compute_begin_picture",
+    "gpu_compute_dispatch_encode", "gpu_compute_dispatch_encode_ext", "gpu_compute_dispatch_me_only",
+    "gpu_compute_get_last_latency_ms", "gpu_compute_end_picture", "gpu_compute_sync",
+    "gpu_compute_submitted_slot", "gpu_compute_sync_slot", "gpu_compute_get_quant_staging_data_slot",
+    "gpu_compute_get_dc_staging_data_slot", "gpu_compute_get_pred_mode_staging_data_slot",
+    "gpu_compute_get_mv_staging_data_slot", "gpu_compute_get_nz_staging_data_slot",
+    "gpu_compute_get_staging_data", "gpu_compute_release_staging_data", "gpu_compute_get_quant_staging_data",
+    "gpu_compute_get_dc_staging_data", "gpu_compute_get_pred_mode_staging_data",
+    "gpu_compute_get_mv_staging_data", "gpu_compute_get_nz_staging_data", "gpu_compute_debug_dump_recon",
+    "b200enc_ctx_configure", "b200enc_ctx_stream", "b200enc_ctx_recon", "b200enc_ctx_device_outputs",
+    "b200enc_ctx_encode_device", "b200enc_ctx_perf", "b200enc_ctx_perf_read",
+]
+
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_lib = None
+
+
+class GpuImage(ctypes.Structure):
+    _fields_ = [("y_plane", _vp), ("y_view", _vp), ("uv_plane", _vp), ("uv_view", _vp), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32), ("current_layout", _i), ("format", _i), ("pitch", ctypes.c_uint32)]
+
+
+class GpuMemory(ctypes.Structure):
+    _fields_ = [("memory", _vp), ("size", ctypes.c_size_t), ("mapped_ptr", _vp)]
+
+
+class GpuContext(ctypes.Structure):
+    _fields_ = [("recon_image", GpuImage), ("recon_memory", GpuMemory), ("has_recon_frame", ctypes.c_bool),
+                ("any_surface_exported", ctypes.c_bool), ("frame_width", ctypes.c_uint32),
+                ("frame_height", ctypes.c_uint32), ("frames_submitted", ctypes.c_uint32), ("current_buf", _i),
+                ("impl", _vp)]
+
+
+def load_library(path=LIB_PATH):
+    """Loads the library without touching the GPU (works on CPU hosts)."""
+    if not os.path.exists(path):
+        raise RuntimeError(f"libb200enc.so is not built ({path}); run __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    lib.b200enc_wavefront_scratch_bytes.restype = ctypes.c_size_t
+    lib.b200enc_wavefront_scratch_bytes.argtypes = [_i]
+    lib.gpu_compute_get_last_latency_ms.restype = ctypes.c_double
+    lib.b200enc_ctx_stream.restype = _vp
+    lib.b200enc_i_frame.argtypes = [_vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i,
+                                    _vp, ctypes.c_size_t, _i, _vp]
+    lib.b200enc_deblock.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, ctypes.c_size_t, _i, _vp]
+    lib.b200enc_me_full_search.argtypes = [_vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp]
+    lib.b200enc_p_frame.argtypes = [_vp, _vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                    _i, _vp]
+    lib.b200enc_wavefront_status.argtypes = [_vp, _vp]
+    lib.gpu_compute_dispatch_encode_ext.argtypes = [ctypes.POINTER(GpuContext), GpuImage, _i, _i, _i, _i, _i, _i, _vp]
+    lib.gpu_compute_begin_picture.argtypes = [ctypes.POINTER(GpuContext), GpuImage]
+    lib.b200enc_ctx_encode_device.argtypes = [ctypes.POINTER(GpuContext), _vp, _vp, _i, _i, _i, _i, _i, _i, _i]
+    return lib
+
+
+def lib():
+    """The loaded library; raises when it is missing or no GPU is present."""
+    global _lib
+    if _lib is None:
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("b200enc needs a CUDA device (sm_100a); none is available")
+        _lib = load_library()
+    return _lib
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"{what} failed (rc={rc})")
+
+
+def _stream(stream):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return _vp(s.cuda_stream)
+
+
+def coded(W, H):
+    return (W + 15) // 16 * 16, (H + 15) // 16 * 16
+
+
+class NV12:
+    """An NV12 frame in device memory at the coded size, 128-byte pitch."""
+
+    def __init__(self, W, H, device="cuda", pitch=None):
+        import torch
+        self.W, self.H = W, H
+        self.CW, self.CH = coded(W, H)
+        self.pitch = pitch or (self.CW + 127) // 128 * 128
+        self.buf = torch.zeros((self.CH + self.CH // 2, self.pitch), dtype=torch.uint8, device=device)
+        self.y = self.buf[: self.CH]
+        self.uv = self.buf[self.CH:]
+
+    @classmethod
+    def from_host(cls, y, uv, device="cuda"):
+        """y: [H, W] uint8, uv: [H/2, W] uint8 (numpy); pads by edge replication."""
+        import numpy as np
+        import torch
+        H, W = y.shape
+        f = cls(W, H, device)
+        yp = np.pad(y, ((0, f.CH - H), (0, f.pitch - W)), mode="edge")
+        uvp = np.pad(uv, ((0, f.CH // 2 - H // 2), (0, f.pitch - W)), mode="edge")
+        f.y.copy_(torch.from_numpy(yp))
+        f.uv.copy_(torch.from_numpy(uvp))
+        return f
+
+    def yp(self):
+        return _vp(self.y.data_ptr())
+
+    def uvp(self):
+        return _vp(self.uv.data_ptr())
+
+
+class Outputs:
+    """Per-frame outputs in device memory (reference staging layouts)."""
+
+    def __init__(self, W, H, device="cuda"):
+        import torch
+        mbs = ((W + 15) // 16) * ((H + 15) // 16)
+        self.levels = torch.zeros((mbs, 24, 16), dtype=torch.int16, device=device)
+        self.dc = torch.zeros((mbs, 24), dtype=torch.int32, device=device)
+        self.nz = torch.zeros((mbs, 24), dtype=torch.int32, device=device)
+        self.pred_mode = torch.zeros((mbs,), dtype=torch.int32, device=device)
+        self.mv = torch.zeros((mbs, 4), dtype=torch.int32, device=device)
+
+    def host(self):
+        import numpy as np
+        return {"levels": self.levels.cpu().numpy(), "dc": self.dc.cpu().numpy(),
+                "nz": self.nz.cpu().numpy().view(np.uint32), "pred_mode": self.pred_mode.cpu().numpy().view(np.uint32),
+                "mv": self.mv.cpu().numpy()}
+
+
+def _p(t):
+    return _vp(t.data_ptr())
+
+
+def me_full_search(cur, ref, W, H, RW, RH, rng, lam, zero_thresh, mv, stream=None):
+    _check(lib().b200enc_me_full_search(cur.yp(), cur.pitch, ref.yp(), ref.pitch, W, H, RW, RH, rng, lam,
+                                        zero_thresh, _p(mv), _stream(stream)), "b200enc_me_full_search")
+
+
+def p_frame(cur, ref, W, H, RW, RH, qp, mv, out, rec, stream=None):
+    _check(lib().b200enc_p_frame(cur.yp(), cur.uvp(), cur.pitch, ref.yp(), ref.uvp(), ref.pitch, W, H, RW, RH, qp,
+                                 _p(mv), _p(out.levels), _p(out.dc), _p(out.nz), _p(out.pred_mode), rec.yp(),
+                                 rec.uvp(), rec.pitch, _stream(stream)), "b200enc_p_frame")
+
+
+def scratch(mbh, device="cuda"):
+    import torch
+    n = lib().b200enc_wavefront_scratch_bytes(mbh)
+    return torch.zeros((n + 3) // 4, dtype=torch.int32, device=device)
+
+
+def i_frame(cur, W, H, RW, RH, qp, num_slices, out, rec, scr, ctas=0, stream=None):
+    _check(lib().b200enc_i_frame(cur.yp(), cur.uvp(), cur.pitch, W, H, RW, RH, qp, num_slices, _p(out.levels),
+                                 _p(out.dc), _p(out.nz), _p(out.pred_mode), _p(out.mv), rec.yp(), rec.uvp(),
+                                 rec.pitch, _p(scr), scr.numel() * 4, ctas, _stream(stream)), "b200enc_i_frame")
+
+
+def deblock(mbw, mbh, qp, is_intra, nz, mv, rec, scr, ctas=0, stream=None):
+    _check(lib().b200enc_deblock(mbw, mbh, qp, int(is_intra), _p(nz), _p(mv), rec.yp(), rec.uvp(), rec.pitch,
+                                 _p(scr), scr.numel() * 4, ctas, _stream(stream)), "b200enc_deblock")
+
+
+def wavefront_status(scr, stream=None):
+    return lib().b200enc_wavefront_status(_p(scr), _stream(stream))
+
+
+class Context:
+    """The reference's gpu_compute_* boundary (include/gpu_compute.h)."""
+
+    def __init__(self):
+        self.ctx = GpuContext()
+        self.L = lib()
+        _check(self.L.bc250_gpu_init(ctypes.byref(self.ctx)), "bc250_gpu_init")
+
+    def close(self):
+        if self.ctx.impl:
+            self.L.bc250_gpu_destroy(ctypes.byref(self.ctx))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def configure(self, search_range=16, lam=-1, zero_thresh=512, coded_clamp=True, deblock=-1):
+        _check(self.L.b200enc_ctx_configure(ctypes.byref(self.ctx), search_range, lam, zero_thresh,
+                                            int(coded_clamp), deblock), "b200enc_ctx_configure")
+
+    def create_image(self, W, H):
+        img, mem = GpuImage(), GpuMemory()
+        _check(self.L.gpu_compute_create_image(ctypes.byref(self.ctx), W, H, 0, ctypes.byref(img),
+                                               ctypes.byref(mem)), "gpu_compute_create_image")
+        return img, mem
+
+    def destroy_image(self, img, mem):
+        self.L.gpu_compute_destroy_image(ctypes.byref(self.ctx), img, mem)
+
+    def upload(self, img, mem, y, uv):
+        H, W = y.shape
+        _check(self.L.gpu_compute_upload_nv12(ctypes.byref(self.ctx), ctypes.byref(img), mem, _vp(y.ctypes.data),
+                                              y.strides[0], _vp(uv.ctypes.data), uv.strides[0], W, H),
+               "gpu_compute_upload_nv12")
+
+    def encode(self, img, W, H, qp, is_intra, num_slices=1, me_mode=0, cpu_mvs=None):
+        """begin_picture + dispatch_encode_ext + end_picture; returns the slot."""
+        c = ctypes.byref(self.ctx)
+        _check(self.L.gpu_compute_begin_picture(c, img), "gpu_compute_begin_picture")
+        mv = _vp(cpu_mvs.ctypes.data) if cpu_mvs is not None else None
+        _check(self.L.gpu_compute_dispatch_encode_ext(c, img, W, H, qp, int(is_intra), num_slices, me_mode, mv),
+               "gpu_compute_dispatch_encode_ext")
+        _check(self.L.gpu_compute_end_picture(c), "gpu_compute_end_picture")
+        return self.L.gpu_compute_submitted_slot(c)
+
+    def sync(self, slot):
+        return self.L.gpu_compute_sync_slot(ctypes.byref(self.ctx), slot)
+
+    def staging(self, slot):
+        """numpy views of the slot's staging buffers (valid until resubmitted)."""
+        import numpy as np
+        c = ctypes.byref(self.ctx)
+        res = {}
+        for name, fn, dt, shape in (("levels", "gpu_compute_get_quant_staging_data_slot", np.int16, (-1, 24, 16)),
+                                    ("dc", "gpu_compute_get_dc_staging_data_slot", np.int32, (-1, 24)),
+                                    ("pred_mode", "gpu_compute_get_pred_mode_staging_data_slot", np.uint32, (-1,)),
+                                    ("mv", "gpu_compute_get_mv_staging_data_slot", np.int32, (-1, 4)),
+                                    ("nz", "gpu_compute_get_nz_staging_data_slot", np.uint32, (-1, 24))):
+            data, size = _vp(), ctypes.c_size_t()
+            _check(getattr(self.L, fn)(c, slot, ctypes.byref(data), ctypes.byref(size)), fn)
+            buf = (ctypes.c_uint8 * size.value).from_address(data.value)
+            res[name] = np.frombuffer(buf, dtype=dt).reshape(shape)
+        return res
+
+    def recon_host(self):
+        """(y, uv) of the latest reconstruction at the coded size, as numpy."""
+        import torch
+        y, uv, pitch = _vp(), _vp(), _i()
+        _check(self.L.b200enc_ctx_recon(ctypes.byref(self.ctx), ctypes.byref(y), ctypes.byref(uv),
+                                        ctypes.byref(pitch)), "b200enc_ctx_recon")
+        CW, CH = coded(self.ctx.frame_width, self.ctx.frame_height)
+        torch.cuda.synchronize()
+        hy = device_view(y.value, CH * pitch.value).cpu().numpy().reshape(CH, pitch.value)
+        huv = device_view(uv.value, CH // 2 * pitch.value).cpu().numpy().reshape(CH // 2, pitch.value)
+        return hy[:, :CW], huv[:, :CW]
+
+    def perf(self, enable=True):
+        _check(self.L.b200enc_ctx_perf(ctypes.byref(self.ctx), int(enable)), "b200enc_ctx_perf")
+
+    def perf_read(self, intra=False):
+        """Summed stage milliseconds: dict(me, chain, deblock, staging, frames)."""
+        vals = [ctypes.c_double() for _ in range(4)]
+        frames = ctypes.c_long()
+        _check(self.L.b200enc_ctx_perf_read(ctypes.byref(self.ctx), int(intra), *[ctypes.byref(v) for v in vals],
+                                            ctypes.byref(frames)), "b200enc_ctx_perf_read")
+        return dict(me=vals[0].value, chain=vals[1].value, deblock=vals[2].value, staging=vals[3].value,
+                    frames=frames.value)
+
+    def encode_device(self, frame, W, H, qp, is_intra, num_slices=1, stage=False):
+        _check(self.L.b200enc_ctx_encode_device(ctypes.byref(self.ctx), frame.yp(), frame.uvp(), frame.pitch, W, H,
+                                                qp, int(is_intra), num_slices, int(stage)),
+               "b200enc_ctx_encode_device")
+
+    def stream(self):
+        return self.L.b200enc_ctx_stream(ctypes.byref(self.ctx))
+
+
+class _DeviceSpan:
+    def __init__(self, ptr, nbytes):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def device_view(ptr, nbytes):
+    """A uint8 torch tensor aliasing library-owned device memory (no copy)."""
+    import torch
+    return torch.as_tensor(_DeviceSpan(ptr, nbytes), device="cuda")

@@ -1,0 +1,8 @@
+// b200enc_internal.h - declarations shared by the library's translation
+// units. The public C-ABI is include/b200enc.h (stage entry points) and
+// include/gpu_compute.h (the reference's drop-in boundary).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/b200enc.h"

@@ -1,0 +1,224 @@
+// common.cuh - shared device helpers for the b200enc kernels (sm_100a).
+//
+// Integer arithmetic of the H.264 compute-encoder stages, written for warp
+// execution: a 4x4 transform block is owned by a quad of lanes (one lane per
+// row), quads exchange rows/columns through shared memory, and every table
+// lives in __constant__ memory. The math is the reference's
+// (A1 = approach1-compute-encoder):
+//   forward 4x4     A1/shaders/dct_transform.comp:34-73
+//   AC quant        A1/shaders/quantize.comp:151-225
+//   dequant/inverse A1/shaders/reconstruct.comp:124-177
+//   DC paths        A1/src/encoder_h264.c:653-797, reconstruct.comp:179-299
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace b200enc {
+
+struct MV {
+  int32_t mvx, mvy;  // quarter-pel
+  uint32_t sad, pad;
+};
+static_assert(sizeof(MV) == 16, "MV must match the reference's 16-byte gpu_mv_t");
+
+// Geometry of one frame. Source reads clamp to (W, H); reference/recon reads
+// clamp to (RW, RH) and recon writes stop there. RW/RH = W/H is the
+// reference shaders' behaviour; RW/RH = coded size is a conforming decoder's.
+struct Geo {
+  int W, H, RW, RH, mbw, mbh;
+};
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+__device__ __forceinline__ int clip1(int v) { return clampi(v, 0, 255); }
+
+__device__ __forceinline__ int chroma_qp(int qpy) {
+  // A1/shaders/quantize.comp:182-187 (Table 8-15, offset 0)
+  if (qpy < 30) return qpy;
+  const int i = qpy - 30;
+  const int t = i < 22 ? i : 21;
+  switch (t) {
+    case 0: return 29; case 1: return 30; case 2: return 31; case 3: return 32; case 4: return 32;
+    case 5: return 33; case 6: return 34; case 7: return 34; case 8: return 35; case 9: return 35;
+    case 10: return 36; case 11: return 36; case 12: return 37; case 13: return 37; case 14: return 37;
+    case 15: return 38; case 16: return 38; case 17: return 38; default: return 39;
+  }
+}
+
+// Position class of raster index p in a 4x4 block: 0 both even, 1 both odd,
+// 2 mixed (A1/shaders/quantize.comp:160-168).
+__device__ __forceinline__ int pos_type(int p) {
+  const int r = (p >> 2) & 1, c = p & 1;
+  return (r & c) ? 1 : ((r | c) ? 2 : 0);
+}
+
+// MF (A1/shaders/quantize.comp:151-158), V (A1/shaders/reconstruct.comp:
+// 124-131) and the DC level scale (reconstruct.comp:92), indexed
+// [qp%6][position class].
+static __constant__ int kMF[6][3] = {{13107, 5243, 8066}, {11916, 4660, 7490}, {10082, 4194, 6554},
+                                     {9362, 3647, 5825},  {8192, 3355, 5243},  {7282, 2893, 4559}};
+static __constant__ int kV[6][3] = {{10, 16, 13}, {11, 18, 14}, {13, 20, 16},
+                                    {14, 23, 18}, {16, 25, 20}, {18, 29, 23}};
+static __constant__ int kDcLs[6] = {160, 176, 208, 224, 256, 288};
+
+__device__ __forceinline__ int mf_of(int rem, int pt) { return kMF[rem][pt]; }
+__device__ __forceinline__ int v_of(int rem, int pt) { return kV[rem][pt]; }
+__device__ __forceinline__ int dc_ls(int rem) { return kDcLs[rem]; }
+
+// Quantizer constants for one QP, computed once per thread.
+struct QP {
+  int per, rem, f_shift, f;  // f = rounding offset of the AC quantizer
+};
+__device__ __forceinline__ QP make_qp(int qp, bool intra) {
+  QP q;
+  q.per = qp / 6;
+  q.rem = qp - 6 * q.per;
+  q.f_shift = 15 + q.per;
+  q.f = (1 << q.f_shift) / (intra ? 3 : 6);
+  return q;
+}
+
+__device__ __forceinline__ int quant_ac(int c, int pos, const QP& q) {
+  const int a = c < 0 ? -c : c;
+  const int l = (a * mf_of(q.rem, pos_type(pos)) + q.f) >> q.f_shift;
+  return c < 0 ? -l : l;
+}
+__device__ __forceinline__ int dequant_ac(int level, int pos, const QP& q) {
+  const int scale = 16 * v_of(q.rem, pos_type(pos));
+  if (q.per >= 4) return (level * scale) << (q.per - 4);
+  return (level * scale + (1 << (3 - q.per))) >> (4 - q.per);
+}
+
+__device__ __forceinline__ int quantize_dc(int v, const QP& q) {
+  // A1/src/encoder_h264.c:653-709 (luma and chroma bodies are identical)
+  const int ls = dc_ls(q.rem);
+  const int a = v < 0 ? -v : v;
+  int num, den;
+  if (q.per >= 5) { num = a; den = ls << (q.per - 5); }
+  else { num = a << (5 - q.per); den = ls; }
+  const int l = (num + den / 2) / den;
+  return v < 0 ? -l : l;
+}
+__device__ __forceinline__ int dequant_dc_luma(int f, const QP& q) {
+  const int ls = dc_ls(q.rem);
+  if (q.per >= 6) return (f * ls) << (q.per - 6);
+  return (f * ls + (1 << (5 - q.per))) >> (6 - q.per);
+}
+__device__ __forceinline__ int dequant_dc_chroma(int f, const QP& q) {
+  const int ls = dc_ls(q.rem);
+  if (q.per >= 5) return (f * ls) << (q.per - 5);
+  return (f * ls) >> (5 - q.per);
+}
+
+// 1-D forward butterfly (dct_transform.comp:45-53).
+__device__ __forceinline__ void fwd4(int& x0, int& x1, int& x2, int& x3) {
+  const int a0 = x0 + x3, a1 = x1 + x2, a2 = x1 - x2, a3 = x0 - x3;
+  x0 = a0 + a1;
+  x1 = (a3 << 1) + a2;
+  x2 = a0 - a1;
+  x3 = a3 - (a2 << 1);
+}
+// 1-D inverse butterfly (reconstruct.comp:168-169).
+__device__ __forceinline__ void inv4(int& x0, int& x1, int& x2, int& x3) {
+  const int z0 = x0 + x2, z1 = x0 - x2, z2 = (x1 >> 1) - x3, z3 = x1 + (x3 >> 1);
+  x0 = z0 + z3;
+  x1 = z1 + z2;
+  x2 = z1 - z2;
+  x3 = z0 - z3;
+}
+
+// Slice index of macroblock mb (A1/shaders/residual_predict.comp:163-171).
+__device__ __forceinline__ uint32_t slice_of(uint32_t mb, uint32_t total, uint32_t ns) {
+  if (ns <= 1u || total == 0u) return 0u;
+  uint32_t s = (mb * ns) / total;
+  if (s >= ns) s = ns - 1u;
+  while (s + 1u < ns && ((s + 1u) * total) / ns <= mb) s++;
+  while (s > 0u && (s * total) / ns > mb) s--;
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// Quad (4-lane) transform block pipeline.
+//
+// Lane `r` of a quad owns row r of one 4x4 block. `sm` is that block's
+// 16-int shared scratch (raster). Functions leave results in registers;
+// callers fence with __syncwarp (every quad of a block sits in one warp).
+// ---------------------------------------------------------------------------
+
+// Forward 4x4 of the residual row x[0..3] held by lane r. Returns column r
+// of the coefficients: c[i] = coef[i][r]. Rows then columns, like
+// dct_transform.comp; the forward transform is exact so order is moot.
+__device__ __forceinline__ void quad_forward(int x[4], int r, int* sm) {
+  fwd4(x[0], x[1], x[2], x[3]);
+  sm[4 * r + 0] = x[0];
+  sm[4 * r + 1] = x[1];
+  sm[4 * r + 2] = x[2];
+  sm[4 * r + 3] = x[3];
+  __syncwarp();
+  x[0] = sm[r];
+  x[1] = sm[4 + r];
+  x[2] = sm[8 + r];
+  x[3] = sm[12 + r];
+  __syncwarp();
+  fwd4(x[0], x[1], x[2], x[3]);
+}
+
+// Inverse 4x4 of the dequantized row d[0..3] (lane r holds row r, +32 already
+// on d[0][0]); returns column r of the residual: out[i] = res[i][r]
+// (reconstruct.comp:162-177: rows first, then columns, >>6).
+__device__ __forceinline__ void quad_inverse(int d[4], int r, int* sm) {
+  inv4(d[0], d[1], d[2], d[3]);
+  sm[4 * r + 0] = d[0];
+  sm[4 * r + 1] = d[1];
+  sm[4 * r + 2] = d[2];
+  sm[4 * r + 3] = d[3];
+  __syncwarp();
+  d[0] = sm[r];
+  d[1] = sm[4 + r];
+  d[2] = sm[8 + r];
+  d[3] = sm[12 + r];
+  __syncwarp();
+  inv4(d[0], d[1], d[2], d[3]);
+  d[0] >>= 6;
+  d[1] >>= 6;
+  d[2] >>= 6;
+  d[3] >>= 6;
+}
+
+// Error codes written by the wavefront kernels' bounded waits.
+enum : uint32_t {
+  kErrNone = 0,
+  kErrWaitTimeout = 1,
+};
+
+// Bounded acquire-wait until *flag >= target. Returns false on timeout.
+__device__ __forceinline__ bool wait_at_least(const uint32_t* flag, uint32_t target, uint32_t max_iters) {
+  uint32_t v;
+  for (uint32_t it = 0; it < max_iters; ++it) {
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+    if (v >= target) return true;
+    if (it > 8) __nanosleep(64);
+  }
+  return false;
+}
+__device__ __forceinline__ void store_release(uint32_t* flag, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t load_acquire(const uint32_t* flag) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+  return v;
+}
+
+// Scratch layout of the wavefront kernels (one region per launch):
+//   [0] ticket counter, [1] error code, [2] error detail, [3] reserved,
+//   [4 .. 4+mbh) per-row progress (macroblocks done in that row).
+struct Scratch {
+  uint32_t* base;
+  __device__ uint32_t* ticket() const { return base; }
+  __device__ uint32_t* err() const { return base + 1; }
+  __device__ uint32_t* err_detail() const { return base + 2; }
+  __device__ uint32_t* progress(int row) const { return base + 4 + row; }
+};
+inline size_t scratch_words(int mbh) { return 4 + (size_t)mbh; }
+
+}  // namespace b200enc

@@ -1,0 +1,385 @@
+// intra.cu - I-frame intra wavefront as ONE persistent kernel.
+//
+// Reference: A1/shaders/intra_wavefront.comp:398-756, dispatched once per
+// anti-diagonal with a barrier between dispatches (A1/src/gpu_compute.c:
+// 3238-3249: 187 dispatches for a 1080p frame). An I16x16 macroblock needs
+// only its left, top and top-left neighbours' reconstruction, so here each
+// CTA takes a whole macroblock row by ticket (atomicAdd; a ticket is only
+// taken by a running CTA, so rows are always owned by resident CTAs and the
+// wait below cannot deadlock whatever the grid size), walks it left to
+// right, and before macroblock x waits until row y-1 has published
+// progress > x. Waits are bounded: on timeout the CTA records an error in
+// the scratch and returns; every waiter also gives up as soon as it sees a
+// recorded error.
+//
+// Within a macroblock the work is the reference's, laid out for warps:
+// 96 threads, each 4x4 block owned by a lane quad (luma blocks in warps
+// 0-1, chroma in warp 2), the 4x4 luma DC Hadamard done by 16 lanes as
+// signed 16-term sums.
+#include "b200enc_internal.h"
+#include "common.cuh"
+
+namespace b200enc {
+
+struct IShared {
+  int top[16], left[16], corner;
+  int tuv[2][8], luv[2][8];
+  int sad[4][3];
+  int mode, dcv, pa, pb, pc, top_av, left_av;
+  int row;
+  int abort_flag;
+  int16_t src[16][16];
+  int16_t srcc[2][8][8];
+  int16_t pred[24][16];
+  int32_t tsm[24][16];
+  alignas(16) int16_t lev[24][16];
+  int32_t ldc[16];     // pre-quant luma DC coefficients (block raster)
+  int32_t ldl[16];     // quantized luma DC (natural order)
+  int32_t ldcval[16];  // dequantized luma DC per block
+  int32_t cdc[8];
+  int32_t cdcval[8];
+  alignas(16) uint8_t ry[16][16];
+  alignas(16) uint8_t ruv[8][16];
+};
+
+__device__ __forceinline__ int hsign(int row, int idx) {
+  // sign of element idx in row `row` of the butterfly used by
+  // luma_dc_hadamard (A1/src/encoder_h264.c:711-730): rows
+  // [+ + + +], [+ + - -], [+ - - +], [+ - + -]
+  const int m = row == 0 ? 0x0 : (row == 1 ? 0xC : (row == 2 ? 0x6 : 0xA));
+  return ((m >> idx) & 1) ? -1 : 1;
+}
+
+__global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__ cur_y,
+                                                     const uint8_t* __restrict__ cur_uv, int cur_pitch, Geo g,
+                                                     int qp, int num_slices, int16_t* __restrict__ levels,
+                                                     int32_t* __restrict__ dc, uint32_t* __restrict__ nzm,
+                                                     uint32_t* __restrict__ pred_mode, MV* __restrict__ mvs,
+                                                     uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch,
+                                                     uint32_t* scratch, uint32_t max_wait) {
+  __shared__ IShared s;
+  const Scratch sc{scratch};
+  const int tid = threadIdx.x;
+  const int b = tid >> 2, r = tid & 3;
+  const bool luma = b < 16;
+  const QP ql = make_qp(qp, true), qc = make_qp(chroma_qp(qp), true);
+  const QP& q = luma ? ql : qc;
+  const uint32_t total = (uint32_t)(g.mbw * g.mbh);
+  const int rmx = g.RW - 1, rmy = g.RH - 1, cmx = g.RW / 2 - 1, cmy = g.RH / 2 - 1;
+
+  for (;;) {
+    if (tid == 0) {
+      s.row = (int)atomicAdd(sc.ticket(), 1u);
+      s.abort_flag = 0;
+    }
+    __syncthreads();
+    const int mby = s.row;
+    if (mby >= g.mbh) return;
+    for (int mbx = 0; mbx < g.mbw; ++mbx) {
+      const int mb = mby * g.mbw + mbx, X = mbx * 16, Y = mby * 16, Xc = X >> 1, Yc = Y >> 1;
+      // ---- wait for the top neighbour ----------------------------------
+      if (tid == 0 && mby > 0) {
+        const uint32_t* pf = sc.progress(mby - 1);
+        bool ok = false;
+        for (uint32_t it = 0; it < max_wait; ++it) {
+          if (load_acquire(pf) >= (uint32_t)(mbx + 1)) { ok = true; break; }
+          if (load_acquire(sc.err()) != 0u) break;
+          if (it > 4) __nanosleep(32);
+        }
+        if (!ok) {
+          if (atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u) atomicExch(sc.err_detail(), (uint32_t)mb);
+          s.abort_flag = 1;
+        }
+      }
+      __syncthreads();
+      if (s.abort_flag) return;
+
+      // ---- neighbours (reconstructed, read from L2) and source ----------
+      const uint32_t sl = slice_of((uint32_t)mb, total, (uint32_t)num_slices);
+      const bool top_exists = mby > 0, left_exists = mbx > 0;
+      const bool top_av = top_exists && slice_of((uint32_t)(mb - g.mbw), total, (uint32_t)num_slices) == sl;
+      const bool left_av = left_exists && slice_of((uint32_t)(mb - 1), total, (uint32_t)num_slices) == sl;
+      if (tid < 16) {
+        s.top[tid] = top_exists ? __ldcg(rec_y + (size_t)clampi(Y - 1, 0, rmy) * rec_pitch + clampi(X + tid, 0, rmx)) : 128;
+      } else if (tid < 32) {
+        const int i = tid - 16;
+        s.left[i] = left_exists ? __ldcg(rec_y + (size_t)clampi(Y + i, 0, rmy) * rec_pitch + clampi(X - 1, 0, rmx)) : 128;
+      } else if (tid < 48) {
+        const int i = tid - 32, pl = i >> 3, k = i & 7;
+        s.tuv[pl][k] = top_av ? __ldcg(rec_uv + (size_t)clampi(Yc - 1, 0, cmy) * rec_pitch + 2 * clampi(Xc + k, 0, cmx) + pl) : 128;
+      } else if (tid < 64) {
+        const int i = tid - 48, pl = i >> 3, k = i & 7;
+        s.luv[pl][k] = left_av ? __ldcg(rec_uv + (size_t)clampi(Yc + k, 0, cmy) * rec_pitch + 2 * clampi(Xc - 1, 0, cmx) + pl) : 128;
+      } else if (tid == 64) {
+        s.corner = (top_exists && left_exists) ? __ldcg(rec_y + (size_t)clampi(Y - 1, 0, rmy) * rec_pitch + clampi(X - 1, 0, rmx)) : 128;
+      }
+      for (int i = tid; i < 256; i += 96)
+        s.src[i >> 4][i & 15] = __ldg(cur_y + (size_t)clampi(Y + (i >> 4), 0, g.H - 1) * cur_pitch + clampi(X + (i & 15), 0, g.W - 1));
+      for (int i = tid; i < 128; i += 96) {
+        const int pl = i >> 6, y = (i >> 3) & 7, x = i & 7;
+        s.srcc[pl][y][x] = __ldg(cur_uv + (size_t)clampi(Yc + y, 0, g.H / 2 - 1) * cur_pitch + 2 * clampi(Xc + x, 0, g.W / 2 - 1) + pl);
+      }
+      __syncthreads();
+
+      // ---- I16x16 candidates (intra_wavefront.comp:454-476) -------------
+      if (tid < 32) {
+        // lane-parallel sums; lane 0 finishes
+        int st = tid < 16 ? s.top[tid] : 0, sl2 = tid < 16 ? s.left[tid] : 0;
+        int hterm = 0, vterm = 0;
+        if (tid < 8) {
+          const int l = (6 - tid >= 0) ? s.top[6 - tid] : s.corner;
+          hterm = (tid + 1) * (s.top[8 + tid] - l);
+          const int a = (6 - tid >= 0) ? s.left[6 - tid] : s.corner;
+          vterm = (tid + 1) * (s.left[8 + tid] - a);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          st += __shfl_xor_sync(0xffffffffu, st, o);
+          sl2 += __shfl_xor_sync(0xffffffffu, sl2, o);
+          hterm += __shfl_xor_sync(0xffffffffu, hterm, o);
+          vterm += __shfl_xor_sync(0xffffffffu, vterm, o);
+        }
+        if (tid == 0) {
+          int dcv;
+          if (top_av && left_av) dcv = (st + sl2 + 16) >> 5;
+          else if (top_av) dcv = (st + 8) >> 4;
+          else if (left_av) dcv = (sl2 + 8) >> 4;
+          else dcv = 128;
+          s.dcv = dcv;
+          if (top_av && left_av) {
+            s.pa = 16 * (s.left[15] + s.top[15]);
+            s.pb = (5 * hterm + 32) >> 6;
+            s.pc = (5 * vterm + 32) >> 6;
+          } else {
+            s.pa = s.pb = s.pc = 0;
+          }
+        }
+      }
+      __syncthreads();
+      {
+        uint32_t sdc = 0, sv = 0, shh = 0, spl = 0;
+        for (int i = tid; i < 256; i += 96) {
+          const int x = i & 15, y = i >> 4, v = s.src[y][x];
+          sdc += (uint32_t)abs(v - s.dcv);
+          if (top_av) sv += (uint32_t)abs(v - s.top[x]);
+          if (left_av) shh += (uint32_t)abs(v - s.left[y]);
+          if (top_av && left_av) spl += (uint32_t)abs(v - clip1((s.pa + s.pb * (x - 7) + s.pc * (y - 7) + 16) >> 5));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          sdc += __shfl_xor_sync(0xffffffffu, sdc, o);
+          sv += __shfl_xor_sync(0xffffffffu, sv, o);
+          shh += __shfl_xor_sync(0xffffffffu, shh, o);
+          spl += __shfl_xor_sync(0xffffffffu, spl, o);
+        }
+        if ((tid & 31) == 0) {
+          s.sad[0][tid >> 5] = (int)sdc;
+          s.sad[1][tid >> 5] = (int)sv;
+          s.sad[2][tid >> 5] = (int)shh;
+          s.sad[3][tid >> 5] = (int)spl;
+        }
+      }
+      __syncthreads();
+      if (tid == 0) {
+        const uint32_t sdc = s.sad[0][0] + s.sad[0][1] + s.sad[0][2], sv = s.sad[1][0] + s.sad[1][1] + s.sad[1][2];
+        const uint32_t shh = s.sad[2][0] + s.sad[2][1] + s.sad[2][2], spl = s.sad[3][0] + s.sad[3][1] + s.sad[3][2];
+        uint32_t best = sdc;
+        int mode = 2;
+        if (top_av && sv < best) { best = sv; mode = 0; }
+        if (left_av && shh < best) { best = shh; mode = 1; }
+        if (top_av && left_av && spl < best) { best = spl; mode = 3; }
+        s.mode = mode;
+        pred_mode[mb] = (uint32_t)mode;  // chroma mode bits 2-3 = 0 (DC)
+        mvs[mb] = MV{0, 0, 0u, 0u};
+      }
+      __syncthreads();
+
+      // ---- predictions -------------------------------------------------
+      const int mode = s.mode;
+      for (int i = tid; i < 256; i += 96) {
+        const int x = i & 15, y = i >> 4;
+        int pv;
+        if (mode == 0) pv = s.top[x];
+        else if (mode == 1) pv = s.left[y];
+        else if (mode == 3) pv = clip1((s.pa + s.pb * (x - 7) + s.pc * (y - 7) + 16) >> 5);
+        else pv = s.dcv;
+        s.pred[(y >> 2) * 4 + (x >> 2)][(y & 3) * 4 + (x & 3)] = (int16_t)pv;
+      }
+      if (tid < 8) {
+        // chroma DC predictor per plane and sub-block (intra_wavefront.comp:612-641)
+        const int pl = tid >> 2, sub = tid & 3;
+        const int t0 = s.tuv[pl][0] + s.tuv[pl][1] + s.tuv[pl][2] + s.tuv[pl][3];
+        const int t1 = s.tuv[pl][4] + s.tuv[pl][5] + s.tuv[pl][6] + s.tuv[pl][7];
+        const int l0 = s.luv[pl][0] + s.luv[pl][1] + s.luv[pl][2] + s.luv[pl][3];
+        const int l1 = s.luv[pl][4] + s.luv[pl][5] + s.luv[pl][6] + s.luv[pl][7];
+        int v;
+        if (sub == 0) v = (top_av && left_av) ? (t0 + l0 + 4) >> 3 : top_av ? (t0 + 2) >> 2 : left_av ? (l0 + 2) >> 2 : 128;
+        else if (sub == 1) v = top_av ? (t1 + 2) >> 2 : left_av ? (l0 + 2) >> 2 : 128;
+        else if (sub == 2) v = left_av ? (l1 + 2) >> 2 : top_av ? (t0 + 2) >> 2 : 128;
+        else v = (top_av && left_av) ? (t1 + l1 + 4) >> 3 : top_av ? (t1 + 2) >> 2 : left_av ? (l1 + 2) >> 2 : 128;
+        s.cdcval[tid] = v;  // temporarily: the predictor value of block 16+tid
+      }
+      __syncthreads();
+      if (!luma) {
+        const int pv = s.cdcval[b - 16];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) s.pred[b][4 * r + i] = (int16_t)pv;
+      }
+
+      // ---- forward + AC quant (position 0 is carried by the DC paths) ----
+      int x[4];
+      if (luma) {
+        const int bx = b & 3, by = b >> 2;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) x[i] = s.src[4 * by + r][4 * bx + i] - s.pred[b][4 * r + i];
+      } else {
+        const int pl = (b - 16) >> 2, sub = (b - 16) & 3;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) x[i] = s.srcc[pl][4 * (sub >> 1) + r][4 * (sub & 1) + i] - s.pred[b][4 * r + i];
+      }
+      quad_forward(x, r, s.tsm[b]);  // x[i] = coef[i][r]
+      uint32_t nz = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int pos = 4 * i + r;
+        const int l = pos == 0 ? 0 : quant_ac(x[i], pos, q);
+        s.lev[b][pos] = (int16_t)clampi(l, -32768, 32767);
+        nz |= (l != 0 ? 1u : 0u) << pos;
+      }
+      nz |= __shfl_xor_sync(0xffffffffu, nz, 1);
+      nz |= __shfl_xor_sync(0xffffffffu, nz, 2);
+      if (r == 0) {
+        nzm[(size_t)mb * 24 + b] = nz;
+        dc[(size_t)mb * 24 + b] = x[0];
+        if (luma) s.ldc[b] = x[0];
+        else s.cdc[b - 16] = x[0];
+      }
+      __syncthreads();
+
+      // ---- DC paths ----------------------------------------------------
+      if (tid < 16) {
+        // luma: out[i][k] = (sum_ab h_k(a) h_i(b) in[a][b] + 1) >> 1, quantize
+        const int i = tid >> 2, k = tid & 3;
+        int sum = 0;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int bb = 0; bb < 4; ++bb) sum += hsign(k, a) * hsign(i, bb) * s.ldc[4 * a + bb];
+        s.ldl[tid] = quantize_dc((sum + 1) >> 1, ql);
+      } else if (tid == 64 || tid == 80) {
+        const int pl = (tid - 64) >> 4;
+        const int c0 = s.cdc[4 * pl], c1 = s.cdc[4 * pl + 1], c2 = s.cdc[4 * pl + 2], c3 = s.cdc[4 * pl + 3];
+        const int l0 = quantize_dc(c0 + c1 + c2 + c3, qc), l1 = quantize_dc(c0 - c1 + c2 - c3, qc);
+        const int l2 = quantize_dc(c0 + c1 - c2 - c3, qc), l3 = quantize_dc(c0 - c1 - c2 + c3, qc);
+        s.cdcval[4 * pl + 0] = dequant_dc_chroma(l0 + l1 + l2 + l3, qc);
+        s.cdcval[4 * pl + 1] = dequant_dc_chroma(l0 - l1 + l2 - l3, qc);
+        s.cdcval[4 * pl + 2] = dequant_dc_chroma(l0 + l1 - l2 - l3, qc);
+        s.cdcval[4 * pl + 3] = dequant_dc_chroma(l0 - l1 - l2 + l3, qc);
+      }
+      __syncwarp();
+      if (tid < 16) {
+        const int i = tid >> 2, k = tid & 3;
+        int f = 0;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int bb = 0; bb < 4; ++bb) f += hsign(k, a) * hsign(i, bb) * s.ldl[4 * a + bb];
+        s.ldcval[tid] = dequant_dc_luma(f, ql);
+      }
+      __syncthreads();
+
+      // ---- dequant + inverse + recon -----------------------------------
+      int d[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) d[i] = dequant_ac(s.lev[b][4 * r + i], 4 * r + i, q);
+      if (r == 0) d[0] = (luma ? s.ldcval[b] : s.cdcval[b - 16]) + 32;
+      quad_inverse(d, r, s.tsm[b]);
+      if (luma) {
+        const int bx = b & 3, by = b >> 2;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) s.ry[4 * by + i][4 * bx + r] = (uint8_t)clip1(s.pred[b][4 * i + r] + d[i]);
+      } else {
+        const int pl = (b - 16) >> 2, sub = (b - 16) & 3;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          s.ruv[4 * (sub >> 1) + i][2 * (4 * (sub & 1) + r) + pl] = (uint8_t)clip1(s.pred[b][4 * i + r] + d[i]);
+      }
+      __syncthreads();
+
+      // ---- stores + publish progress ------------------------------------
+      if (tid < 48) {
+        reinterpret_cast<uint4*>(levels + (size_t)mb * 384)[tid] = reinterpret_cast<const uint4*>(&s.lev[0][0])[tid];
+      } else if (tid < 64) {
+        const int row = tid - 48, gy = Y + row;
+        if (gy < g.RH) {
+          uint8_t* dst = rec_y + (size_t)gy * rec_pitch + X;
+          if (X + 16 <= g.RW) __stcg(reinterpret_cast<uint4*>(dst), *reinterpret_cast<const uint4*>(s.ry[row]));
+          else
+            for (int c = 0; c < 16 && X + c < g.RW; ++c) dst[c] = s.ry[row][c];
+        }
+      } else if (tid < 72) {
+        const int row = tid - 64, gy = Yc + row;
+        if (gy <= cmy) {
+          uint8_t* dst = rec_uv + (size_t)gy * rec_pitch + X;
+          if (Xc + 8 <= cmx + 1) __stcg(reinterpret_cast<uint4*>(dst), *reinterpret_cast<const uint4*>(s.ruv[row]));
+          else
+            for (int c = 0; c < 8 && Xc + c <= cmx; ++c) {
+              dst[2 * c] = s.ruv[row][2 * c];
+              dst[2 * c + 1] = s.ruv[row][2 * c + 1];
+            }
+        }
+      }
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) store_release(sc.progress(mby), (uint32_t)(mbx + 1));
+    }
+  }
+}
+
+}  // namespace b200enc
+
+using namespace b200enc;
+
+extern "C" size_t b200enc_wavefront_scratch_bytes(int mbh) { return scratch_words(mbh < 1 ? 1 : mbh) * sizeof(uint32_t); }
+
+extern "C" int b200enc_wavefront_status(const void* scratch, void* stream) {
+  if (!scratch) return -1;
+  uint32_t e = 0;
+  if (cudaMemcpyAsync(&e, (const uint32_t*)scratch + 1, sizeof(e), cudaMemcpyDeviceToHost, (cudaStream_t)stream) !=
+      cudaSuccess)
+    return -1;
+  if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return -1;
+  return e == 0 ? 0 : 1;
+}
+
+// Upper bound on polls of one progress word before a wavefront CTA gives up
+// (each poll is an L2 round trip plus a short sleep: well over a second).
+static constexpr uint32_t kMaxWaitPolls = 1u << 22;
+
+extern "C" int b200enc_i_frame_launch(const uint8_t* cur_y, const uint8_t* cur_uv, int cur_pitch, int W, int H,
+                                      int RW, int RH, int qp, int num_slices, int16_t* levels, int32_t* dc,
+                                      uint32_t* nz, uint32_t* pred_mode, void* mv, uint8_t* rec_y, uint8_t* rec_uv,
+                                      int rec_pitch, uint32_t* scratch, int ctas, uint32_t max_wait, void* stream) {
+  Geo g{W, H, RW, RH, (W + 15) / 16, (H + 15) / 16};
+  if (ctas <= 0) ctas = g.mbh;
+  if (ctas > g.mbh) ctas = g.mbh;
+  i_frame_kernel<<<ctas, 96, 0, (cudaStream_t)stream>>>(cur_y, cur_uv, cur_pitch, g, qp, num_slices, levels, dc, nz,
+                                                       pred_mode, (MV*)mv, rec_y, rec_uv, rec_pitch, scratch,
+                                                       max_wait);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int b200enc_i_frame(const uint8_t* cur_y, const uint8_t* cur_uv, int cur_pitch, int W, int H, int RW,
+                               int RH, int qp, int num_slices, int16_t* levels, int32_t* dc, uint32_t* nz,
+                               uint32_t* pred_mode, void* mv, uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch,
+                               void* scratch, size_t scratch_bytes, int ctas, void* stream) {
+  if (!cur_y || !cur_uv || !levels || !dc || !nz || !pred_mode || !mv || !rec_y || !rec_uv || !scratch) return -1;
+  if (qp < 0 || qp > 51 || W <= 0 || H <= 0 || RW <= 1 || RH <= 1 || num_slices < 1) return -1;
+  if ((rec_pitch & 15) || (((uintptr_t)rec_y) & 15) || (((uintptr_t)rec_uv) & 15) || (((uintptr_t)levels) & 15))
+    return -1;
+  const int mbh = (H + 15) / 16;
+  if (scratch_bytes < b200enc_wavefront_scratch_bytes(mbh)) return -1;
+  if (cudaMemsetAsync(scratch, 0, b200enc_wavefront_scratch_bytes(mbh), (cudaStream_t)stream) != cudaSuccess) return -1;
+  return b200enc_i_frame_launch(cur_y, cur_uv, cur_pitch, W, H, RW, RH, qp, num_slices, levels, dc, nz, pred_mode, mv,
+                                rec_y, rec_uv, rec_pitch, (uint32_t*)scratch, ctas, kMaxWaitPolls, stream);
+}

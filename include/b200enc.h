@@ -1,0 +1,115 @@
+/*
+ * b200enc.h - stage-level C-ABI of the B200 compute-encoder hot path.
+ *
+ * Every pointer argument named *_y, *_uv, levels, dc, nz, pred_mode, mv,
+ * rec_* and scratch is DEVICE memory; `stream` is a cudaStream_t passed as
+ * void* (NULL = legacy default stream). Planes are 8-bit: luma with a byte
+ * pitch, chroma NV12-interleaved (CbCr pairs) with the same pitch. Each call
+ * only enqueues work and returns 0, or -1 when an argument is rejected or the
+ * launch fails; nothing here allocates. Output layouts are the reference's
+ * staging layouts (approach1-compute-encoder/src/gpu_compute.h:575-648):
+ *   levels    int16 [mbs][24][16]  (blocks 0-15 luma raster, 16-19 Cb, 20-23 Cr;
+ *                                   positions raster within the 4x4 block)
+ *   dc        int32 [mbs][24]      pre-quantisation coefficient 0 of each block
+ *   nz        uint32[mbs][24]      bit p set iff levels[..][p] != 0
+ *   pred_mode uint32[mbs]          I16x16 mode in bits 0-1, chroma mode bits 2-3
+ *   mv        b200enc_mv_t[mbs]    quarter-pel MV + SAD, 16 bytes
+ * Geometry: W x H is the visible frame (source reads clamp to it); RW x RH is
+ * where reference/recon reads clamp and recon writes stop. RW,RH = W,H is the
+ * reference shaders' behaviour; RW,RH = 16*ceil(W/16), 16*ceil(H/16) is what
+ * a conforming H.264 decoder reconstructs (identical when W, H are multiples
+ * of 16). Recon planes must be allocated at the coded size.
+ */
+#ifndef B200ENC_H
+#define B200ENC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int32_t mvx, mvy; /* quarter-pel, points into the reference */
+    uint32_t sad;
+    uint32_t pad;
+} b200enc_mv_t;
+
+/* Plain full-search ME over [-range, range]^2 (range 16 or 32), cost
+ * SAD + lambda*(|dx|+|dy|), then the 8 half-pel and 8 quarter-pel refines.
+ * Replaces Stage 2, approach1-compute-encoder/shaders/motion_estimation.comp:278-469
+ * (dispatched at src/gpu_compute.c:3094-3103). zero_thresh < 0 disables the
+ * zero-MV early-out (the reference uses 512). Pitches and plane bases must be
+ * multiples of 4. */
+int b200enc_me_full_search(const uint8_t *cur_y, int cur_pitch,
+                           const uint8_t *ref_y, int ref_pitch,
+                           int W, int H, int RW, int RH,
+                           int range, int lambda, int zero_thresh,
+                           void *mv_out, void *stream);
+
+/* Fused P-frame chain given MVs: MC prediction, residual, forward 4x4, AC
+ * quant (inter rounding), nz masks, chroma DC, dequant, inverse, recon.
+ * Replaces residual_predict.comp (P path) + dct_transform.comp +
+ * quantize.comp + reconstruct.comp (src/gpu_compute.c:3121-3183). rec pitch
+ * and rec/levels bases must be multiples of 16. */
+int b200enc_p_frame(const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
+                    const uint8_t *ref_y, const uint8_t *ref_uv, int ref_pitch,
+                    int W, int H, int RW, int RH, int qp, const void *mv,
+                    int16_t *levels, int32_t *dc, uint32_t *nz, uint32_t *pred_mode,
+                    uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch, void *stream);
+
+/* Bytes of scratch the wavefront kernels (intra, deblock) need for a frame
+ * of mbh macroblock rows: a row ticket, an error word and one progress word
+ * per row. The scratch must be zeroed before each launch; the *_frame calls
+ * below do that themselves on `stream`. */
+size_t b200enc_wavefront_scratch_bytes(int mbh);
+
+/* I-frame intra wavefront: I16x16 4-mode decision from reconstructed
+ * neighbours, chroma DC prediction, full transform/quant/DC/recon chain per
+ * macroblock, in a persistent kernel whose CTAs take macroblock rows by
+ * ticket and wait (bounded) on per-row progress words for the top
+ * neighbour. Replaces the per-diagonal dispatch loop over
+ * shaders/intra_wavefront.comp (src/gpu_compute.c:3217-3251). Writes
+ * mv[] = 0. rec planes are read and written in place. */
+int b200enc_i_frame(const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
+                    int W, int H, int RW, int RH, int qp, int num_slices,
+                    int16_t *levels, int32_t *dc, uint32_t *nz, uint32_t *pred_mode, void *mv,
+                    uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch,
+                    void *scratch, size_t scratch_bytes, int ctas, void *stream);
+
+/* Spec deblocking (H.264 clause 8.7) of the coded picture, luma and chroma,
+ * bS 0-4 with the strong filter, for this encoder's macroblock kinds
+ * (all-I16x16 or all-P16x16/P_Skip frames, uniform QP, idc 0, zero
+ * offsets). Macroblocks run as a wavefront (left neighbour and top-right
+ * neighbour first), which reproduces raster order exactly. Replaces
+ * shaders/deblock_filter.comp (src/gpu_compute.c:3261-3290), whose
+ * luma-only, no-strong-filter approximation a decoder does not reproduce. */
+int b200enc_deblock(int mbw, int mbh, int qp, int is_intra,
+                    const uint32_t *nz, const void *mv,
+                    uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch,
+                    void *scratch, size_t scratch_bytes, int ctas, void *stream);
+
+/* The two wavefront kernels with a caller-prepared scratch (NOT cleared
+ * here) and an explicit bound on the polls of each progress wait. For
+ * callers that manage the scratch themselves, and for tests of the bounded
+ * wait (a scratch whose row ticket starts past row 0 leaves row 0 unowned,
+ * so every wait on it gives up after max_wait polls and records error 1). */
+int b200enc_i_frame_launch(const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
+                           int W, int H, int RW, int RH, int qp, int num_slices,
+                           int16_t *levels, int32_t *dc, uint32_t *nz, uint32_t *pred_mode, void *mv,
+                           uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch,
+                           uint32_t *scratch, int ctas, uint32_t max_wait, void *stream);
+int b200enc_deblock_launch(int mbw, int mbh, int qp, int is_intra, const uint32_t *nz, const void *mv,
+                           uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch,
+                           uint32_t *scratch, int ctas, uint32_t max_wait, void *stream);
+
+/* Reads the error word a wavefront launch left in its scratch (synchronises
+ * `stream`): 0 = fine, 1 = a bounded wait gave up (the frame's output is
+ * incomplete and must not be used), -1 = the read failed. */
+int b200enc_wavefront_status(const void *scratch, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B200ENC_H */

@@ -1,0 +1,116 @@
+/*
+ * oracle.h - CPU restatement of the reference compute encoder's hot-path
+ * stages, used ONLY as the test checker (tests/, __graft_entry__.smoke(),
+ * bench.py's cpu_baseline leg). Nothing in the product library links or
+ * calls this code; the CUDA path fails loudly when its extension is absent.
+ *
+ * Each function cites the reference file:line it follows (paths relative to
+ * the reference project root, A1 = approach1-compute-encoder).
+ *
+ * Parity pinning: the restatement is checked against (a) the reference's own
+ * C functions compiled from its sources into oracle/_ref (h264_deblock.c,
+ * h264_mc.c, h264_recon.c, cpu_simd_me.c, encoder_h264.c's exported DC
+ * transform) and (b) the reference tests' golden vectors
+ * (A1/tests/test_encode.c:60-96, A1/tests/test_cpu_simd_me.c:16-106).
+ *
+ * Plane conventions shared with the CUDA library:
+ *   - luma: 8-bit, row pitch `pitch` bytes.
+ *   - chroma: NV12 interleaved CbCr, row pitch `pitch` bytes (W/2 pairs).
+ *   - source reads clamp to the visible size (W, H); reference/recon reads
+ *     clamp to (RW, RH) and recon writes are bounded by (RW, RH). RW/RH equal
+ *     to W/H reproduces the reference shaders exactly; RW/RH equal to the
+ *     coded size (16*mbw, 16*mbh) is what a conforming decoder does.
+ */
+#ifndef B200ENC_ORACLE_H
+#define B200ENC_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int32_t mvx, mvy; /* quarter-pel */
+    uint32_t sad;
+    uint32_t pad;
+} orc_mv_t;
+
+typedef struct {
+    int W, H;      /* visible size: source clamp */
+    int RW, RH;    /* recon/reference clamp and recon write bound */
+    int mbw, mbh;
+    int qp;
+    int num_slices;
+} orc_frame_t;
+
+typedef struct {
+    int range;        /* integer search range R: dx, dy in [-R, R] */
+    int lambda;       /* motion cost weight per integer pel of |dx|+|dy| */
+    int zero_thresh;  /* SAD(0,0) <= zero_thresh ends the search; < 0 disables */
+} orc_me_params_t;
+
+/* Per-frame outputs, reference staging layout (A1/src/gpu_compute.h:575-648). */
+typedef struct {
+    int16_t  *levels;    /* [mbs][24][16] */
+    int32_t  *dc;        /* [mbs][24] */
+    uint32_t *nz;        /* [mbs][24] */
+    uint32_t *pred_mode; /* [mbs] */
+    orc_mv_t *mv;        /* [mbs] */
+} orc_out_t;
+
+int  orc_chroma_qp(int qpy);
+uint32_t orc_slice_of(uint32_t mb, uint32_t total_mbs, uint32_t num_slices);
+void orc_forward_4x4(const int in[16], int out[16]);
+void orc_inverse_4x4(int d[16], int r[16]);
+int  orc_quant_ac(int coeff, int pos, int qp, int intra);
+int  orc_dequant_ac(int level, int pos, int qp);
+void orc_luma_dc_hadamard_fwd(const int in[16], int out[16]);
+void orc_luma_dc_hadamard_inv(const int in[16], int out[16]);
+void orc_chroma_dc_hadamard(const int in[4], int out[4]);
+int  orc_quantize_dc_luma(int v, int qp);
+int  orc_quantize_dc_chroma(int v, int qp);
+int  orc_dequant_dc_luma(int f, int qp);
+int  orc_dequant_dc_chroma(int f, int qp);
+/* Spec-order I16x16 DC as handed to CAVLC (transposed), test_encode.c:60-96. */
+void orc_intra16_luma_dc_transform(const int dc_in[16], int qp, int dc_out[16], int pre[16]);
+
+int  orc_interp_luma_qpel(const uint8_t *ref, int pitch, int RW, int RH, int qx, int qy);
+int  orc_interp_chroma(const uint8_t *ref_uv, int pitch, int RW, int RH, int plane, int ex, int ey);
+uint32_t orc_sad16(const uint8_t *a, int pa, const uint8_t *b, int pb);
+
+/* Plain full-search ME for one frame. */
+void orc_me_frame(const orc_frame_t *f, const orc_me_params_t *p,
+                  const uint8_t *cur_y, int cur_pitch,
+                  const uint8_t *ref_y, int ref_pitch, orc_mv_t *mv);
+
+/* P-frame predict + transform + quant + DC + dequant + recon, given MVs. */
+void orc_p_frame(const orc_frame_t *f,
+                 const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
+                 const uint8_t *ref_y, const uint8_t *ref_uv, int ref_pitch,
+                 const orc_mv_t *mv, orc_out_t *out,
+                 uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch);
+
+/* I-frame intra wavefront (run in raster order, which respects the
+ * diagonal dependency), writing recon in place. */
+void orc_i_frame(const orc_frame_t *f,
+                 const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
+                 orc_out_t *out, uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch);
+
+/* Spec deblocking (H.264 8.7) of the coded picture (16*mbw x 16*mbh) for
+ * the macroblock kinds this encoder emits: all-intra (I16x16) frames or
+ * all-inter (P16x16 / P_Skip, one reference) frames, uniform QP,
+ * disable_deblocking_filter_idc = 0, zero filter offsets. */
+void orc_deblock_frame(int mbw, int mbh, int qp, int is_intra,
+                       const uint32_t *nz, const orc_mv_t *mv,
+                       uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch);
+
+/* One whole frame of the hot path: ME (P only) -> P or I chain -> deblock. */
+void orc_encode_frame(const orc_frame_t *f, const orc_me_params_t *p, int is_intra, int deblock,
+                      const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
+                      const uint8_t *ref_y, const uint8_t *ref_uv, int ref_pitch,
+                      orc_out_t *out, uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,74 @@
+"""The reference boundary (gpu_compute_* in include/gpu_compute.h) end to end:
+host frames uploaded, IPPP sequences encoded through begin/dispatch/end/sync,
+staging buffers and the reconstruction compared with the oracle's sequence."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _pad(a, rows, cols):
+    return np.pad(a, ((0, rows - a.shape[0]), (0, cols - a.shape[1])), mode="edge")
+
+
+def _run(gpu, oracle_mod, W, H, frames, qp, rng, me_mode=0, deblock=1, num_slices=1, coded_clamp=True,
+         gop=None, cpu_mv_frames=()):
+    from b200enc import synth
+    seq = synth.Sequence(W, H, seed=11, pan=W >= 640, noise_patch=W >= 1280)
+    ctx = gpu.Context()
+    ctx.configure(search_range=rng, coded_clamp=coded_clamp, deblock=deblock)
+    img, mem = ctx.create_image(W, H)
+    CW, CH = gpu.coded(W, H)
+    f = oracle_mod.frame(W, H, qp, num_slices=num_slices, coded_clamp=coded_clamp)
+    lam = 8 if me_mode == 1 else 5
+    ref_y = ref_uv = None
+    for t in range(frames):
+        y, uv = seq.frame(t)
+        intra = (t == 0) or (gop is not None and t % gop == 0)
+        ctx.upload(img, mem, y, uv)
+        cpu_mvs = None
+        rec_y = np.zeros((CH, CW), np.uint8)
+        rec_uv = np.zeros((CH // 2, CW), np.uint8)
+        if t in cpu_mv_frames and not intra:
+            rs = np.random.Generator(np.random.PCG64(t))
+            cpu_mvs = np.zeros((f.mbw * f.mbh, 4), np.int32)
+            cpu_mvs[:, :2] = rs.integers(-40, 41, (f.mbw * f.mbh, 2))
+            want = oracle_mod.p_frame(f, y, uv, ref_y, ref_uv, cpu_mvs, rec_y, rec_uv)
+            if deblock:
+                oracle_mod.deblock(f.mbw, f.mbh, qp, 0, want["nz"], want["mv"], rec_y, rec_uv)
+        else:
+            if ref_y is None:
+                ref_y, ref_uv = _pad(y, CH, CW), _pad(uv, CH // 2, CW)
+            want = oracle_mod.encode_frame(f, rng, lam, 512, intra, deblock, y, uv, ref_y, ref_uv, rec_y, rec_uv)
+        slot = ctx.encode(img, W, H, qp, intra, num_slices, me_mode, cpu_mvs)
+        assert ctx.sync(slot) == 0
+        got = ctx.staging(slot)
+        for k in ("levels", "dc", "nz", "pred_mode", "mv"):
+            np.testing.assert_array_equal(got[k], want[k], err_msg=f"frame {t} {k}")
+        gy, guv = ctx.recon_host()
+        RW, RH = (CW, CH) if coded_clamp else (W, H)
+        np.testing.assert_array_equal(gy[:RH, :RW], rec_y[:RH, :RW], err_msg=f"frame {t} recon Y")
+        np.testing.assert_array_equal(guv[:RH // 2, :RW], rec_uv[:RH // 2, :RW], err_msg=f"frame {t} recon UV")
+        ref_y, ref_uv = rec_y, rec_uv
+    ctx.destroy_image(img, mem)
+    ctx.close()
+
+
+def test_ippp_640x480(gpu, oracle_mod):
+    _run(gpu, oracle_mod, 640, 480, 6, 26, 16)
+
+
+def test_ippp_640x480_r32_fast_mode_slices(gpu, oracle_mod):
+    _run(gpu, oracle_mod, 640, 480, 4, 30, 32, me_mode=1, num_slices=4, gop=3)
+
+
+def test_ippp_no_deblock_visible_clamp(gpu, oracle_mod):
+    _run(gpu, oracle_mod, 320, 200, 4, 22, 16, deblock=0, coded_clamp=False)
+
+
+def test_cpu_mvs_replace_me(gpu, oracle_mod):
+    _run(gpu, oracle_mod, 160, 96, 4, 28, 16, cpu_mv_frames=(1, 3))
+
+
+def test_ippp_1080p(gpu, oracle_mod):
+    _run(gpu, oracle_mod, 1920, 1080, 3, 27, 16)
