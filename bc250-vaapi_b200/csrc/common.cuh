@@ -190,16 +190,6 @@ enum : uint32_t {
   kErrWaitTimeout = 1,
 };
 
-// Bounded acquire-wait until *flag >= target. Returns false on timeout.
-__device__ __forceinline__ bool wait_at_least(const uint32_t* flag, uint32_t target, uint32_t max_iters) {
-  uint32_t v;
-  for (uint32_t it = 0; it < max_iters; ++it) {
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
-    if (v >= target) return true;
-    if (it > 8) __nanosleep(64);
-  }
-  return false;
-}
 __device__ __forceinline__ void store_release(uint32_t* flag, uint32_t v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(v) : "memory");
 }
@@ -209,9 +199,17 @@ __device__ __forceinline__ uint32_t load_acquire(const uint32_t* flag) {
   return v;
 }
 
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Scratch layout of the wavefront kernels (one region per launch):
 //   [0] ticket counter, [1] error code, [2] error detail, [3] reserved,
-//   [4 .. 4+mbh) per-row progress (macroblocks done in that row).
+//   [4 .. 4+mbh) per-row progress (luma rows for deblocking, the only rows
+//   of the intra wavefront), [4+mbh .. 4+2*mbh) chroma-row progress of the
+//   deblocking wavefront.
 struct Scratch {
   uint32_t* base;
   __device__ uint32_t* ticket() const { return base; }
@@ -219,6 +217,6 @@ struct Scratch {
   __device__ uint32_t* err_detail() const { return base + 2; }
   __device__ uint32_t* progress(int row) const { return base + 4 + row; }
 };
-inline size_t scratch_words(int mbh) { return 4 + (size_t)mbh; }
+inline size_t scratch_words(int mbh) { return 4 + 2 * (size_t)mbh; }
 
 }  // namespace b200enc

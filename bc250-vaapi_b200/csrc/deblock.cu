@@ -4,22 +4,29 @@
 // treats bS 4 like bS 3, and runs all edges of a direction at once, so
 // neighbouring edges race on the samples they share; no decoder reproduces
 // it. This kernel reproduces the reference's C deblocker
-// (A1/src/h264_deblock.c:263-368) exactly: macroblocks in raster order
-// semantics, vertical edges then horizontal, luma and chroma, bS 0-4 with
-// the strong filter.
+// (A1/src/h264_deblock.c:263-368) exactly: raster-order semantics, vertical
+// edges then horizontal per macroblock, luma and chroma, bS 0-4 with the
+// strong filter.
 //
 // Raster order matters only between macroblocks whose sample footprints
-// overlap: (x-1,y), (x-1,y-1), (x,y-1) and (x+1,y-1) before (x,y). So each
-// CTA (one warp) takes a macroblock row by ticket and, before macroblock x,
-// waits until row y-1 has published progress >= min(x+2, mbw): the
-// classic 2-macroblock-skew wavefront, which gives the raster result.
-// Waits are bounded exactly as in the intra kernel.
+// overlap: (x-1,y), (x-1,y-1), (x,y-1) and (x+1,y-1) before (x,y). So rows
+// run as a wavefront with a 2-macroblock skew. Luma and chroma never share a
+// sample, so they are two independent wavefronts.
 //
-// Per macroblock the warp stages a 20x20 luma tile (4-sample halo left and
-// above) and the matching 10x20-byte NV12 chroma tile in shared memory;
-// lanes 0-15 filter one luma line each and lanes 16-31 one chroma line
-// (8 Cb + 8 Cr), first along rows across the vertical edges, then along
-// columns across the horizontal ones.
+// Layout for latency (the wavefront is latency-bound: ~mbw + 2*mbh
+// dependent macroblock steps per frame):
+//   * a CTA owns a group of R consecutive macroblock rows (taken by ticket,
+//     so groups are only owned by running CTAs and waits cannot deadlock);
+//     R luma warps + R chroma warps, one warp per row and plane kind;
+//   * the group's rows (plus a 4-row / 2-row halo above) live in shared
+//     memory for the whole frame: one bulk load, one bulk store at the end;
+//   * inside a CTA a row waits on its upper neighbour through a shared-memory
+//     progress word; only the group's first row waits on global memory,
+//     and only the group's last row publishes (its bottom 4 luma / 2 chroma
+//     sample rows per macroblock, then a release store);
+//   * boundary strengths of the whole group are computed up front.
+// Waits are bounded; on timeout a CTA records the error and leaves, and
+// every waiter gives up as soon as it sees a recorded error.
 #include "b200enc_internal.h"
 #include "common.cuh"
 
@@ -41,9 +48,8 @@ __constant__ uint8_t kTc0[52][3] = {
     {2, 3, 4}, {3, 3, 5}, {3, 4, 6}, {3, 4, 6}, {4, 5, 7}, {4, 5, 8}, {4, 6, 9},  {5, 7, 10}, {6, 8, 11},
     {6, 8, 13}, {7, 10, 14}, {8, 11, 16}, {9, 12, 18}, {10, 13, 20}, {11, 15, 23}, {13, 17, 25}};
 
-constexpr int kTP = 20;  // tile pitch in bytes (luma and NV12 chroma)
-
-// One luma line across one edge (clause 8.7.2.3 / 8.7.2.4).
+// One luma line across one edge (clause 8.7.2.3 / 8.7.2.4); q points at q0,
+// d is the step across the edge.
 __device__ __forceinline__ void filt_luma(uint8_t* q, int d, int bs, int alpha, int beta, int tc0) {
   const int p0 = q[-d], p1 = q[-2 * d], p2 = q[-3 * d], q0 = q[0], q1 = q[d], q2 = q[2 * d];
   if (abs(p0 - q0) >= alpha || abs(p1 - p0) >= beta || abs(q1 - q0) >= beta) return;
@@ -90,145 +96,270 @@ __device__ __forceinline__ void filt_chroma(uint8_t* q, int d, int bs, int alpha
   q[0] = (uint8_t)clip1(q0 - delta);
 }
 
-struct DShared {
-  alignas(16) uint8_t yt[20][kTP];
-  alignas(16) uint8_t ct[10][kTP];
-  uint8_t bsv[4][4];  // [edge][segment] vertical
-  uint8_t bsh[4][4];  // [edge][segment] horizontal
-  int row, abort_flag;
+// Shared-memory plan of one CTA (dynamic shared memory):
+//   luma image  : (16R + 4) rows x sp bytes, row 0 = picture row 16*y0 - 4
+//   chroma image: (8R + 2) rows x sp bytes (NV12), row 0 = picture row 8*y0 - 2
+//   bS          : R x mbw x 32 bytes ([dir][edge][segment] per macroblock)
+//   progress    : 2R words (luma rows, then chroma rows)
+// sp = 16*mbw + 4: a 4-byte skew per row keeps the 16 lanes that walk 16
+// consecutive rows of one column on 16 different banks.
+struct DbPlan {
+  int R, sp;
+  size_t luma_off, chroma_off, bs_off, prog_off, bytes;
 };
 
-__global__ void __launch_bounds__(32) deblock_kernel(int mbw, int mbh, int qp, int is_intra,
-                                                     const uint32_t* __restrict__ nzm, const MV* __restrict__ mvs,
-                                                     uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch,
-                                                     uint32_t* scratch, uint32_t max_wait) {
-  __shared__ DShared s;
+__host__ __device__ inline DbPlan db_plan(int mbw, int R) {
+  DbPlan p;
+  p.R = R;
+  p.sp = 16 * mbw + 4;
+  p.luma_off = 0;
+  p.chroma_off = p.luma_off + (size_t)(16 * R + 4) * p.sp;
+  p.bs_off = p.chroma_off + (size_t)(8 * R + 2) * p.sp;
+  p.prog_off = (p.bs_off + (size_t)R * mbw * 32 + 15) & ~(size_t)15;
+  p.bytes = p.prog_off + 2 * R * sizeof(uint32_t);
+  return p;
+}
+
+// Bounded waits: give up after max_wait_us microseconds of %globaltimer, or
+// as soon as another CTA has recorded an error.
+__device__ __forceinline__ bool wait_global(const Scratch& sc, const uint32_t* flag, uint32_t need,
+                                            uint32_t max_wait_us, uint32_t where) {
+  const uint64_t t0 = global_ns(), budget = (uint64_t)max_wait_us * 1000u;
+  for (uint32_t it = 0;; ++it) {
+    if (load_acquire(flag) >= need) return true;
+    if (load_acquire(sc.err()) != 0u) return false;
+    if ((it & 15) == 15 && global_ns() - t0 > budget) break;
+    if (it > 16) __nanosleep(20);
+  }
+  if (atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u) atomicExch(sc.err_detail(), where);
+  return false;
+}
+
+__device__ __forceinline__ bool wait_shared(const volatile uint32_t* flag, const Scratch& sc, uint32_t need,
+                                            uint32_t max_wait_us, uint32_t where) {
+  const uint64_t t0 = global_ns(), budget = (uint64_t)max_wait_us * 1000u;
+  for (uint32_t it = 0;; ++it) {
+    if (*flag >= need) return true;
+    if ((it & 63) == 63) {
+      if (load_acquire(sc.err()) != 0u) return false;
+      if (global_ns() - t0 > budget) break;
+    }
+  }
+  if (atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u) atomicExch(sc.err_detail(), where);
+  return false;
+}
+
+__global__ void __launch_bounds__(256) deblock_kernel(int mbw, int mbh, int R, int qp, int is_intra,
+                                                      const uint32_t* __restrict__ nzm, const MV* __restrict__ mvs,
+                                                      uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch,
+                                                      uint32_t* scratch, uint32_t max_wait) {  // max_wait in microseconds
+  extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ int s_group, s_abort;
+  const DbPlan P = db_plan(mbw, R);
+  uint8_t* ly = smem + P.luma_off;
+  uint8_t* cy = smem + P.chroma_off;
+  uint8_t* bsm = smem + P.bs_off;
+  volatile uint32_t* prog = reinterpret_cast<volatile uint32_t*>(smem + P.prog_off);
   const Scratch sc{scratch};
-  const int lane = threadIdx.x;
+  uint32_t* gprog_luma = scratch + 4;
+  uint32_t* gprog_chroma = scratch + 4 + mbh;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nthr = blockDim.x;
   const int qpc = chroma_qp(qp);
   const int al = kAlpha[qp], be = kBeta[qp], alc = kAlpha[qpc], bec = kBeta[qpc];
-  const bool luma_on = al && be, chroma_on = alc && bec;
+  const int W16 = 16 * mbw;
 
   for (;;) {
-    if (lane == 0) {
-      s.row = (int)atomicAdd(sc.ticket(), 1u);
-      s.abort_flag = 0;
+    if (tid == 0) {
+      s_group = (int)atomicAdd(sc.ticket(), 1u);
+      s_abort = 0;
     }
-    __syncwarp();
-    const int my = s.row;
-    if (my >= mbh) return;
-    for (int mx = 0; mx < mbw; ++mx) {
-      const int mb = my * mbw + mx;
-      if (lane == 0 && my > 0) {
-        const uint32_t need = (uint32_t)min(mx + 2, mbw);
-        const uint32_t* pf = sc.progress(my - 1);
-        bool ok = false;
-        for (uint32_t it = 0; it < max_wait; ++it) {
-          if (load_acquire(pf) >= need) { ok = true; break; }
-          if (load_acquire(sc.err()) != 0u) break;
-          if (it > 4) __nanosleep(32);
+    __syncthreads();
+    const int y0 = s_group * R;
+    if (y0 >= mbh) return;
+    const int rows = min(R, mbh - y0);
+    const bool has_next = y0 + rows < mbh;
+
+    // ---- prologue: own rows into shared memory, progress, bS ----------
+    for (int i = tid; i < 2 * R; i += nthr) prog[i] = 0u;
+    {
+      const int wpr = W16 / 16;  // uint4 per picture row
+      for (int i = tid; i < 16 * rows * wpr; i += nthr) {
+        const int r = i / wpr, c = i - r * wpr;
+        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(rec_y + (size_t)(16 * y0 + r) * rec_pitch) + c);
+        uint32_t* d = reinterpret_cast<uint32_t*>(ly + (size_t)(4 + r) * P.sp + 16 * c);
+        d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+      }
+      for (int i = tid; i < 8 * rows * wpr; i += nthr) {
+        const int r = i / wpr, c = i - r * wpr;
+        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(rec_uv + (size_t)(8 * y0 + r) * rec_pitch) + c);
+        uint32_t* d = reinterpret_cast<uint32_t*>(cy + (size_t)(2 + r) * P.sp + 16 * c);
+        d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+      }
+    }
+    for (int i = tid; i < rows * mbw * 32; i += nthr) {
+      // clause 8.7.2.1 for this encoder's macroblock kinds
+      const int k = i & 3, e = (i >> 2) & 3, dir = (i >> 4) & 1, m = i >> 5;
+      const int my = y0 + m / mbw, mx = m % mbw, mb = my * mbw + mx;
+      int bs = 0;
+      if (e > 0 || (dir == 0 ? mx > 0 : my > 0)) {
+        if (is_intra) {
+          bs = e == 0 ? 4 : 3;
+        } else {
+          const int mbp = e ? mb : (dir == 0 ? mb - 1 : mb - mbw);
+          const int bq = dir == 0 ? k * 4 + e : e * 4 + k;
+          const int bp = e ? (dir == 0 ? bq - 1 : bq - 4) : (dir == 0 ? k * 4 + 3 : 12 + k);
+          if ((__ldg(nzm + (size_t)mbp * 24 + bp) | __ldg(nzm + (size_t)mb * 24 + bq)) & 0xffffu) {
+            bs = 2;
+          } else if (e == 0) {
+            const int2 a = __ldg(reinterpret_cast<const int2*>(mvs + mbp));
+            const int2 c = __ldg(reinterpret_cast<const int2*>(mvs + mb));
+            bs = (abs(a.x - c.x) >= 4 || abs(a.y - c.y) >= 4) ? 1 : 0;
+          }
+        }
+      }
+      bsm[i] = (uint8_t)bs;
+    }
+    __syncthreads();
+
+    const bool is_luma = warp < R;
+    const int wr = is_luma ? warp : warp - R;  // row within the group
+    const int y = y0 + wr;
+    if (wr < rows) {
+      const uint8_t* bsrow = bsm + (size_t)wr * mbw * 32;
+      volatile uint32_t* my_prog = prog + (is_luma ? 0 : R) + wr;
+      const volatile uint32_t* up_prog = prog + (is_luma ? 0 : R) + wr - 1;
+      uint32_t* gflag_up = (is_luma ? gprog_luma : gprog_chroma) + (y - 1);
+      uint32_t* gflag_me = (is_luma ? gprog_luma : gprog_chroma) + y;
+      for (int mx = 0; mx < mbw; ++mx) {
+        const uint32_t need = (uint32_t)(mx + 1);  // upper row: bottom samples of MB mx final
+        bool ok = true;
+        if (y > 0) {
+          if (wr == 0) {
+            if (lane == 0) ok = wait_global(sc, gflag_up, need, max_wait, (uint32_t)(y * mbw + mx));
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (ok) {
+              // halo above: 4 luma / 2 chroma sample rows of this column
+              if (is_luma) {
+                if (lane < 16) {
+                  const int r = lane >> 2, w = lane & 3;
+                  const uint32_t v = __ldcg(reinterpret_cast<const uint32_t*>(
+                      rec_y + (size_t)(16 * y - 4 + r) * rec_pitch + 16 * mx + 4 * w));
+                  *reinterpret_cast<uint32_t*>(ly + (size_t)r * P.sp + 16 * mx + 4 * w) = v;
+                }
+              } else if (lane < 8) {
+                const int r = lane >> 2, w = lane & 3;
+                const uint32_t v = __ldcg(reinterpret_cast<const uint32_t*>(
+                    rec_uv + (size_t)(8 * y - 2 + r) * rec_pitch + 16 * mx + 4 * w));
+                *reinterpret_cast<uint32_t*>(cy + (size_t)r * P.sp + 16 * mx + 4 * w) = v;
+              }
+            }
+          } else {
+            if (lane == 0) ok = wait_shared(up_prog, sc, need, max_wait, (uint32_t)(y * mbw + mx));
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            __threadfence_block();
+          }
         }
         if (!ok) {
-          if (atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u) atomicExch(sc.err_detail(), 0x80000000u | (uint32_t)mb);
-          s.abort_flag = 1;
+          s_abort = 1;
+          break;
         }
-      }
-      __syncwarp();
-      if (s.abort_flag) return;
-
-      // ---- stage tiles (L2 reads: neighbours were written by other CTAs) ----
-      const int x0 = mx * 16 - 4;  // tile byte column origin (luma and NV12 chroma)
-      for (int i = lane; i < 20 * 5; i += 32) {
-        const int r = i / 5, w = i - r * 5, gy = my * 16 - 4 + r, gx = x0 + 4 * w;
-        uint32_t v = 0;
-        if (gy >= 0 && gx >= 0) v = __ldcg(reinterpret_cast<const uint32_t*>(rec_y + (size_t)gy * rec_pitch + gx));
-        reinterpret_cast<uint32_t*>(s.yt[r])[w] = v;
-      }
-      for (int i = lane; i < 10 * 5; i += 32) {
-        const int r = i / 5, w = i - r * 5, gy = my * 8 - 2 + r, gx = x0 + 4 * w;
-        uint32_t v = 0;
-        if (gy >= 0 && gx >= 0) v = __ldcg(reinterpret_cast<const uint32_t*>(rec_uv + (size_t)gy * rec_pitch + gx));
-        reinterpret_cast<uint32_t*>(s.ct[r])[w] = v;
-      }
-      // ---- boundary strengths (clause 8.7.2.1) -------------------------
-      {
-        const int dir = lane >> 4, e = (lane >> 2) & 3, k = lane & 3;
-        int bs = 0;
-        const bool has_p = e > 0 || (dir == 0 ? mx > 0 : my > 0);
-        if (has_p) {
-          if (is_intra) {
-            bs = e == 0 ? 4 : 3;
-          } else {
-            const int mbp = e ? mb : (dir == 0 ? mb - 1 : mb - mbw);
-            const int bq = dir == 0 ? k * 4 + e : e * 4 + k;
-            const int bp = e ? (dir == 0 ? bq - 1 : bq - 4) : (dir == 0 ? k * 4 + 3 : 12 + k);
-            if ((__ldg(nzm + (size_t)mbp * 24 + bp) | __ldg(nzm + (size_t)mb * 24 + bq)) & 0xffffu) {
-              bs = 2;
-            } else if (e == 0) {
-              const MV a = mvs[mbp], c = mvs[mb];
-              bs = (abs(a.mvx - c.mvx) >= 4 || abs(a.mvy - c.mvy) >= 4) ? 1 : 0;
+        __syncwarp();
+        const uint8_t* bs = bsrow + mx * 32;
+        if (is_luma) {
+          if (al && be && lane < 16) {
+            // vertical edges along sample row lane, then horizontal edges
+            // down sample column lane (left to right, top to bottom)
+            uint8_t* line = ly + (size_t)(4 + 16 * wr + lane) * P.sp + 16 * mx;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int b = bs[e * 4 + (lane >> 2)];
+              if (b) filt_luma(line + 4 * e, 1, b, al, be, b < 4 ? kTc0[qp][b - 1] : 0);
+            }
+          }
+          __syncwarp();
+          if (al && be && lane < 16) {
+            uint8_t* col = ly + (size_t)(4 + 16 * wr) * P.sp + 16 * mx + lane;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int b = bs[16 + e * 4 + (lane >> 2)];
+              if (b) filt_luma(col + (size_t)(4 * e) * P.sp, P.sp, b, al, be, b < 4 ? kTc0[qp][b - 1] : 0);
+            }
+          }
+        } else {
+          if (alc && bec && lane < 16) {
+            const int pl = lane >> 3, i = lane & 7;
+            uint8_t* line = cy + (size_t)(2 + 8 * wr + i) * P.sp + 16 * mx + pl;
+#pragma unroll
+            for (int e = 0; e < 4; e += 2) {
+              const int b = bs[e * 4 + (i >> 1)];
+              if (b) filt_chroma(line + 4 * e, 2, b, alc, bec, b < 4 ? kTc0[qpc][b - 1] : 0);
+            }
+          }
+          __syncwarp();
+          if (alc && bec && lane < 16) {
+            const int pl = lane >> 3, i = lane & 7;
+            uint8_t* col = cy + (size_t)(2 + 8 * wr) * P.sp + 16 * mx + 2 * i + pl;
+#pragma unroll
+            for (int e = 0; e < 4; e += 2) {
+              const int b = bs[16 + e * 4 + (i >> 1)];
+              if (b) filt_chroma(col + (size_t)(2 * e) * P.sp, P.sp, b, alc, bec, b < 4 ? kTc0[qpc][b - 1] : 0);
             }
           }
         }
-        if (dir == 0) s.bsv[e][k] = (uint8_t)bs;
-        else s.bsh[e][k] = (uint8_t)bs;
-      }
-      __syncwarp();
-
-      // ---- vertical edges, left to right -------------------------------
-      if (lane < 16) {
-        if (luma_on) {
-          uint8_t* line = s.yt[4 + lane];
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int bs = s.bsv[e][lane >> 2];
-            if (bs) filt_luma(line + 4 + 4 * e, 1, bs, al, be, bs < 4 ? kTc0[qp][bs - 1] : 0);
+        __syncwarp();
+        // Macroblock mx-1's bottom samples are final now (mx's left edge was
+        // its last change); all of them after the last macroblock.
+        const uint32_t done = (mx == mbw - 1) ? (uint32_t)mbw : (uint32_t)mx;
+        if (wr == rows - 1) {
+          if (has_next && done > 0) {
+            const int first = (mx == mbw - 1 && mbw > 1) ? mx - 1 : mx - 1;
+            for (int bx = first; bx < (int)done; ++bx) {
+              if (is_luma) {
+                if (lane < 16) {
+                  const int r = lane >> 2, w = lane & 3;
+                  __stcg(reinterpret_cast<uint32_t*>(rec_y + (size_t)(16 * y + 12 + r) * rec_pitch + 16 * bx + 4 * w),
+                         *reinterpret_cast<const uint32_t*>(ly + (size_t)(4 + 16 * wr + 12 + r) * P.sp + 16 * bx + 4 * w));
+                }
+              } else if (lane < 8) {
+                const int r = lane >> 2, w = lane & 3;
+                __stcg(reinterpret_cast<uint32_t*>(rec_uv + (size_t)(8 * y + 6 + r) * rec_pitch + 16 * bx + 4 * w),
+                       *reinterpret_cast<const uint32_t*>(cy + (size_t)(2 + 8 * wr + 6 + r) * P.sp + 16 * bx + 4 * w));
+              }
+            }
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) store_release(gflag_me, done);
           }
-        }
-      } else if (chroma_on) {
-        const int j = lane - 16, pl = j >> 3, i = j & 7;
-        uint8_t* line = s.ct[2 + i];
-#pragma unroll
-        for (int e = 0; e < 4; e += 2) {
-          const int bs = s.bsv[e][i >> 1];
-          if (bs) filt_chroma(line + 2 * (2 + 2 * e) + pl, 2, bs, alc, bec, bs < 4 ? kTc0[qpc][bs - 1] : 0);
+        } else {
+          __threadfence_block();
+          __syncwarp();
+          if (lane == 0) *my_prog = done;
         }
       }
-      __syncwarp();
-      // ---- horizontal edges, top to bottom -----------------------------
-      if (lane < 16) {
-        if (luma_on) {
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int bs = s.bsh[e][lane >> 2];
-            if (bs) filt_luma(&s.yt[4 + 4 * e][4 + lane], kTP, bs, al, be, bs < 4 ? kTc0[qp][bs - 1] : 0);
-          }
-        }
-      } else if (chroma_on) {
-        const int j = lane - 16, pl = j >> 3, i = j & 7;
-#pragma unroll
-        for (int e = 0; e < 4; e += 2) {
-          const int bs = s.bsh[e][i >> 1];
-          if (bs) filt_chroma(&s.ct[2 + 2 * e][2 * (2 + i) + pl], kTP, bs, alc, bec, bs < 4 ? kTc0[qpc][bs - 1] : 0);
-        }
-      }
-      __syncwarp();
-
-      // ---- write back everything but the unused top-left corner ---------
-      for (int i = lane; i < 20 * 5; i += 32) {
-        const int r = i / 5, w = i - r * 5, gy = my * 16 - 4 + r, gx = x0 + 4 * w;
-        if (gy < 0 || gx < 0 || (r < 4 && w == 0)) continue;
-        __stcg(reinterpret_cast<uint32_t*>(rec_y + (size_t)gy * rec_pitch + gx), reinterpret_cast<const uint32_t*>(s.yt[r])[w]);
-      }
-      for (int i = lane; i < 10 * 5; i += 32) {
-        const int r = i / 5, w = i - r * 5, gy = my * 8 - 2 + r, gx = x0 + 4 * w;
-        if (gy < 0 || gx < 0 || (r < 2 && w == 0)) continue;
-        __stcg(reinterpret_cast<uint32_t*>(rec_uv + (size_t)gy * rec_pitch + gx), reinterpret_cast<const uint32_t*>(s.ct[r])[w]);
-      }
-      __threadfence();
-      __syncwarp();
-      if (lane == 0) store_release(sc.progress(my), (uint32_t)(mx + 1));
     }
+    __syncthreads();
+    if (s_abort) return;
+
+    // ---- epilogue: write the group's final samples back ------------------
+    // Luma picture rows [16*y0-3, last], chroma [8*y0-1, last], where the
+    // last rows belong to the next group if there is one (it filters and
+    // writes the 3 luma / 1 chroma rows above its first edge itself).
+    {
+      const int wpr = W16 / 4;
+      const int l0 = y0 > 0 ? -3 : 0, l1 = 16 * rows - (has_next ? 3 : 0);
+      for (int i = tid; i < (l1 - l0) * wpr; i += nthr) {
+        const int r = l0 + i / wpr, c = i % wpr;
+        __stcg(reinterpret_cast<uint32_t*>(rec_y + (size_t)(16 * y0 + r) * rec_pitch) + c,
+               *reinterpret_cast<const uint32_t*>(ly + (size_t)(4 + r) * P.sp + 4 * c));
+      }
+      const int c0 = y0 > 0 ? -1 : 0, c1 = 8 * rows - (has_next ? 1 : 0);
+      for (int i = tid; i < (c1 - c0) * wpr; i += nthr) {
+        const int r = c0 + i / wpr, c = i % wpr;
+        __stcg(reinterpret_cast<uint32_t*>(rec_uv + (size_t)(8 * y0 + r) * rec_pitch) + c,
+               *reinterpret_cast<const uint32_t*>(cy + (size_t)(2 + r) * P.sp + 4 * c));
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -236,14 +367,34 @@ __global__ void __launch_bounds__(32) deblock_kernel(int mbw, int mbh, int qp, i
 
 using namespace b200enc;
 
-static constexpr uint32_t kMaxWaitPollsDb = 1u << 22;
+static constexpr uint32_t kMaxWaitUsDb = 2000000u;  // 2 s
+
+// Rows per CTA: as many as fit in shared memory (one luma + one chroma warp
+// each, at most 8 rows = 512 threads... capped at 4 to keep 256 threads).
+static int db_rows_per_cta(int mbw, int mbh) {
+  int dev = 0, maxsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (maxsm <= 0) maxsm = 48 * 1024;
+  int R = 4;
+  while (R > 1 && db_plan(mbw, R).bytes + 64 > (size_t)maxsm) --R;
+  if (R > mbh) R = mbh;
+  if (db_plan(mbw, R).bytes + 64 > (size_t)maxsm) return 0;
+  return R;
+}
 
 extern "C" int b200enc_deblock_launch(int mbw, int mbh, int qp, int is_intra, const uint32_t* nz, const void* mv,
                                       uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch, uint32_t* scratch, int ctas,
                                       uint32_t max_wait, void* stream) {
-  if (ctas <= 0 || ctas > mbh) ctas = mbh;
-  deblock_kernel<<<ctas, 32, 0, (cudaStream_t)stream>>>(mbw, mbh, qp, is_intra, nz, (const MV*)mv, rec_y, rec_uv,
-                                                        rec_pitch, scratch, max_wait);
+  const int R = db_rows_per_cta(mbw, mbh);
+  if (R <= 0) return -1;
+  const DbPlan P = db_plan(mbw, R);
+  const int groups = (mbh + R - 1) / R;
+  if (ctas <= 0 || ctas > groups) ctas = groups;
+  if (cudaFuncSetAttribute(deblock_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.bytes) != cudaSuccess)
+    return -1;
+  deblock_kernel<<<ctas, 64 * R, P.bytes, (cudaStream_t)stream>>>(mbw, mbh, R, qp, is_intra, nz, (const MV*)mv, rec_y,
+                                                                  rec_uv, rec_pitch, scratch, max_wait);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -251,10 +402,10 @@ extern "C" int b200enc_deblock(int mbw, int mbh, int qp, int is_intra, const uin
                                uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch, void* scratch, size_t scratch_bytes,
                                int ctas, void* stream) {
   if (!nz || !mv || !rec_y || !rec_uv || !scratch || mbw <= 0 || mbh <= 0 || qp < 0 || qp > 51) return -1;
-  if ((rec_pitch & 3) || (((uintptr_t)rec_y) & 3) || (((uintptr_t)rec_uv) & 3)) return -1;
+  if ((rec_pitch & 15) || (((uintptr_t)rec_y) & 15) || (((uintptr_t)rec_uv) & 15)) return -1;
   if (rec_pitch < mbw * 16) return -1;
   if (scratch_bytes < b200enc_wavefront_scratch_bytes(mbh)) return -1;
   if (cudaMemsetAsync(scratch, 0, b200enc_wavefront_scratch_bytes(mbh), (cudaStream_t)stream) != cudaSuccess) return -1;
   return b200enc_deblock_launch(mbw, mbh, qp, is_intra, nz, mv, rec_y, rec_uv, rec_pitch, (uint32_t*)scratch, ctas,
-                                kMaxWaitPollsDb, stream);
+                                kMaxWaitUsDb, stream);
 }

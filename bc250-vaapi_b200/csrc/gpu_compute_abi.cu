@@ -24,7 +24,7 @@
 
 namespace {
 
-constexpr uint32_t kWavefrontMaxPolls = 1u << 22;
+constexpr uint32_t kWavefrontMaxWaitUs = 2000000u;  // 2 s per progress wait
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -233,7 +233,7 @@ int encode_frame(gpu_context_t* ctx, Impl* m, const uint8_t* y, const uint8_t* u
     perf_mark(m, 1);  // intra frames have no ME stage
     rc |= cudaMemsetAsync(scr0, 0, m->scratch_words * 4, m->stream) == cudaSuccess ? 0 : -1;
     rc |= b200enc_i_frame_launch(y, uv, src_pitch, W, H, RW, RH, qp, num_slices, m->d_levels, m->d_dc, m->d_nz,
-                                 m->d_pred_mode, m->d_mv, out_y, out_uv, m->pitch, scr0, 0, kWavefrontMaxPolls,
+                                 m->d_pred_mode, m->d_mv, out_y, out_uv, m->pitch, scr0, 0, kWavefrontMaxWaitUs,
                                  m->stream);
   } else {
     if (cpu_mvs) {
@@ -254,7 +254,7 @@ int encode_frame(gpu_context_t* ctx, Impl* m, const uint8_t* y, const uint8_t* u
   if (db) {
     rc |= cudaMemsetAsync(scr1, 0, m->scratch_words * 4, m->stream) == cudaSuccess ? 0 : -1;
     rc |= b200enc_deblock_launch(m->mbw, m->mbh, qp, is_intra, m->d_nz, m->d_mv, out_y, out_uv, m->pitch, scr1, 0,
-                                 kWavefrontMaxPolls, m->stream);
+                                 kWavefrontMaxWaitUs, m->stream);
   }
   perf_mark(m, 3);
   if (stage) {

@@ -80,14 +80,16 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
       // ---- wait for the top neighbour ----------------------------------
       if (tid == 0 && mby > 0) {
         const uint32_t* pf = sc.progress(mby - 1);
-        bool ok = false;
-        for (uint32_t it = 0; it < max_wait; ++it) {
+        bool ok = false, other = false;
+        const uint64_t t0 = global_ns(), budget = (uint64_t)max_wait * 1000u;  // max_wait in microseconds
+        for (uint32_t it = 0;; ++it) {
           if (load_acquire(pf) >= (uint32_t)(mbx + 1)) { ok = true; break; }
-          if (load_acquire(sc.err()) != 0u) break;
+          if (load_acquire(sc.err()) != 0u) { other = true; break; }
+          if ((it & 15) == 15 && global_ns() - t0 > budget) break;
           if (it > 4) __nanosleep(32);
         }
         if (!ok) {
-          if (atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u) atomicExch(sc.err_detail(), (uint32_t)mb);
+          if (!other && atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u) atomicExch(sc.err_detail(), (uint32_t)mb);
           s.abort_flag = 1;
         }
       }
@@ -352,9 +354,8 @@ extern "C" int b200enc_wavefront_status(const void* scratch, void* stream) {
   return e == 0 ? 0 : 1;
 }
 
-// Upper bound on polls of one progress word before a wavefront CTA gives up
-// (each poll is an L2 round trip plus a short sleep: well over a second).
-static constexpr uint32_t kMaxWaitPolls = 1u << 22;
+// Time budget of one progress wait before a wavefront CTA gives up.
+static constexpr uint32_t kMaxWaitUs = 2000000u;  // 2 s
 
 extern "C" int b200enc_i_frame_launch(const uint8_t* cur_y, const uint8_t* cur_uv, int cur_pitch, int W, int H,
                                       int RW, int RH, int qp, int num_slices, int16_t* levels, int32_t* dc,
@@ -381,5 +382,5 @@ extern "C" int b200enc_i_frame(const uint8_t* cur_y, const uint8_t* cur_uv, int 
   if (scratch_bytes < b200enc_wavefront_scratch_bytes(mbh)) return -1;
   if (cudaMemsetAsync(scratch, 0, b200enc_wavefront_scratch_bytes(mbh), (cudaStream_t)stream) != cudaSuccess) return -1;
   return b200enc_i_frame_launch(cur_y, cur_uv, cur_pitch, W, H, RW, RH, qp, num_slices, levels, dc, nz, pred_mode, mv,
-                                rec_y, rec_uv, rec_pitch, (uint32_t*)scratch, ctas, kMaxWaitPolls, stream);
+                                rec_y, rec_uv, rec_pitch, (uint32_t*)scratch, ctas, kMaxWaitUs, stream);
 }

@@ -60,8 +60,8 @@ int b200enc_p_frame(const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
                     uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch, void *stream);
 
 /* Bytes of scratch the wavefront kernels (intra, deblock) need for a frame
- * of mbh macroblock rows: a row ticket, an error word and one progress word
- * per row. The scratch must be zeroed before each launch; the *_frame calls
+ * of mbh macroblock rows: a ticket, an error word and two progress words per
+ * row (luma and chroma wavefronts). The scratch must be zeroed before each launch; the *_frame calls
  * below do that themselves on `stream`. */
 size_t b200enc_wavefront_scratch_bytes(int mbh);
 
@@ -91,10 +91,11 @@ int b200enc_deblock(int mbw, int mbh, int qp, int is_intra,
                     void *scratch, size_t scratch_bytes, int ctas, void *stream);
 
 /* The two wavefront kernels with a caller-prepared scratch (NOT cleared
- * here) and an explicit bound on the polls of each progress wait. For
- * callers that manage the scratch themselves, and for tests of the bounded
- * wait (a scratch whose row ticket starts past row 0 leaves row 0 unowned,
- * so every wait on it gives up after max_wait polls and records error 1). */
+ * here) and an explicit time bound, in microseconds, on each progress wait.
+ * For callers that manage the scratch themselves, and for tests of the
+ * bounded wait (a scratch whose ticket starts past the first row (group)
+ * leaves it unowned, so every wait on it gives up after max_wait us and
+ * records error 1). */
 int b200enc_i_frame_launch(const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
                            int W, int H, int RW, int RH, int qp, int num_slices,
                            int16_t *levels, int32_t *dc, uint32_t *nz, uint32_t *pred_mode, void *mv,

@@ -35,7 +35,7 @@ def test_rejects_bad_arguments_without_a_gpu():
     assert lib.b200enc_me_full_search(vp(16), 63, vp(16), 64, 64, 64, 64, 64, 16, 5, 512, vp(16), None) == -1
     assert lib.b200enc_p_frame(None, None, 64, None, None, 64, 64, 64, 64, 64, 26, *([None] * 7), 64, None) == -1
     assert lib.b200enc_deblock(4, 4, 60, 0, vp(16), vp(16), vp(16), vp(16), 64, vp(16), 1024, 0, None) == -1
-    assert lib.b200enc_wavefront_scratch_bytes(68) == 4 * (4 + 68)
+    assert lib.b200enc_wavefront_scratch_bytes(68) == 4 * (4 + 2 * 68)
     assert lib.gpu_compute_sync_slot(None, 0) == -1
     assert lib.gpu_compute_begin_picture(None, b200enc.GpuImage()) == -1
 
