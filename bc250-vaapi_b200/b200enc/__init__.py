@@ -17,6 +17,7 @@ EXPORTS = [
     # include/b200enc.h
     "b200enc_me_full_search", "b200enc_p_frame", "b200enc_wavefront_scratch_bytes", "b200enc_i_frame",
     "b200enc_deblock", "b200enc_wavefront_status", "b200enc_i_frame_launch", "b200enc_deblock_launch",
+    "b200enc_deblock_noalloc",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
     "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",

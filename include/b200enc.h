@@ -105,6 +105,30 @@ int b200enc_deblock_launch(int mbw, int mbh, int qp, int is_intra, const uint32_
                            uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch,
                            uint32_t *scratch, int ctas, uint32_t max_wait, void *stream);
 
+/* b200enc_deblock for callers that cannot allocate device memory. No
+ * counterpart in the reference. A real-time encode thread (a streaming
+ * server's per-frame encode, a VA-API EndPicture under the driver lock) must
+ * not call cudaMalloc, which synchronises the whole device and can stall for
+ * milliseconds, and a plug-in whose device memory is budgeted at start-up may
+ * not allocate later; neither can provide the scratch b200enc_deblock wants.
+ * This variant uses a fixed scratch array built into the library (4112
+ * bytes per device, resident until the process exits) and allocates nothing;
+ * the caller still passes the planes, nz and MVs.
+ *   - Limit: mbh <= 512 macroblock rows (frames up to 8192 lines); larger
+ *     frames return -2 with a message on stderr. Bad arguments return -1.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress, with that device current); make that first call
+ *     before any stream capture.
+ *   - Every call on a device shares the one array and zeroes the part it
+ *     uses on `stream` before launching: calls whose work overlaps on the GPU
+ *     (two streams at once) race on it and must be serialised by the caller.
+ * Status: there is no scratch pointer to hand to b200enc_wavefront_status,
+ * so a bounded wait that gave up (only if the GPU stopped running the
+ * kernel's CTAs for 2 s) is not reported through this entry point. */
+int b200enc_deblock_noalloc(int mbw, int mbh, int qp, int is_intra,
+                            const uint32_t *nz, const void *mv,
+                            uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch, void *stream);
+
 /* Reads the error word a wavefront launch left in its scratch (synchronises
  * `stream`): 0 = fine, 1 = a bounded wait gave up (the frame's output is
  * incomplete and must not be used), -1 = the read failed. */
