@@ -67,7 +67,7 @@ def load_library(path=LIB_PATH):
     lib.gpu_compute_get_last_latency_ms.restype = ctypes.c_double
     lib.b200enc_ctx_stream.restype = _vp
     lib.b200enc_i_frame.argtypes = [_vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i,
-                                    _vp, ctypes.c_size_t, _i, _vp]
+                                    _vp, ctypes.c_size_t, _i, _i, _vp]
     lib.b200enc_deblock.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, ctypes.c_size_t, _i, _vp]
     lib.b200enc_me_full_search.argtypes = [_vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp]
     lib.b200enc_p_frame.argtypes = [_vp, _vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
@@ -177,10 +177,14 @@ def scratch(mbh, device="cuda"):
     return torch.zeros((n + 3) // 4, dtype=torch.int32, device=device)
 
 
-def i_frame(cur, W, H, RW, RH, qp, num_slices, out, rec, scr, ctas=0, stream=None):
+INTRA_CORNER_CHECK = 1
+
+
+def i_frame(cur, W, H, RW, RH, qp, num_slices, out, rec, scr, ctas=0, stream=None, flags=INTRA_CORNER_CHECK):
     _check(lib().b200enc_i_frame(cur.yp(), cur.uvp(), cur.pitch, W, H, RW, RH, qp, num_slices, _p(out.levels),
                                  _p(out.dc), _p(out.nz), _p(out.pred_mode), _p(out.mv), rec.yp(), rec.uvp(),
-                                 rec.pitch, _p(scr), scr.numel() * 4, ctas, _stream(stream)), "b200enc_i_frame")
+                                 rec.pitch, _p(scr), scr.numel() * 4, ctas, flags, _stream(stream)),
+           "b200enc_i_frame")
 
 
 def deblock(mbw, mbh, qp, is_intra, nz, mv, rec, scr, ctas=0, stream=None):

@@ -96,6 +96,59 @@ __device__ __forceinline__ void filt_chroma(uint8_t* q, int d, int bs, int alpha
   q[0] = (uint8_t)clip1(q0 - delta);
 }
 
+// The same filters on samples held in registers (the caller unrolls the
+// edge loop, so every index is a compile-time constant); a lane whose edge
+// has bS 0 or fails the sample tests leaves at once, as in the reference.
+__device__ __forceinline__ void luma_regs(int& p3, int& p2, int& p1, int& p0, int& q0, int& q1, int& q2, int& q3,
+                                          int bs, int alpha, int beta, int tc0) {
+  if (!bs) return;
+  const int d0 = abs(p0 - q0);
+  if (d0 >= alpha || abs(p1 - p0) >= beta || abs(q1 - q0) >= beta) return;
+  const bool ap = abs(p2 - p0) < beta, aq = abs(q2 - q0) < beta;
+  if (bs == 4) {
+    const bool small = d0 < ((alpha >> 2) + 2);
+    const int o_p0 = p0, o_p1 = p1, o_q0 = q0, o_q1 = q1;
+    if (ap && small) {
+      p0 = (p2 + 2 * o_p1 + 2 * o_p0 + 2 * o_q0 + o_q1 + 4) >> 3;
+      p1 = (p2 + o_p1 + o_p0 + o_q0 + 2) >> 2;
+      p2 = (2 * p3 + 3 * p2 + o_p1 + o_p0 + o_q0 + 4) >> 3;
+    } else {
+      p0 = (2 * o_p1 + o_p0 + o_q1 + 2) >> 2;
+    }
+    if (aq && small) {
+      q0 = (q2 + 2 * o_q1 + 2 * o_q0 + 2 * o_p0 + o_p1 + 4) >> 3;
+      q1 = (q2 + o_q1 + o_q0 + o_p0 + 2) >> 2;
+      q2 = (2 * q3 + 3 * q2 + o_q1 + o_q0 + o_p0 + 4) >> 3;
+    } else {
+      q0 = (2 * o_q1 + o_q0 + o_p1 + 2) >> 2;
+    }
+    return;
+  }
+  const int tc = tc0 + (ap ? 1 : 0) + (aq ? 1 : 0);
+  const int delta = clampi(((q0 - p0) * 4 + (p1 - q1) + 4) >> 3, -tc, tc);
+  const int avg = (p0 + q0 + 1) >> 1;
+  if (ap) p1 += clampi((p2 + avg - (p1 << 1)) >> 1, -tc0, tc0);
+  if (aq) q1 += clampi((q2 + avg - (q1 << 1)) >> 1, -tc0, tc0);
+  p0 = clip1(p0 + delta);
+  q0 = clip1(q0 - delta);
+}
+
+__device__ __forceinline__ void chroma_regs(int p1, int& p0, int& q0, int q1, int bs, int alpha, int beta, int tc0) {
+  if (!bs) return;
+  if (abs(p0 - q0) >= alpha || abs(p1 - p0) >= beta || abs(q1 - q0) >= beta) return;
+  if (bs == 4) {
+    p0 = (2 * p1 + p0 + q1 + 2) >> 2;
+    q0 = (2 * q1 + q0 + p1 + 2) >> 2;
+    return;
+  }
+  const int tc = tc0 + 1;
+  const int delta = clampi(((q0 - p0) * 4 + (p1 - q1) + 4) >> 3, -tc, tc);
+  p0 = clip1(p0 + delta);
+  q0 = clip1(q0 - delta);
+}
+
+__device__ __forceinline__ int tc0_for(int bs, int t1, int t2, int t3) { return bs == 1 ? t1 : (bs == 2 ? t2 : t3); }
+
 // Shared-memory plan of one CTA (dynamic shared memory):
 //   luma image  : (16R + 4) rows x sp bytes, row 0 = picture row 16*y0 - 4
 //   chroma image: (8R + 2) rows x sp bytes (NV12), row 0 = picture row 8*y0 - 2
@@ -144,6 +197,7 @@ __device__ __forceinline__ bool wait_shared(const volatile uint32_t* flag, const
       if (load_acquire(sc.err()) != 0u) return false;
       if (global_ns() - t0 > budget) break;
     }
+    __nanosleep(32);  // leave the issue slots to the warps doing the work
   }
   if (atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u) atomicExch(sc.err_detail(), where);
   return false;
@@ -166,6 +220,8 @@ __global__ void __launch_bounds__(256) deblock_kernel(int mbw, int mbh, int R, i
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nthr = blockDim.x;
   const int qpc = chroma_qp(qp);
   const int al = kAlpha[qp], be = kBeta[qp], alc = kAlpha[qpc], bec = kBeta[qpc];
+  const int tcl1 = kTc0[qp][0], tcl2 = kTc0[qp][1], tcl3 = kTc0[qp][2];
+  const int tcc1 = kTc0[qpc][0], tcc2 = kTc0[qpc][1], tcc3 = kTc0[qpc][2];
   const int W16 = 16 * mbw;
 
   for (;;) {
@@ -267,43 +323,97 @@ __global__ void __launch_bounds__(256) deblock_kernel(int mbw, int mbh, int R, i
         const uint8_t* bs = bsrow + mx * 32;
         if (is_luma) {
           if (al && be && lane < 16) {
-            // vertical edges along sample row lane, then horizontal edges
-            // down sample column lane (left to right, top to bottom)
-            uint8_t* line = ly + (size_t)(4 + 16 * wr + lane) * P.sp + 16 * mx;
+            // vertical edges: this lane's sample row, 20 samples from p3 of
+            // the left edge to q3 of the last internal edge, in registers
+            uint8_t* row = ly + (size_t)(4 + 16 * wr + lane) * P.sp + 16 * mx;
+            int v[20];
+            const uint32_t* rw = reinterpret_cast<const uint32_t*>(row);
+            const uint32_t w0 = mx > 0 ? rw[-1] : 0u;
+            const uint32_t w1 = rw[0], w2 = rw[1], w3 = rw[2], w4 = rw[3];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              v[k] = (w0 >> (8 * k)) & 255;
+              v[4 + k] = (w1 >> (8 * k)) & 255;
+              v[8 + k] = (w2 >> (8 * k)) & 255;
+              v[12 + k] = (w3 >> (8 * k)) & 255;
+              v[16 + k] = (w4 >> (8 * k)) & 255;
+            }
+            const int seg = lane >> 2;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-              const int b = bs[e * 4 + (lane >> 2)];
-              if (b) filt_luma(line + 4 * e, 1, b, al, be, b < 4 ? kTc0[qp][b - 1] : 0);
+              const int b = bs[e * 4 + seg];
+              const int i = 4 + 4 * e;
+              luma_regs(v[i - 4], v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], v[i + 3], b, al, be,
+                        tc0_for(b, tcl1, tcl2, tcl3));
             }
+            uint32_t o[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k)
+              o[k] = (uint32_t)v[4 * k] | ((uint32_t)v[4 * k + 1] << 8) | ((uint32_t)v[4 * k + 2] << 16) |
+                     ((uint32_t)v[4 * k + 3] << 24);
+            uint32_t* ww = reinterpret_cast<uint32_t*>(row);
+            if (mx > 0) ww[-1] = o[0];
+            ww[0] = o[1];
+            ww[1] = o[2];
+            ww[2] = o[3];
+            ww[3] = o[4];
           }
           __syncwarp();
           if (al && be && lane < 16) {
-            uint8_t* col = ly + (size_t)(4 + 16 * wr) * P.sp + 16 * mx + lane;
+            // horizontal edges: this lane's sample column, rows -4..15
+            uint8_t* col = ly + (size_t)(16 * wr) * P.sp + 16 * mx + lane;
+            int v[20];
+#pragma unroll
+            for (int r = 0; r < 20; ++r) v[r] = col[(size_t)r * P.sp];
+            const int seg = lane >> 2;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-              const int b = bs[16 + e * 4 + (lane >> 2)];
-              if (b) filt_luma(col + (size_t)(4 * e) * P.sp, P.sp, b, al, be, b < 4 ? kTc0[qp][b - 1] : 0);
+              const int b = bs[16 + e * 4 + seg];
+              const int i = 4 + 4 * e;
+              luma_regs(v[i - 4], v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], v[i + 3], b, al, be,
+                        tc0_for(b, tcl1, tcl2, tcl3));
             }
+#pragma unroll
+            for (int r = 1; r < 19; ++r) col[(size_t)r * P.sp] = (uint8_t)v[r];
           }
         } else {
           if (alc && bec && lane < 16) {
+            // vertical edges of one chroma plane's sample row: chroma
+            // samples 8mx-2 .. 8mx+7 (every other byte of the NV12 row)
             const int pl = lane >> 3, i = lane & 7;
-            uint8_t* line = cy + (size_t)(2 + 8 * wr + i) * P.sp + 16 * mx + pl;
+            uint8_t* row = cy + (size_t)(2 + 8 * wr + i) * P.sp + 16 * mx + pl;
+            int v[10];
+            v[0] = mx > 0 ? row[-4] : 0;
+            v[1] = mx > 0 ? row[-2] : 0;
+#pragma unroll
+            for (int k = 2; k < 10; ++k) v[k] = row[2 * (k - 2)];
+            const int seg = i >> 1;
 #pragma unroll
             for (int e = 0; e < 4; e += 2) {
-              const int b = bs[e * 4 + (i >> 1)];
-              if (b) filt_chroma(line + 4 * e, 2, b, alc, bec, b < 4 ? kTc0[qpc][b - 1] : 0);
+              const int b = bs[e * 4 + seg];
+              const int j = 2 + 2 * e;
+              chroma_regs(v[j - 2], v[j - 1], v[j], v[j + 1], b, alc, bec, tc0_for(b, tcc1, tcc2, tcc3));
             }
+            if (mx > 0) row[-2] = (uint8_t)v[1];
+#pragma unroll
+            for (int k = 2; k < 10; ++k) row[2 * (k - 2)] = (uint8_t)v[k];
           }
           __syncwarp();
           if (alc && bec && lane < 16) {
             const int pl = lane >> 3, i = lane & 7;
-            uint8_t* col = cy + (size_t)(2 + 8 * wr) * P.sp + 16 * mx + 2 * i + pl;
+            uint8_t* col = cy + (size_t)(8 * wr) * P.sp + 16 * mx + 2 * i + pl;
+            int v[10];
+#pragma unroll
+            for (int r = 0; r < 10; ++r) v[r] = col[(size_t)r * P.sp];
+            const int seg = i >> 1;
 #pragma unroll
             for (int e = 0; e < 4; e += 2) {
-              const int b = bs[16 + e * 4 + (i >> 1)];
-              if (b) filt_chroma(col + (size_t)(2 * e) * P.sp, P.sp, b, alc, bec, b < 4 ? kTc0[qpc][b - 1] : 0);
+              const int b = bs[16 + e * 4 + seg];
+              const int j = 2 + 2 * e;
+              chroma_regs(v[j - 2], v[j - 1], v[j], v[j + 1], b, alc, bec, tc0_for(b, tcc1, tcc2, tcc3));
             }
+#pragma unroll
+            for (int r = 1; r < 9; ++r) col[(size_t)r * P.sp] = (uint8_t)v[r];
           }
         }
         __syncwarp();

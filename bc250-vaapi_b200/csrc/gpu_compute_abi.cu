@@ -64,6 +64,7 @@ struct Impl {
   double last_latency_ms = 0.0;
   // parameters
   int range = 16, lambda = -1, zero_thresh = 512, clamp_coded = 1, deblock = -1;
+  int intra_flags = B200ENC_INTRA_CORNER_CHECK;
   std::map<void*, Shadow> shadows;
   // Per-stage timing (the reference's BC250_PERF_STATS timestamps,
   // gpu_compute.c:50-67): a ring of event sets, one per frame, folded into
@@ -234,7 +235,7 @@ int encode_frame(gpu_context_t* ctx, Impl* m, const uint8_t* y, const uint8_t* u
     rc |= cudaMemsetAsync(scr0, 0, m->scratch_words * 4, m->stream) == cudaSuccess ? 0 : -1;
     rc |= b200enc_i_frame_launch(y, uv, src_pitch, W, H, RW, RH, qp, num_slices, m->d_levels, m->d_dc, m->d_nz,
                                  m->d_pred_mode, m->d_mv, out_y, out_uv, m->pitch, scr0, 0, kWavefrontMaxWaitUs,
-                                 m->stream);
+                                 m->intra_flags, m->stream);
   } else {
     if (cpu_mvs) {
       // caller-supplied MVs replace Stage 2 (gpu_compute.c:3078-3092)
@@ -311,6 +312,8 @@ int bc250_gpu_init(bc250_gpu_context_t* ctx) {
   m->range = (r == 32) ? 32 : 16;
   const char* cl = getenv("B200ENC_RECON_CLAMP");
   m->clamp_coded = (cl && strcmp(cl, "visible") == 0) ? 0 : 1;
+  const char* ip = getenv("B200ENC_INTRA_PLANE");
+  m->intra_flags = (ip && strcmp(ip, "shader") == 0) ? 0 : B200ENC_INTRA_CORNER_CHECK;
   ctx->impl = m;
   return 0;
 }

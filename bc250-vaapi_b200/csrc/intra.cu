@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
                                                      int32_t* __restrict__ dc, uint32_t* __restrict__ nzm,
                                                      uint32_t* __restrict__ pred_mode, MV* __restrict__ mvs,
                                                      uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch,
-                                                     uint32_t* scratch, uint32_t max_wait) {
+                                                     uint32_t* scratch, uint32_t max_wait, int flags) {
   __shared__ IShared s;
   const Scratch sc{scratch};
   const int tid = threadIdx.x;
@@ -101,6 +101,12 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
       const bool top_exists = mby > 0, left_exists = mbx > 0;
       const bool top_av = top_exists && slice_of((uint32_t)(mb - g.mbw), total, (uint32_t)num_slices) == sl;
       const bool left_av = left_exists && slice_of((uint32_t)(mb - 1), total, (uint32_t)num_slices) == sl;
+      // Plane also predicts from the top-left sample; with the corner check
+      // it needs the top-left macroblock in this slice as well (the
+      // reference shader checks only top and left).
+      const bool plane_av = top_av && left_av &&
+                            (!(flags & B200ENC_INTRA_CORNER_CHECK) ||
+                             slice_of((uint32_t)(mb - g.mbw - 1), total, (uint32_t)num_slices) == sl);
       if (tid < 16) {
         s.top[tid] = top_exists ? __ldcg(rec_y + (size_t)clampi(Y - 1, 0, rmy) * rec_pitch + clampi(X + tid, 0, rmx)) : 128;
       } else if (tid < 32) {
@@ -148,7 +154,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
           else if (left_av) dcv = (sl2 + 8) >> 4;
           else dcv = 128;
           s.dcv = dcv;
-          if (top_av && left_av) {
+          if (plane_av) {
             s.pa = 16 * (s.left[15] + s.top[15]);
             s.pb = (5 * hterm + 32) >> 6;
             s.pc = (5 * vterm + 32) >> 6;
@@ -165,7 +171,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
           sdc += (uint32_t)abs(v - s.dcv);
           if (top_av) sv += (uint32_t)abs(v - s.top[x]);
           if (left_av) shh += (uint32_t)abs(v - s.left[y]);
-          if (top_av && left_av) spl += (uint32_t)abs(v - clip1((s.pa + s.pb * (x - 7) + s.pc * (y - 7) + 16) >> 5));
+          if (plane_av) spl += (uint32_t)abs(v - clip1((s.pa + s.pb * (x - 7) + s.pc * (y - 7) + 16) >> 5));
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -189,7 +195,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
         int mode = 2;
         if (top_av && sv < best) { best = sv; mode = 0; }
         if (left_av && shh < best) { best = shh; mode = 1; }
-        if (top_av && left_av && spl < best) { best = spl; mode = 3; }
+        if (plane_av && spl < best) { best = spl; mode = 3; }
         s.mode = mode;
         pred_mode[mb] = (uint32_t)mode;  // chroma mode bits 2-3 = 0 (DC)
         mvs[mb] = MV{0, 0, 0u, 0u};
@@ -360,20 +366,21 @@ static constexpr uint32_t kMaxWaitUs = 2000000u;  // 2 s
 extern "C" int b200enc_i_frame_launch(const uint8_t* cur_y, const uint8_t* cur_uv, int cur_pitch, int W, int H,
                                       int RW, int RH, int qp, int num_slices, int16_t* levels, int32_t* dc,
                                       uint32_t* nz, uint32_t* pred_mode, void* mv, uint8_t* rec_y, uint8_t* rec_uv,
-                                      int rec_pitch, uint32_t* scratch, int ctas, uint32_t max_wait, void* stream) {
+                                      int rec_pitch, uint32_t* scratch, int ctas, uint32_t max_wait, int flags,
+                                      void* stream) {
   Geo g{W, H, RW, RH, (W + 15) / 16, (H + 15) / 16};
   if (ctas <= 0) ctas = g.mbh;
   if (ctas > g.mbh) ctas = g.mbh;
   i_frame_kernel<<<ctas, 96, 0, (cudaStream_t)stream>>>(cur_y, cur_uv, cur_pitch, g, qp, num_slices, levels, dc, nz,
                                                        pred_mode, (MV*)mv, rec_y, rec_uv, rec_pitch, scratch,
-                                                       max_wait);
+                                                       max_wait, flags);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int b200enc_i_frame(const uint8_t* cur_y, const uint8_t* cur_uv, int cur_pitch, int W, int H, int RW,
                                int RH, int qp, int num_slices, int16_t* levels, int32_t* dc, uint32_t* nz,
                                uint32_t* pred_mode, void* mv, uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch,
-                               void* scratch, size_t scratch_bytes, int ctas, void* stream) {
+                               void* scratch, size_t scratch_bytes, int ctas, int flags, void* stream) {
   if (!cur_y || !cur_uv || !levels || !dc || !nz || !pred_mode || !mv || !rec_y || !rec_uv || !scratch) return -1;
   if (qp < 0 || qp > 51 || W <= 0 || H <= 0 || RW <= 1 || RH <= 1 || num_slices < 1) return -1;
   if ((rec_pitch & 15) || (((uintptr_t)rec_y) & 15) || (((uintptr_t)rec_uv) & 15) || (((uintptr_t)levels) & 15))
@@ -382,5 +389,5 @@ extern "C" int b200enc_i_frame(const uint8_t* cur_y, const uint8_t* cur_uv, int 
   if (scratch_bytes < b200enc_wavefront_scratch_bytes(mbh)) return -1;
   if (cudaMemsetAsync(scratch, 0, b200enc_wavefront_scratch_bytes(mbh), (cudaStream_t)stream) != cudaSuccess) return -1;
   return b200enc_i_frame_launch(cur_y, cur_uv, cur_pitch, W, H, RW, RH, qp, num_slices, levels, dc, nz, pred_mode, mv,
-                                rec_y, rec_uv, rec_pitch, (uint32_t*)scratch, ctas, kMaxWaitUs, stream);
+                                rec_y, rec_uv, rec_pitch, (uint32_t*)scratch, ctas, kMaxWaitUs, flags, stream);
 }

@@ -65,6 +65,16 @@ int b200enc_p_frame(const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
  * below do that themselves on `stream`. */
 size_t b200enc_wavefront_scratch_bytes(int mbh);
 
+/* Intra flag: Intra16x16 Plane also requires the top-left macroblock to be
+ * in the current slice (Plane predicts from p[-1,-1], so a decoder needs it).
+ * Without the flag the decision is the reference shader's
+ * (shaders/intra_wavefront.comp:463-497 checks only top and left), which can
+ * pick Plane across a slice that starts at the top neighbour; the reference
+ * host encoder then writes a non-conforming stream that decoders
+ * reconstruct differently. The gpu_compute_* layer sets the flag unless
+ * B200ENC_INTRA_PLANE=shader. */
+#define B200ENC_INTRA_CORNER_CHECK 1
+
 /* I-frame intra wavefront: I16x16 4-mode decision from reconstructed
  * neighbours, chroma DC prediction, full transform/quant/DC/recon chain per
  * macroblock, in a persistent kernel whose CTAs take macroblock rows by
@@ -76,7 +86,7 @@ int b200enc_i_frame(const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
                     int W, int H, int RW, int RH, int qp, int num_slices,
                     int16_t *levels, int32_t *dc, uint32_t *nz, uint32_t *pred_mode, void *mv,
                     uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch,
-                    void *scratch, size_t scratch_bytes, int ctas, void *stream);
+                    void *scratch, size_t scratch_bytes, int ctas, int flags, void *stream);
 
 /* Spec deblocking (H.264 clause 8.7) of the coded picture, luma and chroma,
  * bS 0-4 with the strong filter, for this encoder's macroblock kinds
@@ -100,7 +110,7 @@ int b200enc_i_frame_launch(const uint8_t *cur_y, const uint8_t *cur_uv, int cur_
                            int W, int H, int RW, int RH, int qp, int num_slices,
                            int16_t *levels, int32_t *dc, uint32_t *nz, uint32_t *pred_mode, void *mv,
                            uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch,
-                           uint32_t *scratch, int ctas, uint32_t max_wait, void *stream);
+                           uint32_t *scratch, int ctas, uint32_t max_wait, int flags, void *stream);
 int b200enc_deblock_launch(int mbw, int mbh, int qp, int is_intra, const uint32_t *nz, const void *mv,
                            uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch,
                            uint32_t *scratch, int ctas, uint32_t max_wait, void *stream);

@@ -23,6 +23,8 @@
  *   B200ENC_SEARCH_RANGE=16|32 integer full-search range (default 16)
  *   B200ENC_RECON_CLAMP=coded|visible  where reference reads clamp
  *                              (default coded = what a decoder does)
+ *   B200ENC_INTRA_PLANE=shader the reference shader's Plane availability
+ *                              (default: also require the top-left slice)
  */
 #ifndef GPU_COMPUTE_H
 #define GPU_COMPUTE_H

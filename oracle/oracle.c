@@ -514,6 +514,9 @@ void orc_i_frame(const orc_frame_t *f,
             const int top_exists = mby > 0, left_exists = mbx > 0;
             const int top_av = top_exists && orc_slice_of((uint32_t)(mb - f->mbw), total, (uint32_t)f->num_slices) == sl;
             const int left_av = left_exists && orc_slice_of((uint32_t)(mb - 1), total, (uint32_t)f->num_slices) == sl;
+            const int plane_av = top_av && left_av &&
+                (!(f->flags & ORC_INTRA_CORNER_CHECK) ||
+                 orc_slice_of((uint32_t)(mb - f->mbw - 1), total, (uint32_t)f->num_slices) == sl);
             int top[16], left[16], corner;
             for (int i = 0; i < 16; i++) {
                 top[i] = top_exists ? rec_y[(size_t)clampi(Y - 1, 0, rmy) * rp + clampi(X + i, 0, rmx)] : 128;
@@ -528,7 +531,7 @@ void orc_i_frame(const orc_frame_t *f,
             else if (left_av) dcv = (sl_ + 8) >> 4;
             else dcv = 128;
             int pa = 0, pb = 0, pc = 0;
-            if (top_av && left_av) {
+            if (plane_av) {
                 int Hs = 0, Vs = 0;
                 for (int k = 0; k < 8; k++) {
                     int l = (6 - k >= 0) ? top[6 - k] : corner;
@@ -550,13 +553,13 @@ void orc_i_frame(const orc_frame_t *f,
                     sdc += (uint32_t)iabs(s - dcv);
                     if (top_av) sv += (uint32_t)iabs(s - top[x]);
                     if (left_av) sh += (uint32_t)iabs(s - left[y]);
-                    if (top_av && left_av) spl += (uint32_t)iabs(s - clip1((pa + pb * (x - 7) + pc * (y - 7) + 16) >> 5));
+                    if (plane_av) spl += (uint32_t)iabs(s - clip1((pa + pb * (x - 7) + pc * (y - 7) + 16) >> 5));
                 }
             uint32_t best = sdc;
             int mode = 2;
             if (top_av && sv < best) { best = sv; mode = 0; }
             if (left_av && sh < best) { best = sh; mode = 1; }
-            if (top_av && left_av && spl < best) { best = spl; mode = 3; }
+            if (plane_av && spl < best) { best = spl; mode = 3; }
             out->pred_mode[mb] = (uint32_t)mode;
             out->mv[mb].mvx = out->mv[mb].mvy = 0;
             out->mv[mb].sad = out->mv[mb].pad = 0;

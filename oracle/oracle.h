@@ -41,7 +41,15 @@ typedef struct {
     int mbw, mbh;
     int qp;
     int num_slices;
+    int flags;     /* ORC_INTRA_CORNER_CHECK: Plane also needs the top-left MB's slice */
 } orc_frame_t;
+
+/* Intra16x16 Plane predicts from p[-1,-1] too, so a conforming encoder only
+ * picks it when the top-left macroblock is available. The reference shader
+ * only checks top and left (A1/shaders/intra_wavefront.comp:463, :486, :497),
+ * which lets it pick Plane across a slice boundary that starts at the top
+ * neighbour; with this flag the top-left slice is checked as well. */
+#define ORC_INTRA_CORNER_CHECK 1
 
 typedef struct {
     int range;        /* integer search range R: dx, dy in [-R, R] */

@@ -20,7 +20,11 @@ _u8p = ctypes.POINTER(ctypes.c_uint8)
 
 class Frame(ctypes.Structure):
     _fields_ = [("W", ctypes.c_int), ("H", ctypes.c_int), ("RW", ctypes.c_int), ("RH", ctypes.c_int),
-                ("mbw", ctypes.c_int), ("mbh", ctypes.c_int), ("qp", ctypes.c_int), ("num_slices", ctypes.c_int)]
+                ("mbw", ctypes.c_int), ("mbh", ctypes.c_int), ("qp", ctypes.c_int), ("num_slices", ctypes.c_int),
+                ("flags", ctypes.c_int)]
+
+
+INTRA_CORNER_CHECK = 1
 
 
 class MeParams(ctypes.Structure):
@@ -66,10 +70,10 @@ def _p(a):
     return ctypes.c_void_p(a.ctypes.data)
 
 
-def frame(W, H, qp, num_slices=1, coded_clamp=True):
+def frame(W, H, qp, num_slices=1, coded_clamp=True, corner_check=True):
     mbw, mbh = (W + 15) // 16, (H + 15) // 16
     RW, RH = (mbw * 16, mbh * 16) if coded_clamp else (W, H)
-    return Frame(W, H, RW, RH, mbw, mbh, qp, num_slices)
+    return Frame(W, H, RW, RH, mbw, mbh, qp, num_slices, INTRA_CORNER_CHECK if corner_check else 0)
 
 
 def alloc_outputs(mbs):

@@ -99,10 +99,10 @@ def test_p_frame(gpu, oracle_mod, W, H, coded_clamp, qp):
 
 
 @pytest.mark.parametrize("W,H", SIZES + [(1920, 1080)])
-@pytest.mark.parametrize("num_slices", [1, 4])
+@pytest.mark.parametrize("num_slices", [1, 4, 7])
 @pytest.mark.parametrize("qp", [10, 26, 40])
-@pytest.mark.parametrize("coded_clamp", [True, False])
-def test_i_frame(gpu, oracle_mod, W, H, num_slices, qp, coded_clamp):
+@pytest.mark.parametrize("coded_clamp,corner_check", [(True, True), (False, False), (True, False)])
+def test_i_frame(gpu, oracle_mod, W, H, num_slices, qp, coded_clamp, corner_check):
     import torch
     (y0, uv0), = _frames(W, H, 1, seed=W + 7 * qp)
     CW, CH = gpu.coded(W, H)
@@ -111,9 +111,9 @@ def test_i_frame(gpu, oracle_mod, W, H, num_slices, qp, coded_clamp):
     out = gpu.Outputs(W, H)
     rec = gpu.NV12(W, H)
     scr = gpu.scratch(CH // 16)
-    gpu.i_frame(cur, W, H, RW, RH, qp, num_slices, out, rec, scr)
+    gpu.i_frame(cur, W, H, RW, RH, qp, num_slices, out, rec, scr, flags=int(corner_check))
     assert gpu.wavefront_status(scr) == 0
-    f = oracle_mod.frame(W, H, qp, num_slices=num_slices, coded_clamp=coded_clamp)
+    f = oracle_mod.frame(W, H, qp, num_slices=num_slices, coded_clamp=coded_clamp, corner_check=corner_check)
     rec_y = np.zeros((CH, CW), np.uint8)
     rec_uv = np.zeros((CH // 2, CW), np.uint8)
     want = oracle_mod.i_frame(f, np.ascontiguousarray(y0), np.ascontiguousarray(uv0), rec_y, rec_uv)
@@ -158,7 +158,7 @@ def test_wavefront_bounded_wait_reports_error(gpu):
     scr = gpu.scratch(mbh)
     nz = torch.zeros((mbw * mbh, 24), dtype=torch.int32, device="cuda")
     mv = torch.zeros((mbw * mbh, 4), dtype=torch.int32, device="cuda")
-    scr[0] = 1  # row ticket starts past row 0: row 0 is never filtered or published
+    scr[0] = 1  # ticket starts past the first row group: it is never filtered or published
     stream = torch.cuda.current_stream().cuda_stream
     rc = L.b200enc_deblock_launch(mbw, mbh, 30, 1, ctypes.c_void_p(nz.data_ptr()), ctypes.c_void_p(mv.data_ptr()),
                                   ctypes.c_void_p(rec.y.data_ptr()), ctypes.c_void_p(rec.uv.data_ptr()), rec.pitch,
@@ -168,4 +168,28 @@ def test_wavefront_bounded_wait_reports_error(gpu):
     # the device is still fine afterwards
     scr.zero_()
     gpu.deblock(mbw, mbh, 30, 1, nz, mv, rec, scr)
+    assert gpu.wavefront_status(scr) == 0
+
+
+def test_intra_bounded_wait_reports_error(gpu):
+    """The intra wavefront with row 0 left unowned gives up within its
+    budget, reports error 1, and the next launch on the context is fine."""
+    import ctypes
+    import torch
+    L = gpu.lib()
+    W, H = 96, 64
+    cur = gpu.NV12(W, H)
+    out = gpu.Outputs(W, H)
+    rec = gpu.NV12(W, H)
+    scr = gpu.scratch(H // 16)
+    scr[0] = 1
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = L.b200enc_i_frame_launch(p(cur.y), p(cur.uv), cur.pitch, W, H, W, H, 26, 1, p(out.levels), p(out.dc),
+                                  p(out.nz), p(out.pred_mode), p(out.mv), p(rec.y), p(rec.uv), rec.pitch, p(scr), 0,
+                                  ctypes.c_uint32(2000), 1, stream)
+    assert rc == 0
+    assert gpu.wavefront_status(scr) == 1
+    scr.zero_()
+    gpu.i_frame(cur, W, H, W, H, 26, 1, out, rec, scr)
     assert gpu.wavefront_status(scr) == 0
