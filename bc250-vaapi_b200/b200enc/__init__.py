@@ -17,7 +17,7 @@ EXPORTS = [
     # include/b200enc.h
     "b200enc_me_full_search", "b200enc_p_frame", "b200enc_wavefront_scratch_bytes", "b200enc_i_frame",
     "b200enc_deblock", "b200enc_wavefront_status", "b200enc_i_frame_launch", "b200enc_deblock_launch",
-    "b200enc_deblock_noalloc",
+    "b200enc_deblock_noalloc", "b200enc_gemm_bf16",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
     "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",
@@ -76,6 +76,8 @@ def load_library(path=LIB_PATH):
     lib.gpu_compute_dispatch_encode_ext.argtypes = [ctypes.POINTER(GpuContext), GpuImage, _i, _i, _i, _i, _i, _i, _vp]
     lib.gpu_compute_begin_picture.argtypes = [ctypes.POINTER(GpuContext), GpuImage]
     lib.b200enc_ctx_encode_device.argtypes = [ctypes.POINTER(GpuContext), _vp, _vp, _i, _i, _i, _i, _i, _i, _i]
+    lib.b200enc_gemm_bf16.argtypes = [_i, _i, _i, _vp, ctypes.c_longlong, ctypes.c_longlong, _vp, ctypes.c_longlong,
+                                      ctypes.c_longlong, _vp, ctypes.c_longlong, _vp, _i, _vp, _vp]
     return lib
 
 
@@ -190,6 +192,17 @@ def i_frame(cur, W, H, RW, RH, qp, num_slices, out, rec, scr, ctas=0, stream=Non
 def deblock(mbw, mbh, qp, is_intra, nz, mv, rec, scr, ctas=0, stream=None):
     _check(lib().b200enc_deblock(mbw, mbh, qp, int(is_intra), _p(nz), _p(mv), rec.yp(), rec.uvp(), rec.pitch,
                                  _p(scr), scr.numel() * 4, ctas, _stream(stream)), "b200enc_deblock")
+
+
+GEMM_ACCUMULATE, GEMM_RELU = 1, 2
+
+
+def gemm_bf16(A, B, C, M, N, K, a_strides, b_strides, bias=None, flags=0, err=None, stream=None):
+    """C[:M,:N] = epilogue(A(m,k) . B(n,k)) on the tensor cores; A, B bf16
+    tensors addressed through (row, k) element strides, C float32."""
+    _check(lib().b200enc_gemm_bf16(M, N, K, _p(A), a_strides[0], a_strides[1], _p(B), b_strides[0], b_strides[1],
+                                   _p(C), C.stride(0), _p(bias) if bias is not None else None, flags,
+                                   _p(err) if err is not None else None, _stream(stream)), "b200enc_gemm_bf16")
 
 
 def wavefront_status(scr, stream=None):

@@ -171,7 +171,7 @@ def run_reference(args):
     if rank != 0:
         return
     frames = make_frames(0, 2)
-    budget = max(2.0, min(15.0, 150.0 / max(1, args.steps + args.warmup)))
+    budget = max(0.25, min(15.0, 120.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
         cpu_reference_frame_time(frames, budget_s=budget / 4)
     times = []

@@ -139,6 +139,20 @@ int b200enc_deblock_noalloc(int mbw, int mbh, int qp, int is_intra,
                             const uint32_t *nz, const void *mv,
                             uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch, void *stream);
 
+/* BF16 GEMM on the tcgen05 tensor cores with FP32 accumulation in tensor
+ * memory: C[m][n] (row pitch ldc floats) = epilogue(sum_k A(m,k) * B(n,k)),
+ * where A(m,k) = A[m*a_rs + k*a_ks] and B(n,k) = B[n*b_rs + k*b_ks] (BF16,
+ * element strides, so transposed operands need no copy). Epilogue flags:
+ * ACCUMULATE adds the existing C, then bias[n] (if bias != NULL), then RELU
+ * clamps at zero. `err` (device word, may be NULL) is set to 1 if an
+ * mbarrier wait gave up. Used by the motion-proposal network; no reference
+ * counterpart (the reference has no dense contraction). */
+#define B200ENC_GEMM_ACCUMULATE 1
+#define B200ENC_GEMM_RELU 2
+int b200enc_gemm_bf16(int M, int N, int K, const void *A, long long a_rs, long long a_ks,
+                      const void *B, long long b_rs, long long b_ks, float *C, long long ldc,
+                      const float *bias, int flags, uint32_t *err, void *stream);
+
 /* Reads the error word a wavefront launch left in its scratch (synchronises
  * `stream`): 0 = fine, 1 = a bounded wait gave up (the frame's output is
  * incomplete and must not be used), -1 = the read failed. */
