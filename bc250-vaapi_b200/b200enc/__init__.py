@@ -17,7 +17,11 @@ EXPORTS = [
     # include/b200enc.h
     "b200enc_me_full_search", "b200enc_p_frame", "b200enc_wavefront_scratch_bytes", "b200enc_i_frame",
     "b200enc_deblock", "b200enc_wavefront_status", "b200enc_i_frame_launch", "b200enc_deblock_launch",
-    "b200enc_deblock_noalloc", "b200enc_gemm_bf16",
+    "b200enc_deblock_noalloc", "b200enc_gemm_bf16", "b200enc_me_full_search_ex",
+    "b200enc_proposal_num_params", "b200enc_proposal_create", "b200enc_proposal_destroy",
+    "b200enc_proposal_set_params", "b200enc_proposal_get_params", "b200enc_proposal_prepare",
+    "b200enc_proposal_forward", "b200enc_proposal_labels", "b200enc_proposal_backward", "b200enc_proposal_adam",
+    "b200enc_proposal_train_step", "b200enc_proposal_me", "b200enc_proposal_tensor",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
     "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",
@@ -70,6 +74,8 @@ def load_library(path=LIB_PATH):
                                     _vp, ctypes.c_size_t, _i, _i, _vp]
     lib.b200enc_deblock.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, ctypes.c_size_t, _i, _vp]
     lib.b200enc_me_full_search.argtypes = [_vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp]
+    lib.b200enc_me_full_search_ex.argtypes = [_vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _i, _i,
+                                              _vp]
     lib.b200enc_p_frame.argtypes = [_vp, _vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                     _i, _vp]
     lib.b200enc_wavefront_status.argtypes = [_vp, _vp]
@@ -78,6 +84,22 @@ def load_library(path=LIB_PATH):
     lib.b200enc_ctx_encode_device.argtypes = [ctypes.POINTER(GpuContext), _vp, _vp, _i, _i, _i, _i, _i, _i, _i]
     lib.b200enc_gemm_bf16.argtypes = [_i, _i, _i, _vp, ctypes.c_longlong, ctypes.c_longlong, _vp, ctypes.c_longlong,
                                       ctypes.c_longlong, _vp, ctypes.c_longlong, _vp, _i, _vp, _vp]
+    lib.b200enc_proposal_create.restype = _vp
+    lib.b200enc_proposal_create.argtypes = [_i]
+    lib.b200enc_proposal_destroy.argtypes = [_vp]
+    lib.b200enc_proposal_destroy.restype = None
+    lib.b200enc_proposal_set_params.argtypes = [_vp, _vp, _i]
+    lib.b200enc_proposal_get_params.argtypes = [_vp, _vp, _i]
+    lib.b200enc_proposal_prepare.argtypes = [_vp, _vp, _i, _vp, _i, _i, _i, _i, _i, _vp, _i, _i, _vp]
+    lib.b200enc_proposal_forward.argtypes = [_vp, _i, _vp]
+    lib.b200enc_proposal_labels.argtypes = [_vp, _i, _vp, _vp, _vp]
+    lib.b200enc_proposal_backward.argtypes = [_vp, _i, _vp]
+    lib.b200enc_proposal_adam.argtypes = [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _i,
+                                          _vp]
+    lib.b200enc_proposal_train_step.argtypes = [_vp, _i, ctypes.c_float, _i, _vp]
+    lib.b200enc_proposal_me.argtypes = [_vp, _vp, _i, _vp, _i, _i, _i, _i, _i, _vp, _i, _i, _i, ctypes.c_float, _vp,
+                                        _vp]
+    lib.b200enc_proposal_tensor.argtypes = [_vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_size_t)]
     return lib
 
 
@@ -167,6 +189,25 @@ def me_full_search(cur, ref, W, H, RW, RH, rng, lam, zero_thresh, mv, stream=Non
                                         zero_thresh, _p(mv), _stream(stream)), "b200enc_me_full_search")
 
 
+ME_LOG_INTEGER = 1
+
+
+def me_full_search_ex(cur, ref, W, H, RW, RH, rng, lam, zero_thresh, mv, mb_list=None, mb_count=None,
+                      capacity=0, flags=0, stream=None):
+    _check(lib().b200enc_me_full_search_ex(cur.yp(), cur.pitch, ref.yp(), ref.pitch, W, H, RW, RH, rng, lam,
+                                           zero_thresh, _p(mv), _p(mb_list) if mb_list is not None else None,
+                                           _p(mb_count) if mb_count is not None else None, capacity, flags,
+                                           _stream(stream)), "b200enc_me_full_search_ex")
+
+
+def me_log_decode(pad):
+    """(valid, early_out, dx, dy) arrays from ME_LOG_INTEGER words."""
+    import numpy as np
+    pad = np.asarray(pad).astype(np.uint32)
+    return ((pad >> 31) & 1).astype(bool), ((pad >> 30) & 1).astype(bool), \
+        (pad & 0xFF).astype(np.int32) - 128, ((pad >> 8) & 0xFF).astype(np.int32) - 128
+
+
 def p_frame(cur, ref, W, H, RW, RH, qp, mv, out, rec, stream=None):
     _check(lib().b200enc_p_frame(cur.yp(), cur.uvp(), cur.pitch, ref.yp(), ref.uvp(), ref.pitch, W, H, RW, RH, qp,
                                  _p(mv), _p(out.levels), _p(out.dc), _p(out.nz), _p(out.pred_mode), rec.yp(),
@@ -194,7 +235,11 @@ def deblock(mbw, mbh, qp, is_intra, nz, mv, rec, scr, ctas=0, stream=None):
                                  _p(scr), scr.numel() * 4, ctas, _stream(stream)), "b200enc_deblock")
 
 
-GEMM_ACCUMULATE, GEMM_RELU = 1, 2
+GEMM_ACCUMULATE, GEMM_RELU, GEMM_OUT_BF16 = 1, 2, 4
+
+
+def GEMM_SPLITK(n):
+    return n << 16
 
 
 def gemm_bf16(A, B, C, M, N, K, a_strides, b_strides, bias=None, flags=0, err=None, stream=None):

@@ -15,70 +15,10 @@
 // window byte is read once per column. SAD is the byte-SIMD
 // vabsdiff4-with-add; the integer path uses no tensor cores. The column
 // dx = +R is scored directly, one candidate per thread, after the sweep.
-#include "common.cuh"
 #include "b200enc_internal.h"
+#include "me_common.cuh"
 
 namespace b200enc {
-
-__device__ __forceinline__ uint32_t sad4_acc(uint32_t a, uint32_t b, uint32_t c) {
-  uint32_t d;
-  asm("vabsdiff4.u32.u32.u32.add %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
-  return d;
-}
-
-template <int NT>
-__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* red) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if (NT == 32) return v;
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  uint32_t s = 0;
-#pragma unroll
-  for (int i = 0; i < NT / 32; ++i) s += red[i];
-  return s;
-}
-
-template <int NT>
-__device__ __forceinline__ uint32_t block_min(uint32_t v, uint32_t* red) {
-  v = __reduce_min_sync(0xffffffffu, v);
-  if (NT == 32) return v;
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  uint32_t m = 0xffffffffu;
-#pragma unroll
-  for (int i = 0; i < NT / 32; ++i) m = min(m, red[i]);
-  return m;
-}
-
-// Quarter-pel sample from precomputed half-pel planes, with the letters and
-// averages of motion_estimation.comp:197-213.
-__device__ __forceinline__ int qpel_sample(int phase, int G, int H, int M, int b, int h, int m, int s, int j) {
-  switch (phase) {
-    case 0: return G;
-    case 1: return (G + b + 1) >> 1;
-    case 2: return b;
-    case 3: return (b + H + 1) >> 1;
-    case 4: return (G + h + 1) >> 1;
-    case 5: return (b + h + 1) >> 1;
-    case 6: return (b + j + 1) >> 1;
-    case 7: return (b + m + 1) >> 1;
-    case 8: return h;
-    case 9: return (h + j + 1) >> 1;
-    case 10: return j;
-    case 11: return (j + m + 1) >> 1;
-    case 12: return (h + M + 1) >> 1;
-    case 13: return (h + s + 1) >> 1;
-    case 14: return (j + s + 1) >> 1;
-    default: return (m + s + 1) >> 1;
-  }
-}
-
-// Candidate offsets in quarter pels, motion_estimation.comp:395-398, :435-438.
-__constant__ int8_t kHalfOff[8][2] = {{2, 0}, {-2, 0}, {0, 2}, {0, -2}, {2, 2}, {2, -2}, {-2, 2}, {-2, -2}};
-__constant__ int8_t kQtrOff[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
 
 template <int R>
 struct MeShared {
@@ -87,25 +27,27 @@ struct MeShared {
   uint32_t win[WP * WW];
   uint32_t cur[64];
   uint32_t red[8];
-  uint32_t part[8][4];
-  // Refine planes over coordinates relative to the integer winner:
-  // columns -1..16 and rows -1..16 (18 x 18); raw horizontal 6-tap sums
-  // for rows -3..19 (23 x 18).
-  int16_t pb[18][18], ph[18][18], pj[18][18];
-  int32_t hr[23][18];
+  RefineShared rf;
 };
 
 template <int R>
 __global__ void __launch_bounds__(2 * R) me_full_search_kernel(const uint8_t* __restrict__ cur, int cur_pitch,
                                                                const uint8_t* __restrict__ ref, int ref_pitch,
                                                                Geo g, int lambda, int zero_thresh,
-                                                               MV* __restrict__ out) {
+                                                               MV* __restrict__ out, const int* __restrict__ mb_list,
+                                                               const int* __restrict__ mb_count, int flags) {
   constexpr int NT = 2 * R;
   using S = MeShared<R>;
   constexpr int WP = S::WP, WW = S::WW, SIDE = 2 * R + 1;
   __shared__ S sh;
   const int tid = threadIdx.x;
-  const int mbx = blockIdx.x, mby = blockIdx.y;
+  int mbx = blockIdx.x, mby = blockIdx.y;
+  if (mb_list) {  // list mode: one CTA per listed MB, the rest exit
+    if ((int)blockIdx.x >= *mb_count) return;
+    const int mb = mb_list[blockIdx.x];
+    mby = mb / g.mbw;
+    mbx = mb - mby * g.mbw;
+  }
   const int X = mbx * 16, Y = mby * 16;
   const int ox = X - R - 4, oy = Y - R - 4;  // window origin (multiple of 4)
 
@@ -149,7 +91,7 @@ __global__ void __launch_bounds__(2 * R) me_full_search_kernel(const uint8_t* __
   const uint32_t sad0 = block_sum<NT>(z, sh.red);
   MV* o = out + (size_t)mby * g.mbw + mbx;
   if (zero_thresh >= 0 && sad0 <= (uint32_t)zero_thresh) {
-    if (tid == 0) *o = MV{0, 0, sad0, 0u};
+    if (tid == 0) *o = MV{0, 0, sad0, (flags & B200ENC_ME_LOG_INTEGER) ? me_log_word(0, 0, true) : 0u};
     return;
   }
 
@@ -215,106 +157,51 @@ __global__ void __launch_bounds__(2 * R) me_full_search_kernel(const uint8_t* __
   const int mx = idx % SIDE - R, my = idx / SIDE - R;
   const uint32_t int_sad = (best >> 14) - (uint32_t)lambda * (uint32_t)(abs(mx) + abs(my));
 
-  // ---- half-pel planes around the winner --------------------------------
+  // ---- half/quarter-pel refine around the winner -------------------------
   const uint8_t* wb8 = reinterpret_cast<const uint8_t*>(sh.win);
   const int px0 = mx + R + 4, py0 = my + R + 4;  // window coords of the winner
   auto G8 = [&](int rx, int ry) -> int { return wb8[(py0 + ry) * WP + px0 + rx]; };
-  for (int i = tid; i < 23 * 18; i += NT) {
-    const int ry = i / 18 - 3, rx = i % 18 - 1;
-    sh.hr[ry + 3][rx + 1] = G8(rx - 2, ry) - 5 * G8(rx - 1, ry) + 20 * G8(rx, ry) + 20 * G8(rx + 1, ry) -
-                             5 * G8(rx + 2, ry) + G8(rx + 3, ry);
-  }
-  __syncthreads();
-  for (int i = tid; i < 18 * 18; i += NT) {
-    const int ry = i / 18 - 1, rx = i % 18 - 1;
-    sh.pb[ry + 1][rx + 1] = (int16_t)clip1((sh.hr[ry + 3][rx + 1] + 16) >> 5);
-    const int v = G8(rx, ry - 2) - 5 * G8(rx, ry - 1) + 20 * G8(rx, ry) + 20 * G8(rx, ry + 1) -
-                  5 * G8(rx, ry + 2) + G8(rx, ry + 3);
-    sh.ph[ry + 1][rx + 1] = (int16_t)clip1((v + 16) >> 5);
-    const int j1 = sh.hr[ry + 1][rx + 1] - 5 * sh.hr[ry + 2][rx + 1] + 20 * sh.hr[ry + 3][rx + 1] +
-                   20 * sh.hr[ry + 4][rx + 1] - 5 * sh.hr[ry + 5][rx + 1] + sh.hr[ry + 6][rx + 1];
-    sh.pj[ry + 1][rx + 1] = (int16_t)clip1((j1 + 512) >> 10);
-  }
-  __syncthreads();
-
-  // Eight candidates at once: per-thread partial SADs, then one reduction.
-  auto score8 = [&](const int8_t (*off)[2], int bx, int by, uint32_t* res) {
-    uint32_t p[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) p[c] = 0;
-    const uint8_t* cb = reinterpret_cast<const uint8_t*>(sh.cur);
-    for (int pix = tid; pix < 256; pix += NT) {
-      const int x = pix & 15, y = pix >> 4;
-      const int cv = cb[y * 16 + x];
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const int ox_ = bx + off[c][0], oy_ = by + off[c][1];  // quarter-pel offset from the integer winner
-        const int rx = x + (ox_ >> 2), ry = y + (oy_ >> 2);
-        const int phase = (oy_ & 3) * 4 + (ox_ & 3);
-        const int v = qpel_sample(phase, G8(rx, ry), G8(rx + 1, ry), G8(rx, ry + 1), sh.pb[ry + 1][rx + 1],
-                                  sh.ph[ry + 1][rx + 1], sh.ph[ry + 1][rx + 2], sh.pb[ry + 2][rx + 1],
-                                  sh.pj[ry + 1][rx + 1]);
-        p[c] += (uint32_t)abs(cv - v);
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-#pragma unroll
-      for (int o2 = 16; o2 > 0; o2 >>= 1) p[c] += __shfl_xor_sync(0xffffffffu, p[c], o2);
-    }
-    __syncthreads();
-    if ((tid & 31) == 0)
-#pragma unroll
-      for (int c = 0; c < 8; ++c) sh.part[c][tid >> 5] = p[c];
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      uint32_t s = 0;
-#pragma unroll
-      for (int w = 0; w < NT / 32; ++w) s += sh.part[c][w];
-      res[c] = s;
-    }
-  };
-
-  uint32_t cs[8];
-  score8(kHalfOff, 0, 0, cs);
-  uint32_t bsad = int_sad;
-  int hx = 0, hy = 0;
-#pragma unroll
-  for (int c = 0; c < 8; ++c)
-    if (cs[c] < bsad) { bsad = cs[c]; hx = kHalfOff[c][0]; hy = kHalfOff[c][1]; }
-  score8(kQtrOff, hx, hy, cs);
-  int qx = 0, qy = 0;
-#pragma unroll
-  for (int c = 0; c < 8; ++c)
-    if (cs[c] < bsad) { bsad = cs[c]; qx = kQtrOff[c][0]; qy = kQtrOff[c][1]; }
-  if (tid == 0) *o = MV{4 * mx + hx + qx, 4 * my + hy + qy, bsad, 0u};
+  int qx, qy;
+  const uint32_t bsad =
+      qpel_refine<NT>(sh.rf, G8, reinterpret_cast<const uint8_t*>(sh.cur), int_sad, &qx, &qy);
+  if (tid == 0)
+    *o = MV{4 * mx + qx, 4 * my + qy, bsad, (flags & B200ENC_ME_LOG_INTEGER) ? me_log_word(mx, my, false) : 0u};
 }
 
 }  // namespace b200enc
 
 using namespace b200enc;
 
-extern "C" int b200enc_me_full_search(const uint8_t* cur_y, int cur_pitch, const uint8_t* ref_y, int ref_pitch,
-                                      int W, int H, int RW, int RH, int range, int lambda, int zero_thresh,
-                                      void* mv_out, void* stream) {
+extern "C" int b200enc_me_full_search_ex(const uint8_t* cur_y, int cur_pitch, const uint8_t* ref_y, int ref_pitch,
+                                         int W, int H, int RW, int RH, int range, int lambda, int zero_thresh,
+                                         void* mv_out, const int* mb_list, const int* mb_count, int list_capacity,
+                                         int flags, void* stream) {
   if (!cur_y || !ref_y || !mv_out || W <= 0 || H <= 0 || RW <= 0 || RH <= 0) return -1;
   if ((cur_pitch & 3) || (ref_pitch & 3) || (((uintptr_t)cur_y) & 3) || (((uintptr_t)ref_y) & 3)) return -1;
   if (lambda < 0 || lambda > 1023) return -1;
+  if ((mb_list == nullptr) != (mb_count == nullptr)) return -1;
   Geo g{W, H, RW, RH, (W + 15) / 16, (H + 15) / 16};
-  dim3 grid(g.mbw, g.mbh);
+  if (mb_list && (list_capacity <= 0 || list_capacity > g.mbw * g.mbh)) return -1;
+  dim3 grid = mb_list ? dim3(list_capacity) : dim3(g.mbw, g.mbh);
   cudaStream_t st = (cudaStream_t)stream;
   switch (range) {
     case 16:
       me_full_search_kernel<16><<<grid, 32, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda, zero_thresh,
-                                                     (MV*)mv_out);
+                                                     (MV*)mv_out, mb_list, mb_count, flags);
       break;
     case 32:
       me_full_search_kernel<32><<<grid, 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda, zero_thresh,
-                                                     (MV*)mv_out);
+                                                     (MV*)mv_out, mb_list, mb_count, flags);
       break;
     default:
       return -1;
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int b200enc_me_full_search(const uint8_t* cur_y, int cur_pitch, const uint8_t* ref_y, int ref_pitch,
+                                      int W, int H, int RW, int RH, int range, int lambda, int zero_thresh,
+                                      void* mv_out, void* stream) {
+  return b200enc_me_full_search_ex(cur_y, cur_pitch, ref_y, ref_pitch, W, H, RW, RH, range, lambda, zero_thresh,
+                                   mv_out, nullptr, nullptr, 0, 0, stream);
 }

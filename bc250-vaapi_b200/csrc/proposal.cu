@@ -1,0 +1,754 @@
+// proposal.cu - the learned motion-proposal network: candidate preparation,
+// BF16 forward/backward on the tcgen05 GEMM, loss, Adam, candidate selection
+// and exact integer re-scoring with the plain search's refine.
+//
+// The reference has no learned part; this stands in for most of the
+// exhaustive search of me.cu. Per MB:
+//   candidates  c0 = the previous frame's co-located MV, c1..c8 its eight
+//               neighbours (raster order of the 3x3 block), c9 = zero; each
+//               rounded to integer pels, clamped to [-(R-2), R-2]
+//   features    exact SAD at every candidate, candidate offsets, duplicate
+//               flags, the previous frame's SADs, block gradients
+//   network     input 2 x 16x16 (current luma, residual against c0), four
+//               2x2 stride-2 convolutions of 32 channels (16x16 -> 1x1), then
+//               fc 96 -> 64 -> 16: logits of the 10 candidates and "none"
+//               (the full-search winner is within +-2 pels of no candidate),
+//               a no-residual logit, 4 unused
+//   decision    the 4 most probable distinct candidates; if their summed
+//               probability is under the confidence threshold the MB falls
+//               back to full search, otherwise every integer MV within +-2 of
+//               them is scored exactly with the full search's cost and
+//               tie-break key, and the winner gets the same half/quarter-pel
+//               refine. Whenever the full-search winner is inside those
+//               windows the result equals the plain search's bit for bit.
+//
+// Layout: conv rows are kept in Morton order inside each MB (row m of layer
+// l covers grid cell (x, y) with x = even bits of m, y = odd bits), so the
+// four rows of every 2x2 patch are consecutive and each 2x2 stride-2
+// convolution is a plain GEMM over the previous output viewed as
+// [rows/4][4*channels]; the backward pass needs no im2col or col2im either.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "b200enc_internal.h"
+#include "me_common.cuh"
+
+namespace b200enc {
+
+constexpr int kCand = 10;
+constexpr int kClasses = 11;  // candidates + none
+constexpr int kOut = 16;
+constexpr int kFeat = 64;
+constexpr int kFIn = 96;  // fc1 input: 32 conv features + 64 side features
+static_assert(kFIn == 32 + kFeat, "fc1 input = conv features + side features");
+constexpr int kLayers = 6;
+__host__ __device__ constexpr int layer_in(int l) { return l == 0 ? 8 : (l < 4 ? 128 : (l == 4 ? kFIn : 64)); }
+__host__ __device__ constexpr int layer_out(int l) { return l < 4 ? 32 : (l == 4 ? 64 : kOut); }
+__host__ __device__ constexpr int layer_woff(int l) {
+  return l == 0 ? 0 : layer_woff(l - 1) + layer_out(l - 1) * layer_in(l - 1) + layer_out(l - 1);
+}
+__host__ __device__ constexpr int layer_boff(int l) { return layer_woff(l) + layer_out(l) * layer_in(l); }
+constexpr int kParams = layer_boff(kLayers - 1) + layer_out(kLayers - 1);
+
+// per-MB state word
+constexpr uint32_t kStEarly = 1u, kStNoHist = 2u;  // dup mask in bits 8..17
+
+__constant__ int8_t kNb[9][2] = {{0, 0}, {-1, -1}, {0, -1}, {1, -1}, {-1, 0}, {1, 0}, {-1, 1}, {0, 1}, {1, 1}};
+
+struct LpBuf {
+  __nv_bfloat16 *x0, *y1, *y2, *y3, *f, *h;
+  float* logits;
+  int32_t* cand;      // [mbs][10] packed (cy << 16) | (cx & 0xffff)
+  uint32_t* cand_sad;  // [mbs][10]
+  uint32_t* state;     // [mbs]
+  uint32_t* sel;       // [mbs] 4 x int8 candidate indices (-1 unused)
+  float* p_norez;      // [mbs]
+  int* lists;          // learned [mbs], fallback [mbs]
+  int* counters;       // [0] learned, [1] fallback, [2] valid training samples, [3] early-outs
+};
+
+__device__ __forceinline__ int cand_x(int32_t p) { return (int)(int16_t)(p & 0xffff); }
+__device__ __forceinline__ int cand_y(int32_t p) { return p >> 16; }
+__device__ __forceinline__ int morton_x(int m) { return (m & 1) | ((m >> 1) & 2) | ((m >> 2) & 4); }
+__device__ __forceinline__ int morton_y(int m) { return ((m >> 1) & 1) | ((m >> 2) & 2) | ((m >> 3) & 4); }
+
+// ---------------------------------------------------------------------------
+// Preparation: candidates, their SADs, the network input and side features.
+// 64 threads per MB.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restrict__ cur, int cur_pitch,
+                                                        const uint8_t* __restrict__ ref, int ref_pitch, Geo g,
+                                                        const MV* __restrict__ prev, int R, int zero_thresh,
+                                                        LpBuf b) {
+  __shared__ uint8_t sc[256];
+  __shared__ int scx[kCand], scy[kCand];
+  __shared__ uint32_t ssad[kCand], sprev[9];
+  __shared__ uint32_t sgrad[2][2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int mb = blockIdx.x;
+  const int mby = mb / g.mbw, mbx = mb - mby * g.mbw;
+  const int X = mbx * 16, Y = mby * 16;
+  for (int i = tid; i < 256; i += 64) {
+    const int r = i >> 4, c = i & 15;
+    sc[i] = cur[(size_t)clampi(Y + r, 0, g.H - 1) * cur_pitch + min(X + c, g.W - 1)];
+  }
+  if (tid < kCand) {
+    int cx = 0, cy = 0;
+    if (tid < 9 && prev) {
+      const int nx = clampi(mbx + kNb[tid][0], 0, g.mbw - 1), ny = clampi(mby + kNb[tid][1], 0, g.mbh - 1);
+      const MV m = prev[ny * g.mbw + nx];
+      cx = clampi((m.mvx + 2) >> 2, -(R - 2), R - 2);
+      cy = clampi((m.mvy + 2) >> 2, -(R - 2), R - 2);
+      sprev[tid] = m.sad;
+    } else if (tid < 9) {
+      sprev[tid] = 0;
+    }
+    scx[tid] = cx;
+    scy[tid] = cy;
+  }
+  if (tid < 2) sgrad[0][tid] = sgrad[1][tid] = 0;
+  __syncthreads();
+
+  // exact SAD at each candidate: warp w scores candidates w, w+2, ...
+  for (int c = warp; c < kCand; c += 2) {
+    const int cx = scx[c], cy = scy[c];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int i = lane * 8 + k, y = i >> 4, x = i & 15;
+      const int rv = ref[(size_t)clampi(Y + y + cy, 0, g.RH - 1) * ref_pitch + clampi(X + x + cx, 0, g.RW - 1)];
+      s += (uint32_t)abs((int)sc[i] - rv);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) ssad[c] = s;
+  }
+  // block gradients: sum |horizontal| and |vertical| neighbour differences
+  {
+    uint32_t gh = 0, gv = 0;
+    for (int i = tid; i < 256; i += 64) {
+      const int y = i >> 4, x = i & 15;
+      if (x < 15) gh += (uint32_t)abs((int)sc[i] - (int)sc[i + 1]);
+      if (y < 15) gv += (uint32_t)abs((int)sc[i] - (int)sc[i + 16]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      gh += __shfl_xor_sync(0xffffffffu, gh, o);
+      gv += __shfl_xor_sync(0xffffffffu, gv, o);
+    }
+    if (lane == 0) {
+      sgrad[warp][0] = gh;
+      sgrad[warp][1] = gv;
+    }
+  }
+  __syncthreads();
+
+  uint32_t dup = 0;
+  uint32_t smin = 0xffffffffu;
+  for (int c = 0; c < kCand; ++c) {
+    for (int d = 0; d < c; ++d)
+      if (scx[d] == scx[c] && scy[d] == scy[c]) {
+        dup |= 1u << c;
+        break;
+      }
+    smin = min(smin, ssad[c]);
+  }
+  const bool early = zero_thresh >= 0 && ssad[9] <= (uint32_t)zero_thresh;
+
+  // network input: row m (Morton cell (ox, oy) of the 8x8 grid) holds the
+  // 2x2 pels (dy, dx) x (current, residual against c0) at k = (dy*2+dx)*2+ch
+  {
+    const int m = tid, ox = morton_x(m), oy = morton_y(m);
+    const int c0x = scx[0], c0y = scy[0];
+    __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+      for (int dx = 0; dx < 2; ++dx) {
+        const int y = 2 * oy + dy, x = 2 * ox + dx;
+        const int cv = sc[y * 16 + x];
+        const int rv =
+            ref[(size_t)clampi(Y + y + c0y, 0, g.RH - 1) * ref_pitch + clampi(X + x + c0x, 0, g.RW - 1)];
+        v[(dy * 2 + dx) * 2 + 0] = __float2bfloat16_rn((float)(cv - 128) * 0.015625f);
+        v[(dy * 2 + dx) * 2 + 1] = __float2bfloat16_rn((float)(cv - rv) * 0.015625f);
+      }
+    *reinterpret_cast<uint4*>(b.x0 + ((size_t)mb * 64 + m) * 8) = *reinterpret_cast<const uint4*>(v);
+  }
+  // side features (64), columns 32..95 of the fc1 input row
+  {
+    const int t = tid;
+    float f = 0.f;
+    if (t < 10) f = (float)min(ssad[t], 32767u) * (1.f / 4096.f);
+    else if (t < 20) f = (float)min(ssad[t - 10] - smin, 32767u) * (1.f / 4096.f);
+    else if (t < 30) f = (float)(scx[t - 20] - scx[0]) * 0.125f;
+    else if (t < 40) f = (float)(scy[t - 30] - scy[0]) * 0.125f;
+    else if (t < 50) f = (dup >> (t - 40)) & 1u ? 1.f : 0.f;
+    else if (t < 59) f = (float)min(sprev[t - 50], 32767u) * (1.f / 4096.f);
+    else if (t == 59) f = (float)abs(scx[0]) * 0.03125f;
+    else if (t == 60) f = (float)abs(scy[0]) * 0.03125f;
+    else if (t == 61) f = (float)(sgrad[0][0] + sgrad[1][0]) / 7680.f;
+    else if (t == 62) f = (float)(sgrad[0][1] + sgrad[1][1]) / 7680.f;
+    else f = prev ? 0.f : 1.f;
+    b.f[(size_t)mb * kFIn + 32 + t] = __float2bfloat16_rn(f);
+  }
+  if (tid < kCand) {
+    b.cand[mb * kCand + tid] = (scy[tid] << 16) | (scx[tid] & 0xffff);
+    b.cand_sad[mb * kCand + tid] = ssad[tid];
+  }
+  if (tid == 0) b.state[mb] = (early ? kStEarly : 0u) | (prev ? 0u : kStNoHist) | (dup << 8);
+}
+
+// ---------------------------------------------------------------------------
+// Selection: masked softmax over the distinct candidates and "none", the
+// top 4, the confidence test, and the learned / fallback lists.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void masked_softmax(const float* z, uint32_t dup, float* p) {
+  float mx = -INFINITY;
+  for (int j = 0; j < kClasses; ++j)
+    if (!((dup >> j) & 1u)) mx = fmaxf(mx, z[j]);
+  float s = 0.f;
+  for (int j = 0; j < kClasses; ++j) {
+    p[j] = ((dup >> j) & 1u) ? 0.f : expf(z[j] - mx);
+    s += p[j];
+  }
+  const float inv = 1.f / s;
+  for (int j = 0; j < kClasses; ++j) p[j] *= inv;
+}
+
+__global__ void lp_select_kernel(int mbs, LpBuf b, float conf_thresh, MV* __restrict__ mv_out) {
+  const int mb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mb >= mbs) return;
+  const uint32_t st = b.state[mb];
+  if (st & kStEarly) {
+    mv_out[mb] = MV{0, 0, b.cand_sad[mb * kCand + 9], 0u};
+    atomicAdd(&b.counters[3], 1);
+    b.sel[mb] = 0xffffffffu;
+    return;
+  }
+  if (st & kStNoHist) {
+    b.lists[mbs + atomicAdd(&b.counters[1], 1)] = mb;
+    b.sel[mb] = 0xffffffffu;
+    return;
+  }
+  const uint32_t dup = (st >> 8) & 0x3ffu;
+  float z[kClasses], p[kClasses];
+  for (int j = 0; j < kClasses; ++j) z[j] = b.logits[(size_t)mb * kOut + j];
+  masked_softmax(z, dup, p);
+  b.p_norez[mb] = 1.f / (1.f + expf(-b.logits[(size_t)mb * kOut + 11]));
+  uint32_t chosen = dup, sel = 0xffffffffu;
+  float conf = 0.f;
+  for (int k = 0; k < 4; ++k) {
+    int best = -1;
+    for (int c = 0; c < kCand; ++c)
+      if (!((chosen >> c) & 1u) && (best < 0 || p[c] > p[best])) best = c;
+    if (best < 0) break;
+    chosen |= 1u << best;
+    conf += p[best];
+    sel = (sel & ~(0xffu << (8 * k))) | ((uint32_t)best << (8 * k));
+  }
+  b.sel[mb] = sel;
+  if (conf < conf_thresh) {
+    b.lists[mbs + atomicAdd(&b.counters[1], 1)] = mb;
+  } else {
+    b.lists[atomicAdd(&b.counters[0], 1)] = mb;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Exact re-scoring of the selected candidates' +-2 windows, then the refine.
+// 64 threads per MB, persistent over the learned list.
+// ---------------------------------------------------------------------------
+struct RescoreShared {
+  uint32_t patch[4][20][6];  // candidate k: rows cy-2 .. cy+17, words from xa = (X+cx-2) & ~3
+  uint32_t cur[64];
+  uint8_t win[23][24];  // refine neighbourhood of the winner: rows/cols -3..19
+  uint32_t red[2];
+  RefineShared rf;
+};
+
+__device__ __forceinline__ uint32_t load_word_clamped(const uint8_t* row, int gx, int RW) {
+  if (gx >= 0 && gx + 3 < RW) return __ldg(reinterpret_cast<const uint32_t*>(row + gx));
+  return (uint32_t)__ldg(row + clampi(gx, 0, RW - 1)) | ((uint32_t)__ldg(row + clampi(gx + 1, 0, RW - 1)) << 8) |
+         ((uint32_t)__ldg(row + clampi(gx + 2, 0, RW - 1)) << 16) |
+         ((uint32_t)__ldg(row + clampi(gx + 3, 0, RW - 1)) << 24);
+}
+
+__global__ void __launch_bounds__(64) lp_rescore_kernel(const uint8_t* __restrict__ cur, int cur_pitch,
+                                                        const uint8_t* __restrict__ ref, int ref_pitch, Geo g,
+                                                        int R, int lambda, int mbs, LpBuf b,
+                                                        MV* __restrict__ mv_out) {
+  __shared__ RescoreShared sh;
+  const int tid = threadIdx.x;
+  const int n = b.counters[0];
+  const int SIDE = 2 * R + 1;
+  for (int li = blockIdx.x; li < n; li += gridDim.x) {
+    const int mb = b.lists[li];
+    const int mby = mb / g.mbw, mbx = mb - mby * g.mbw;
+    const int X = mbx * 16, Y = mby * 16;
+    const uint32_t sel = b.sel[mb];
+    int nk = 0, ccx[4], ccy[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int c = (int)((sel >> (8 * k)) & 0xffu);
+      if (c < kCand) {
+        const int32_t p = b.cand[mb * kCand + c];
+        ccx[nk] = cand_x(p);
+        ccy[nk] = cand_y(p);
+        ++nk;
+      }
+    }
+    // stage the current MB (clamped to W, H) and the candidate patches
+    for (int i = tid; i < 64; i += 64) {
+      const int r = i >> 2, w = i & 3;
+      const uint8_t* cp = cur + (size_t)clampi(Y + r, 0, g.H - 1) * cur_pitch;
+      const int gx = X + 4 * w;
+      uint32_t v;
+      if (gx + 3 < g.W) {
+        v = __ldg(reinterpret_cast<const uint32_t*>(cp + gx));
+      } else {
+        v = (uint32_t)__ldg(cp + min(gx, g.W - 1)) | ((uint32_t)__ldg(cp + min(gx + 1, g.W - 1)) << 8) |
+            ((uint32_t)__ldg(cp + min(gx + 2, g.W - 1)) << 16) | ((uint32_t)__ldg(cp + min(gx + 3, g.W - 1)) << 24);
+      }
+      sh.cur[i] = v;
+    }
+    for (int i = tid; i < nk * 20 * 6; i += 64) {
+      const int k = i / 120, rem = i - k * 120, r = rem / 6, w = rem - r * 6;
+      const int xa = (X + ccx[k] - 2) & ~3;
+      const uint8_t* rp = ref + (size_t)clampi(Y + ccy[k] - 2 + r, 0, g.RH - 1) * ref_pitch;
+      sh.patch[k][r][w] = load_word_clamped(rp, xa + 4 * w, g.RW);
+    }
+    __syncthreads();
+
+    // 25 offsets per candidate, up to 100 positions over 64 threads
+    uint32_t best = 0xffffffffu;
+    for (int pos = tid; pos < nk * 25; pos += 64) {
+      const int k = pos / 25, o = pos - k * 25, oy = o / 5, ox = o - oy * 5;
+      const int dx = ccx[k] - 2 + ox, dy = ccy[k] - 2 + oy;
+      const int xa = (X + ccx[k] - 2) & ~3;
+      const int byte0 = (X + dx) - xa;  // 0..7
+      const int w0 = byte0 >> 2, shft = (byte0 & 3) * 8;
+      uint32_t s = 0;
+#pragma unroll 4
+      for (int r = 0; r < 16; ++r) {
+        const uint32_t* rw = sh.patch[k][oy + r] + w0;
+        const uint32_t a0 = rw[0], a1 = rw[1], a2 = rw[2], a3 = rw[3], a4 = rw[4];
+        s = sad4_acc(__funnelshift_r(a0, a1, shft), sh.cur[r * 4 + 0], s);
+        s = sad4_acc(__funnelshift_r(a1, a2, shft), sh.cur[r * 4 + 1], s);
+        s = sad4_acc(__funnelshift_r(a2, a3, shft), sh.cur[r * 4 + 2], s);
+        s = sad4_acc(__funnelshift_r(a3, a4, shft), sh.cur[r * 4 + 3], s);
+      }
+      const uint32_t cost = s + (uint32_t)lambda * (uint32_t)(abs(dx) + abs(dy));
+      best = min(best, (cost << 14) | (uint32_t)((dy + R) * SIDE + (dx + R)));
+    }
+    best = block_min<64>(best, sh.red);
+    const int idx = (int)(best & 0x3fffu);
+    const int mx = idx % SIDE - R, my = idx / SIDE - R;
+    const uint32_t int_sad = (best >> 14) - (uint32_t)lambda * (uint32_t)(abs(mx) + abs(my));
+
+    // refine neighbourhood of the winner, clamped like the full search's window
+    for (int i = tid; i < 23 * 23; i += 64) {
+      const int ry = i / 23 - 3, rx = i % 23 - 3;
+      sh.win[ry + 3][rx + 3] = ref[(size_t)clampi(Y + my + ry, 0, g.RH - 1) * ref_pitch +
+                                   clampi(X + mx + rx, 0, g.RW - 1)];
+    }
+    __syncthreads();
+    auto G8 = [&](int rx, int ry) -> int { return sh.win[ry + 3][rx + 3]; };
+    int qx, qy;
+    const uint32_t bsad = qpel_refine<64>(sh.rf, G8, reinterpret_cast<const uint8_t*>(sh.cur), int_sad, &qx, &qy);
+    if (tid == 0) mv_out[mb] = MV{4 * mx + qx, 4 * my + qy, bsad, 0u};
+    __syncthreads();  // shared memory is restaged for the next MB
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Training: labels, loss + logit gradient, ReLU backward, bias sums, Adam.
+// ---------------------------------------------------------------------------
+// Label of an MB from the full search's log word (B200ENC_ME_LOG_INTEGER):
+// the first distinct candidate whose +-2 window holds the integer winner,
+// else 10 ("none"); early-outs and MBs without history get weight 0. The
+// no-residual target is 1 iff all 24 nz words of the plain encode are 0.
+__global__ void lp_label_kernel(int mbs, LpBuf b, const MV* __restrict__ logged, const uint32_t* __restrict__ nz,
+                                int* __restrict__ label, float* __restrict__ norez, float* __restrict__ weight) {
+  const int mb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mb >= mbs) return;
+  const uint32_t st = b.state[mb];
+  const uint32_t w = logged[mb].pad;
+  const bool valid = (w >> 31) && !((w >> 30) & 1u) && !(st & (kStEarly | kStNoHist));
+  int lab = kClasses - 1;
+  if (valid) {
+    const int dx = (int)(w & 0xffu) - 128, dy = (int)((w >> 8) & 0xffu) - 128;
+    const uint32_t dup = (st >> 8) & 0x3ffu;
+    for (int c = 0; c < kCand; ++c) {
+      if ((dup >> c) & 1u) continue;
+      const int32_t p = b.cand[mb * kCand + c];
+      if (abs(dx - cand_x(p)) <= 2 && abs(dy - cand_y(p)) <= 2) {
+        lab = c;
+        break;
+      }
+    }
+  }
+  bool zero_res = true;
+  if (nz)
+    for (int k = 0; k < 24; ++k) zero_res = zero_res && nz[mb * 24 + k] == 0u;
+  label[mb] = lab;
+  norez[mb] = zero_res ? 1.f : 0.f;
+  weight[mb] = valid ? 1.f : 0.f;
+  if (valid) atomicAdd(&b.counters[2], 1);
+}
+
+// Mean over valid samples of CE(11-way masked softmax) + 0.5 BCE(no-residual);
+// writes dLoss/dlogits as BF16 and adds the loss sum to *loss.
+__global__ void lp_loss_kernel(int mbs, LpBuf b, const int* __restrict__ label, const float* __restrict__ norez,
+                               const float* __restrict__ weight, __nv_bfloat16* __restrict__ g5,
+                               float* __restrict__ loss) {
+  const int mb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mb >= mbs) return;
+  const float nval = (float)max(b.counters[2], 1);
+  const float w = weight[mb] / nval;
+  const uint32_t dup = (b.state[mb] >> 8) & 0x3ffu;
+  float z[kClasses], p[kClasses];
+  for (int j = 0; j < kClasses; ++j) z[j] = b.logits[(size_t)mb * kOut + j];
+  masked_softmax(z, dup, p);
+  const int y = label[mb];
+  const float zs = b.logits[(size_t)mb * kOut + 11];
+  const float ps = 1.f / (1.f + expf(-zs));
+  const float t = norez[mb];
+  __nv_bfloat16* gr = g5 + (size_t)mb * kOut;
+  for (int j = 0; j < kClasses; ++j) gr[j] = __float2bfloat16_rn(w * (p[j] - (j == y ? 1.f : 0.f)));
+  gr[11] = __float2bfloat16_rn(w * 0.5f * (ps - t));
+  for (int j = 12; j < kOut; ++j) gr[j] = __float2bfloat16_rn(0.f);
+  if (weight[mb] > 0.f) {
+    // softplus forms of -log p_y and the BCE
+    const float ce = -logf(fmaxf(p[y], 1e-30f));
+    const float bce = fmaxf(zs, 0.f) - zs * t + log1pf(expf(-fabsf(zs)));
+    atomicAdd(loss, w * (ce + 0.5f * bce));
+  }
+}
+
+// G[r][c] = bf16(dA[r*lda + c] * (Y[r*ldy + c] > 0)), c < C
+__global__ void lp_relu_bwd_kernel(long long rows, int C, const float* __restrict__ dA, int lda,
+                                   const __nv_bfloat16* __restrict__ Y, int ldy, __nv_bfloat16* __restrict__ G) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * C) return;
+  const long long r = i / C;
+  const int c = (int)(i - r * C);
+  const float y = __bfloat162float(Y[r * ldy + c]);
+  G[i] = __float2bfloat16_rn(y > 0.f ? dA[r * lda + c] : 0.f);
+}
+
+// out[c] += sum over rows of G[r][c] (G is [rows][C] BF16)
+__global__ void lp_colsum_kernel(long long rows, int C, const __nv_bfloat16* __restrict__ G, float* __restrict__ out) {
+  const int c = threadIdx.x % C;
+  const int lanes = blockDim.x / C;
+  const int sub = threadIdx.x / C;
+  if (sub >= lanes) return;
+  float s = 0.f;
+  for (long long r = (long long)blockIdx.x * lanes + sub; r < rows; r += (long long)gridDim.x * lanes)
+    s += __bfloat162float(G[r * C + c]);
+  atomicAdd(out + c, s);
+}
+
+__global__ void lp_adam_kernel(int n, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                               float* __restrict__ v, __nv_bfloat16* __restrict__ pb, float lr_t, float b1, float b2,
+                               float eps) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float pi = p[i] - lr_t * mi / (sqrtf(vi) + eps);
+  p[i] = pi;
+  pb[i] = __float2bfloat16_rn(pi);
+}
+
+__global__ void lp_to_bf16_kernel(int n, const float* __restrict__ p, __nv_bfloat16* __restrict__ pb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) pb[i] = __float2bfloat16_rn(p[i]);
+}
+
+// ---------------------------------------------------------------------------
+// Host runtime
+// ---------------------------------------------------------------------------
+struct Proposal {
+  int max_mbs = 0;
+  float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+  __nv_bfloat16* wb = nullptr;
+  LpBuf b{};
+  uint32_t* err = nullptr;
+  // training buffers (allocated on first use)
+  bool train_ready = false;
+  int *label = nullptr;
+  float *norez = nullptr, *weight = nullptr, *loss = nullptr;
+  __nv_bfloat16 *g5 = nullptr, *g4 = nullptr, *g3 = nullptr, *g2 = nullptr, *g1 = nullptr, *g0 = nullptr;
+  float *da5 = nullptr, *da4 = nullptr, *da3 = nullptr, *da2 = nullptr, *da1 = nullptr;
+  std::vector<void*> allocs;
+
+  template <class T>
+  bool alloc(T** p, size_t count) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, count * sizeof(T) + 16) != cudaSuccess) return false;
+    allocs.push_back(q);
+    *p = static_cast<T*>(q);
+    return true;
+  }
+  ~Proposal() {
+    for (void* p : allocs) cudaFree(p);
+  }
+  bool init(int mbs) {
+    max_mbs = mbs;
+    const size_t B = (size_t)mbs;
+    return alloc(&params, kParams) && alloc(&grads, kParams) && alloc(&adam_m, kParams) && alloc(&adam_v, kParams) &&
+           alloc(&wb, kParams) && alloc(&b.x0, B * 64 * 8) && alloc(&b.y1, B * 64 * 32) && alloc(&b.y2, B * 16 * 32) &&
+           alloc(&b.y3, B * 4 * 32) && alloc(&b.f, B * kFIn) && alloc(&b.h, B * 64) && alloc(&b.logits, B * kOut) &&
+           alloc(&b.cand, B * kCand) && alloc(&b.cand_sad, B * kCand) && alloc(&b.state, B) && alloc(&b.sel, B) &&
+           alloc(&b.p_norez, B) && alloc(&b.lists, 2 * B) && alloc(&b.counters, 8) && alloc(&err, 1) &&
+           cudaMemset(params, 0, kParams * 4) == cudaSuccess && cudaMemset(adam_m, 0, kParams * 4) == cudaSuccess &&
+           cudaMemset(adam_v, 0, kParams * 4) == cudaSuccess && cudaMemset(wb, 0, kParams * 2) == cudaSuccess &&
+           cudaMemset(b.counters, 0, 32) == cudaSuccess && cudaMemset(err, 0, 4) == cudaSuccess &&
+           cudaMemset(b.f, 0, B * kFIn * 2) == cudaSuccess;
+  }
+  bool init_train() {
+    if (train_ready) return true;
+    const size_t B = (size_t)max_mbs;
+    train_ready = alloc(&label, B) && alloc(&norez, B) && alloc(&weight, B) && alloc(&loss, 1) &&
+                  alloc(&g5, B * kOut) && alloc(&g4, B * 64) && alloc(&g3, B * 32) && alloc(&g2, B * 128) &&
+                  alloc(&g1, B * 512) && alloc(&g0, B * 2048) && alloc(&da5, B * 64) && alloc(&da4, B * kFIn) &&
+                  alloc(&da3, B * 128) && alloc(&da2, B * 512) && alloc(&da1, B * 2048) &&
+                  cudaMemset(loss, 0, 4) == cudaSuccess;
+    return train_ready;
+  }
+  const __nv_bfloat16* W(int l) const { return wb + layer_woff(l); }
+  const float* bias(int l) const { return params + layer_boff(l); }
+  float* gW(int l) const { return grads + layer_woff(l); }
+  float* gb(int l) const { return grads + layer_boff(l); }
+};
+
+static int splits_for(long long k) {
+  const long long chunks = (k + 63) / 64;
+  long long s = chunks / 16;
+  return (int)(s < 1 ? 1 : (s > 255 ? 255 : s));
+}
+
+#define LP_TRY(x) \
+  do {            \
+    if ((x) != 0) return -1; \
+  } while (0)
+
+static int lp_forward(Proposal* P, int mbs, cudaStream_t st) {
+  const long long B = mbs;
+  const int relu_bf = B200ENC_GEMM_RELU | B200ENC_GEMM_OUT_BF16;
+  void* s = (void*)st;
+  LP_TRY(b200enc_gemm_bf16((int)(B * 64), 32, 8, P->b.x0, 8, 1, P->W(0), 8, 1, (float*)P->b.y1, 32, P->bias(0),
+                           relu_bf, P->err, s));
+  LP_TRY(b200enc_gemm_bf16((int)(B * 16), 32, 128, P->b.y1, 128, 1, P->W(1), 128, 1, (float*)P->b.y2, 32,
+                           P->bias(1), relu_bf, P->err, s));
+  LP_TRY(b200enc_gemm_bf16((int)(B * 4), 32, 128, P->b.y2, 128, 1, P->W(2), 128, 1, (float*)P->b.y3, 32, P->bias(2),
+                           relu_bf, P->err, s));
+  LP_TRY(b200enc_gemm_bf16((int)B, 32, 128, P->b.y3, 128, 1, P->W(3), 128, 1, (float*)P->b.f, kFIn, P->bias(3),
+                           relu_bf, P->err, s));
+  LP_TRY(b200enc_gemm_bf16((int)B, 64, kFIn, P->b.f, kFIn, 1, P->W(4), kFIn, 1, (float*)P->b.h, 64, P->bias(4),
+                           relu_bf, P->err, s));
+  LP_TRY(b200enc_gemm_bf16((int)B, kOut, 64, P->b.h, 64, 1, P->W(5), 64, 1, P->b.logits, kOut, P->bias(5), 0, P->err,
+                           s));
+  return 0;
+}
+
+// Gradient of one layer given its BF16 output gradient G [rows][out]:
+// dW += G^T A (split K over the rows), db += column sums of G, and, when dA
+// is non-null, dA = G W (FP32, [rows][in]).
+static int lp_layer_bwd(Proposal* P, int l, long long rows, const __nv_bfloat16* G, const __nv_bfloat16* A, int lda,
+                        float* dA, cudaStream_t st) {
+  const int in = layer_in(l), out = layer_out(l);
+  void* s = (void*)st;
+  LP_TRY(b200enc_gemm_bf16(out, in, (int)rows, G, 1, out, A, 1, lda, P->gW(l), in, nullptr,
+                           B200ENC_GEMM_SPLITK(splits_for(rows)), P->err, s));
+  const int lanes = 256 / out;
+  long long blocks = (rows + lanes * 64 - 1) / (lanes * 64);
+  if (blocks > 1184) blocks = 1184;
+  if (blocks < 1) blocks = 1;
+  lp_colsum_kernel<<<(int)blocks, lanes * out, 0, st>>>(rows, out, G, P->gb(l));
+  if (dA) LP_TRY(b200enc_gemm_bf16((int)rows, in, out, G, out, 1, P->W(l), 1, in, dA, in, nullptr, 0, P->err, s));
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+static void relu_bwd(long long rows, int C, const float* dA, int lda, const __nv_bfloat16* Y, int ldy,
+                     __nv_bfloat16* G, cudaStream_t st) {
+  const long long n = rows * C;
+  lp_relu_bwd_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rows, C, dA, lda, Y, ldy, G);
+}
+
+static int lp_backward(Proposal* P, int mbs, cudaStream_t st) {
+  const long long B = mbs;
+  if (cudaMemsetAsync(P->grads, 0, kParams * 4, st) != cudaSuccess) return -1;
+  lp_loss_kernel<<<(mbs + 127) / 128, 128, 0, st>>>(mbs, P->b, P->label, P->norez, P->weight, P->g5, P->loss);
+  LP_TRY(lp_layer_bwd(P, 5, B, P->g5, P->b.h, 64, P->da5, st));
+  relu_bwd(B, 64, P->da5, 64, P->b.h, 64, P->g4, st);
+  LP_TRY(lp_layer_bwd(P, 4, B, P->g4, P->b.f, kFIn, P->da4, st));
+  relu_bwd(B, 32, P->da4, kFIn, P->b.f, kFIn, P->g3, st);
+  LP_TRY(lp_layer_bwd(P, 3, B, P->g3, P->b.y3, 128, P->da3, st));
+  relu_bwd(B * 4, 32, P->da3, 32, P->b.y3, 32, P->g2, st);
+  LP_TRY(lp_layer_bwd(P, 2, B * 4, P->g2, P->b.y2, 128, P->da2, st));
+  relu_bwd(B * 16, 32, P->da2, 32, P->b.y2, 32, P->g1, st);
+  LP_TRY(lp_layer_bwd(P, 1, B * 16, P->g1, P->b.y1, 128, P->da1, st));
+  relu_bwd(B * 64, 32, P->da1, 32, P->b.y1, 32, P->g0, st);
+  LP_TRY(lp_layer_bwd(P, 0, B * 64, P->g0, P->b.x0, 8, nullptr, st));
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+}  // namespace b200enc
+
+using namespace b200enc;
+
+extern "C" {
+
+int b200enc_proposal_num_params(void) { return kParams; }
+
+void* b200enc_proposal_create(int max_mbs) {
+  if (max_mbs <= 0 || max_mbs > (1 << 20)) return nullptr;
+  Proposal* P = new (std::nothrow) Proposal();
+  if (!P) return nullptr;
+  if (!P->init(max_mbs)) {
+    delete P;
+    return nullptr;
+  }
+  return P;
+}
+
+void b200enc_proposal_destroy(void* h) { delete static_cast<Proposal*>(h); }
+
+int b200enc_proposal_set_params(void* h, const float* host_params, int n) {
+  Proposal* P = static_cast<Proposal*>(h);
+  if (!P || !host_params || n != kParams) return -1;
+  if (cudaMemcpy(P->params, host_params, kParams * 4, cudaMemcpyHostToDevice) != cudaSuccess) return -1;
+  lp_to_bf16_kernel<<<(kParams + 255) / 256, 256>>>(kParams, P->params, P->wb);
+  return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_proposal_get_params(void* h, float* host_params, int n) {
+  Proposal* P = static_cast<Proposal*>(h);
+  if (!P || !host_params || n != kParams) return -1;
+  return cudaMemcpy(host_params, P->params, kParams * 4, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_proposal_prepare(void* h, const uint8_t* cur_y, int cur_pitch, const uint8_t* ref_y, int ref_pitch,
+                             int W, int H, int RW, int RH, const void* prev_mv, int range, int zero_thresh,
+                             void* stream) {
+  Proposal* P = static_cast<Proposal*>(h);
+  if (!P || !cur_y || !ref_y || W <= 0 || H <= 0 || RW <= 0 || RH <= 0) return -1;
+  if (range != 16 && range != 32) return -1;
+  Geo g{W, H, RW, RH, (W + 15) / 16, (H + 15) / 16};
+  const int mbs = g.mbw * g.mbh;
+  if (mbs > P->max_mbs) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemsetAsync(P->b.counters, 0, 32, st) != cudaSuccess) return -1;
+  lp_prepare_kernel<<<mbs, 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, (const MV*)prev_mv, range,
+                                        zero_thresh, P->b);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_proposal_forward(void* h, int mbs, void* stream) {
+  Proposal* P = static_cast<Proposal*>(h);
+  if (!P || mbs <= 0 || mbs > P->max_mbs) return -1;
+  return lp_forward(P, mbs, (cudaStream_t)stream);
+}
+
+int b200enc_proposal_labels(void* h, int mbs, const void* logged_mv, const uint32_t* nz, void* stream) {
+  Proposal* P = static_cast<Proposal*>(h);
+  if (!P || mbs <= 0 || mbs > P->max_mbs || !logged_mv || !P->init_train()) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  lp_label_kernel<<<(mbs + 127) / 128, 128, 0, st>>>(mbs, P->b, (const MV*)logged_mv, nz, P->label, P->norez,
+                                                     P->weight);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_proposal_backward(void* h, int mbs, void* stream) {
+  Proposal* P = static_cast<Proposal*>(h);
+  if (!P || mbs <= 0 || mbs > P->max_mbs || !P->init_train()) return -1;
+  return lp_backward(P, mbs, (cudaStream_t)stream);
+}
+
+int b200enc_proposal_adam(void* h, float lr, float beta1, float beta2, float eps, int step, void* stream) {
+  Proposal* P = static_cast<Proposal*>(h);
+  if (!P || step < 1) return -1;
+  const double c1 = 1.0 - std::pow((double)beta1, step), c2 = 1.0 - std::pow((double)beta2, step);
+  const float lr_t = (float)(lr * std::sqrt(c2) / c1);
+  lp_adam_kernel<<<(kParams + 255) / 256, 256, 0, (cudaStream_t)stream>>>(kParams, P->params, P->grads, P->adam_m,
+                                                                         P->adam_v, P->wb, lr_t, beta1, beta2, eps);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_proposal_train_step(void* h, int mbs, float lr, int step, void* stream) {
+  if (b200enc_proposal_forward(h, mbs, stream) != 0) return -1;
+  if (b200enc_proposal_backward(h, mbs, stream) != 0) return -1;
+  return b200enc_proposal_adam(h, lr, 0.9f, 0.999f, 1e-8f, step, stream);
+}
+
+int b200enc_proposal_me(void* h, const uint8_t* cur_y, int cur_pitch, const uint8_t* ref_y, int ref_pitch, int W,
+                        int H, int RW, int RH, const void* prev_mv, int range, int lambda, int zero_thresh,
+                        float conf_thresh, void* mv_out, void* stream) {
+  Proposal* P = static_cast<Proposal*>(h);
+  if (!P || !mv_out) return -1;
+  if (!prev_mv)  // no motion history: the plain search
+    return b200enc_me_full_search(cur_y, cur_pitch, ref_y, ref_pitch, W, H, RW, RH, range, lambda, zero_thresh,
+                                  mv_out, stream);
+  if (lambda < 0 || lambda > 1023) return -1;
+  if ((cur_pitch & 3) || (ref_pitch & 3) || (((uintptr_t)cur_y) & 3) || (((uintptr_t)ref_y) & 3)) return -1;
+  if (b200enc_proposal_prepare(h, cur_y, cur_pitch, ref_y, ref_pitch, W, H, RW, RH, prev_mv, range, zero_thresh,
+                               stream) != 0)
+    return -1;
+  Geo g{W, H, RW, RH, (W + 15) / 16, (H + 15) / 16};
+  const int mbs = g.mbw * g.mbh;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (lp_forward(P, mbs, st) != 0) return -1;
+  lp_select_kernel<<<(mbs + 127) / 128, 128, 0, st>>>(mbs, P->b, conf_thresh, (MV*)mv_out);
+  lp_rescore_kernel<<<std::min(mbs, 148 * 16), 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, range, lambda,
+                                                           mbs, P->b, (MV*)mv_out);
+  if (cudaGetLastError() != cudaSuccess) return -1;
+  return b200enc_me_full_search_ex(cur_y, cur_pitch, ref_y, ref_pitch, W, H, RW, RH, range, lambda, zero_thresh,
+                                   mv_out, P->b.lists + mbs, P->b.counters + 1, mbs, 0, stream);
+}
+
+// Device pointers of the runtime's tensors, for tests and the training
+// driver: 0 params f32, 1 grads f32, 2 x0, 3 y1, 4 y2, 5 y3, 6 f, 7 h (bf16),
+// 8 logits f32, 9 cand, 10 cand_sad, 11 state, 12 sel, 13 p_norez,
+// 14 lists, 15 counters, 16 label, 17 norez target, 18 weight, 19 loss, 20 err.
+int b200enc_proposal_tensor(void* h, int which, void** ptr, size_t* bytes) {
+  Proposal* P = static_cast<Proposal*>(h);
+  if (!P || !ptr || !bytes) return -1;
+  const size_t B = (size_t)P->max_mbs;
+  if (which >= 16 && !P->init_train()) return -1;
+  switch (which) {
+    case 0: *ptr = P->params; *bytes = kParams * 4; break;
+    case 1: *ptr = P->grads; *bytes = kParams * 4; break;
+    case 2: *ptr = P->b.x0; *bytes = B * 64 * 8 * 2; break;
+    case 3: *ptr = P->b.y1; *bytes = B * 64 * 32 * 2; break;
+    case 4: *ptr = P->b.y2; *bytes = B * 16 * 32 * 2; break;
+    case 5: *ptr = P->b.y3; *bytes = B * 4 * 32 * 2; break;
+    case 6: *ptr = P->b.f; *bytes = B * kFIn * 2; break;
+    case 7: *ptr = P->b.h; *bytes = B * 64 * 2; break;
+    case 8: *ptr = P->b.logits; *bytes = B * kOut * 4; break;
+    case 9: *ptr = P->b.cand; *bytes = B * kCand * 4; break;
+    case 10: *ptr = P->b.cand_sad; *bytes = B * kCand * 4; break;
+    case 11: *ptr = P->b.state; *bytes = B * 4; break;
+    case 12: *ptr = P->b.sel; *bytes = B * 4; break;
+    case 13: *ptr = P->b.p_norez; *bytes = B * 4; break;
+    case 14: *ptr = P->b.lists; *bytes = 2 * B * 4; break;
+    case 15: *ptr = P->b.counters; *bytes = 32; break;
+    case 16: *ptr = P->label; *bytes = B * 4; break;
+    case 17: *ptr = P->norez; *bytes = B * 4; break;
+    case 18: *ptr = P->weight; *bytes = B * 4; break;
+    case 19: *ptr = P->loss; *bytes = 4; break;
+    case 20: *ptr = P->err; *bytes = 4; break;
+    default: return -1;
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -8,6 +8,10 @@
 // operands of the backward pass need no copies, FP32 accumulation in tensor
 // memory, and an epilogue of optional FP32 accumulate-into-C, bias and ReLU.
 //
+// Split K (grid z > 1) gives each z slice a range of 64-wide K chunks and
+// adds the slices' FP32 partial products into C with atomics, for the weight
+// gradients of the backward pass, whose reduction runs over every sample.
+//
 // Per CTA: a 128 x BN output tile, 4 warps. For each 64-wide K chunk the
 // threads stage A (128 x 64) and B (BN x 64) in shared memory in the
 // canonical K-major no-swizzle UMMA layout (8-row x 16-byte core matrices,
@@ -82,13 +86,14 @@ struct TcShared {
   int failed;
 };
 
-// Loads one K chunk of an operand (rows x 64) into the canonical layout:
-// element (r, kk) at ((kk/8) * rows/8 + r/8) * 64 + (r%8) * 8 + kk%8.
-__device__ __forceinline__ void stage_chunk(uint16_t* dst, int rows, const __nv_bfloat16* src, long long rs,
+// Loads the first kw (a multiple of 16, at most 64) columns of one K chunk
+// of an operand (rows x kw) into the canonical layout: element (r, kk) at
+// ((kk/8) * rows/8 + r/8) * 64 + (r%8) * 8 + kk%8.
+__device__ __forceinline__ void stage_chunk(uint16_t* dst, int rows, int kw, const __nv_bfloat16* src, long long rs,
                                             long long ks, int r0, int rmax, int k0, int kmax) {
-  const int total = rows * kTcK;
+  const int total = rows * kw;
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
-    const int kk = i % kTcK, r = i / kTcK;  // consecutive threads walk k: coalesced for K-contiguous sources
+    const int kk = i % kw, r = i / kw;  // consecutive threads walk k: coalesced for K-contiguous sources
     const int gr = r0 + r, gk = k0 + kk;
     uint16_t v = 0;
     if (gr < rmax && gk < kmax) v = __bfloat16_as_ushort(src[(long long)gr * rs + (long long)gk * ks]);
@@ -125,27 +130,32 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(int M, int N, int K, const
   const uint32_t tmem = s.tmem;
   constexpr uint32_t idesc = umma_idesc_bf16(kTcM, BN);
 
+  // split K: blockIdx.z takes chunks [c_begin, c_end) and adds its partial
+  // product into C atomically
+  const int splits = gridDim.z;
+  const int nchunks_all = (K + kTcK - 1) / kTcK;
+  const int per = (nchunks_all + splits - 1) / splits;
+  const int c_begin = blockIdx.z * per, c_end = min(nchunks_all, c_begin + per);
   uint32_t phase = 0;
-  const int nchunks = (K + kTcK - 1) / kTcK;
-  for (int c = 0; c < nchunks; ++c) {
-    if (c > 0) {
+  for (int c = c_begin; c < c_end; ++c) {
+    if (c > c_begin) {
       // the MMAs reading the previous chunk must be done before restaging
       if (!mbar_wait(&s.bar, phase, 2000000000ull)) s.failed = 1;
       phase ^= 1;
     }
-    stage_chunk(s.a, kTcM, A, a_rs, a_ks, m0, M, c * kTcK, K);
-    stage_chunk(s.b, BN, B, b_rs, b_ks, n0, N, c * kTcK, K);
+    const int ksteps = min(kTcK, K - c * kTcK + 15) / 16;  // 16-wide MMA steps holding real K
+    stage_chunk(s.a, kTcM, ksteps * 16, A, a_rs, a_ks, m0, M, c * kTcK, K);
+    stage_chunk(s.b, BN, ksteps * 16, B, b_rs, b_ks, n0, N, c * kTcK, K);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (s.failed) break;
     if (threadIdx.x == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-      for (int k = 0; k < kTcK / 16; ++k) {
+      for (int k = 0; k < ksteps; ++k) {
         // K step k covers the core-matrix chunks 2k and 2k+1
         const uint64_t da = umma_desc(smem_u32(s.a) + (uint32_t)(2 * k * (kTcM / 8) * 128), kTcM * 16, 128);
         const uint64_t db = umma_desc(smem_u32(s.b) + (uint32_t)(2 * k * (BN / 8) * 128), BN * 16, 128);
-        const uint32_t acc = (c > 0 || k > 0) ? 1u : 0u;
+        const uint32_t acc = (c > c_begin || k > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "setp.ne.b32 p, %4, 0;\n\t"
@@ -158,11 +168,12 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(int M, int N, int K, const
                    : "memory");
     }
   }
-  if (!s.failed && !mbar_wait(&s.bar, phase, 2000000000ull)) s.failed = 1;
+  const bool any = c_end > c_begin;
+  if (any && !s.failed && !mbar_wait(&s.bar, phase, 2000000000ull)) s.failed = 1;
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-  if (!s.failed) {
+  if (any && !s.failed) {
     // epilogue: warp w owns TMEM lanes (= rows) 32w .. 32w+31
     const int row = m0 + warp * 32 + lane;
 #pragma unroll
@@ -176,16 +187,32 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(int M, int N, int K, const
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (row < M) {
+        if (splits > 1) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = n0 + cb + j;
-          if (col >= N) continue;
-          float x = __uint_as_float(v[j]);
-          float* dst = C + (long long)row * ldc + col;
-          if (flags & B200ENC_GEMM_ACCUMULATE) x += *dst;
-          if (bias) x += bias[col];
-          if ((flags & B200ENC_GEMM_RELU) && x < 0.f) x = 0.f;
-          *dst = x;
+          for (int j = 0; j < 16; ++j) {
+            const int col = n0 + cb + j;
+            if (col < N) atomicAdd(C + (long long)row * ldc + col, __uint_as_float(v[j]));
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int col = n0 + cb + j;
+            if (col >= N) continue;
+            float x = __uint_as_float(v[j]);
+            if (flags & B200ENC_GEMM_OUT_BF16) {
+              __nv_bfloat16* dst = reinterpret_cast<__nv_bfloat16*>(C) + (long long)row * ldc + col;
+              if (flags & B200ENC_GEMM_ACCUMULATE) x += __bfloat162float(*dst);
+              if (bias) x += bias[col];
+              if ((flags & B200ENC_GEMM_RELU) && x < 0.f) x = 0.f;
+              *dst = __float2bfloat16_rn(x);
+            } else {
+              float* dst = C + (long long)row * ldc + col;
+              if (flags & B200ENC_GEMM_ACCUMULATE) x += *dst;
+              if (bias) x += bias[col];
+              if ((flags & B200ENC_GEMM_RELU) && x < 0.f) x = 0.f;
+              *dst = x;
+            }
+          }
         }
       }
     }
@@ -206,7 +233,8 @@ static int launch_tc(int M, int N, int K, const void* A, long long a_rs, long lo
   const size_t smem = sizeof(TcShared<BN>) + 128;
   if (cudaFuncSetAttribute(tc_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return -1;
-  dim3 grid((M + kTcM - 1) / kTcM, (N + BN - 1) / BN);
+  const int splits = (flags >> 16) & 0xFF;
+  dim3 grid((M + kTcM - 1) / kTcM, (N + BN - 1) / BN, splits > 1 ? splits : 1);
   tc_gemm_kernel<BN><<<grid, 128, smem, st>>>(M, N, K, (const __nv_bfloat16*)A, a_rs, a_ks,
                                               (const __nv_bfloat16*)B, b_rs, b_ks, C, ldc, bias, flags, err);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
@@ -220,6 +248,10 @@ extern "C" int b200enc_gemm_bf16(int M, int N, int K, const void* A, long long a
                                  long long b_rs, long long b_ks, float* C, long long ldc, const float* bias, int flags,
                                  uint32_t* err, void* stream) {
   if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !C) return -1;
+  const int splits = (flags >> 16) & 0xFF;
+  // split-K adds FP32 partial products atomically: no per-element epilogue
+  if (splits > 1 && (flags & (B200ENC_GEMM_OUT_BF16 | B200ENC_GEMM_RELU | B200ENC_GEMM_ACCUMULATE) || bias))
+    return -1;
   cudaStream_t st = (cudaStream_t)stream;
   if (N <= 32) return launch_tc<32>(M, N, K, A, a_rs, a_ks, B, b_rs, b_ks, C, ldc, bias, flags, err, st);
   if (N <= 64) return launch_tc<64>(M, N, K, A, a_rs, a_ks, B, b_rs, b_ks, C, ldc, bias, flags, err, st);

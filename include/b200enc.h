@@ -48,6 +48,23 @@ int b200enc_me_full_search(const uint8_t *cur_y, int cur_pitch,
                            int range, int lambda, int zero_thresh,
                            void *mv_out, void *stream);
 
+/* The same search over a device list of MB indices (raster mby*mbw+mbx):
+ * mb_list[0 .. *mb_count) with *mb_count <= list_capacity (device words,
+ * written by an earlier kernel, so the host never reads the count); only
+ * listed MBs' mv_out entries are written. mb_list == mb_count == NULL
+ * searches every MB. flags B200ENC_ME_LOG_INTEGER writes the integer winner
+ * into mv.pad: bit 31 set, bit 30 = zero-MV early-out, bits 8-15 dy+128,
+ * bits 0-7 dx+128 (the qpel refine can move the MV up to 3/4 pel, so the
+ * integer winner is not recoverable from mvx, mvy); used to log training
+ * labels for the motion-proposal network. No reference counterpart. */
+#define B200ENC_ME_LOG_INTEGER 1
+int b200enc_me_full_search_ex(const uint8_t *cur_y, int cur_pitch,
+                              const uint8_t *ref_y, int ref_pitch,
+                              int W, int H, int RW, int RH,
+                              int range, int lambda, int zero_thresh,
+                              void *mv_out, const int *mb_list, const int *mb_count,
+                              int list_capacity, int flags, void *stream);
+
 /* Fused P-frame chain given MVs: MC prediction, residual, forward 4x4, AC
  * quant (inter rounding), nz masks, chroma DC, dequant, inverse, recon.
  * Replaces residual_predict.comp (P path) + dct_transform.comp +
@@ -144,14 +161,59 @@ int b200enc_deblock_noalloc(int mbw, int mbh, int qp, int is_intra,
  * where A(m,k) = A[m*a_rs + k*a_ks] and B(n,k) = B[n*b_rs + k*b_ks] (BF16,
  * element strides, so transposed operands need no copy). Epilogue flags:
  * ACCUMULATE adds the existing C, then bias[n] (if bias != NULL), then RELU
- * clamps at zero. `err` (device word, may be NULL) is set to 1 if an
+ * clamps at zero, then OUT_BF16 stores BF16 instead of FP32. `err` (device word, may be NULL) is set to 1 if an
  * mbarrier wait gave up. Used by the motion-proposal network; no reference
  * counterpart (the reference has no dense contraction). */
 #define B200ENC_GEMM_ACCUMULATE 1
 #define B200ENC_GEMM_RELU 2
+#define B200ENC_GEMM_OUT_BF16 4 /* C is BF16 (ldc in elements), rounded to nearest even */
+/* Split the K reduction over n CTAs (2..255) that add FP32 partial products
+ * into C atomically (C += A.B^T); excludes bias, RELU, ACCUMULATE, OUT_BF16. */
+#define B200ENC_GEMM_SPLITK(n) ((n) << 16)
 int b200enc_gemm_bf16(int M, int N, int K, const void *A, long long a_rs, long long a_ks,
                       const void *B, long long b_rs, long long b_ks, float *C, long long ldc,
                       const float *bias, int flags, uint32_t *err, void *stream);
+
+/* ---- Learned motion proposal (no reference counterpart) -----------------
+ * A small network ranks ten integer MV candidates per MB (the previous
+ * frame's co-located MV, its 8 neighbours, zero) from the current 16x16 luma,
+ * the residual at the co-located MV and the candidates' exact SADs; the top
+ * four distinct candidates' +-2 pel windows are searched exactly with the
+ * full search's cost, tie-break and half/quarter-pel refine, and MBs whose
+ * top-4 probability is under conf_thresh take the full search. Where the
+ * full-search winner lies inside the chosen windows the MV equals
+ * b200enc_me_full_search's. A handle owns the parameters (FP32 master + BF16
+ * copy), the activations for up to max_mbs MBs, and (on first training use)
+ * the gradients and Adam state. Calls on one handle are stream-ordered and
+ * must not overlap. */
+int b200enc_proposal_num_params(void);
+void *b200enc_proposal_create(int max_mbs);
+void b200enc_proposal_destroy(void *h);
+int b200enc_proposal_set_params(void *h, const float *host_params, int n);
+int b200enc_proposal_get_params(void *h, float *host_params, int n);
+/* Candidates, their SADs, the network input and side features for every MB
+ * of a frame; prev_mv = the previous frame's b200enc_mv_t field (NULL: no
+ * history). Resets the handle's counters. */
+int b200enc_proposal_prepare(void *h, const uint8_t *cur_y, int cur_pitch, const uint8_t *ref_y, int ref_pitch,
+                             int W, int H, int RW, int RH, const void *prev_mv, int range, int zero_thresh,
+                             void *stream);
+int b200enc_proposal_forward(void *h, int mbs, void *stream);
+/* Training targets from a full search logged with B200ENC_ME_LOG_INTEGER on
+ * the same frame (and, optionally, the plain encode's nz words). */
+int b200enc_proposal_labels(void *h, int mbs, const void *logged_mv, const uint32_t *nz, void *stream);
+/* Loss gradient through every layer (after forward); gradients overwrite. */
+int b200enc_proposal_backward(void *h, int mbs, void *stream);
+int b200enc_proposal_adam(void *h, float lr, float beta1, float beta2, float eps, int step, void *stream);
+/* forward + backward + Adam (beta 0.9, 0.999, eps 1e-8), step counts from 1 */
+int b200enc_proposal_train_step(void *h, int mbs, float lr, int step, void *stream);
+/* Motion estimation of one frame in the learned form; prev_mv NULL runs the
+ * full search. Same geometry, range, lambda, zero_thresh, mv_out and
+ * alignment rules as b200enc_me_full_search. */
+int b200enc_proposal_me(void *h, const uint8_t *cur_y, int cur_pitch, const uint8_t *ref_y, int ref_pitch,
+                        int W, int H, int RW, int RH, const void *prev_mv, int range, int lambda,
+                        int zero_thresh, float conf_thresh, void *mv_out, void *stream);
+/* Device pointer and size of an internal tensor (index list in proposal.cu). */
+int b200enc_proposal_tensor(void *h, int which, void **ptr, size_t *bytes);
 
 /* Reads the error word a wavefront launch left in its scratch (synchronises
  * `stream`): 0 = fine, 1 = a bounded wait gave up (the frame's output is

@@ -320,6 +320,54 @@ static uint32_t sad_qpel(const orc_frame_t *f, const int cur[256], const uint8_t
 static const int HALF_OFF[8][2] = {{2, 0}, {-2, 0}, {0, 2}, {0, -2}, {2, 2}, {2, -2}, {-2, 2}, {-2, -2}};
 static const int QTR_OFF[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
 
+void orc_me_refine(const orc_frame_t *f, const uint8_t *cur_y, int cp, const uint8_t *ref_y, int rp,
+                   int mbx, int mby, int imx, int imy, uint32_t int_sad, orc_mv_t *o)
+{
+    /* Steps 3-4 of the plain search below, for a given integer winner. */
+    int cur[256];
+    load_cur_mb(f, cur_y, cp, mbx, mby, cur);
+    const int X = mbx * 16, Y = mby * 16;
+    int bx = imx * 4, by = imy * 4;
+    uint32_t best = int_sad;
+    int hx = 0, hy = 0;
+    for (int c = 0; c < 8; c++) {
+        uint32_t s = sad_qpel(f, cur, ref_y, rp, X, Y, bx + HALF_OFF[c][0], by + HALF_OFF[c][1]);
+        if (s < best) { best = s; hx = HALF_OFF[c][0]; hy = HALF_OFF[c][1]; }
+    }
+    bx += hx; by += hy;
+    int qx = 0, qy = 0;
+    for (int c = 0; c < 8; c++) {
+        uint32_t s = sad_qpel(f, cur, ref_y, rp, X, Y, bx + QTR_OFF[c][0], by + QTR_OFF[c][1]);
+        if (s < best) { best = s; qx = QTR_OFF[c][0]; qy = QTR_OFF[c][1]; }
+    }
+    o->mvx = bx + qx;
+    o->mvy = by + qy;
+    o->sad = best;
+    o->pad = 0;
+}
+
+uint32_t orc_me_rect_key(const orc_frame_t *f, const orc_me_params_t *p, const uint8_t *cur_y, int cp,
+                         const uint8_t *ref_y, int rp, int mbx, int mby, int x0, int y0, int x1, int y1)
+{
+    /* The plain search's key (cost << 14 | raster index over [-R,R]^2)
+     * minimised over the integer MVs of [x0,x1] x [y0,y1] only. */
+    const int R = p->range, side = 2 * R + 1, X = mbx * 16, Y = mby * 16;
+    int cur[256];
+    load_cur_mb(f, cur_y, cp, mbx, mby, cur);
+    uint32_t best_key = 0xffffffffu;
+    for (int dy = y0; dy <= y1; dy++)
+        for (int dx = x0; dx <= x1; dx++) {
+            uint32_t s = 0;
+            for (int y = 0; y < 16; y++)
+                for (int x = 0; x < 16; x++)
+                    s += (uint32_t)iabs(cur[y * 16 + x] - refY(ref_y, rp, f->RW, f->RH, X + x + dx, Y + y + dy));
+            uint32_t cost = s + (uint32_t)p->lambda * (uint32_t)(iabs(dx) + iabs(dy));
+            uint32_t key = (cost << 14) | (uint32_t)((dy + R) * side + (dx + R));
+            if (key < best_key) best_key = key;
+        }
+    return best_key;
+}
+
 void orc_me_frame(const orc_frame_t *f, const orc_me_params_t *p,
                   const uint8_t *cur_y, int cp, const uint8_t *ref_y, int rp, orc_mv_t *mv)
 {
@@ -363,24 +411,7 @@ void orc_me_frame(const orc_frame_t *f, const orc_me_params_t *p,
                     if (key < best_key) { best_key = key; best_sad = s; }
                 }
             int idx = (int)(best_key & 0x3fff);
-            int imx = idx % side - R, imy = idx / side - R;
-            int bx = imx * 4, by = imy * 4;
-            uint32_t best = best_sad;
-            int hx = 0, hy = 0;
-            for (int c = 0; c < 8; c++) {
-                uint32_t s = sad_qpel(f, cur, ref_y, rp, X, Y, bx + HALF_OFF[c][0], by + HALF_OFF[c][1]);
-                if (s < best) { best = s; hx = HALF_OFF[c][0]; hy = HALF_OFF[c][1]; }
-            }
-            bx += hx; by += hy;
-            int qx = 0, qy = 0;
-            for (int c = 0; c < 8; c++) {
-                uint32_t s = sad_qpel(f, cur, ref_y, rp, X, Y, bx + QTR_OFF[c][0], by + QTR_OFF[c][1]);
-                if (s < best) { best = s; qx = QTR_OFF[c][0]; qy = QTR_OFF[c][1]; }
-            }
-            o->mvx = bx + qx;
-            o->mvy = by + qy;
-            o->sad = best;
-            o->pad = 0;
+            orc_me_refine(f, cur_y, cp, ref_y, rp, mbx, mby, idx % side - R, idx / side - R, best_sad, o);
         }
 }
 

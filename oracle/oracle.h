@@ -91,6 +91,17 @@ void orc_me_frame(const orc_frame_t *f, const orc_me_params_t *p,
                   const uint8_t *cur_y, int cur_pitch,
                   const uint8_t *ref_y, int ref_pitch, orc_mv_t *mv);
 
+/* Half- then quarter-pel refine of the plain search around integer winner
+ * (imx, imy) whose integer SAD is int_sad; writes mvx, mvy, sad, pad = 0. */
+void orc_me_refine(const orc_frame_t *f, const uint8_t *cur_y, int cur_pitch, const uint8_t *ref_y, int ref_pitch,
+                   int mbx, int mby, int imx, int imy, uint32_t int_sad, orc_mv_t *o);
+
+/* The plain search's selection key minimised over the integer MVs of the
+ * rectangle [x0,x1] x [y0,y1] (inside [-R,R]^2); key >> 14 = SAD + lambda
+ * cost, key & 0x3fff = (dy+R)*(2R+1) + dx+R. */
+uint32_t orc_me_rect_key(const orc_frame_t *f, const orc_me_params_t *p, const uint8_t *cur_y, int cur_pitch,
+                         const uint8_t *ref_y, int ref_pitch, int mbx, int mby, int x0, int y0, int x1, int y1);
+
 /* P-frame predict + transform + quant + DC + dequant + recon, given MVs. */
 void orc_p_frame(const orc_frame_t *f,
                  const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,

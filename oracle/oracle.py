@@ -98,6 +98,22 @@ def me_frame(f, cur_y, ref_y, rng, lam, zero_thresh=512):
     return mv
 
 
+def me_refine(f, cur_y, ref_y, mbx, mby, imx, imy, int_sad):
+    """Half/quarter-pel refine of the plain search around integer winner (imx, imy)."""
+    o = np.zeros(4, np.int32)
+    lib().orc_me_refine(ctypes.byref(f), _p(cur_y), cur_y.shape[1], _p(ref_y), ref_y.shape[1], int(mbx), int(mby),
+                        int(imx), int(imy), ctypes.c_uint32(int(int_sad)), _p(o))
+    return o
+
+
+def me_rect_key(f, cur_y, ref_y, rng, lam, mbx, mby, x0, y0, x1, y1):
+    """The plain search's key minimised over the integer MVs of [x0,x1] x [y0,y1]."""
+    lib().orc_me_rect_key.restype = ctypes.c_uint32
+    return int(lib().orc_me_rect_key(ctypes.byref(f), ctypes.byref(MeParams(rng, lam, -1)), _p(cur_y),
+                                     cur_y.shape[1], _p(ref_y), ref_y.shape[1], int(mbx), int(mby), int(x0), int(y0),
+                                     int(x1), int(y1)))
+
+
 def p_frame(f, cur_y, cur_uv, ref_y, ref_uv, mv, rec_y, rec_uv):
     o = alloc_outputs(f.mbw * f.mbh)
     o["mv"][:] = mv

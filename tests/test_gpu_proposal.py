@@ -1,0 +1,280 @@
+"""GPU parity of the learned motion proposal (csrc/proposal.cu) against the
+CPU oracle (oracle/proposal_ref.py, oracle.c):
+
+* preparation (candidates, exact SADs, state words, network input, side
+  features): bit-exact;
+* forward pass, layer by layer from the GPU's own BF16 inputs: every output
+  within one BF16 rounding of the exact value plus the FP32 accumulation
+  bound 1e-5 x sum|a w|;
+* backward pass (the gradient check): per-layer relative L2 error of the
+  weight and bias gradients <= 2e-2 against the oracle's backward on the same
+  activations, and the loss within 1e-4 relative;
+* the learned search: MBs that fall back equal the full search bit for bit;
+  learned MBs equal the oracle's exact search over the selected candidates'
+  +-2 windows followed by the plain refine, and equal the full search
+  whenever its integer winner lies inside those windows.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
+import proposal_ref as pr  # noqa: E402
+
+
+def _frames(W, H, n, seed):
+    from b200enc import synth
+    seq = synth.Sequence(W, H, seed=seed, pan=True, noise_patch=True)
+    return [seq.frame(t) for t in range(n)]
+
+
+def _pad(y, CW, CH):
+    return np.ascontiguousarray(np.pad(y, ((0, CH - y.shape[0]), (0, CW - y.shape[1])), mode="edge"))
+
+
+def _decode_cand(c):
+    c = c.astype(np.int64)
+    cx = ((c & 0xFFFF) ^ 0x8000) - 0x8000
+    cy = c >> 16
+    return np.stack([cx, cy], axis=-1)
+
+
+def _bf(t):
+    import torch
+    return t.float().cpu().numpy() if t.dtype == torch.bfloat16 else t.cpu().numpy()
+
+
+def _random_params(seed):
+    from b200enc import proposal
+    rs = np.random.Generator(np.random.PCG64(seed))
+    p = proposal.init_params(seed)
+    for wo, bo, i, n in proposal.layer_offsets():
+        p[bo:bo + n] = rs.standard_normal(n).astype(np.float32) * 0.1
+    return p
+
+
+def _prepared(gpu, W, H, R, prev_kind, coded, seed):
+    import torch
+    from b200enc import proposal
+    (y0, uv0), (y1, uv1) = _frames(W, H, 2, seed)
+    CW, CH = gpu.coded(W, H)
+    RW, RH = (CW, CH) if coded else (W, H)
+    ref = gpu.NV12.from_host(y0, uv0)
+    cur = gpu.NV12.from_host(y1, uv1)
+    mbs = (CW // 16) * (CH // 16)
+    rs = np.random.Generator(np.random.PCG64(seed + 1))
+    prev = None
+    if prev_kind == "random":
+        prev = np.zeros((mbs, 4), np.int32)
+        prev[:, :2] = rs.integers(-4 * (R + 12), 4 * (R + 12) + 1, (mbs, 2))  # beyond +-R: exercises the clamp
+        prev[:, 2] = rs.integers(0, 40000, mbs)
+        prev[rs.random(mbs) < 0.3, :2] = 0
+    P = proposal.Proposal(mbs)
+    P.prepare(cur, ref, W, H, RW, RH, torch.from_numpy(prev).cuda() if prev is not None else None, R, 512)
+    torch.cuda.synchronize()
+    refh = _pad(y0, CW, CH) if coded else np.ascontiguousarray(y0)
+    want = pr.prepare(np.ascontiguousarray(y1), refh, W, H, RW, RH, prev, R, 512)
+    return P, want, mbs, (cur, ref, RW, RH, y0, y1, refh)
+
+
+@pytest.mark.parametrize("W,H", [(96, 64), (200, 120), (16, 16)])
+@pytest.mark.parametrize("R", [16, 32])
+@pytest.mark.parametrize("prev_kind", ["random", None])
+@pytest.mark.parametrize("coded", [True, False])
+def test_prepare_bit_exact(gpu, W, H, R, prev_kind, coded):
+    import torch
+    from b200enc import proposal as pp
+    P, want, mbs, _ = _prepared(gpu, W, H, R, prev_kind, coded, seed=W + R)
+    got_cand = _decode_cand(P.tensor(pp.T_CAND, torch.int32, (mbs, 10)).cpu().numpy())
+    np.testing.assert_array_equal(got_cand, want["cand"])
+    np.testing.assert_array_equal(P.tensor(pp.T_CAND_SAD, torch.int32, (mbs, 10)).cpu().numpy().view(np.uint32),
+                                  want["cand_sad"])
+    np.testing.assert_array_equal(P.tensor(pp.T_STATE, torch.int32, (mbs,)).cpu().numpy().view(np.uint32),
+                                  want["state"])
+    np.testing.assert_array_equal(_bf(P.tensor(pp.T_X0, "bf16", (mbs * 64, 8))), want["x0"])
+    np.testing.assert_array_equal(_bf(P.tensor(pp.T_F, "bf16", (mbs, 96)))[:, 32:], want["side"])
+
+
+def _acts(P, mbs):
+    from b200enc import proposal as pp
+    import torch
+    f = _bf(P.tensor(pp.T_F, "bf16", (mbs, 96)))
+    return {"a0": _bf(P.tensor(pp.T_X0, "bf16", (mbs * 64, 8))), "y0": _bf(P.tensor(pp.T_Y1, "bf16", (mbs * 64, 32))),
+            "y1": _bf(P.tensor(pp.T_Y2, "bf16", (mbs * 16, 32))), "y2": _bf(P.tensor(pp.T_Y3, "bf16", (mbs * 4, 32))),
+            "y3": f[:, :32], "f": f, "h": _bf(P.tensor(pp.T_H, "bf16", (mbs, 64))),
+            "logits": P.tensor(pp.T_LOGITS, torch.float32, (mbs, 16)).cpu().numpy()}
+
+
+def test_forward_layerwise(gpu):
+    import torch
+    P, _, mbs, _ = _prepared(gpu, 320, 192, 32, "random", True, seed=11)
+    params = _random_params(3)
+    P.set_params(params)
+    P.forward(mbs)
+    torch.cuda.synchronize()
+    a = _acts(P, mbs)
+    L = pr.unpack(params)
+    ins = [a["a0"], a["y0"].reshape(-1, 128), a["y1"].reshape(-1, 128), a["y2"].reshape(-1, 128), a["f"], a["h"]]
+    outs = [a["y0"], a["y1"], a["y2"], a["y3"], a["h"], a["logits"]]
+    for l in range(6):
+        W, b = L[l]
+        Wb = pr.bf16(W).astype(np.float64)
+        A = ins[l].astype(np.float64)
+        z = A @ Wb.T + b
+        bound = np.abs(A) @ np.abs(Wb).T + np.abs(b)
+        if l < 5:
+            want = np.maximum(z, 0)
+            tol = 2.0 ** -8 * want + 1e-5 * bound + 1e-6
+        else:
+            want = z
+            tol = 1e-5 * bound + 1e-6
+        err = np.abs(outs[l] - want)
+        assert (err <= tol).all(), (l, float((err - tol).max()))
+        assert np.abs(want).max() > 0.01  # a live layer, not all zero
+
+
+def test_gradient_check(gpu):
+    """The BF16 backward kernels against the oracle's backward pass."""
+    import torch
+    from b200enc import proposal as pp
+    P, want, mbs, (cur, ref, RW, RH, *_rest) = _prepared(gpu, 320, 192, 32, "random", True, seed=12)
+    params = _random_params(4)
+    P.set_params(params)
+    logged = torch.zeros((mbs, 4), dtype=torch.int32, device="cuda")
+    gpu.me_full_search_ex(cur, ref, 320, 192, RW, RH, 32, 5, 512, logged, flags=gpu.ME_LOG_INTEGER)
+    rs = np.random.Generator(np.random.PCG64(5))
+    nz = torch.from_numpy((rs.random((mbs, 24)) < 0.05).astype(np.int32)).cuda()
+    P.labels(mbs, logged, nz)
+    P.forward(mbs)
+    P.backward(mbs)
+    torch.cuda.synchronize()
+    a = _acts(P, mbs)
+    state = want["state"]
+    lab, norez, w = pr.labels(state, want["cand"], logged.cpu().numpy()[:, 3], nz.cpu().numpy())
+    np.testing.assert_array_equal(P.tensor(pp.T_LABEL, torch.int32, (mbs,)).cpu().numpy(), lab)
+    np.testing.assert_array_equal(P.tensor(pp.T_WEIGHT, torch.float32, (mbs,)).cpu().numpy(), w)
+    np.testing.assert_array_equal(P.tensor(pp.T_NOREZ_T, torch.float32, (mbs,)).cpu().numpy(), norez)
+    assert w.sum() > mbs // 4 and len(set(lab[w > 0])) > 2
+    loss, g5 = pr.loss_and_grad(a["logits"], lab, norez, w, (state >> 8) & 0x3FF)
+    got_loss = float(P.tensor(pp.T_LOSS, torch.float32, (1,)).cpu()[0])
+    assert abs(got_loss - loss) <= 1e-4 * abs(loss)
+    want_g = pr.backward(params, a, g5.astype(np.float32))
+    got_g = P.tensor(pp.T_GRADS, torch.float32, (pp.NUM_PARAMS,)).cpu().numpy().astype(np.float64)
+    for l, (wo, bo, i, n) in enumerate(pp.layer_offsets()):
+        for lo, hi, what in ((wo, bo, "W"), (bo, bo + n, "b")):
+            ref_n = np.linalg.norm(want_g[lo:hi])
+            assert ref_n > 0, (l, what)
+            rel = np.linalg.norm(got_g[lo:hi] - want_g[lo:hi]) / ref_n
+            assert rel <= 2e-2, (l, what, rel)
+
+
+def test_training_reduces_loss(gpu):
+    """A few hundred Adam steps on logged full-search decisions: the loss
+    falls and the parameters stay finite."""
+    import torch
+    from b200enc import proposal as pp
+    W, H, R = 320, 192, 32
+    CW, CH = gpu.coded(W, H)
+    mbs = (CW // 16) * (CH // 16)
+    batches = []
+    for s in range(3):
+        fr = _frames(W, H, 3, seed=100 + s)
+        nv = [gpu.NV12.from_host(y, uv) for y, uv in fr]
+        mv1 = torch.zeros((mbs, 4), dtype=torch.int32, device="cuda")
+        gpu.me_full_search_ex(nv[1], nv[0], W, H, CW, CH, R, 5, 512, mv1)
+        mv2 = torch.zeros((mbs, 4), dtype=torch.int32, device="cuda")
+        gpu.me_full_search_ex(nv[2], nv[1], W, H, CW, CH, R, 5, 512, mv2, flags=gpu.ME_LOG_INTEGER)
+        batches.append((nv[2], nv[1], mv1, mv2))
+    P = pp.Proposal(mbs, pp.init_params(0))
+    loss_t = P.tensor(pp.T_LOSS, torch.float32, (1,))
+    hist = []
+    step = 0
+    for epoch in range(60):
+        loss_t.zero_()
+        for cur, ref, prev, logged in batches:
+            step += 1
+            P.prepare(cur, ref, W, H, CW, CH, prev, R, 512)
+            P.labels(mbs, logged)
+            P.train_step(mbs, 3e-3, step)
+        torch.cuda.synchronize()
+        hist.append(float(loss_t.cpu()[0]) / len(batches))
+    assert np.isfinite(P.get_params()).all()
+    assert hist[-1] < 0.6 * hist[0], hist[::10]
+
+
+def _learned_case(gpu, seed, conf, params_seed):
+    import torch
+    from b200enc import proposal as pp
+    W, H, R, lam = 320, 192, 32, 5
+    CW, CH = gpu.coded(W, H)
+    mbs = (CW // 16) * (CH // 16)
+    fr = _frames(W, H, 3, seed)
+    nv = [gpu.NV12.from_host(y, uv) for y, uv in fr]
+    prev = torch.zeros((mbs, 4), dtype=torch.int32, device="cuda")
+    gpu.me_full_search_ex(nv[1], nv[0], W, H, CW, CH, R, lam, 512, prev)
+    full = torch.zeros((mbs, 4), dtype=torch.int32, device="cuda")
+    gpu.me_full_search_ex(nv[2], nv[1], W, H, CW, CH, R, lam, 512, full, flags=gpu.ME_LOG_INTEGER)
+    P = pp.Proposal(mbs, _random_params(params_seed))
+    out = torch.full((mbs, 4), -7, dtype=torch.int32, device="cuda")
+    P.me(nv[2], nv[1], W, H, CW, CH, prev, R, lam, 512, conf, out)
+    torch.cuda.synchronize()
+    return P, mbs, out.cpu().numpy(), full.cpu().numpy(), fr, (W, H, CW, CH, R, lam)
+
+
+def test_learned_me_all_fallback_equals_full_search(gpu):
+    P, mbs, got, full, _, _ = _learned_case(gpu, 21, 1.01, 1)
+    c = P.counters()
+    assert c[0] == 0 and c[1] + c[3] == mbs
+    np.testing.assert_array_equal(got[:, :3], full[:, :3])
+
+
+@pytest.mark.parametrize("seed,params_seed,conf", [(22, 2, 0.0), (23, 5, 0.0), (24, 6, 0.6)])
+def test_learned_me_rescoring_exact(gpu, oracle_mod, seed, params_seed, conf):
+    import torch
+    from b200enc import proposal as pp
+    P, mbs, got, full, fr, (W, H, CW, CH, R, lam) = _learned_case(gpu, seed, conf, params_seed)
+    state = P.tensor(pp.T_STATE, torch.int32, (mbs,)).cpu().numpy().view(np.uint32)
+    sel = P.tensor(pp.T_SEL, torch.int32, (mbs,)).cpu().numpy().view(np.uint32)
+    cand = _decode_cand(P.tensor(pp.T_CAND, torch.int32, (mbs, 10)).cpu().numpy())
+    lists = P.tensor(pp.T_LISTS, torch.int32, (2 * mbs,)).cpu().numpy()
+    c = P.counters()
+    learned = set(lists[:c[0]].tolist())
+    fallback = set(lists[mbs:mbs + c[1]].tolist())
+    assert not (learned & fallback) and len(learned) + len(fallback) + c[3] == mbs
+    if conf == 0.0:
+        assert len(fallback) == 0 and len(learned) > mbs // 2
+    # selection agrees with the oracle's on the GPU's logits
+    logits = P.tensor(pp.T_LOGITS, torch.float32, (mbs, 16)).cpu().numpy()
+    osel, olearned, _ = pr.select(logits, state, conf)
+    gsel = np.array([[(s >> (8 * k)) & 0xFF for k in range(4)] for s in sel], np.int64)
+    gsel[gsel == 0xFF] = -1
+    for mb in learned:
+        np.testing.assert_array_equal(gsel[mb], osel[mb], err_msg=f"sel mb {mb}")
+    f = oracle_mod.frame(W, H, 26, coded_clamp=True)
+    cur = np.ascontiguousarray(fr[2][0])
+    ref = _pad(fr[1][0], CW, CH)
+    mbw = CW // 16
+    covered = 0
+    for mb in range(mbs):
+        if state[mb] & 1 or mb in fallback:
+            np.testing.assert_array_equal(got[mb, :3], full[mb, :3], err_msg=f"mb {mb}")
+            continue
+        mby, mbx = divmod(mb, mbw)
+        keys = [oracle_mod.me_rect_key(f, cur, ref, R, lam, mbx, mby, cand[mb, k, 0] - 2, cand[mb, k, 1] - 2,
+                                       cand[mb, k, 0] + 2, cand[mb, k, 1] + 2) for k in gsel[mb] if k >= 0]
+        key = min(keys)
+        idx = key & 0x3FFF
+        mx, my = idx % (2 * R + 1) - R, idx // (2 * R + 1) - R
+        int_sad = (key >> 14) - lam * (abs(mx) + abs(my))
+        want = oracle_mod.me_refine(f, cur, ref, mbx, mby, mx, my, int_sad)
+        np.testing.assert_array_equal(got[mb, :3], want[:3], err_msg=f"learned mb {mb}")
+        w = int(full[mb, 3]) & 0xFFFFFFFF
+        fx, fy = (w & 0xFF) - 128, ((w >> 8) & 0xFF) - 128
+        if any(abs(fx - cand[mb, k, 0]) <= 2 and abs(fy - cand[mb, k, 1]) <= 2 for k in gsel[mb] if k >= 0):
+            covered += 1
+            np.testing.assert_array_equal(got[mb, :3], full[mb, :3], err_msg=f"covered mb {mb}")
+    assert covered > 0

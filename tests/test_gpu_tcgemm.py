@@ -74,3 +74,52 @@ def test_gemm_bf16_epilogue(gpu, flags, with_bias):
                   flags=flags)
     torch.cuda.synchronize()
     _check(C.cpu(), A, B, C0, bias, flags)
+
+
+@pytest.mark.parametrize("M,N,K", [(300, 32, 8), (1000, 64, 128), (513, 96, 40)])
+@pytest.mark.parametrize("relu", [False, True])
+def test_gemm_bf16_out(gpu, M, N, K, relu):
+    """BF16 output: the FP32 result (bias, ReLU) rounded to nearest even."""
+    import torch
+    rs = np.random.Generator(np.random.PCG64(M + N + K + relu))
+    A, B = _bf16(rs, (M, K)), _bf16(rs, (N, K))
+    bias = torch.from_numpy(rs.standard_normal(N).astype(np.float32))
+    C = torch.zeros((M, N + 8), dtype=torch.bfloat16, device="cuda")
+    gpu.gemm_bf16(A.cuda(), B.cuda(), C, M, N, K, (K, 1), (K, 1), bias=bias.cuda(),
+                  flags=gpu.GEMM_OUT_BF16 | (gpu.GEMM_RELU if relu else 0))
+    torch.cuda.synchronize()
+    want = A.double() @ B.double().T + bias.double()[None, :]
+    if relu:
+        want = want.clamp_min(0)
+    got = C[:, :N].cpu().double()
+    # one BF16 rounding of a value within the FP32 tolerance of the exact sum
+    bound = A.double().abs() @ B.double().abs().T + bias.double().abs()[None, :]
+    err = (got - want).abs()
+    tol = 2.0 ** -8 * want.abs() + 1e-4 * bound + 1e-6
+    assert (err <= tol).all()
+    assert (C[:, N:].cpu() == 0).all()
+
+
+@pytest.mark.parametrize("M,N,K,splits", [(32, 128, 100000, 37), (128, 288, 5000, 8), (64, 17, 700, 3),
+                                          (32, 32, 64, 5)])
+def test_gemm_bf16_splitk(gpu, M, N, K, splits):
+    """Split K: slices add into C atomically (C += A.B^T), including slices
+    that own no K chunk."""
+    import torch
+    rs = np.random.Generator(np.random.PCG64(K + splits))
+    A, B = _bf16(rs, (M, K)), _bf16(rs, (N, K))
+    C0 = torch.from_numpy(rs.standard_normal((M, N)).astype(np.float32))
+    C = C0.cuda()
+    # transposed storage of A exercises strided staging too
+    Ad = A.T.contiguous().cuda()
+    gpu.gemm_bf16(Ad, B.cuda(), C, M, N, K, (1, M), (K, 1), flags=gpu.GEMM_SPLITK(splits))
+    torch.cuda.synchronize()
+    _check(C.cpu(), A, B, C0, None, 1)
+
+
+def test_gemm_bf16_rejects_bad_splitk(gpu):
+    import torch
+    A = torch.zeros((128, 64), dtype=torch.bfloat16, device="cuda")
+    C = torch.zeros((128, 64), dtype=torch.float32, device="cuda")
+    with pytest.raises(RuntimeError):
+        gpu.gemm_bf16(A, A, C, 128, 64, 64, (64, 1), (64, 1), flags=gpu.GEMM_SPLITK(4) | gpu.GEMM_RELU)
