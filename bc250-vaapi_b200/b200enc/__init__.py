@@ -21,7 +21,8 @@ EXPORTS = [
     "b200enc_proposal_num_params", "b200enc_proposal_create", "b200enc_proposal_destroy",
     "b200enc_proposal_set_params", "b200enc_proposal_get_params", "b200enc_proposal_prepare",
     "b200enc_proposal_forward", "b200enc_proposal_labels", "b200enc_proposal_backward", "b200enc_proposal_adam",
-    "b200enc_proposal_train_step", "b200enc_proposal_me", "b200enc_proposal_tensor",
+    "b200enc_proposal_train_step", "b200enc_proposal_me", "b200enc_proposal_tensor", "b200enc_proposal_load",
+    "b200enc_ctx_set_me", "b200enc_ctx_me_stats",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
     "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",
@@ -97,9 +98,11 @@ def load_library(path=LIB_PATH):
     lib.b200enc_proposal_adam.argtypes = [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _i,
                                           _vp]
     lib.b200enc_proposal_train_step.argtypes = [_vp, _i, ctypes.c_float, _i, _vp]
-    lib.b200enc_proposal_me.argtypes = [_vp, _vp, _i, _vp, _i, _i, _i, _i, _i, _vp, _i, _i, _i, ctypes.c_float, _vp,
-                                        _vp]
+    lib.b200enc_proposal_me.argtypes = [_vp, _vp, _i, _vp, _i, _i, _i, _i, _i, _vp, _i, _i, _i, _i, ctypes.c_float,
+                                        _vp, _vp]
     lib.b200enc_proposal_tensor.argtypes = [_vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_size_t)]
+    lib.b200enc_proposal_load.argtypes = [_vp, ctypes.c_char_p]
+    lib.b200enc_ctx_set_me.argtypes = [ctypes.POINTER(GpuContext), _i, ctypes.c_char_p, ctypes.c_float]
     return lib
 
 
@@ -351,6 +354,21 @@ class Context:
 
     def stream(self):
         return self.L.b200enc_ctx_stream(ctypes.byref(self.ctx))
+
+    ME_PLAIN, ME_LEARNED, ME_CANDIDATES = 0, 1, 2
+
+    def set_me(self, mode, weights=None, conf=0.9):
+        """Motion estimation form of P frames (plain / learned / candidates)."""
+        rc = self.L.b200enc_ctx_set_me(ctypes.byref(self.ctx), mode, weights.encode() if weights else None, conf)
+        if rc != 0:
+            raise RuntimeError(f"b200enc_ctx_set_me failed (rc={rc})")
+
+    def me_stats(self):
+        """(learned, fallback, early-out) MB counts of the last P frame."""
+        v = [ctypes.c_int() for _ in range(3)]
+        _check(self.L.b200enc_ctx_me_stats(ctypes.byref(self.ctx), *[ctypes.byref(x) for x in v]),
+               "b200enc_ctx_me_stats")
+        return tuple(x.value for x in v)
 
 
 class _DeviceSpan:

@@ -129,6 +129,12 @@ class Proposal:
         p = np.ascontiguousarray(params, np.float32)
         self._ck(self._lib.b200enc_proposal_set_params(self.h, p.ctypes.data, p.size), "set_params")
 
+    def load(self, path):
+        """Parameters from a checkpoint, read and SHA-256-checked by the library."""
+        rc = self._lib.b200enc_proposal_load(self.h, os.fsencode(path))
+        if rc != 0:
+            raise RuntimeError(f"b200enc_proposal_load({path}) failed (rc={rc})")
+
     def get_params(self):
         p = np.zeros(NUM_PARAMS, np.float32)
         self._ck(self._lib.b200enc_proposal_get_params(self.h, p.ctypes.data, p.size), "get_params")
@@ -173,11 +179,16 @@ class Proposal:
         from . import _stream
         self._ck(self._lib.b200enc_proposal_train_step(self.h, mbs, lr, step, _stream(stream)), "train_step")
 
-    def me(self, cur, ref, W, H, RW, RH, prev_mv, rng, lam, zero_thresh, conf, mv_out, stream=None):
+    NETWORK, CANDIDATES = 1, 2
+
+    def me(self, cur, ref, W, H, RW, RH, prev_mv, rng, lam, zero_thresh, param, mv_out, mode=1, stream=None):
+        """Learned-form ME of one frame: mode NETWORK (param = confidence
+        threshold) or CANDIDATES (no network; param = fallback cost per pel,
+        < 0 never)."""
         from . import _p, _stream
         self._ck(self._lib.b200enc_proposal_me(self.h, cur.yp(), cur.pitch, ref.yp(), ref.pitch, W, H, RW, RH,
                                                _p(prev_mv) if prev_mv is not None else None, rng, lam, zero_thresh,
-                                               conf, _p(mv_out), _stream(stream)), "proposal_me")
+                                               mode, param, _p(mv_out), _stream(stream)), "proposal_me")
 
     def counters(self):
         """[learned, fallback, valid training samples, early-outs] (synchronises)."""

@@ -8,6 +8,7 @@
 // event and sync_slot waits on it (bounded) and checks the wavefront status
 // word that was staged with the outputs.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 #include <fcntl.h>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -65,6 +66,15 @@ struct Impl {
   // parameters
   int range = 16, lambda = -1, zero_thresh = 512, clamp_coded = 1, deblock = -1;
   int intra_flags = B200ENC_INTRA_CORNER_CHECK;
+  // learned proposal (me_mode 1: network, 2: candidates only)
+  int me_mode = 0;
+  float conf = 0.9f;
+  std::string weights;
+  void* prop = nullptr;
+  int prop_mbs = 0;
+  b200enc_mv_t* d_mv_prev = nullptr;
+  bool mv_hist = false;  // d_mv holds the previous P frame's field
+  bool last_learned = false;  // the last P frame ran b200enc_proposal_me
   std::map<void*, Shadow> shadows;
   // Per-stage timing (the reference's BC250_PERF_STATS timestamps,
   // gpu_compute.c:50-67): a ring of event sets, one per frame, folded into
@@ -97,7 +107,13 @@ void free_frame_buffers(Impl* m) {
   cudaFree(m->d_nz);
   cudaFree(m->d_pred_mode);
   cudaFree(m->d_mv);
+  cudaFree(m->d_mv_prev);
   cudaFree(m->d_scratch);
+  if (m->prop) b200enc_proposal_destroy(m->prop);
+  m->prop = nullptr;
+  m->prop_mbs = 0;
+  m->d_mv_prev = nullptr;
+  m->mv_hist = false;
   m->rec[0] = m->rec[1] = nullptr;
   m->d_levels = nullptr;
   m->d_dc = nullptr;
@@ -137,7 +153,7 @@ int ensure_buffers(gpu_context_t* ctx, Impl* m, int W, int H) {
   bool ok = cudaMalloc(&m->rec[0], m->rec_bytes) == cudaSuccess && cudaMalloc(&m->rec[1], m->rec_bytes) == cudaSuccess &&
             cudaMalloc(&m->d_levels, mbs * 384 * 2) == cudaSuccess && cudaMalloc(&m->d_dc, mbs * 24 * 4) == cudaSuccess &&
             cudaMalloc(&m->d_nz, mbs * 24 * 4) == cudaSuccess && cudaMalloc(&m->d_pred_mode, mbs * 4) == cudaSuccess &&
-            cudaMalloc(&m->d_mv, mbs * 16) == cudaSuccess &&
+            cudaMalloc(&m->d_mv, mbs * 16) == cudaSuccess && cudaMalloc(&m->d_mv_prev, mbs * 16) == cudaSuccess &&
             cudaMalloc(&m->d_scratch, m->scratch_words * 2 * 4) == cudaSuccess;
   for (Slot& s : m->slot) {
     ok = ok && cudaMallocHost(&s.levels, mbs * 384 * 2) == cudaSuccess &&
@@ -203,6 +219,39 @@ int wait_event(cudaEvent_t ev) {
   }
 }
 
+// The packaged network parameters: <dir of libb200enc.so>/../b200enc/data/.
+std::string default_weights() {
+  Dl_info info;
+  if (dladdr((void*)&default_weights, &info) && info.dli_fname) {
+    std::string p = info.dli_fname;
+    const size_t cut = p.find_last_of('/');
+    p = (cut == std::string::npos) ? std::string(".") : p.substr(0, cut);
+    return p + "/../b200enc/data/proposal_h264.b2pn";
+  }
+  return "proposal_h264.b2pn";
+}
+
+// Creates the proposal runtime for the current frame size and loads the
+// parameters; 0, -1 on allocation failure, -2 on a missing or bad file.
+int ensure_proposal(Impl* m) {
+  const int mbs = m->mbw * m->mbh;
+  if (m->prop && m->prop_mbs == mbs) return 0;
+  if (m->prop) b200enc_proposal_destroy(m->prop);
+  m->prop = b200enc_proposal_create(mbs);
+  m->prop_mbs = mbs;
+  if (!m->prop) return -1;
+  if (m->me_mode == 2) return 0;  // the candidate search without the network needs no parameters
+  const std::string path = m->weights.empty() ? default_weights() : m->weights;
+  const int rc = b200enc_proposal_load(m->prop, path.c_str());
+  if (rc != 0) {
+    b200enc_proposal_destroy(m->prop);
+    m->prop = nullptr;
+    m->prop_mbs = 0;
+    return rc == -2 ? -2 : -1;
+  }
+  return 0;
+}
+
 // The whole hot path of one frame, enqueued on the context stream.
 int encode_frame(gpu_context_t* ctx, Impl* m, const uint8_t* y, const uint8_t* uv, int src_pitch, int W, int H, int qp,
                  int is_intra, int num_slices, int me_mode, const gpu_mv_t* cpu_mvs, bool stage) {
@@ -231,6 +280,8 @@ int encode_frame(gpu_context_t* ctx, Impl* m, const uint8_t* y, const uint8_t* u
   uint32_t* scr1 = m->d_scratch + m->scratch_words;
   int rc = 0;
   if (is_intra) {
+    m->mv_hist = false;
+    m->last_learned = false;
     perf_mark(m, 1);  // intra frames have no ME stage
     rc |= cudaMemsetAsync(scr0, 0, m->scratch_words * 4, m->stream) == cudaSuccess ? 0 : -1;
     rc |= b200enc_i_frame_launch(y, uv, src_pitch, W, H, RW, RH, qp, num_slices, m->d_levels, m->d_dc, m->d_nz,
@@ -242,10 +293,23 @@ int encode_frame(gpu_context_t* ctx, Impl* m, const uint8_t* y, const uint8_t* u
       memcpy(sl.mv, cpu_mvs, mbs * 16);
       rc |= cudaMemcpyAsync(m->d_mv, sl.mv, mbs * 16, cudaMemcpyHostToDevice, m->stream) == cudaSuccess ? 0 : -1;
     } else {
+      m->last_learned = false;
       const int lambda = m->lambda >= 0 ? m->lambda : (me_mode == 1 ? 8 : 5);
-      rc |= b200enc_me_full_search(y, src_pitch, ref_y, ref_pitch, W, H, ref_RW, ref_RH, m->range, lambda,
-                                   m->zero_thresh, m->d_mv, m->stream);
+      if (m->me_mode != 0 && have_ref && m->mv_hist) {
+        // the learned form fails loudly without its parameters
+        if (ensure_proposal(m) != 0) return -1;
+        rc |= cudaMemcpyAsync(m->d_mv_prev, m->d_mv, mbs * 16, cudaMemcpyDeviceToDevice, m->stream) == cudaSuccess
+                  ? 0
+                  : -1;
+        rc |= b200enc_proposal_me(m->prop, y, src_pitch, ref_y, ref_pitch, W, H, ref_RW, ref_RH, m->d_mv_prev,
+                                  m->range, lambda, m->zero_thresh, m->me_mode, m->conf, m->d_mv, m->stream);
+        m->last_learned = true;
+      } else {
+        rc |= b200enc_me_full_search(y, src_pitch, ref_y, ref_pitch, W, H, ref_RW, ref_RH, m->range, lambda,
+                                     m->zero_thresh, m->d_mv, m->stream);
+      }
     }
+    m->mv_hist = have_ref;
     perf_mark(m, 1);
     rc |= b200enc_p_frame(y, uv, src_pitch, ref_y, ref_uv, ref_pitch, W, H, RW, RH, qp, m->d_mv, m->d_levels, m->d_dc,
                           m->d_nz, m->d_pred_mode, out_y, out_uv, m->pitch, m->stream);
@@ -314,6 +378,13 @@ int bc250_gpu_init(bc250_gpu_context_t* ctx) {
   m->clamp_coded = (cl && strcmp(cl, "visible") == 0) ? 0 : 1;
   const char* ip = getenv("B200ENC_INTRA_PLANE");
   m->intra_flags = (ip && strcmp(ip, "shader") == 0) ? 0 : B200ENC_INTRA_CORNER_CHECK;
+  const char* me = getenv("B200ENC_ME");
+  if (me && strcmp(me, "learned") == 0) m->me_mode = 1;
+  if (me && strcmp(me, "candidates") == 0) m->me_mode = 2;
+  const char* wp = getenv("B200ENC_PROPOSAL_WEIGHTS");
+  if (wp && *wp) m->weights = wp;
+  const char* cf = getenv("B200ENC_PROPOSAL_CONF");
+  if (cf && *cf) m->conf = (float)atof(cf);
   ctx->impl = m;
   return 0;
 }
@@ -619,6 +690,46 @@ int b200enc_ctx_configure(gpu_context_t* ctx, int search_range, int lambda, int 
   if (m->clamp_coded != (recon_clamp_coded ? 1 : 0)) ctx->has_recon_frame = false;
   m->clamp_coded = recon_clamp_coded ? 1 : 0;
   m->deblock = deblock;
+  return 0;
+}
+
+int b200enc_ctx_set_me(gpu_context_t* ctx, int mode, const char* weights, float conf) {
+  Impl* m = impl_of(ctx);
+  if (!m || mode < 0 || mode > 2) return -1;
+  cudaStreamSynchronize(m->stream);
+  m->me_mode = mode;
+  m->weights = weights ? weights : "";
+  m->conf = conf;
+  if (m->prop) {
+    b200enc_proposal_destroy(m->prop);
+    m->prop = nullptr;
+    m->prop_mbs = 0;
+  }
+  if (mode != 0 && m->mbw > 0) return ensure_proposal(m);
+  if (mode == 1 && m->mbw == 0) {  // check the checkpoint now, before the first frame
+    void* probe = b200enc_proposal_create(1);
+    if (!probe) return -1;
+    const int rc = b200enc_proposal_load(probe, (m->weights.empty() ? default_weights() : m->weights).c_str());
+    b200enc_proposal_destroy(probe);
+    return rc;
+  }
+  return 0;
+}
+
+int b200enc_ctx_me_stats(gpu_context_t* ctx, int* learned, int* fallback, int* early) {
+  Impl* m = impl_of(ctx);
+  if (!m) return -1;
+  int c[4] = {0, 0, 0, 0};
+  if (m->prop && m->last_learned) {
+    void* ptr = nullptr;
+    size_t n = 0;
+    if (b200enc_proposal_tensor(m->prop, 15, &ptr, &n) != 0) return -1;
+    if (cudaMemcpyAsync(c, ptr, sizeof(c), cudaMemcpyDeviceToHost, m->stream) != cudaSuccess) return -1;
+    if (cudaStreamSynchronize(m->stream) != cudaSuccess) return -1;
+  }
+  if (learned) *learned = c[0];
+  if (fallback) *fallback = c[1];
+  if (early) *early = c[3];
   return 0;
 }
 

@@ -31,6 +31,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -220,7 +221,11 @@ __device__ __forceinline__ void masked_softmax(const float* z, uint32_t dup, flo
   for (int j = 0; j < kClasses; ++j) p[j] *= inv;
 }
 
-__global__ void lp_select_kernel(int mbs, LpBuf b, float conf_thresh, MV* __restrict__ mv_out) {
+// mode 1: the network's 4 most probable distinct candidates, falling back
+// when their probability sum is under `param`. mode 2 (no network): the 4
+// distinct candidates of lowest exact cost (SAD + lambda * |c|), falling
+// back when that lowest cost exceeds param * 256 (param < 0: never).
+__global__ void lp_select_kernel(int mbs, LpBuf b, int mode, float param, int lambda, MV* __restrict__ mv_out) {
   const int mb = blockIdx.x * blockDim.x + threadIdx.x;
   if (mb >= mbs) return;
   const uint32_t st = b.state[mb];
@@ -236,10 +241,23 @@ __global__ void lp_select_kernel(int mbs, LpBuf b, float conf_thresh, MV* __rest
     return;
   }
   const uint32_t dup = (st >> 8) & 0x3ffu;
-  float z[kClasses], p[kClasses];
-  for (int j = 0; j < kClasses; ++j) z[j] = b.logits[(size_t)mb * kOut + j];
-  masked_softmax(z, dup, p);
-  b.p_norez[mb] = 1.f / (1.f + expf(-b.logits[(size_t)mb * kOut + 11]));
+  float p[kClasses];
+  const bool heuristic = mode == 2;
+  uint32_t min_cost = 0xffffffffu;
+  if (heuristic) {
+    for (int c = 0; c < kCand; ++c) {
+      const int32_t q = b.cand[mb * kCand + c];
+      const uint32_t cost = b.cand_sad[mb * kCand + c] + (uint32_t)lambda * (uint32_t)(abs(cand_x(q)) + abs(cand_y(q)));
+      p[c] = -(float)cost;
+      min_cost = min(min_cost, cost);
+    }
+    p[kCand] = -INFINITY;
+  } else {
+    float z[kClasses];
+    for (int j = 0; j < kClasses; ++j) z[j] = b.logits[(size_t)mb * kOut + j];
+    masked_softmax(z, dup, p);
+    b.p_norez[mb] = 1.f / (1.f + expf(-b.logits[(size_t)mb * kOut + 11]));
+  }
   uint32_t chosen = dup, sel = 0xffffffffu;
   float conf = 0.f;
   for (int k = 0; k < 4; ++k) {
@@ -252,7 +270,8 @@ __global__ void lp_select_kernel(int mbs, LpBuf b, float conf_thresh, MV* __rest
     sel = (sel & ~(0xffu << (8 * k))) | ((uint32_t)best << (8 * k));
   }
   b.sel[mb] = sel;
-  if (conf < conf_thresh) {
+  const bool fall = heuristic ? (param >= 0.f && (float)min_cost > param * 256.f) : (conf < param);
+  if (fall) {
     b.lists[mbs + atomicAdd(&b.counters[1], 1)] = mb;
   } else {
     b.lists[atomicAdd(&b.counters[0], 1)] = mb;
@@ -368,10 +387,11 @@ __global__ void __launch_bounds__(64) lp_rescore_kernel(const uint8_t* __restric
 // ---------------------------------------------------------------------------
 // Training: labels, loss + logit gradient, ReLU backward, bias sums, Adam.
 // ---------------------------------------------------------------------------
-// Label of an MB from the full search's log word (B200ENC_ME_LOG_INTEGER):
-// the first distinct candidate whose +-2 window holds the integer winner,
-// else 10 ("none"); early-outs and MBs without history get weight 0. The
-// no-residual target is 1 iff all 24 nz words of the plain encode are 0.
+// Target of an MB from the full search's log word (B200ENC_ME_LOG_INTEGER):
+// the set (bit mask over the 11 classes) of distinct candidates whose +-2
+// window holds the integer winner, or {10} ("none") if there is none;
+// early-outs and MBs without history get weight 0. The no-residual target
+// is 1 iff all 24 nz words of the plain encode are 0.
 __global__ void lp_label_kernel(int mbs, LpBuf b, const MV* __restrict__ logged, const uint32_t* __restrict__ nz,
                                 int* __restrict__ label, float* __restrict__ norez, float* __restrict__ weight) {
   const int mb = blockIdx.x * blockDim.x + threadIdx.x;
@@ -379,19 +399,17 @@ __global__ void lp_label_kernel(int mbs, LpBuf b, const MV* __restrict__ logged,
   const uint32_t st = b.state[mb];
   const uint32_t w = logged[mb].pad;
   const bool valid = (w >> 31) && !((w >> 30) & 1u) && !(st & (kStEarly | kStNoHist));
-  int lab = kClasses - 1;
+  int lab = 0;
   if (valid) {
     const int dx = (int)(w & 0xffu) - 128, dy = (int)((w >> 8) & 0xffu) - 128;
     const uint32_t dup = (st >> 8) & 0x3ffu;
     for (int c = 0; c < kCand; ++c) {
       if ((dup >> c) & 1u) continue;
       const int32_t p = b.cand[mb * kCand + c];
-      if (abs(dx - cand_x(p)) <= 2 && abs(dy - cand_y(p)) <= 2) {
-        lab = c;
-        break;
-      }
+      if (abs(dx - cand_x(p)) <= 2 && abs(dy - cand_y(p)) <= 2) lab |= 1 << c;
     }
   }
+  if (lab == 0) lab = 1 << (kClasses - 1);
   bool zero_res = true;
   if (nz)
     for (int k = 0; k < 24; ++k) zero_res = zero_res && nz[mb * 24 + k] == 0u;
@@ -401,8 +419,10 @@ __global__ void lp_label_kernel(int mbs, LpBuf b, const MV* __restrict__ logged,
   if (valid) atomicAdd(&b.counters[2], 1);
 }
 
-// Mean over valid samples of CE(11-way masked softmax) + 0.5 BCE(no-residual);
-// writes dLoss/dlogits as BF16 and adds the loss sum to *loss.
+// Mean over valid samples of -log(probability mass of the target set under
+// the 11-way masked softmax) + 0.5 BCE(no-residual); writes dLoss/dlogits
+// (p_j - [j in set] p_j / P_set for the set term) as BF16 and adds the loss
+// sum to *loss.
 __global__ void lp_loss_kernel(int mbs, LpBuf b, const int* __restrict__ label, const float* __restrict__ norez,
                                const float* __restrict__ weight, __nv_bfloat16* __restrict__ g5,
                                float* __restrict__ loss) {
@@ -414,17 +434,22 @@ __global__ void lp_loss_kernel(int mbs, LpBuf b, const int* __restrict__ label, 
   float z[kClasses], p[kClasses];
   for (int j = 0; j < kClasses; ++j) z[j] = b.logits[(size_t)mb * kOut + j];
   masked_softmax(z, dup, p);
-  const int y = label[mb];
+  const uint32_t y = (uint32_t)label[mb];
+  float pset = 0.f;
+  for (int j = 0; j < kClasses; ++j)
+    if ((y >> j) & 1u) pset += p[j];
+  pset = fmaxf(pset, 1e-30f);
   const float zs = b.logits[(size_t)mb * kOut + 11];
   const float ps = 1.f / (1.f + expf(-zs));
   const float t = norez[mb];
   __nv_bfloat16* gr = g5 + (size_t)mb * kOut;
-  for (int j = 0; j < kClasses; ++j) gr[j] = __float2bfloat16_rn(w * (p[j] - (j == y ? 1.f : 0.f)));
+  for (int j = 0; j < kClasses; ++j)
+    gr[j] = __float2bfloat16_rn(w * (p[j] - (((y >> j) & 1u) ? p[j] / pset : 0.f)));
   gr[11] = __float2bfloat16_rn(w * 0.5f * (ps - t));
   for (int j = 12; j < kOut; ++j) gr[j] = __float2bfloat16_rn(0.f);
   if (weight[mb] > 0.f) {
     // softplus forms of -log p_y and the BCE
-    const float ce = -logf(fmaxf(p[y], 1e-30f));
+    const float ce = -logf(pset);
     const float bce = fmaxf(zs, 0.f) - zs * t + log1pf(expf(-fabsf(zs)));
     atomicAdd(loss, w * (ce + 0.5f * bce));
   }
@@ -530,6 +555,61 @@ struct Proposal {
   float* gb(int l) const { return grads + layer_boff(l); }
 };
 
+// SHA-256 (FIPS 180-4) for checkpoint integrity.
+struct Sha256 {
+  uint32_t h[8] = {0x6a09e667u, 0xbb67ae85u, 0x3c6ef372u, 0xa54ff53au, 0x510e527fu, 0x9b05688cu, 0x1f83d9abu, 0x5be0cd19u};
+  uint8_t buf[64];
+  size_t nbuf = 0;
+  uint64_t total = 0;
+  static uint32_t rotr(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
+  void block(const uint8_t* p) {
+    static const uint32_t k[64] = {
+        0x428a2f98u, 0x71374491u, 0xb5c0fbcfu, 0xe9b5dba5u, 0x3956c25bu, 0x59f111f1u, 0x923f82a4u, 0xab1c5ed5u,
+        0xd807aa98u, 0x12835b01u, 0x243185beu, 0x550c7dc3u, 0x72be5d74u, 0x80deb1feu, 0x9bdc06a7u, 0xc19bf174u,
+        0xe49b69c1u, 0xefbe4786u, 0x0fc19dc6u, 0x240ca1ccu, 0x2de92c6fu, 0x4a7484aau, 0x5cb0a9dcu, 0x76f988dau,
+        0x983e5152u, 0xa831c66du, 0xb00327c8u, 0xbf597fc7u, 0xc6e00bf3u, 0xd5a79147u, 0x06ca6351u, 0x14292967u,
+        0x27b70a85u, 0x2e1b2138u, 0x4d2c6dfcu, 0x53380d13u, 0x650a7354u, 0x766a0abbu, 0x81c2c92eu, 0x92722c85u,
+        0xa2bfe8a1u, 0xa81a664bu, 0xc24b8b70u, 0xc76c51a3u, 0xd192e819u, 0xd6990624u, 0xf40e3585u, 0x106aa070u,
+        0x19a4c116u, 0x1e376c08u, 0x2748774cu, 0x34b0bcb5u, 0x391c0cb3u, 0x4ed8aa4au, 0x5b9cca4fu, 0x682e6ff3u,
+        0x748f82eeu, 0x78a5636fu, 0x84c87814u, 0x8cc70208u, 0x90befffau, 0xa4506cebu, 0xbef9a3f7u, 0xc67178f2u};
+    uint32_t w[64];
+    for (int i = 0; i < 16; ++i)
+      w[i] = (uint32_t)p[4 * i] << 24 | (uint32_t)p[4 * i + 1] << 16 | (uint32_t)p[4 * i + 2] << 8 | p[4 * i + 3];
+    for (int i = 16; i < 64; ++i) {
+      const uint32_t s0 = rotr(w[i - 15], 7) ^ rotr(w[i - 15], 18) ^ (w[i - 15] >> 3);
+      const uint32_t s1 = rotr(w[i - 2], 17) ^ rotr(w[i - 2], 19) ^ (w[i - 2] >> 10);
+      w[i] = w[i - 16] + s0 + w[i - 7] + s1;
+    }
+    uint32_t a = h[0], b = h[1], c = h[2], d = h[3], e = h[4], f = h[5], g = h[6], hh = h[7];
+    for (int i = 0; i < 64; ++i) {
+      const uint32_t t1 = hh + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) + ((e & f) ^ (~e & g)) + k[i] + w[i];
+      const uint32_t t2 = (rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
+      hh = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + t2;
+    }
+    h[0] += a; h[1] += b; h[2] += c; h[3] += d; h[4] += e; h[5] += f; h[6] += g; h[7] += hh;
+  }
+  void update(const uint8_t* p, size_t n) {
+    total += n;
+    while (n) {
+      const size_t take = std::min(n, 64 - nbuf);
+      memcpy(buf + nbuf, p, take);
+      nbuf += take; p += take; n -= take;
+      if (nbuf == 64) { block(buf); nbuf = 0; }
+    }
+  }
+  void finish(uint8_t out[32]) {
+    const uint64_t bits = total * 8;
+    const uint8_t one = 0x80, zero = 0;
+    update(&one, 1);
+    while (nbuf != 56) update(&zero, 1);
+    uint8_t len[8];
+    for (int i = 0; i < 8; ++i) len[i] = (uint8_t)(bits >> (56 - 8 * i));
+    update(len, 8);
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 4; ++j) out[4 * i + j] = (uint8_t)(h[i] >> (24 - 8 * j));
+  }
+};
+
 static int splits_for(long long k) {
   const long long chunks = (k + 63) / 64;
   long long s = chunks / 16;
@@ -631,6 +711,37 @@ int b200enc_proposal_set_params(void* h, const float* host_params, int n) {
   return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1;
 }
 
+// Loads the parameters of a checkpoint file written by b200enc.proposal
+// (magic "B2PN", version 1, little-endian header n/step/meta length/has-Adam,
+// meta JSON, FP32 parameters, optional Adam moments, SHA-256 trailer).
+// Returns -2 on a checksum or format mismatch, -1 on I/O or device errors.
+int b200enc_proposal_load(void* h, const char* path) {
+  Proposal* P = static_cast<Proposal*>(h);
+  if (!P || !path) return -1;
+  FILE* f = fopen(path, "rb");
+  if (!f) return -1;
+  std::vector<uint8_t> data;
+  uint8_t tmp[65536];
+  size_t n;
+  while ((n = fread(tmp, 1, sizeof(tmp), f)) > 0) data.insert(data.end(), tmp, tmp + n);
+  fclose(f);
+  if (data.size() < 24 + 32) return -2;
+  const size_t body = data.size() - 32;
+  Sha256 sh;
+  sh.update(data.data(), body);
+  uint8_t dig[32];
+  sh.finish(dig);
+  if (memcmp(dig, data.data() + body, 32) != 0 || memcmp(data.data(), "B2PN", 4) != 0) return -2;
+  uint32_t hdr[5];
+  memcpy(hdr, data.data() + 4, 20);
+  if (hdr[0] != 1 || hdr[1] != (uint32_t)kParams) return -2;
+  const size_t off = 24 + (size_t)hdr[3];
+  if (off + (size_t)kParams * 4 > body) return -2;
+  std::vector<float> params(kParams);
+  memcpy(params.data(), data.data() + off, (size_t)kParams * 4);
+  return b200enc_proposal_set_params(h, params.data(), kParams);
+}
+
 int b200enc_proposal_get_params(void* h, float* host_params, int n) {
   Proposal* P = static_cast<Proposal*>(h);
   if (!P || !host_params || n != kParams) return -1;
@@ -691,10 +802,10 @@ int b200enc_proposal_train_step(void* h, int mbs, float lr, int step, void* stre
 }
 
 int b200enc_proposal_me(void* h, const uint8_t* cur_y, int cur_pitch, const uint8_t* ref_y, int ref_pitch, int W,
-                        int H, int RW, int RH, const void* prev_mv, int range, int lambda, int zero_thresh,
-                        float conf_thresh, void* mv_out, void* stream) {
+                        int H, int RW, int RH, const void* prev_mv, int range, int lambda, int zero_thresh, int mode,
+                        float param, void* mv_out, void* stream) {
   Proposal* P = static_cast<Proposal*>(h);
-  if (!P || !mv_out) return -1;
+  if (!P || !mv_out || (mode != 1 && mode != 2)) return -1;
   if (!prev_mv)  // no motion history: the plain search
     return b200enc_me_full_search(cur_y, cur_pitch, ref_y, ref_pitch, W, H, RW, RH, range, lambda, zero_thresh,
                                   mv_out, stream);
@@ -706,8 +817,8 @@ int b200enc_proposal_me(void* h, const uint8_t* cur_y, int cur_pitch, const uint
   Geo g{W, H, RW, RH, (W + 15) / 16, (H + 15) / 16};
   const int mbs = g.mbw * g.mbh;
   cudaStream_t st = (cudaStream_t)stream;
-  if (lp_forward(P, mbs, st) != 0) return -1;
-  lp_select_kernel<<<(mbs + 127) / 128, 128, 0, st>>>(mbs, P->b, conf_thresh, (MV*)mv_out);
+  if (mode == 1 && lp_forward(P, mbs, st) != 0) return -1;
+  lp_select_kernel<<<(mbs + 127) / 128, 128, 0, st>>>(mbs, P->b, mode, param, lambda, (MV*)mv_out);
   lp_rescore_kernel<<<std::min(mbs, 148 * 16), 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, range, lambda,
                                                            mbs, P->b, (MV*)mv_out);
   if (cudaGetLastError() != cudaSuccess) return -1;

@@ -191,6 +191,9 @@ void *b200enc_proposal_create(int max_mbs);
 void b200enc_proposal_destroy(void *h);
 int b200enc_proposal_set_params(void *h, const float *host_params, int n);
 int b200enc_proposal_get_params(void *h, float *host_params, int n);
+/* Parameters from a checkpoint file (b200enc.proposal.save_checkpoint format,
+ * SHA-256 verified): 0, -1 on I/O or device error, -2 on a bad file. */
+int b200enc_proposal_load(void *h, const char *path);
 /* Candidates, their SADs, the network input and side features for every MB
  * of a frame; prev_mv = the previous frame's b200enc_mv_t field (NULL: no
  * history). Resets the handle's counters. */
@@ -208,10 +211,14 @@ int b200enc_proposal_adam(void *h, float lr, float beta1, float beta2, float eps
 int b200enc_proposal_train_step(void *h, int mbs, float lr, int step, void *stream);
 /* Motion estimation of one frame in the learned form; prev_mv NULL runs the
  * full search. Same geometry, range, lambda, zero_thresh, mv_out and
- * alignment rules as b200enc_me_full_search. */
+ * alignment rules as b200enc_me_full_search. mode 1: the network ranks the
+ * candidates and MBs whose top-4 probability is under `param` fall back to
+ * the full search. mode 2, the baseline the network is measured against:
+ * the 4 distinct candidates of lowest exact cost, falling back when that
+ * cost exceeds param * 256 (param < 0: never). */
 int b200enc_proposal_me(void *h, const uint8_t *cur_y, int cur_pitch, const uint8_t *ref_y, int ref_pitch,
                         int W, int H, int RW, int RH, const void *prev_mv, int range, int lambda,
-                        int zero_thresh, float conf_thresh, void *mv_out, void *stream);
+                        int zero_thresh, int mode, float param, void *mv_out, void *stream);
 /* Device pointer and size of an internal tensor (index list in proposal.cu). */
 int b200enc_proposal_tensor(void *h, int which, void **ptr, size_t *bytes);
 

@@ -190,6 +190,21 @@ int b200enc_ctx_encode_device(gpu_context_t *ctx, const uint8_t *y, const uint8_
                               int width, int height, int qp, int is_intra, int num_slices,
                               int stage_outputs);
 
+/* Motion estimation form of P frames: mode 0 = plain full search (default),
+ * 1 = learned proposal (b200enc_proposal_me) with the network parameters of
+ * checkpoint `weights` (NULL: the packaged proposal_h264.b2pn next to the
+ * library's b200enc package) and confidence threshold conf, 2 = the same
+ * candidate search without the network, falling back when the best
+ * candidate's cost per pel exceeds conf (conf < 0: never). The first P frame
+ * after an I frame, and any P frame without a previous MV field, uses the
+ * full search. Env: B200ENC_ME=learned|candidates, B200ENC_PROPOSAL_WEIGHTS,
+ * B200ENC_PROPOSAL_CONF. Returns -2 if the checkpoint is missing or bad. */
+int b200enc_ctx_set_me(gpu_context_t *ctx, int mode, const char *weights, float conf);
+/* Learned-form counters of the last P frame: MBs re-scored from the network's
+ * candidates, MBs that fell back to the full search, zero-MV early-outs
+ * (synchronises the context stream). */
+int b200enc_ctx_me_stats(gpu_context_t *ctx, int *learned, int *fallback, int *early);
+
 /* Per-stage GPU timing with CUDA events, the equivalent of the reference's
  * BC250_PERF_STATS timestamps (gpu_compute.c:50-67). enable resets the
  * sums. perf_read synchronises the stream and returns, for P (intra = 0) or

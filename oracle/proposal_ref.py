@@ -84,21 +84,22 @@ def _masked_softmax(z, dup):
 
 
 def loss_and_grad(logits, label, norez, weight, dup):
-    """Mean over weighted samples of 11-way masked CE + 0.5 BCE on logit 11.
-    Returns (loss, dloss/dlogits [B][16])."""
+    """Mean over weighted samples of -log(probability mass of the target set
+    `label` (bit mask over the 11 classes) under the masked softmax) + 0.5 BCE
+    on logit 11. Returns (loss, dloss/dlogits [B][16])."""
     z = logits.astype(np.float64)
     p = _masked_softmax(z, dup)
     n = max(float((weight > 0).sum()), 1.0)
     w = weight.astype(np.float64) / n
     B = z.shape[0]
-    onehot = np.zeros((B, N_CLASSES))
-    onehot[np.arange(B), label] = 1.0
+    inset = ((np.asarray(label, np.int64)[:, None] >> np.arange(N_CLASSES)[None, :]) & 1).astype(bool)
+    pset = np.maximum((p * inset).sum(axis=1), 1e-30)
     g = np.zeros((B, N_OUT))
-    g[:, :N_CLASSES] = w[:, None] * (p - onehot)
+    g[:, :N_CLASSES] = w[:, None] * (p - np.where(inset, p / pset[:, None], 0.0))
     zs = z[:, 11]
     ps = 1.0 / (1.0 + np.exp(-zs))
     g[:, 11] = w * 0.5 * (ps - norez)
-    ce = -np.log(np.maximum(p[np.arange(B), label], 1e-30))
+    ce = -np.log(pset)
     bce = np.maximum(zs, 0) - zs * norez + np.log1p(np.exp(-np.abs(zs)))
     loss = float(np.sum(np.where(weight > 0, w * (ce + 0.5 * bce), 0.0)))
     return loss, g
@@ -224,9 +225,11 @@ def prepare(cur, ref, W, H, RW, RH, prev_mv, R, zero_thresh):
 
 
 def labels(state, cand, logged_pad, nz=None):
-    """Training targets from full-search log words (see lp_label_kernel)."""
+    """Training targets from full-search log words (see lp_label_kernel):
+    a bit mask of the distinct candidates whose +-2 window holds the integer
+    winner, or of class 10 ("none") when no window does."""
     mbs = state.shape[0]
-    lab = np.full(mbs, N_CLASSES - 1, np.int32)
+    lab = np.zeros(mbs, np.int32)
     w = np.zeros(mbs, np.float32)
     pad = logged_pad.astype(np.uint32)
     for mb in range(mbs):
@@ -240,8 +243,8 @@ def labels(state, cand, logged_pad, nz=None):
             if (dup >> k) & 1:
                 continue
             if abs(dx - cand[mb, k, 0]) <= 2 and abs(dy - cand[mb, k, 1]) <= 2:
-                lab[mb] = k
-                break
+                lab[mb] |= 1 << k
+    lab[lab == 0] = 1 << (N_CLASSES - 1)
     norez = np.ones(mbs, np.float32) if nz is None else (nz.reshape(mbs, -1) == 0).all(axis=1).astype(np.float32)
     return lab, norez, w
 

@@ -73,6 +73,10 @@ def _prepared(gpu, W, H, R, prev_kind, coded, seed):
         prev[:, :2] = rs.integers(-4 * (R + 12), 4 * (R + 12) + 1, (mbs, 2))  # beyond +-R: exercises the clamp
         prev[:, 2] = rs.integers(0, 40000, mbs)
         prev[rs.random(mbs) < 0.3, :2] = 0
+    elif prev_kind == "near":  # candidates within +-3 pels: overlapping windows, multi-candidate targets
+        prev = np.zeros((mbs, 4), np.int32)
+        prev[:, :2] = rs.integers(-12, 13, (mbs, 2))
+        prev[:, 2] = rs.integers(0, 40000, mbs)
     P = proposal.Proposal(mbs)
     P.prepare(cur, ref, W, H, RW, RH, torch.from_numpy(prev).cuda() if prev is not None else None, R, 512)
     torch.cuda.synchronize()
@@ -141,7 +145,7 @@ def test_gradient_check(gpu):
     """The BF16 backward kernels against the oracle's backward pass."""
     import torch
     from b200enc import proposal as pp
-    P, want, mbs, (cur, ref, RW, RH, *_rest) = _prepared(gpu, 320, 192, 32, "random", True, seed=12)
+    P, want, mbs, (cur, ref, RW, RH, *_rest) = _prepared(gpu, 320, 192, 32, "near", True, seed=12)
     params = _random_params(4)
     P.set_params(params)
     logged = torch.zeros((mbs, 4), dtype=torch.int32, device="cuda")
@@ -158,7 +162,7 @@ def test_gradient_check(gpu):
     np.testing.assert_array_equal(P.tensor(pp.T_LABEL, torch.int32, (mbs,)).cpu().numpy(), lab)
     np.testing.assert_array_equal(P.tensor(pp.T_WEIGHT, torch.float32, (mbs,)).cpu().numpy(), w)
     np.testing.assert_array_equal(P.tensor(pp.T_NOREZ_T, torch.float32, (mbs,)).cpu().numpy(), norez)
-    assert w.sum() > mbs // 4 and len(set(lab[w > 0])) > 2
+    assert w.sum() > mbs // 4 and len(set(lab[w > 0])) > 2 and (lab[w > 0] & (lab[w > 0] - 1)).any()
     loss, g5 = pr.loss_and_grad(a["logits"], lab, norez, w, (state >> 8) & 0x3FF)
     got_loss = float(P.tensor(pp.T_LOSS, torch.float32, (1,)).cpu()[0])
     assert abs(got_loss - loss) <= 1e-4 * abs(loss)
@@ -220,7 +224,7 @@ def _learned_case(gpu, seed, conf, params_seed):
     gpu.me_full_search_ex(nv[2], nv[1], W, H, CW, CH, R, lam, 512, full, flags=gpu.ME_LOG_INTEGER)
     P = pp.Proposal(mbs, _random_params(params_seed))
     out = torch.full((mbs, 4), -7, dtype=torch.int32, device="cuda")
-    P.me(nv[2], nv[1], W, H, CW, CH, prev, R, lam, 512, conf, out)
+    P.me(nv[2], nv[1], W, H, CW, CH, prev, R, lam, 512, conf, out, mode=pp.Proposal.NETWORK)
     torch.cuda.synchronize()
     return P, mbs, out.cpu().numpy(), full.cpu().numpy(), fr, (W, H, CW, CH, R, lam)
 

@@ -62,7 +62,7 @@ def test_oracle_backward_matches_finite_differences(seed):
     params = _rand_params(rs)
     x0 = rs.standard_normal((B * 64, 8))
     side = rs.standard_normal((B, 64))
-    label = np.array([0, 10, 3], np.int32)
+    label = np.array([0b1, 0b10000000000, 0b1001000], np.int32)
     norez = np.array([1.0, 0.0, 1.0])
     weight = np.array([1.0, 1.0, 0.0])
     dup = np.array([0b10, 0, 0b1000000000])
@@ -96,7 +96,7 @@ def test_loss_gradient_rows_sum_to_zero_over_classes():
     rs = np.random.Generator(np.random.PCG64(9))
     z = rs.standard_normal((5, 16))
     dup = np.array([0, 0b110, 0, 0b1000000000, 0])
-    _, g = pr.loss_and_grad(z, np.array([0, 0, 10, 4, 9]), np.zeros(5), np.ones(5), dup)
+    _, g = pr.loss_and_grad(z, np.array([1, 0b1001, 1 << 10, 1 << 4, 1 << 9 | 1]), np.zeros(5), np.ones(5), dup)
     np.testing.assert_allclose(g[:, :11].sum(axis=1), 0, atol=1e-12)
     assert g[1, 1] == 0 and g[1, 2] == 0 and g[3, 9] == 0
 
