@@ -15,6 +15,8 @@
 // window byte is read once per column. SAD is the byte-SIMD
 // vabsdiff4-with-add; the integer path uses no tensor cores. The column
 // dx = +R is scored directly, one candidate per thread, after the sweep.
+#include <algorithm>
+
 #include "b200enc_internal.h"
 #include "me_common.cuh"
 
@@ -30,7 +32,7 @@ struct MeShared {
   RefineShared rf;
 };
 
-template <int R>
+template <int R, bool LIST>
 __global__ void __launch_bounds__(2 * R) me_full_search_kernel(const uint8_t* __restrict__ cur, int cur_pitch,
                                                                const uint8_t* __restrict__ ref, int ref_pitch,
                                                                Geo g, int lambda, int zero_thresh,
@@ -41,12 +43,15 @@ __global__ void __launch_bounds__(2 * R) me_full_search_kernel(const uint8_t* __
   constexpr int WP = S::WP, WW = S::WW, SIDE = 2 * R + 1;
   __shared__ S sh;
   const int tid = threadIdx.x;
+  // list mode: a persistent grid walks the listed MBs; otherwise one CTA per MB
+  const int n_items = LIST ? *mb_count : 1;
+  for (int item = LIST ? (int)blockIdx.x : 0; item < n_items; item += LIST ? (int)gridDim.x : 1) {
   int mbx = blockIdx.x, mby = blockIdx.y;
-  if (mb_list) {  // list mode: one CTA per listed MB, the rest exit
-    if ((int)blockIdx.x >= *mb_count) return;
-    const int mb = mb_list[blockIdx.x];
+  if (LIST) {
+    const int mb = mb_list[item];
     mby = mb / g.mbw;
     mbx = mb - mby * g.mbw;
+    __syncthreads();  // the previous item's shared memory is no longer read
   }
   const int X = mbx * 16, Y = mby * 16;
   const int ox = X - R - 4, oy = Y - R - 4;  // window origin (multiple of 4)
@@ -92,7 +97,7 @@ __global__ void __launch_bounds__(2 * R) me_full_search_kernel(const uint8_t* __
   MV* o = out + (size_t)mby * g.mbw + mbx;
   if (zero_thresh >= 0 && sad0 <= (uint32_t)zero_thresh) {
     if (tid == 0) *o = MV{0, 0, sad0, (flags & B200ENC_ME_LOG_INTEGER) ? me_log_word(0, 0, true) : 0u};
-    return;
+    continue;
   }
 
   // ---- integer full search: column sweep ---------------------------------
@@ -166,6 +171,7 @@ __global__ void __launch_bounds__(2 * R) me_full_search_kernel(const uint8_t* __
       qpel_refine<NT>(sh.rf, G8, reinterpret_cast<const uint8_t*>(sh.cur), int_sad, &qx, &qy);
   if (tid == 0)
     *o = MV{4 * mx + qx, 4 * my + qy, bsad, (flags & B200ENC_ME_LOG_INTEGER) ? me_log_word(mx, my, false) : 0u};
+  }
 }
 
 }  // namespace b200enc
@@ -182,16 +188,28 @@ extern "C" int b200enc_me_full_search_ex(const uint8_t* cur_y, int cur_pitch, co
   if ((mb_list == nullptr) != (mb_count == nullptr)) return -1;
   Geo g{W, H, RW, RH, (W + 15) / 16, (H + 15) / 16};
   if (mb_list && (list_capacity <= 0 || list_capacity > g.mbw * g.mbh)) return -1;
-  dim3 grid = mb_list ? dim3(list_capacity) : dim3(g.mbw, g.mbh);
+  int sms = 148, dev = 0;
+  if (mb_list && cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // list mode: a persistent grid of up to 8 CTAs per SM walks the list
+  dim3 grid = mb_list ? dim3(std::min(list_capacity, 8 * sms)) : dim3(g.mbw, g.mbh);
   cudaStream_t st = (cudaStream_t)stream;
+  const bool list = mb_list != nullptr;
   switch (range) {
     case 16:
-      me_full_search_kernel<16><<<grid, 32, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda, zero_thresh,
-                                                     (MV*)mv_out, mb_list, mb_count, flags);
+      if (list)
+        me_full_search_kernel<16, true><<<grid, 32, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda,
+                                                             zero_thresh, (MV*)mv_out, mb_list, mb_count, flags);
+      else
+        me_full_search_kernel<16, false><<<grid, 32, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda,
+                                                              zero_thresh, (MV*)mv_out, mb_list, mb_count, flags);
       break;
     case 32:
-      me_full_search_kernel<32><<<grid, 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda, zero_thresh,
-                                                     (MV*)mv_out, mb_list, mb_count, flags);
+      if (list)
+        me_full_search_kernel<32, true><<<grid, 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda,
+                                                             zero_thresh, (MV*)mv_out, mb_list, mb_count, flags);
+      else
+        me_full_search_kernel<32, false><<<grid, 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda,
+                                                              zero_thresh, (MV*)mv_out, mb_list, mb_count, flags);
       break;
     default:
       return -1;

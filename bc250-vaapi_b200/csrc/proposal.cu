@@ -36,47 +36,10 @@
 #include <new>
 #include <vector>
 
-#include "b200enc_internal.h"
 #include "me_common.cuh"
+#include "proposal.cuh"
 
 namespace b200enc {
-
-constexpr int kCand = 10;
-constexpr int kClasses = 11;  // candidates + none
-constexpr int kOut = 16;
-constexpr int kFeat = 64;
-constexpr int kFIn = 96;  // fc1 input: 32 conv features + 64 side features
-static_assert(kFIn == 32 + kFeat, "fc1 input = conv features + side features");
-constexpr int kLayers = 6;
-__host__ __device__ constexpr int layer_in(int l) { return l == 0 ? 8 : (l < 4 ? 128 : (l == 4 ? kFIn : 64)); }
-__host__ __device__ constexpr int layer_out(int l) { return l < 4 ? 32 : (l == 4 ? 64 : kOut); }
-__host__ __device__ constexpr int layer_woff(int l) {
-  return l == 0 ? 0 : layer_woff(l - 1) + layer_out(l - 1) * layer_in(l - 1) + layer_out(l - 1);
-}
-__host__ __device__ constexpr int layer_boff(int l) { return layer_woff(l) + layer_out(l) * layer_in(l); }
-constexpr int kParams = layer_boff(kLayers - 1) + layer_out(kLayers - 1);
-
-// per-MB state word
-constexpr uint32_t kStEarly = 1u, kStNoHist = 2u;  // dup mask in bits 8..17
-
-__constant__ int8_t kNb[9][2] = {{0, 0}, {-1, -1}, {0, -1}, {1, -1}, {-1, 0}, {1, 0}, {-1, 1}, {0, 1}, {1, 1}};
-
-struct LpBuf {
-  __nv_bfloat16 *x0, *y1, *y2, *y3, *f, *h;
-  float* logits;
-  int32_t* cand;      // [mbs][10] packed (cy << 16) | (cx & 0xffff)
-  uint32_t* cand_sad;  // [mbs][10]
-  uint32_t* state;     // [mbs]
-  uint32_t* sel;       // [mbs] 4 x int8 candidate indices (-1 unused)
-  float* p_norez;      // [mbs]
-  int* lists;          // learned [mbs], fallback [mbs]
-  int* counters;       // [0] learned, [1] fallback, [2] valid training samples, [3] early-outs
-};
-
-__device__ __forceinline__ int cand_x(int32_t p) { return (int)(int16_t)(p & 0xffff); }
-__device__ __forceinline__ int cand_y(int32_t p) { return p >> 16; }
-__device__ __forceinline__ int morton_x(int m) { return (m & 1) | ((m >> 1) & 2) | ((m >> 2) & 4); }
-__device__ __forceinline__ int morton_y(int m) { return ((m >> 1) & 1) | ((m >> 2) & 2) | ((m >> 3) & 4); }
 
 // ---------------------------------------------------------------------------
 // Preparation: candidates, their SADs, the network input and side features.
@@ -86,7 +49,8 @@ __global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restric
                                                         const uint8_t* __restrict__ ref, int ref_pitch, Geo g,
                                                         const MV* __restrict__ prev, int R, int zero_thresh,
                                                         LpBuf b) {
-  __shared__ uint8_t sc[256];
+  __shared__ uint32_t scw[64];   // current MB, 16 rows x 4 words (clamped to W, H)
+  __shared__ uint32_t rfw[64];   // reference block at candidate 0
   __shared__ int scx[kCand], scy[kCand];
   __shared__ uint32_t ssad[kCand], sprev[9];
   __shared__ uint32_t sgrad[2][2];
@@ -94,9 +58,18 @@ __global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restric
   const int mb = blockIdx.x;
   const int mby = mb / g.mbw, mbx = mb - mby * g.mbw;
   const int X = mbx * 16, Y = mby * 16;
-  for (int i = tid; i < 256; i += 64) {
-    const int r = i >> 4, c = i & 15;
-    sc[i] = cur[(size_t)clampi(Y + r, 0, g.H - 1) * cur_pitch + min(X + c, g.W - 1)];
+  {
+    const int r = tid >> 2, w = tid & 3;
+    const uint8_t* cp = cur + (size_t)clampi(Y + r, 0, g.H - 1) * cur_pitch;
+    const int gx = X + 4 * w;
+    uint32_t v;
+    if (gx + 3 < g.W) {
+      v = __ldg(reinterpret_cast<const uint32_t*>(cp + gx));
+    } else {
+      v = (uint32_t)__ldg(cp + min(gx, g.W - 1)) | ((uint32_t)__ldg(cp + min(gx + 1, g.W - 1)) << 8) |
+          ((uint32_t)__ldg(cp + min(gx + 2, g.W - 1)) << 16) | ((uint32_t)__ldg(cp + min(gx + 3, g.W - 1)) << 24);
+    }
+    scw[tid] = v;
   }
   if (tid < kCand) {
     int cx = 0, cy = 0;
@@ -111,26 +84,31 @@ __global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restric
     }
     scx[tid] = cx;
     scy[tid] = cy;
+    ssad[tid] = 0;
   }
-  if (tid < 2) sgrad[0][tid] = sgrad[1][tid] = 0;
   __syncthreads();
 
-  // exact SAD at each candidate: warp w scores candidates w, w+2, ...
-  for (int c = warp; c < kCand; c += 2) {
-    const int cx = scx[c], cy = scy[c];
-    uint32_t s = 0;
+  // exact SAD at each candidate: one (candidate, row) per task, 4 byte-SIMD
+  // words off 5 aligned (clamped) loads of the reference row
+  for (int task = tid; task < kCand * 16; task += 64) {
+    const int c = task >> 4, r = task & 15;
+    const int x0 = X + scx[c], xa = x0 & ~3, shft = (x0 - xa) * 8;
+    const uint8_t* rp = ref + (size_t)clampi(Y + r + scy[c], 0, g.RH - 1) * ref_pitch;
+    uint32_t w[5];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int i = lane * 8 + k, y = i >> 4, x = i & 15;
-      const int rv = ref[(size_t)clampi(Y + y + cy, 0, g.RH - 1) * ref_pitch + clampi(X + x + cx, 0, g.RW - 1)];
-      s += (uint32_t)abs((int)sc[i] - rv);
+    for (int i = 0; i < 5; ++i) w[i] = load_word_clamped(rp, xa + 4 * i, g.RW);
+    uint32_t sad = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint32_t rv = __funnelshift_r(w[i], w[i + 1], shft);
+      sad = sad4_acc(rv, scw[r * 4 + i], sad);
+      if (c == 0) rfw[r * 4 + i] = rv;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) ssad[c] = s;
+    atomicAdd(&ssad[c], sad);
   }
   // block gradients: sum |horizontal| and |vertical| neighbour differences
   {
+    const uint8_t* sc = reinterpret_cast<const uint8_t*>(scw);
     uint32_t gh = 0, gv = 0;
     for (int i = tid; i < 256; i += 64) {
       const int y = i >> 4, x = i & 15;
@@ -164,17 +142,16 @@ __global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restric
   // network input: row m (Morton cell (ox, oy) of the 8x8 grid) holds the
   // 2x2 pels (dy, dx) x (current, residual against c0) at k = (dy*2+dx)*2+ch
   {
+    const uint8_t* sc = reinterpret_cast<const uint8_t*>(scw);
+    const uint8_t* r0 = reinterpret_cast<const uint8_t*>(rfw);
     const int m = tid, ox = morton_x(m), oy = morton_y(m);
-    const int c0x = scx[0], c0y = scy[0];
     __align__(16) __nv_bfloat16 v[8];
 #pragma unroll
     for (int dy = 0; dy < 2; ++dy)
 #pragma unroll
       for (int dx = 0; dx < 2; ++dx) {
-        const int y = 2 * oy + dy, x = 2 * ox + dx;
-        const int cv = sc[y * 16 + x];
-        const int rv =
-            ref[(size_t)clampi(Y + y + c0y, 0, g.RH - 1) * ref_pitch + clampi(X + x + c0x, 0, g.RW - 1)];
+        const int i = (2 * oy + dy) * 16 + 2 * ox + dx;
+        const int cv = sc[i], rv = r0[i];
         v[(dy * 2 + dx) * 2 + 0] = __float2bfloat16_rn((float)(cv - 128) * 0.015625f);
         v[(dy * 2 + dx) * 2 + 1] = __float2bfloat16_rn((float)(cv - rv) * 0.015625f);
       }
@@ -204,125 +181,58 @@ __global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restric
   if (tid == 0) b.state[mb] = (early ? kStEarly : 0u) | (prev ? 0u : kStNoHist) | (dup << 8);
 }
 
-// ---------------------------------------------------------------------------
-// Selection: masked softmax over the distinct candidates and "none", the
-// top 4, the confidence test, and the learned / fallback lists.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void masked_softmax(const float* z, uint32_t dup, float* p) {
-  float mx = -INFINITY;
-  for (int j = 0; j < kClasses; ++j)
-    if (!((dup >> j) & 1u)) mx = fmaxf(mx, z[j]);
-  float s = 0.f;
-  for (int j = 0; j < kClasses; ++j) {
-    p[j] = ((dup >> j) & 1u) ? 0.f : expf(z[j] - mx);
-    s += p[j];
-  }
-  const float inv = 1.f / s;
-  for (int j = 0; j < kClasses; ++j) p[j] *= inv;
-}
-
-// mode 1: the network's 4 most probable distinct candidates, falling back
-// when their probability sum is under `param`. mode 2 (no network): the 4
-// distinct candidates of lowest exact cost (SAD + lambda * |c|), falling
-// back when that lowest cost exceeds param * 256 (param < 0: never).
 __global__ void lp_select_kernel(int mbs, LpBuf b, int mode, float param, int lambda, MV* __restrict__ mv_out) {
   const int mb = blockIdx.x * blockDim.x + threadIdx.x;
   if (mb >= mbs) return;
-  const uint32_t st = b.state[mb];
-  if (st & kStEarly) {
-    mv_out[mb] = MV{0, 0, b.cand_sad[mb * kCand + 9], 0u};
-    atomicAdd(&b.counters[3], 1);
-    b.sel[mb] = 0xffffffffu;
-    return;
-  }
-  if (st & kStNoHist) {
-    b.lists[mbs + atomicAdd(&b.counters[1], 1)] = mb;
-    b.sel[mb] = 0xffffffffu;
-    return;
-  }
-  const uint32_t dup = (st >> 8) & 0x3ffu;
-  float p[kClasses];
-  const bool heuristic = mode == 2;
-  uint32_t min_cost = 0xffffffffu;
-  if (heuristic) {
-    for (int c = 0; c < kCand; ++c) {
-      const int32_t q = b.cand[mb * kCand + c];
-      const uint32_t cost = b.cand_sad[mb * kCand + c] + (uint32_t)lambda * (uint32_t)(abs(cand_x(q)) + abs(cand_y(q)));
-      p[c] = -(float)cost;
-      min_cost = min(min_cost, cost);
-    }
-    p[kCand] = -INFINITY;
-  } else {
-    float z[kClasses];
-    for (int j = 0; j < kClasses; ++j) z[j] = b.logits[(size_t)mb * kOut + j];
-    masked_softmax(z, dup, p);
-    b.p_norez[mb] = 1.f / (1.f + expf(-b.logits[(size_t)mb * kOut + 11]));
-  }
-  uint32_t chosen = dup, sel = 0xffffffffu;
-  float conf = 0.f;
-  for (int k = 0; k < 4; ++k) {
-    int best = -1;
-    for (int c = 0; c < kCand; ++c)
-      if (!((chosen >> c) & 1u) && (best < 0 || p[c] > p[best])) best = c;
-    if (best < 0) break;
-    chosen |= 1u << best;
-    conf += p[best];
-    sel = (sel & ~(0xffu << (8 * k))) | ((uint32_t)best << (8 * k));
-  }
-  b.sel[mb] = sel;
-  const bool fall = heuristic ? (param >= 0.f && (float)min_cost > param * 256.f) : (conf < param);
-  if (fall) {
-    b.lists[mbs + atomicAdd(&b.counters[1], 1)] = mb;
-  } else {
-    b.lists[atomicAdd(&b.counters[0], 1)] = mb;
-  }
+  float z[kOut];
+  if (mode == 1)
+    for (int j = 0; j < kOut; ++j) z[j] = b.logits[(size_t)mb * kOut + j];
+  lp_select_one(mb, mbs, b, mode, param, lambda, z, mv_out);
 }
 
 // ---------------------------------------------------------------------------
 // Exact re-scoring of the selected candidates' +-2 windows, then the refine.
 // 64 threads per MB, persistent over the learned list.
 // ---------------------------------------------------------------------------
-struct RescoreShared {
+// One warp per MB, four independent warps per block; every warp walks the
+// learned list on its own and synchronises only itself.
+struct RescoreWarp {
   uint32_t patch[4][20][6];  // candidate k: rows cy-2 .. cy+17, words from xa = (X+cx-2) & ~3
   uint32_t cur[64];
   uint8_t win[23][24];  // refine neighbourhood of the winner: rows/cols -3..19
-  uint32_t red[2];
+  int ccx[4], ccy[4];
   RefineShared rf;
 };
 
-__device__ __forceinline__ uint32_t load_word_clamped(const uint8_t* row, int gx, int RW) {
-  if (gx >= 0 && gx + 3 < RW) return __ldg(reinterpret_cast<const uint32_t*>(row + gx));
-  return (uint32_t)__ldg(row + clampi(gx, 0, RW - 1)) | ((uint32_t)__ldg(row + clampi(gx + 1, 0, RW - 1)) << 8) |
-         ((uint32_t)__ldg(row + clampi(gx + 2, 0, RW - 1)) << 16) |
-         ((uint32_t)__ldg(row + clampi(gx + 3, 0, RW - 1)) << 24);
-}
-
-__global__ void __launch_bounds__(64) lp_rescore_kernel(const uint8_t* __restrict__ cur, int cur_pitch,
-                                                        const uint8_t* __restrict__ ref, int ref_pitch, Geo g,
-                                                        int R, int lambda, int mbs, LpBuf b,
-                                                        MV* __restrict__ mv_out) {
-  __shared__ RescoreShared sh;
-  const int tid = threadIdx.x;
+__global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restrict__ cur, int cur_pitch,
+                                                         const uint8_t* __restrict__ ref, int ref_pitch, Geo g,
+                                                         int R, int lambda, int mbs, LpBuf b,
+                                                         MV* __restrict__ mv_out) {
+  __shared__ RescoreWarp shw[4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  RescoreWarp& sh = shw[wid];
   const int n = b.counters[0];
   const int SIDE = 2 * R + 1;
-  for (int li = blockIdx.x; li < n; li += gridDim.x) {
+  for (int li = blockIdx.x * 4 + wid; li < n; li += gridDim.x * 4) {
     const int mb = b.lists[li];
     const int mby = mb / g.mbw, mbx = mb - mby * g.mbw;
     const int X = mbx * 16, Y = mby * 16;
     const uint32_t sel = b.sel[mb];
-    int nk = 0, ccx[4], ccy[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int c = (int)((sel >> (8 * k)) & 0xffu);
+    int valid = 0;
+    if (lane < 4) {
+      const int c = (int)((sel >> (8 * lane)) & 0xffu);
       if (c < kCand) {
         const int32_t p = b.cand[mb * kCand + c];
-        ccx[nk] = cand_x(p);
-        ccy[nk] = cand_y(p);
-        ++nk;
+        sh.ccx[lane] = cand_x(p);
+        sh.ccy[lane] = cand_y(p);
+        valid = 1;
       }
     }
+    // selected candidates occupy the low slots (the selection fills them in order)
+    const int nk = __popc(__ballot_sync(0xffffffffu, valid) & 0xfu);
+    __syncwarp();
     // stage the current MB (clamped to W, H) and the candidate patches
-    for (int i = tid; i < 64; i += 64) {
+    for (int i = lane; i < 64; i += 32) {
       const int r = i >> 2, w = i & 3;
       const uint8_t* cp = cur + (size_t)clampi(Y + r, 0, g.H - 1) * cur_pitch;
       const int gx = X + 4 * w;
@@ -335,52 +245,53 @@ __global__ void __launch_bounds__(64) lp_rescore_kernel(const uint8_t* __restric
       }
       sh.cur[i] = v;
     }
-    for (int i = tid; i < nk * 20 * 6; i += 64) {
+    for (int i = lane; i < nk * 120; i += 32) {
       const int k = i / 120, rem = i - k * 120, r = rem / 6, w = rem - r * 6;
-      const int xa = (X + ccx[k] - 2) & ~3;
-      const uint8_t* rp = ref + (size_t)clampi(Y + ccy[k] - 2 + r, 0, g.RH - 1) * ref_pitch;
+      const int xa = (X + sh.ccx[k] - 2) & ~3;
+      const uint8_t* rp = ref + (size_t)clampi(Y + sh.ccy[k] - 2 + r, 0, g.RH - 1) * ref_pitch;
       sh.patch[k][r][w] = load_word_clamped(rp, xa + 4 * w, g.RW);
     }
-    __syncthreads();
+    __syncwarp();
 
-    // 25 offsets per candidate, up to 100 positions over 64 threads
+    // 25 integer offsets per candidate, up to 100 positions over 32 lanes
     uint32_t best = 0xffffffffu;
-    for (int pos = tid; pos < nk * 25; pos += 64) {
+    for (int pos = lane; pos < nk * 25; pos += 32) {
       const int k = pos / 25, o = pos - k * 25, oy = o / 5, ox = o - oy * 5;
-      const int dx = ccx[k] - 2 + ox, dy = ccy[k] - 2 + oy;
-      const int xa = (X + ccx[k] - 2) & ~3;
+      const int cx = sh.ccx[k], cy = sh.ccy[k];
+      const int dx = cx - 2 + ox, dy = cy - 2 + oy;
+      const int xa = (X + cx - 2) & ~3;
       const int byte0 = (X + dx) - xa;  // 0..7
       const int w0 = byte0 >> 2, shft = (byte0 & 3) * 8;
-      uint32_t s = 0;
+      uint32_t sad = 0;
 #pragma unroll 4
       for (int r = 0; r < 16; ++r) {
         const uint32_t* rw = sh.patch[k][oy + r] + w0;
         const uint32_t a0 = rw[0], a1 = rw[1], a2 = rw[2], a3 = rw[3], a4 = rw[4];
-        s = sad4_acc(__funnelshift_r(a0, a1, shft), sh.cur[r * 4 + 0], s);
-        s = sad4_acc(__funnelshift_r(a1, a2, shft), sh.cur[r * 4 + 1], s);
-        s = sad4_acc(__funnelshift_r(a2, a3, shft), sh.cur[r * 4 + 2], s);
-        s = sad4_acc(__funnelshift_r(a3, a4, shft), sh.cur[r * 4 + 3], s);
+        sad = sad4_acc(__funnelshift_r(a0, a1, shft), sh.cur[r * 4 + 0], sad);
+        sad = sad4_acc(__funnelshift_r(a1, a2, shft), sh.cur[r * 4 + 1], sad);
+        sad = sad4_acc(__funnelshift_r(a2, a3, shft), sh.cur[r * 4 + 2], sad);
+        sad = sad4_acc(__funnelshift_r(a3, a4, shft), sh.cur[r * 4 + 3], sad);
       }
-      const uint32_t cost = s + (uint32_t)lambda * (uint32_t)(abs(dx) + abs(dy));
+      const uint32_t cost = sad + (uint32_t)lambda * (uint32_t)(abs(dx) + abs(dy));
       best = min(best, (cost << 14) | (uint32_t)((dy + R) * SIDE + (dx + R)));
     }
-    best = block_min<64>(best, sh.red);
+    best = __reduce_min_sync(0xffffffffu, best);
     const int idx = (int)(best & 0x3fffu);
     const int mx = idx % SIDE - R, my = idx / SIDE - R;
     const uint32_t int_sad = (best >> 14) - (uint32_t)lambda * (uint32_t)(abs(mx) + abs(my));
 
     // refine neighbourhood of the winner, clamped like the full search's window
-    for (int i = tid; i < 23 * 23; i += 64) {
+    for (int i = lane; i < 23 * 23; i += 32) {
       const int ry = i / 23 - 3, rx = i % 23 - 3;
       sh.win[ry + 3][rx + 3] = ref[(size_t)clampi(Y + my + ry, 0, g.RH - 1) * ref_pitch +
                                    clampi(X + mx + rx, 0, g.RW - 1)];
     }
-    __syncthreads();
+    __syncwarp();
     auto G8 = [&](int rx, int ry) -> int { return sh.win[ry + 3][rx + 3]; };
     int qx, qy;
-    const uint32_t bsad = qpel_refine<64>(sh.rf, G8, reinterpret_cast<const uint8_t*>(sh.cur), int_sad, &qx, &qy);
-    if (tid == 0) mv_out[mb] = MV{4 * mx + qx, 4 * my + qy, bsad, 0u};
-    __syncthreads();  // shared memory is restaged for the next MB
+    const uint32_t bsad = qpel_refine<32>(sh.rf, G8, reinterpret_cast<const uint8_t*>(sh.cur), int_sad, &qx, &qy);
+    if (lane == 0) mv_out[mb] = MV{4 * mx + qx, 4 * my + qy, bsad, 0u};
+    __syncwarp();  // the warp's shared memory is restaged for its next MB
   }
 }
 
@@ -507,6 +418,10 @@ struct Proposal {
   __nv_bfloat16* wb = nullptr;
   LpBuf b{};
   uint32_t* err = nullptr;
+  // the fallback full search runs on a side stream, concurrently with the
+  // re-scoring of the learned MBs (disjoint MBs of the same MV field)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_sel = nullptr, ev_fb = nullptr;
   // training buffers (allocated on first use)
   bool train_ready = false;
   int *label = nullptr;
@@ -524,7 +439,11 @@ struct Proposal {
     return true;
   }
   ~Proposal() {
+    if (side) cudaStreamSynchronize(side);
     for (void* p : allocs) cudaFree(p);
+    if (ev_sel) cudaEventDestroy(ev_sel);
+    if (ev_fb) cudaEventDestroy(ev_fb);
+    if (side) cudaStreamDestroy(side);
   }
   bool init(int mbs) {
     max_mbs = mbs;
@@ -537,7 +456,10 @@ struct Proposal {
            cudaMemset(params, 0, kParams * 4) == cudaSuccess && cudaMemset(adam_m, 0, kParams * 4) == cudaSuccess &&
            cudaMemset(adam_v, 0, kParams * 4) == cudaSuccess && cudaMemset(wb, 0, kParams * 2) == cudaSuccess &&
            cudaMemset(b.counters, 0, 32) == cudaSuccess && cudaMemset(err, 0, 4) == cudaSuccess &&
-           cudaMemset(b.f, 0, B * kFIn * 2) == cudaSuccess;
+           cudaMemset(b.f, 0, B * kFIn * 2) == cudaSuccess &&
+           cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking) == cudaSuccess &&
+           cudaEventCreateWithFlags(&ev_sel, cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventCreateWithFlags(&ev_fb, cudaEventDisableTiming) == cudaSuccess;
   }
   bool init_train() {
     if (train_ready) return true;
@@ -817,13 +739,23 @@ int b200enc_proposal_me(void* h, const uint8_t* cur_y, int cur_pitch, const uint
   Geo g{W, H, RW, RH, (W + 15) / 16, (H + 15) / 16};
   const int mbs = g.mbw * g.mbh;
   cudaStream_t st = (cudaStream_t)stream;
-  if (mode == 1 && lp_forward(P, mbs, st) != 0) return -1;
-  lp_select_kernel<<<(mbs + 127) / 128, 128, 0, st>>>(mbs, P->b, mode, param, lambda, (MV*)mv_out);
-  lp_rescore_kernel<<<std::min(mbs, 148 * 16), 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, range, lambda,
-                                                           mbs, P->b, (MV*)mv_out);
-  if (cudaGetLastError() != cudaSuccess) return -1;
-  return b200enc_me_full_search_ex(cur_y, cur_pitch, ref_y, ref_pitch, W, H, RW, RH, range, lambda, zero_thresh,
-                                   mv_out, P->b.lists + mbs, P->b.counters + 1, mbs, 0, stream);
+  if (mode == 1) {
+    if (lp_net_launch(mbs, P->b, P->wb, P->params, param, lambda, (MV*)mv_out, P->err, st) != 0) return -1;
+  } else {
+    lp_select_kernel<<<(mbs + 127) / 128, 128, 0, st>>>(mbs, P->b, mode, param, lambda, (MV*)mv_out);
+  }
+  // fork: the fallback full search on the side stream, the re-scoring here
+  if (cudaEventRecord(P->ev_sel, st) != cudaSuccess || cudaStreamWaitEvent(P->side, P->ev_sel, 0) != cudaSuccess)
+    return -1;
+  const int rc = b200enc_me_full_search_ex(cur_y, cur_pitch, ref_y, ref_pitch, W, H, RW, RH, range, lambda,
+                                           zero_thresh, mv_out, P->b.lists + mbs, P->b.counters + 1, mbs, 0,
+                                           (void*)P->side);
+  lp_rescore_kernel<<<std::max(1, std::min((mbs + 3) / 4, 148 * 8)), 128, 0, st>>>(
+      cur_y, cur_pitch, ref_y, ref_pitch, g, range, lambda, mbs, P->b, (MV*)mv_out);
+  // join
+  if (cudaEventRecord(P->ev_fb, P->side) != cudaSuccess || cudaStreamWaitEvent(st, P->ev_fb, 0) != cudaSuccess)
+    return -1;
+  return (rc == 0 && cudaGetLastError() == cudaSuccess) ? 0 : -1;
 }
 
 // Device pointers of the runtime's tensors, for tests and the training

@@ -24,58 +24,11 @@
 #include <cuda_bf16.h>
 
 #include "b200enc_internal.h"
-#include "common.cuh"
+#include "umma.cuh"
 
 namespace b200enc {
 
 constexpr int kTcM = 128, kTcK = 64;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// Shared-memory matrix descriptor, K-major, no swizzle (layout type 0),
-// Blackwell version 1: start address, leading byte offset (between K
-// chunks) and stride byte offset (between 8-row groups), all >> 4.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1u << 46;  // version
-  return d;
-}
-
-// Instruction descriptor of kind::f16: D F32, A and B BF16, both K-major.
-__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
-  return (1u << 4)                        // c_format F32
-         | (1u << 7)                      // a_format BF16
-         | (1u << 10)                     // b_format BF16
-         | ((uint32_t)(N >> 3) << 17)     // n_dim
-         | ((uint32_t)(M >> 4) << 24);    // m_dim
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-// Bounded wait on an mbarrier phase; false after ~max_ns without completion.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint64_t max_ns) {
-  const uint32_t a = smem_u32(bar);
-  const uint64_t t0 = global_ns();
-  for (;;) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(a), "r"(phase)
-        : "memory");
-    if (ok) return true;
-    if (global_ns() - t0 > max_ns) return false;
-  }
-}
 
 template <int BN>
 struct TcShared {

@@ -1,24 +1,38 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 compute-encoder hot path: 1080p encode fps.
+"""Benchmark of the B200 compute-encoder hot path: 1080p encode fps of the
+learned-proposal form against the plain full-search form.
 
-Workload (plain full-search form): 1920x1080 8-bit NV12, IPPP with an IDR
-every 60 frames, QP 27 (a point of the 22/27/32/37 sweep), integer full
-search over [-32,32]^2 + half/quarter-pel refine, spec deblocking on. A step
-is one frame through ME -> P chain (or intra wavefront) -> deblock. Inputs
-are 60 seeded synthetic frames resident in HBM (187 MB, larger than L2), so
-every step reads a frame that is not in L2.
+Workload: S concurrent streams (default 8, one context and CUDA stream each)
+of 1920x1080 8-bit NV12, IPPP with an IDR every 60 frames, QP 27 (a point of
+the 22/27/32/37 sweep), search range 32, lambda 5, spec deblocking on. A step
+is one frame of every stream through ME -> P chain (or intra wavefront) ->
+deblock. Each stream cycles 60 seeded synthetic frames resident in HBM
+(S x 187 MB, far larger than L2). The learned form (value) ranks candidates
+with the packaged network and re-scores the top 4 exactly, falling back to
+the full search under the confidence threshold; the first P frame of each
+GOP has no motion history and takes the full search. The plain form is the
+full search on every P frame. Both are timed in the same run, and again with
+one stream (single_stream).
 
-  value  frames/s over K timed steps, device-timed with CUDA events on the
-         library's stream, max over ranks, summed over ranks (weak scaling:
-         one independent stream per GPU, no collective on the data path).
-  e2e    the same through the reference boundary (gpu_compute_upload_nv12
-         from pinned host memory, begin/dispatch/end_picture, sync_slot and
-         the staging read-back of levels/dc/nz/pred_mode/mv every step).
+  value  learned-form frames/s summed over the S streams and over ranks,
+         device-timed with CUDA events (start event on a control stream that
+         every context stream waits on, end event after every context stream
+         has drained), max over ranks (weak scaling: independent streams per
+         GPU, no collective on the data path).
+  e2e    the learned form through the reference boundary (per stream
+         gpu_compute_upload_nv12 from pinned host memory,
+         begin/dispatch/end_picture; then sync_slot and a host read of the
+         staged outputs), S streams.
+  bd_rate the learned form's BD-rate against the plain form (bits from the
+         reference's host encoder, CABAC, QP 22/27/32/37, 60 1080p frames),
+         measured on a B200 with tests/rd_report.py and recorded in
+         profiles/rd_h264_1080p_learned_vs_plain.json.
 
 `--impl reference` times the reference's CPU implementation of the same
-frame on the host cores (oracle/_ref: the reference's AVX2 SAD in the
-exhaustive search, its C deblocking filter; the P chain from the CPU
-restatement), each step a bounded sample of one frame.
+frame (the plain form; the reference has no learned form) on the host cores
+(oracle/_ref: the reference's AVX2 SAD in the exhaustive search, its C
+deblocking filter; the P chain from the CPU restatement), each step a
+bounded sample of one frame.
 """
 import argparse
 import json
@@ -180,7 +194,8 @@ def run_reference(args):
         t, info = cpu_reference_frame_time(frames, budget_s=budget)
         times.append(t)
     fps = len(times) / sum(times)
-    line = {"metric": "1080p encode fps (plain full-search form)", "value": round(fps, 4), "unit": "frames/s",
+    line = {"metric": "1080p encode fps, learned-proposal form (vs plain full-search form)", "value": round(fps, 4),
+            "unit": "frames/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 / fps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
             "data": "synthetic (seeded generator, 1080p NV12)", "impl": "reference",
@@ -193,6 +208,32 @@ def run_reference(args):
 
 
 # ----------------------------------------------------------------- GPU arm
+
+def _frames_pool(seeds, n):
+    """Synthetic frames of several streams, generated on the host cores (a
+    spawned pool: no CUDA state is forked)."""
+    import multiprocessing as mp
+    if len(seeds) == 1:
+        return [make_frames(seeds[0], n)]
+    with mp.get_context("spawn").Pool(min(len(seeds), max(1, (os.cpu_count() or 2) - 1))) as pool:
+        return pool.starmap(make_frames, [(s, n) for s in seeds])
+
+
+def rd_record():
+    p = os.path.join(ROOT, "profiles", "rd_h264_1080p_learned_vs_plain.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return {"value_pct": round(d["bd_rate_learned_vs_plain_pct"], 3), "metric": "BD-rate (YUV PSNR) vs plain",
+            "no_network_pct": round(d["bd_rate_no_network_vs_plain_pct"], 3), "conf": d["conf"],
+            "source": "profiles/rd_h264_1080p_learned_vs_plain.json (tests/rd_report.py on B200)",
+            "workload": d["workload"]}
+
+
+# kernels per frame of each kind (counted from the launch sites)
+LAUNCHES = {"i": 2, "p_full": 3, "p_learned": 12}
+
 
 def run_gpu(args):
     import numpy as np
@@ -210,129 +251,179 @@ def run_gpu(args):
                                 device_id=torch.device("cuda", local))
         pg = dist
 
-    frames = make_frames(rank, NFRAMES)
-    dev = [b200enc.NV12.from_host(y, uv) for (y, uv) in frames]
-    ctx = b200enc.Context()
-    ctx.configure(search_range=RANGE, lam=LAMBDA, zero_thresh=512, coded_clamp=True, deblock=1)
-    stream = torch.cuda.ExternalStream(ctx.stream())
-
-    def step(t, stage=False):
-        ctx.encode_device(dev[t % NFRAMES], W, H, QP, (t % GOP) == 0, 1, stage)
-
-    t = 0
-    for _ in range(args.warmup):
-        step(t)
-        t += 1
-    torch.cuda.synchronize()
-    ctx.perf(True)
+    S = args.streams
+    host_frames = _frames_pool([rank * 1000 + s for s in range(S)], NFRAMES)
+    dev = [[b200enc.NV12.from_host(y, uv) for (y, uv) in fr] for fr in host_frames]
+    ctxs = []
+    for s in range(S):
+        c = b200enc.Context()
+        c.configure(search_range=RANGE, lam=LAMBDA, zero_thresh=512, coded_clamp=True, deblock=1)
+        ctxs.append(c)
+    streams = [torch.cuda.ExternalStream(c.stream()) for c in ctxs]
+    control = torch.cuda.Stream()
 
     def barrier():
         if pg:
             pg.barrier()
         torch.cuda.synchronize()
 
-    clocks = Clocks(local) if rank == 0 else None
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    launches = 0
-    for _ in range(args.steps):
-        launches += 2 if (t % GOP) == 0 else 3
-        step(t)
-        t += 1
-    e1.record(stream)
-    barrier()
-    clk = clocks.stop() if clocks else None
-    ms = e0.elapsed_time(e1)
-    if pg:
-        tt = torch.tensor([ms], device="cuda")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        ms = float(tt.item())
-    fps = ws * args.steps / (ms / 1000.0)
-    perf_p = ctx.perf_read(False)
-    perf_i = ctx.perf_read(True)
+    def max_over_ranks(ms):
+        if pg:
+            tt = torch.tensor([ms], device="cuda")
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+            return float(tt.item())
+        return ms
 
-    # searched macroblocks of the last P frame (zero-MV early-outs do no search)
-    out = {}
-    ok = ctx.L.b200enc_ctx_device_outputs(b200enc.ctypes.byref(ctx.ctx), None, None, None, None,
-                                          b200enc.ctypes.byref(mvp := b200enc.ctypes.c_void_p()))
-    mvh = b200enc.device_view(mvp.value, MBS * 16).cpu().numpy().view(np.int32).reshape(MBS, 4)
-    searched = int(np.sum(~((mvh[:, 0] == 0) & (mvh[:, 1] == 0) & (mvh[:, 2].view(np.uint32) <= 512))))
+    def arm(mode, nstreams, steps, warmup, perf=False, clocks=False):
+        """Encodes warmup + steps frames on each of the first nstreams
+        contexts from the start of a GOP; returns (ms, launches, perf, clk)."""
+        for c in ctxs[:nstreams]:
+            c.set_me(mode, conf=args.conf)
+            c.perf(False)
+        t = 0
+
+        def one_step(t):
+            n = 0
+            intra = (t % GOP) == 0
+            for s in range(nstreams):
+                ctxs[s].encode_device(dev[s][t % NFRAMES], W, H, QP, intra, 1, False)
+            if intra:
+                n = LAUNCHES["i"]
+            elif mode == 0 or (t % GOP) == 1:
+                n = LAUNCHES["p_full"]
+            else:
+                n = LAUNCHES["p_learned"]
+            return n * nstreams
+
+        for _ in range(warmup):
+            one_step(t)
+            t += 1
+        barrier()
+        if perf:
+            ctxs[0].perf(True)
+        clk = Clocks(local) if (clocks and rank == 0) else None
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(control)
+        for st in streams[:nstreams]:
+            st.wait_event(e0)
+        launches = 0
+        for _ in range(steps):
+            launches += one_step(t)
+            t += 1
+        for st in streams[:nstreams]:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            control.wait_event(ev)
+        e1.record(control)
+        barrier()
+        c = clk.stop() if clk else None
+        pf = (ctxs[0].perf_read(False), ctxs[0].perf_read(True)) if perf else None
+        return max_over_ranks(e0.elapsed_time(e1)), launches, pf, c
+
+    K, Wm = args.steps, args.warmup
+    ms_l, launches, _, clk = arm(1, S, K, Wm, clocks=True)
+    ms_p, _, _, _ = arm(0, S, K, Wm)
+    k1 = max(K, 2 * GOP)
+    ms_l1, _, perf_l1, _ = arm(1, 1, k1, Wm, perf=True)
+    ms_p1, _, perf_p1, _ = arm(0, 1, k1, Wm, perf=True)
+    fps = ws * S * K / (ms_l / 1000.0)
+    fps_plain = ws * S * K / (ms_p / 1000.0)
+    me_counts = ctxs[0].me_stats()
 
     # ---- e2e through the reference boundary, host buffers -----------------
-    pinned = []
-    for (y, uv) in frames[:8]:
-        py = torch.from_numpy(np.ascontiguousarray(y)).pin_memory()
-        puv = torch.from_numpy(np.ascontiguousarray(uv)).pin_memory()
-        pinned.append((py, puv))
-    img, mem = ctx.create_image(W, H)
-    L, c = ctx.L, b200enc.ctypes.byref(ctx.ctx)
+    NP = 30
+    pinned = [[(torch.from_numpy(np.ascontiguousarray(y)).pin_memory(),
+                torch.from_numpy(np.ascontiguousarray(uv)).pin_memory()) for (y, uv) in fr[:NP]]
+              for fr in host_frames]
+    imgs = [c.create_image(W, H) for c in ctxs]
+    for c in ctxs:
+        c.set_me(1, conf=args.conf)
 
     def e2e_step(k):
-        py, puv = pinned[k % len(pinned)]
-        rc = L.gpu_compute_upload_nv12(c, b200enc.ctypes.byref(img), mem, b200enc.ctypes.c_void_p(py.data_ptr()), W,
-                                       b200enc.ctypes.c_void_p(puv.data_ptr()), W, W, H)
-        assert rc == 0
-        slot = ctx.encode(img, W, H, QP, (k % GOP) == 0, 1, 0, None)
-        assert ctx.sync(slot) == 0
-        st = ctx.staging(slot)
-        return int(st["nz"][0, 0])  # a read of the step's result on the host
+        slots = []
+        for s, c in enumerate(ctxs):
+            py, puv = pinned[s][k % NP]
+            img, mem = imgs[s]
+            rc = c.L.gpu_compute_upload_nv12(b200enc.ctypes.byref(c.ctx), b200enc.ctypes.byref(img), mem,
+                                             b200enc.ctypes.c_void_p(py.data_ptr()), W,
+                                             b200enc.ctypes.c_void_p(puv.data_ptr()), W, W, H)
+            assert rc == 0
+            slots.append(c.encode(img, W, H, QP, (k % GOP) == 0, 1, 0, None))
+        acc = 0
+        for c, slot in zip(ctxs, slots):
+            assert c.sync(slot) == 0
+            acc += int(c.staging(slot)["nz"][0, 0])  # a host read of each step's result
+        return acc
 
-    for k in range(args.warmup):
+    k = 0
+    for _ in range(Wm):
         e2e_step(k)
+        k += 1
     barrier()
     s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s0.record(stream)
-    for k in range(args.steps):
-        e2e_step(k + 1)
-    s1.record(stream)
+    s0.record(control)
+    for _ in range(K):
+        e2e_step(k)
+        k += 1
+    s1.record(control)
     barrier()
-    ems = s0.elapsed_time(s1)
-    if pg:
-        tt = torch.tensor([ems], device="cuda")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        ems = float(tt.item())
-    e2e_fps = ws * args.steps / (ems / 1000.0)
-    ctx.destroy_image(img, mem)
+    e2e_fps = ws * S * K / (max_over_ranks(s0.elapsed_time(s1)) / 1000.0)
+    for c, (img, mem) in zip(ctxs, imgs):
+        c.destroy_image(img, mem)
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        nP = max(1, perf_p["frames"])
-        stage_ms = {k: perf_p[k] / nP for k in ("me", "chain", "deblock", "staging")}
-        dom = max(("me", "chain", "deblock"), key=lambda k: stage_ms[k])
+        pp1, pi1 = perf_l1
+        nP = max(1, pp1["frames"])
+        stage_ms = {k2: pp1[k2] / nP for k2 in ("me", "chain", "deblock", "staging")}
+        plain_stage_ms = {k2: perf_p1[0][k2] / max(1, perf_p1[0]["frames"]) for k2 in ("me", "chain", "deblock")}
+        dom = max(("me", "chain", "deblock"), key=lambda k2: stage_ms[k2])
         algo = ALGO_BYTES_PER_MB[dom] * MBS
         ach = algo / (stage_ms[dom] / 1000.0) / 1e9
         tr = traffic_from_profiles(dom)
-        me_ops = searched * ((2 * RANGE + 1) ** 2 * 256 + 16 * 256)
+        pipe_bytes = (ALGO_BYTES_PER_MB["me"] + ALGO_BYTES_PER_MB["chain"] + ALGO_BYTES_PER_MB["deblock"]) * MBS
         line = {
-            "metric": "1080p encode fps (plain full-search form)", "value": round(fps, 3), "unit": "frames/s",
-            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
+            "metric": "1080p encode fps, learned-proposal form (vs plain full-search form)", "value": round(fps, 2),
+            "unit": "frames/s", "n_gpus": ws, "steps": K, "warmup": Wm,
+            "ms_per_step": round(ms_l / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u8/int32 (integer path), bf16 (proposal network)",
             "data": "synthetic (seeded generator: gradients, sigma-8 texture, 6 moving rectangles, pan, noise patch)",
-            "config": {"workload": WORKLOAD, "width": W, "height": H, "qp": QP, "search_range": RANGE,
-                       "lambda": LAMBDA, "gop": GOP, "deblock": True, "recon_clamp": "coded",
-                       "l2": f"inputs cycle through {NFRAMES} resident frames ({NFRAMES * W * H * 3 // 2 >> 20} MiB > L2)",
-                       "parallelism": f"replicas x{ws} (one stream per GPU)"},
+            "config": {"workload": f"{WORKLOAD}_x{S}_streams", "streams_per_gpu": S, "width": W, "height": H,
+                       "qp": QP, "search_range": RANGE, "lambda": LAMBDA, "gop": GOP, "deblock": True,
+                       "recon_clamp": "coded", "proposal_conf": args.conf,
+                       "l2": f"each stream cycles {NFRAMES} resident frames ({S * NFRAMES * W * H * 3 // 2 >> 20} MiB "
+                             "> L2)",
+                       "parallelism": f"replicas x{ws} (independent streams per GPU)"},
+            "plain": {"value": round(fps_plain, 2), "unit": "frames/s", "ms_per_step": round(ms_p / K, 4)},
+            "speedup_vs_plain": round(fps / fps_plain, 3),
+            "single_stream": {"learned_fps": round(k1 / (ms_l1 / 1000.0), 2),
+                              "plain_fps": round(k1 / (ms_p1 / 1000.0), 2),
+                              "learned_stage_ms_per_p_frame": {k2: round(v, 4) for k2, v in stage_ms.items()},
+                              "plain_stage_ms_per_p_frame": {k2: round(v, 4) for k2, v in plain_stage_ms.items()},
+                              "last_p_frame_mbs": dict(zip(("learned", "fallback", "early"), me_counts))},
+            "bd_rate": rd_record(),
             "gpu_launches": launches,
-            "e2e": {"value": round(e2e_fps, 3), "unit": "frames/s", "h2d_bytes_per_step": H2D_PER_STEP,
-                    "d2h_bytes_per_step": D2H_PER_STEP},
+            "e2e": {"value": round(e2e_fps, 2), "unit": "frames/s", "h2d_bytes_per_step": S * H2D_PER_STEP,
+                    "d2h_bytes_per_step": S * D2H_PER_STEP},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(ach / peak, 5), "peak_kind": peak_kind,
                          "traffic": (round(tr * MBS) if tr is not None else None),
-                         "algorithmic_bytes": int(algo)},
-            "stages_ms_per_p_frame": {k: round(v, 4) for k, v in stage_ms.items()},
-            "stages_ms_per_i_frame": ({k: round(perf_i[k] / perf_i["frames"], 4) for k in ("chain", "deblock")}
-                                      if perf_i["frames"] else None),
-            "me_int": {"searched_mbs": searched, "abs_diff_per_s": round(me_ops / (stage_ms["me"] / 1000.0), 1)},
+                         "algorithmic_bytes": int(algo),
+                         "timing": "single-stream learned run, stage events on the context stream"},
+            "hbm_pipeline": {"achieved": round(pipe_bytes * fps / ws / 1e9, 2), "unit": "GB/s",
+                             "frac": round(pipe_bytes * fps / ws / 1e9 / peak, 5),
+                             "note": "algorithmic bytes of ME + P chain + deblock per P frame x learned-form fps"},
             "clocks": clk,
         }
         if ws == 1 and not args.no_cpu_baseline:
-            spf, info = cpu_reference_frame_time(frames[:2], budget_s=15.0)
+            spf, info = cpu_reference_frame_time(host_frames[0][:2], budget_s=15.0)
             line["cpu_baseline"] = {"value": round(1.0 / spf, 4), "unit": "frames/s", "cores": info["cores"],
                                     "kind": info["kind"], "sample": info["sample"],
-                                    "stage_s": {k: round(v, 4) for k, v in info["stage_s"].items()}}
+                                    "stage_s": {k2: round(v, 4) for k2, v in info["stage_s"].items()}}
         print(json.dumps(line), flush=True)
-    ctx.close()
+    for c in ctxs:
+        c.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()
@@ -341,10 +432,12 @@ def run_gpu(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=120)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--streams", type=int, default=8)
+    ap.add_argument("--conf", type=float, default=0.9)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
