@@ -169,4 +169,101 @@ __device__ __forceinline__ uint32_t qpel_refine(RefineShared& rf, G8F G8, const 
   return bsad;
 }
 
+// ---------------------------------------------------------------------------
+// The same refine for one warp, on byte-SIMD words: the half-pel planes are
+// bytes (their values are clipped to 0..255), every quarter-pel sample is
+// either a plane value or the rounded byte average (a + b + 1) >> 1 of two,
+// which vavgu4 forms for 4 pels at once, and vabsdiff4 accumulates the SAD.
+// Results are identical to qpel_refine.
+struct RefineSimd {
+  int32_t hr[23][18];
+  alignas(4) uint8_t pl[3][18][20];  // b, h, j at [ry+1][rx+1], ry, rx in -1..16
+};
+
+// The operands of each quarter-pel phase (fy*4+fx), motion_estimation.comp:
+// 197-213: {plane, sx, sy} twice (plane 0 G, 1 b, 2 h, 3 j, -1 none); the
+// sample is the first operand or the rounded average of both.
+__constant__ int8_t kQpelOp[16][6] = {
+    {0, 0, 0, -1, 0, 0}, {0, 0, 0, 1, 0, 0}, {1, 0, 0, -1, 0, 0}, {1, 0, 0, 0, 1, 0},
+    {0, 0, 0, 2, 0, 0},  {1, 0, 0, 2, 0, 0}, {1, 0, 0, 3, 0, 0},  {1, 0, 0, 2, 1, 0},
+    {2, 0, 0, -1, 0, 0}, {2, 0, 0, 3, 0, 0}, {3, 0, 0, -1, 0, 0}, {3, 0, 0, 2, 1, 0},
+    {2, 0, 0, 0, 0, 1},  {2, 0, 0, 1, 0, 1}, {3, 0, 0, 1, 0, 1},  {2, 1, 0, 1, 0, 1}};
+
+// Two words (8 pels) of a byte row starting at byte offset c of a 4-aligned row.
+__device__ __forceinline__ void row8(const uint8_t* row, int c, uint32_t& w0, uint32_t& w1) {
+  const uint32_t* r = reinterpret_cast<const uint32_t*>(row) + (c >> 2);
+  const int sh = (c & 3) * 8;
+  const uint32_t a0 = r[0], a1 = r[1], a2 = r[2];
+  w0 = __funnelshift_r(a0, a1, sh);
+  w1 = __funnelshift_r(a1, a2, sh);
+}
+
+// g: 4-aligned rows of the reference, gstride bytes apart; the integer
+// winner's top-left pel is at row g_r0, byte g_c0 (rows g_r0-3 .. g_r0+19
+// and bytes g_c0-3 .. g_c0+19+8 must be readable). cur: the 64 words of the
+// current MB. Every lane of the warp returns the same result.
+__device__ __forceinline__ uint32_t qpel_refine_warp_simd(RefineSimd& rf, const uint8_t* g, int gstride, int g_r0,
+                                                          int g_c0, const uint32_t* cur, uint32_t int_sad,
+                                                          int* qx_out, int* qy_out) {
+  const int lane = threadIdx.x & 31;
+  auto G8 = [&](int rx, int ry) -> int { return g[(g_r0 + ry) * gstride + g_c0 + rx]; };
+  for (int i = lane; i < 23 * 18; i += 32) {
+    const int ry = i / 18 - 3, rx = i % 18 - 1;
+    rf.hr[ry + 3][rx + 1] = G8(rx - 2, ry) - 5 * G8(rx - 1, ry) + 20 * G8(rx, ry) + 20 * G8(rx + 1, ry) -
+                             5 * G8(rx + 2, ry) + G8(rx + 3, ry);
+  }
+  __syncwarp();
+  for (int i = lane; i < 18 * 18; i += 32) {
+    const int ry = i / 18 - 1, rx = i % 18 - 1;
+    rf.pl[0][ry + 1][rx + 1] = (uint8_t)clip1((rf.hr[ry + 3][rx + 1] + 16) >> 5);
+    const int v = G8(rx, ry - 2) - 5 * G8(rx, ry - 1) + 20 * G8(rx, ry) + 20 * G8(rx, ry + 1) -
+                  5 * G8(rx, ry + 2) + G8(rx, ry + 3);
+    rf.pl[1][ry + 1][rx + 1] = (uint8_t)clip1((v + 16) >> 5);
+    const int j1 = rf.hr[ry + 1][rx + 1] - 5 * rf.hr[ry + 2][rx + 1] + 20 * rf.hr[ry + 3][rx + 1] +
+                   20 * rf.hr[ry + 4][rx + 1] - 5 * rf.hr[ry + 5][rx + 1] + rf.hr[ry + 6][rx + 1];
+    rf.pl[2][ry + 1][rx + 1] = (uint8_t)clip1((j1 + 512) >> 10);
+  }
+  __syncwarp();
+
+  const int y = lane >> 1, half = lane & 1;
+  const uint32_t c0 = cur[y * 4 + 2 * half], c1 = cur[y * 4 + 2 * half + 1];
+  // operand (plane p: 0 G, 1 b, 2 h, 3 j; extra shifts sx, sy) of the lane's
+  // 8 pels at integer offset (dx, dy) from the winner
+  auto operand = [&](int p, int dx, int dy, int sx, int sy, uint32_t& w0, uint32_t& w1) {
+    const int ry = y + dy + sy, rx = dx + sx + 8 * half;
+    if (p == 0) row8(g + (g_r0 + ry) * gstride, g_c0 + rx, w0, w1);
+    else row8(&rf.pl[p - 1][ry + 1][0], rx + 1, w0, w1);
+  };
+  auto score = [&](int ox, int oy) -> uint32_t {  // SAD at quarter-pel offset (ox, oy) from the winner
+    const int dx = ox >> 2, dy = oy >> 2, ph = (oy & 3) * 4 + (ox & 3);
+    uint32_t a0, a1;
+    operand(kQpelOp[ph][0], dx, dy, kQpelOp[ph][1], kQpelOp[ph][2], a0, a1);
+    if (kQpelOp[ph][3] >= 0) {
+      uint32_t b0, b1;
+      operand(kQpelOp[ph][3], dx, dy, kQpelOp[ph][4], kQpelOp[ph][5], b0, b1);
+      a0 = __vavgu4(a0, b0);
+      a1 = __vavgu4(a1, b1);
+    }
+    uint32_t sad = sad4_acc(a0, c0, 0u);
+    sad = sad4_acc(a1, c1, sad);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sad += __shfl_xor_sync(0xffffffffu, sad, o);
+    return sad;
+  };
+  uint32_t bsad = int_sad;
+  int hx = 0, hy = 0;
+  for (int c = 0; c < 8; ++c) {
+    const uint32_t v = score(kHalfOff[c][0], kHalfOff[c][1]);
+    if (v < bsad) { bsad = v; hx = kHalfOff[c][0]; hy = kHalfOff[c][1]; }
+  }
+  int qx = 0, qy = 0;
+  for (int c = 0; c < 8; ++c) {
+    const uint32_t v = score(hx + kQtrOff[c][0], hy + kQtrOff[c][1]);
+    if (v < bsad) { bsad = v; qx = kQtrOff[c][0]; qy = kQtrOff[c][1]; }
+  }
+  *qx_out = hx + qx;
+  *qy_out = hy + qy;
+  return bsad;
+}
+
 }  // namespace b200enc

@@ -196,12 +196,15 @@ __global__ void lp_select_kernel(int mbs, LpBuf b, int mode, float param, int la
 // ---------------------------------------------------------------------------
 // One warp per MB, four independent warps per block; every warp walks the
 // learned list on its own and synchronises only itself.
+// Candidate k's patch covers rows cy-5 .. cy+21 and 32 bytes from
+// xa = (X+cx-5) & ~3: the +-2 search window plus the refine's -3..+19 reach
+// around any winner inside that window, so the refine reads no global memory.
+constexpr int kPatchRows = 27, kPatchWords = 8;
 struct RescoreWarp {
-  uint32_t patch[4][20][6];  // candidate k: rows cy-2 .. cy+17, words from xa = (X+cx-2) & ~3
+  uint32_t patch[4][kPatchRows][kPatchWords];
   uint32_t cur[64];
-  uint8_t win[23][24];  // refine neighbourhood of the winner: rows/cols -3..19
   int ccx[4], ccy[4];
-  RefineShared rf;
+  RefineSimd rf;
 };
 
 __global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restrict__ cur, int cur_pitch,
@@ -245,10 +248,11 @@ __global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restri
       }
       sh.cur[i] = v;
     }
-    for (int i = lane; i < nk * 120; i += 32) {
-      const int k = i / 120, rem = i - k * 120, r = rem / 6, w = rem - r * 6;
-      const int xa = (X + sh.ccx[k] - 2) & ~3;
-      const uint8_t* rp = ref + (size_t)clampi(Y + sh.ccy[k] - 2 + r, 0, g.RH - 1) * ref_pitch;
+    for (int i = lane; i < nk * kPatchRows * kPatchWords; i += 32) {
+      const int k = i / (kPatchRows * kPatchWords), rem = i - k * (kPatchRows * kPatchWords);
+      const int r = rem / kPatchWords, w = rem - r * kPatchWords;
+      const int xa = (X + sh.ccx[k] - 5) & ~3;
+      const uint8_t* rp = ref + (size_t)clampi(Y + sh.ccy[k] - 5 + r, 0, g.RH - 1) * ref_pitch;
       sh.patch[k][r][w] = load_word_clamped(rp, xa + 4 * w, g.RW);
     }
     __syncwarp();
@@ -259,13 +263,13 @@ __global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restri
       const int k = pos / 25, o = pos - k * 25, oy = o / 5, ox = o - oy * 5;
       const int cx = sh.ccx[k], cy = sh.ccy[k];
       const int dx = cx - 2 + ox, dy = cy - 2 + oy;
-      const int xa = (X + cx - 2) & ~3;
-      const int byte0 = (X + dx) - xa;  // 0..7
+      const int xa = (X + cx - 5) & ~3;
+      const int byte0 = (X + dx) - xa;  // 3..10
       const int w0 = byte0 >> 2, shft = (byte0 & 3) * 8;
       uint32_t sad = 0;
 #pragma unroll 4
       for (int r = 0; r < 16; ++r) {
-        const uint32_t* rw = sh.patch[k][oy + r] + w0;
+        const uint32_t* rw = sh.patch[k][oy + 3 + r] + w0;
         const uint32_t a0 = rw[0], a1 = rw[1], a2 = rw[2], a3 = rw[3], a4 = rw[4];
         sad = sad4_acc(__funnelshift_r(a0, a1, shft), sh.cur[r * 4 + 0], sad);
         sad = sad4_acc(__funnelshift_r(a1, a2, shft), sh.cur[r * 4 + 1], sad);
@@ -280,16 +284,16 @@ __global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restri
     const int mx = idx % SIDE - R, my = idx / SIDE - R;
     const uint32_t int_sad = (best >> 14) - (uint32_t)lambda * (uint32_t)(abs(mx) + abs(my));
 
-    // refine neighbourhood of the winner, clamped like the full search's window
-    for (int i = lane; i < 23 * 23; i += 32) {
-      const int ry = i / 23 - 3, rx = i % 23 - 3;
-      sh.win[ry + 3][rx + 3] = ref[(size_t)clampi(Y + my + ry, 0, g.RH - 1) * ref_pitch +
-                                   clampi(X + mx + rx, 0, g.RW - 1)];
-    }
-    __syncwarp();
-    auto G8 = [&](int rx, int ry) -> int { return sh.win[ry + 3][rx + 3]; };
+    // the refine reads the patch of the first candidate whose window holds
+    // the winner (clamped like the full search's window)
+    int kw = 0;
+    for (int k = nk - 1; k >= 0; --k)
+      if (abs(mx - sh.ccx[k]) <= 2 && abs(my - sh.ccy[k]) <= 2) kw = k;
+    const uint8_t* pb8 = reinterpret_cast<const uint8_t*>(&sh.patch[kw][0][0]);
+    const int row0 = my - (sh.ccy[kw] - 5), col0 = (X + mx) - ((X + sh.ccx[kw] - 5) & ~3);
     int qx, qy;
-    const uint32_t bsad = qpel_refine<32>(sh.rf, G8, reinterpret_cast<const uint8_t*>(sh.cur), int_sad, &qx, &qy);
+    const uint32_t bsad =
+        qpel_refine_warp_simd(sh.rf, pb8, kPatchWords * 4, row0, col0, sh.cur, int_sad, &qx, &qy);
     if (lane == 0) mv_out[mb] = MV{4 * mx + qx, 4 * my + qy, bsad, 0u};
     __syncwarp();  // the warp's shared memory is restaged for its next MB
   }

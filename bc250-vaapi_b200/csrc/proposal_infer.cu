@@ -2,11 +2,12 @@
 // persistent kernel on the tcgen05 tensor cores, with the candidate
 // selection fused into its last epilogue.
 //
-// One CTA per SM (192 KB of shared memory), 4 warps, looping over tiles of
+// One CTA per SM (192 KB of shared memory), 16 warps, looping over tiles of
 // 16 MBs. The BF16 weights of all six layers are staged once per CTA as
 // UMMA B operands. Per tile every layer is a handful of M=128 MMAs into
 // TMEM, issued by one thread and committed to an mbarrier; the epilogue
-// (warp w reads TMEM lanes 32w..32w+31 = rows) adds the bias, applies ReLU,
+// (warp w reads TMEM lanes 32(w%4).. = rows; the four warps of a lane
+// quadrant split the column blocks between them) adds the bias, applies ReLU,
 // rounds to BF16 and writes the next layer's A operand directly in the
 // canonical K-major layout. Because conv rows are in Morton order inside
 // each MB, the four rows of every 2x2 stride-2 patch are consecutive: output
@@ -67,47 +68,47 @@ __device__ __forceinline__ void store8_relu(uint16_t* dst, const uint32_t* acc, 
   *reinterpret_cast<uint4*>(dst) = v;
 }
 
-// 32 channels of TMEM row (lane) 32*warp + lane, columns col .. col+31.
-__device__ __forceinline__ void tmem_row32(uint32_t tmem, int warp, int col, uint32_t (&v)[32]) {
-  uint32_t (&lo)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[0]);
-  uint32_t (&hi)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[16]);
-  const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col;
-  tmem_ld16(base, lo);
-  tmem_ld16(base + 16, hi);
+// 16 channels of TMEM row (lane) 32*quad + lane, columns col .. col+15.
+__device__ __forceinline__ void tmem_row16(uint32_t tmem, int quad, int col, uint32_t (&v)[16]) {
+  tmem_ld16(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)col, v);
   tmem_wait_ld();
 }
 
-// Writes conv output row R (32 channels in v) into the next layer's operand
-// tile set `dst` (128-row tiles of K=128): row R/4, K offset (R%4)*32.
-__device__ __forceinline__ void store_conv_row(uint16_t* dst_tiles, int R, const uint32_t (&v)[32], const float* bias) {
+// Writes channels ch0 .. ch0+15 of conv output row R into the next layer's
+// operand tile set `dst` (128-row tiles of K=128): row R/4, K offset
+// (R%4)*32 + ch0.
+__device__ __forceinline__ void store_conv_row16(uint16_t* dst_tiles, int R, int ch0, const uint32_t (&v)[16],
+                                                 const float* bias) {
   const int q = R >> 2, j = R & 3;
   uint16_t* tile = dst_tiles + (size_t)(q >> 7) * (128 * 128);
-#pragma unroll
-  for (int c8 = 0; c8 < 4; ++c8)
-    store8_relu(tile + canon_off(q & 127, j * 32 + c8 * 8, 128), &v[c8 * 8], bias + c8 * 8);
+  store8_relu(tile + canon_off(q & 127, j * 32 + ch0, 128), &v[0], bias + ch0);
+  store8_relu(tile + canon_off(q & 127, j * 32 + ch0 + 8, 128), &v[8], bias + ch0 + 8);
 }
 
-__global__ void __launch_bounds__(128, 1) lp_net_kernel(int mbs, LpBuf b, const __nv_bfloat16* __restrict__ wb,
+constexpr int kNetThreads = 512;
+
+__global__ void __launch_bounds__(kNetThreads, 1) lp_net_kernel(int mbs, LpBuf b, const __nv_bfloat16* __restrict__ wb,
                                                        const float* __restrict__ params, float param, int lambda,
                                                        MV* __restrict__ mv_out, uint32_t* __restrict__ err) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
   NetSmem& s = *reinterpret_cast<NetSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int quad = warp & 3, wq = warp >> 2;  // TMEM lane quadrant, warp index within it (0..3)
   const uint16_t* w16 = reinterpret_cast<const uint16_t*>(wb);
 
   // ---- weights and biases, once per CTA --------------------------------
-  for (int i = tid; i < 32 * 16; i += 128) {
+  for (int i = tid; i < 32 * 16; i += kNetThreads) {
     const int n = i >> 4, k = i & 15;
     s.w1[canon_off(n, k, 32)] = k < 8 ? w16[layer_woff(0) + n * 8 + k] : (uint16_t)0;
   }
-  for (int i = tid; i < 32 * 128; i += 128) {
+  for (int i = tid; i < 32 * 128; i += kNetThreads) {
     const int n = i >> 7, k = i & 127;
     s.w2[canon_off(n, k, 32)] = w16[layer_woff(1) + i];
     s.w3[canon_off(n, k, 32)] = w16[layer_woff(2) + i];
     s.w4[canon_off(n, k, 32)] = w16[layer_woff(3) + i];
   }
-  for (int i = tid; i < 64 * 96; i += 128) s.wf1[canon_off(i / 96, i % 96, 64)] = w16[layer_woff(4) + i];
-  for (int i = tid; i < 16 * 64; i += 128) s.wf2[canon_off(i >> 6, i & 63, 16)] = w16[layer_woff(5) + i];
+  for (int i = tid; i < 64 * 96; i += kNetThreads) s.wf1[canon_off(i / 96, i % 96, 64)] = w16[layer_woff(4) + i];
+  for (int i = tid; i < 16 * 64; i += kNetThreads) s.wf2[canon_off(i >> 6, i & 63, 16)] = w16[layer_woff(5) + i];
   if (tid < 32) {
     s.b1[tid] = params[layer_boff(0) + tid];
     s.b2[tid] = params[layer_boff(1) + tid];
@@ -152,23 +153,39 @@ __global__ void __launch_bounds__(128, 1) lp_net_kernel(int mbs, LpBuf b, const 
   };
 
   const int ntiles = (mbs + kNetTileMbs - 1) / kNetTileMbs;
+  // The next tile's inputs are loaded into registers while the current tile
+  // computes: 1024 network rows (16 B each, two per thread) and the 16 x 8
+  // chunks of side features (threads 0..127).
+  constexpr int kRowsPerThread = kNetTileMbs * 64 / kNetThreads;
+  uint4 pre_x[kRowsPerThread], pre_f = make_uint4(0, 0, 0, 0);
+  auto prefetch = [&](int tile) {
+    const int mb0 = tile * kNetTileMbs, nmb = min(kNetTileMbs, mbs - mb0);
+#pragma unroll
+    for (int i = 0; i < kRowsPerThread; ++i) {
+      const int R = tid + i * kNetThreads;
+      pre_x[i] = (R >> 6) < nmb ? *reinterpret_cast<const uint4*>(b.x0 + ((size_t)mb0 * 64 + R) * 8)
+                                : make_uint4(0, 0, 0, 0);
+    }
+    if (tid < 128) {
+      const int m = tid >> 3, c8 = tid & 7;
+      pre_f = m < nmb ? *reinterpret_cast<const uint4*>(b.f + (size_t)(mb0 + m) * kFIn + 32 + c8 * 8)
+                      : make_uint4(0, 0, 0, 0);
+    }
+  };
+  if ((int)blockIdx.x < ntiles) prefetch(blockIdx.x);
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int mb0 = tile * kNetTileMbs;
     const int nmb = min(kNetTileMbs, mbs - mb0);
     // ---- inputs: network rows (both K chunks) and side features ---------
-    for (int R = tid; R < kNetTileMbs * 64; R += 128) {
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if ((R >> 6) < nmb) v = *reinterpret_cast<const uint4*>(b.x0 + ((size_t)mb0 * 64 + R) * 8);
+#pragma unroll
+    for (int i = 0; i < kRowsPerThread; ++i) {
+      const int R = tid + i * kNetThreads;
       uint16_t* t = s.x0[R >> 7];
-      *reinterpret_cast<uint4*>(t + canon_off(R & 127, 0, 128)) = v;
+      *reinterpret_cast<uint4*>(t + canon_off(R & 127, 0, 128)) = pre_x[i];
       *reinterpret_cast<uint4*>(t + canon_off(R & 127, 8, 128)) = make_uint4(0, 0, 0, 0);
     }
-    {
-      const int m = tid >> 3, c8 = tid & 7;  // 16 MBs x 8 chunks of the 64 side features
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (m < nmb) v = *reinterpret_cast<const uint4*>(b.f + (size_t)(mb0 + m) * kFIn + 32 + c8 * 8);
-      *reinterpret_cast<uint4*>(s.f + canon_off(m, 32 + c8 * 8, 128)) = v;
-    }
+    if (tid < 128) *reinterpret_cast<uint4*>(s.f + canon_off(tid >> 3, 32 + (tid & 7) * 8, 128)) = pre_f;
+    if (tile + (int)gridDim.x < ntiles) prefetch(tile + gridDim.x);
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
@@ -183,10 +200,12 @@ __global__ void __launch_bounds__(128, 1) lp_net_kernel(int mbs, LpBuf b, const 
       umma_commit(&s.bar);
     }
     if (!sync_mma()) break;
-    for (int t = 0; t < 8; ++t) {
-      uint32_t v[32];
-      tmem_row32(tmem, warp, 32 * t, v);
-      store_conv_row(&s.a2[0][0], 128 * t + 32 * warp + lane, v, s.b1);
+    // 8 tiles x 2 channel halves per lane quadrant, 4 warps per quadrant
+    for (int job = wq; job < 16; job += 4) {
+      const int t = job >> 1, h = job & 1;
+      uint32_t v[16];
+      tmem_row16(tmem, quad, 32 * t + 16 * h, v);
+      store_conv_row16(&s.a2[0][0], 128 * t + 32 * quad + lane, 16 * h, v, s.b1);
     }
     publish();
 
@@ -201,10 +220,11 @@ __global__ void __launch_bounds__(128, 1) lp_net_kernel(int mbs, LpBuf b, const 
       umma_commit(&s.bar);
     }
     if (!sync_mma()) break;
-    for (int t = 0; t < 2; ++t) {
-      uint32_t v[32];
-      tmem_row32(tmem, warp, 32 * t, v);
-      store_conv_row(s.a3, 128 * t + 32 * warp + lane, v, s.b2);
+    {  // 2 tiles x 2 halves per quadrant: one job per warp
+      const int t = wq >> 1, h = wq & 1;
+      uint32_t v[16];
+      tmem_row16(tmem, quad, 32 * t + 16 * h, v);
+      store_conv_row16(s.a3, 128 * t + 32 * quad + lane, 16 * h, v, s.b2);
     }
     publish();
 
@@ -218,10 +238,10 @@ __global__ void __launch_bounds__(128, 1) lp_net_kernel(int mbs, LpBuf b, const 
       umma_commit(&s.bar);
     }
     if (!sync_mma()) break;
-    if (warp < 2) {
-      uint32_t v[32];
-      tmem_row32(tmem, warp, 0, v);
-      store_conv_row(a4, 32 * warp + lane, v, s.b3);
+    if (quad < 2 && wq < 2) {  // rows 0..63: quadrants 0, 1; two halves
+      uint32_t v[16];
+      tmem_row16(tmem, quad, 16 * wq, v);
+      store_conv_row16(a4, 32 * quad + lane, 16 * wq, v, s.b3);
     }
     publish();
 
@@ -235,12 +255,13 @@ __global__ void __launch_bounds__(128, 1) lp_net_kernel(int mbs, LpBuf b, const 
       umma_commit(&s.bar);
     }
     if (!sync_mma()) break;
-    if (warp == 0) {
-      uint32_t v[32];
-      tmem_row32(tmem, 0, 0, v);
-      if (lane < 16)
-#pragma unroll
-        for (int c8 = 0; c8 < 4; ++c8) store8_relu(s.f + canon_off(lane, c8 * 8, 128), &v[c8 * 8], s.b4 + c8 * 8);
+    if (quad == 0 && wq < 2) {  // rows 0..15, two halves of the 32 channels
+      uint32_t v[16];
+      tmem_row16(tmem, 0, 16 * wq, v);
+      if (lane < 16) {
+        store8_relu(s.f + canon_off(lane, 16 * wq, 128), &v[0], s.b4 + 16 * wq);
+        store8_relu(s.f + canon_off(lane, 16 * wq + 8, 128), &v[8], s.b4 + 16 * wq + 8);
+      }
     }
     publish();
 
@@ -254,14 +275,12 @@ __global__ void __launch_bounds__(128, 1) lp_net_kernel(int mbs, LpBuf b, const 
       umma_commit(&s.bar);
     }
     if (!sync_mma()) break;
-    if (warp == 0) {
-      uint32_t v[32];
-      for (int h = 0; h < 2; ++h) {
-        tmem_row32(tmem, 0, 32 * h, v);
-        if (lane < 16)
-#pragma unroll
-          for (int c8 = 0; c8 < 4; ++c8)
-            store8_relu(hd + canon_off(lane, 32 * h + c8 * 8, 128), &v[c8 * 8], s.bf1 + 32 * h + c8 * 8);
+    if (quad == 0) {  // rows 0..15, 64 channels: 16 per warp of quadrant 0
+      uint32_t v[16];
+      tmem_row16(tmem, 0, 16 * wq, v);
+      if (lane < 16) {
+        store8_relu(hd + canon_off(lane, 16 * wq, 128), &v[0], s.bf1 + 16 * wq);
+        store8_relu(hd + canon_off(lane, 16 * wq + 8, 128), &v[8], s.bf1 + 16 * wq + 8);
       }
     }
     publish();
@@ -308,7 +327,7 @@ int lp_net_launch(int mbs, const LpBuf& b, const __nv_bfloat16* wb, const float*
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int ntiles = (mbs + kNetTileMbs - 1) / kNetTileMbs;
-  lp_net_kernel<<<std::min(ntiles, sms), 128, smem, st>>>(mbs, b, wb, params, conf, lambda, mv_out, err);
+  lp_net_kernel<<<std::min(ntiles, sms), kNetThreads, smem, st>>>(mbs, b, wb, params, conf, lambda, mv_out, err);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
