@@ -21,9 +21,11 @@
 //   * the group's rows (plus a 4-row / 2-row halo above) live in shared
 //     memory for the whole frame: one bulk load, one bulk store at the end;
 //   * inside a CTA a row waits on its upper neighbour through a shared-memory
-//     progress word; only the group's first row waits on global memory,
-//     and only the group's last row publishes (its bottom 4 luma / 2 chroma
-//     sample rows per macroblock, then a release store);
+//     progress word; only the group's first row waits on global memory;
+//   * two publisher warps (luma, chroma) follow the group's last row through
+//     its shared progress word and publish its final macroblocks in batches
+//     (their bottom 4 luma / 2 chroma sample rows, one fence, a release
+//     store), so no row warp ever waits on a device-scope fence;
 //   * boundary strengths of the whole group are computed up front.
 // Waits are bounded; on timeout a CTA records the error and leaves, and
 // every waiter gives up as soon as it sees a recorded error.
@@ -203,7 +205,7 @@ __device__ __forceinline__ bool wait_shared(const volatile uint32_t* flag, const
   return false;
 }
 
-__global__ void __launch_bounds__(256) deblock_kernel(int mbw, int mbh, int R, int qp, int is_intra,
+__global__ void __launch_bounds__(320) deblock_kernel(int mbw, int mbh, int R, int qp, int is_intra,
                                                       const uint32_t* __restrict__ nzm, const MV* __restrict__ mvs,
                                                       uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch,
                                                       uint32_t* scratch, uint32_t max_wait) {  // max_wait in microseconds
@@ -280,12 +282,50 @@ __global__ void __launch_bounds__(256) deblock_kernel(int mbw, int mbh, int R, i
     const bool is_luma = warp < R;
     const int wr = is_luma ? warp : warp - R;  // row within the group
     const int y = y0 + wr;
-    if (wr < rows) {
+    if (warp >= 2 * R) {
+      // ---- publisher: luma (warp 2R) or chroma (warp 2R+1) -------------------
+      const bool pl_luma = warp == 2 * R;
+      const int last = rows - 1, yl = y0 + last;
+      const volatile uint32_t* lp = prog + (pl_luma ? 0 : R) + last;
+      uint32_t* gflag = (pl_luma ? gprog_luma : gprog_chroma) + yl;
+      uint32_t published = 0;
+      while (has_next && published < (uint32_t)mbw) {
+        bool ok = true;
+        if (lane == 0) ok = wait_shared(lp, sc, published + 1, max_wait, (uint32_t)(yl * mbw + (int)published));
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+          s_abort = 1;
+          break;
+        }
+        __threadfence_block();
+        // one read, broadcast: the last row keeps advancing the word, and the
+        // loop below must stay uniform across the warp
+        uint32_t done = 0;
+        if (lane == 0) done = *lp;
+        done = __shfl_sync(0xffffffffu, done, 0);
+        for (int bx = (int)published; bx < (int)done; ++bx) {
+          if (pl_luma) {
+            if (lane < 16) {
+              const int r = lane >> 2, w = lane & 3;
+              __stcg(reinterpret_cast<uint32_t*>(rec_y + (size_t)(16 * yl + 12 + r) * rec_pitch + 16 * bx + 4 * w),
+                     *reinterpret_cast<const uint32_t*>(ly + (size_t)(4 + 16 * last + 12 + r) * P.sp + 16 * bx + 4 * w));
+            }
+          } else if (lane < 8) {
+            const int r = lane >> 2, w = lane & 3;
+            __stcg(reinterpret_cast<uint32_t*>(rec_uv + (size_t)(8 * yl + 6 + r) * rec_pitch + 16 * bx + 4 * w),
+                   *reinterpret_cast<const uint32_t*>(cy + (size_t)(2 + 8 * last + 6 + r) * P.sp + 16 * bx + 4 * w));
+          }
+        }
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) store_release(gflag, done);
+        published = done;
+      }
+    } else if (wr < rows) {
       const uint8_t* bsrow = bsm + (size_t)wr * mbw * 32;
       volatile uint32_t* my_prog = prog + (is_luma ? 0 : R) + wr;
       const volatile uint32_t* up_prog = prog + (is_luma ? 0 : R) + wr - 1;
       uint32_t* gflag_up = (is_luma ? gprog_luma : gprog_chroma) + (y - 1);
-      uint32_t* gflag_me = (is_luma ? gprog_luma : gprog_chroma) + y;
       for (int mx = 0; mx < mbw; ++mx) {
         const uint32_t need = (uint32_t)(mx + 1);  // upper row: bottom samples of MB mx final
         bool ok = true;
@@ -420,31 +460,9 @@ __global__ void __launch_bounds__(256) deblock_kernel(int mbw, int mbh, int R, i
         // Macroblock mx-1's bottom samples are final now (mx's left edge was
         // its last change); all of them after the last macroblock.
         const uint32_t done = (mx == mbw - 1) ? (uint32_t)mbw : (uint32_t)mx;
-        if (wr == rows - 1) {
-          if (has_next && done > 0) {
-            const int first = (mx == mbw - 1 && mbw > 1) ? mx - 1 : mx - 1;
-            for (int bx = first; bx < (int)done; ++bx) {
-              if (is_luma) {
-                if (lane < 16) {
-                  const int r = lane >> 2, w = lane & 3;
-                  __stcg(reinterpret_cast<uint32_t*>(rec_y + (size_t)(16 * y + 12 + r) * rec_pitch + 16 * bx + 4 * w),
-                         *reinterpret_cast<const uint32_t*>(ly + (size_t)(4 + 16 * wr + 12 + r) * P.sp + 16 * bx + 4 * w));
-                }
-              } else if (lane < 8) {
-                const int r = lane >> 2, w = lane & 3;
-                __stcg(reinterpret_cast<uint32_t*>(rec_uv + (size_t)(8 * y + 6 + r) * rec_pitch + 16 * bx + 4 * w),
-                       *reinterpret_cast<const uint32_t*>(cy + (size_t)(2 + 8 * wr + 6 + r) * P.sp + 16 * bx + 4 * w));
-              }
-            }
-            __threadfence();
-            __syncwarp();
-            if (lane == 0) store_release(gflag_me, done);
-          }
-        } else {
-          __threadfence_block();
-          __syncwarp();
-          if (lane == 0) *my_prog = done;
-        }
+        __threadfence_block();
+        __syncwarp();
+        if (lane == 0) *my_prog = done;
       }
     }
     __syncthreads();
@@ -503,7 +521,7 @@ extern "C" int b200enc_deblock_launch(int mbw, int mbh, int qp, int is_intra, co
   if (ctas <= 0 || ctas > groups) ctas = groups;
   if (cudaFuncSetAttribute(deblock_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.bytes) != cudaSuccess)
     return -1;
-  deblock_kernel<<<ctas, 64 * R, P.bytes, (cudaStream_t)stream>>>(mbw, mbh, R, qp, is_intra, nz, (const MV*)mv, rec_y,
+  deblock_kernel<<<ctas, 64 * R + 64, P.bytes, (cudaStream_t)stream>>>(mbw, mbh, R, qp, is_intra, nz, (const MV*)mv, rec_y,
                                                                   rec_uv, rec_pitch, scratch, max_wait);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
