@@ -23,6 +23,8 @@ EXPORTS = [
     "b200enc_proposal_forward", "b200enc_proposal_labels", "b200enc_proposal_backward", "b200enc_proposal_adam",
     "b200enc_proposal_train_step", "b200enc_proposal_me", "b200enc_proposal_tensor", "b200enc_proposal_load",
     "b200enc_ctx_set_me", "b200enc_ctx_me_stats",
+    "b200enc_hevc_transform_quant_4x4", "b200enc_hevc_dequant_itransform_4x4", "b200enc_hevc_transform_quant_8x8",
+    "b200enc_hevc_dequant_itransform_8x8", "b200enc_hevc_build_hpel",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
     "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",
@@ -102,6 +104,11 @@ def load_library(path=LIB_PATH):
                                         _vp, _vp]
     lib.b200enc_proposal_tensor.argtypes = [_vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_size_t)]
     lib.b200enc_proposal_load.argtypes = [_vp, ctypes.c_char_p]
+    lib.b200enc_hevc_transform_quant_4x4.argtypes = [_vp, _vp, _i, _i, _i, _i, _i, _vp]
+    lib.b200enc_hevc_dequant_itransform_4x4.argtypes = [_vp, _vp, _i, _i, _i, _i, _vp]
+    lib.b200enc_hevc_transform_quant_8x8.argtypes = [_vp, _vp, _i, _i, _i, _i, _vp]
+    lib.b200enc_hevc_dequant_itransform_8x8.argtypes = [_vp, _vp, _i, _i, _i, _vp]
+    lib.b200enc_hevc_build_hpel.argtypes = [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp]
     lib.b200enc_ctx_set_me.argtypes = [ctypes.POINTER(GpuContext), _i, ctypes.c_char_p, ctypes.c_float]
     return lib
 
@@ -251,6 +258,36 @@ def gemm_bf16(A, B, C, M, N, K, a_strides, b_strides, bias=None, flags=0, err=No
     _check(lib().b200enc_gemm_bf16(M, N, K, _p(A), a_strides[0], a_strides[1], _p(B), b_strides[0], b_strides[1],
                                    _p(C), C.stride(0), _p(bias) if bias is not None else None, flags,
                                    _p(err) if err is not None else None, _stream(stream)), "b200enc_gemm_bf16")
+
+
+def hevc_transform_quant_4x4(residual, coeff, qp, use_dst, round_q12, bit_depth=8, stream=None):
+    """residual, coeff: int16 device tensors [n][16]."""
+    _check(lib().b200enc_hevc_transform_quant_4x4(_p(residual), _p(coeff), residual.shape[0], qp, int(use_dst),
+                                                  round_q12, bit_depth, _stream(stream)), "hevc_transform_quant_4x4")
+
+
+def hevc_dequant_itransform_4x4(coeff, residual, qp, use_dst, bit_depth=8, stream=None):
+    _check(lib().b200enc_hevc_dequant_itransform_4x4(_p(coeff), _p(residual), coeff.shape[0], qp, int(use_dst),
+                                                     bit_depth, _stream(stream)), "hevc_dequant_itransform_4x4")
+
+
+def hevc_transform_quant_8x8(residual, coeff, qp, round_q12, bit_depth=8, stream=None):
+    """residual, coeff: int16 device tensors [n][64]."""
+    _check(lib().b200enc_hevc_transform_quant_8x8(_p(residual), _p(coeff), residual.shape[0], qp, bit_depth,
+                                                  round_q12, _stream(stream)), "hevc_transform_quant_8x8")
+
+
+def hevc_dequant_itransform_8x8(coeff, residual, qp, bit_depth=8, stream=None):
+    _check(lib().b200enc_hevc_dequant_itransform_8x8(_p(coeff), _p(residual), coeff.shape[0], qp, bit_depth,
+                                                     _stream(stream)), "hevc_dequant_itransform_8x8")
+
+
+def hevc_build_hpel(recon, w, h, margin, planes, stream=None):
+    """recon: uint8 device tensor [>=h][pitch]; planes: uint8 device tensor
+    [4][h + 2*margin][pitch >= w + 2*margin] (I, H, V, HV)."""
+    _check(lib().b200enc_hevc_build_hpel(_p(recon), recon.stride(0), w, h, margin, _p(planes[0]), _p(planes[1]),
+                                         _p(planes[2]), _p(planes[3]), planes.stride(1), _stream(stream)),
+           "hevc_build_hpel")
 
 
 def wavefront_status(scr, stream=None):

@@ -1,0 +1,362 @@
+// hevc.cu - HEVC encoder primitives the reference's host RD loop calls per
+// block, as batched GPU kernels:
+//   H1  half-sample planes of the previous reconstruction for the motion
+//       search (approach1-compute-encoder/src/hevc_enc_template.c:312-400,
+//       build_hpel / hpel_pass): the whole-sample plane and the H, V and HV
+//       planes of the 8-tap filter -1 4 -11 40 40 -11 4 -1, with a margin;
+//   H4  forward transform + quantisation of 4x4 (DCT-II or DST-VII) and 8x8
+//       (DCT-II) residual blocks at 8 or 10 bits (hevc_intra.c:468, :565, :720);
+//   H5  dequantisation + inverse transform of the same blocks
+//       (hevc_intra.c:484, :586, :761).
+// Arithmetic is the reference's compiled (SSE2) path: both transform passes
+// round, shift and saturate to int16 exactly where its packs instructions
+// do; the quantiser divides by levelScale through the same reciprocal
+// multiply, which is exact over the reachable range.
+#include <algorithm>
+
+#include "b200enc_internal.h"
+#include "common.cuh"
+
+namespace b200enc {
+
+// H.265 transform matrices and levelScale (standard constants; the decoder
+// uses the same values).
+__constant__ int16_t kHDct4[4][4] = {{64, 64, 64, 64}, {83, 36, -36, -83}, {64, -64, -64, 64}, {36, -83, 83, -36}};
+__constant__ int16_t kHDst4[4][4] = {{29, 55, 74, 84}, {74, 74, 0, -74}, {84, -29, -74, 55}, {55, -84, 74, -29}};
+__constant__ int16_t kHDct8[8][8] = {{64, 64, 64, 64, 64, 64, 64, 64},     {89, 75, 50, 18, -18, -50, -75, -89},
+                                     {83, 36, -36, -83, -83, -36, 36, 83}, {75, -18, -89, -50, 50, 89, 18, -75},
+                                     {64, -64, -64, 64, 64, -64, -64, 64}, {50, -89, 18, 75, -75, -18, 89, -50},
+                                     {36, -83, 83, -36, -36, 83, -83, 36}, {18, -50, 75, -89, 89, -75, 50, -18}};
+__constant__ int kHLevelScale[6] = {40, 45, 51, 57, 64, 72};
+
+__device__ __forceinline__ int sat16(int v) { return v > 32767 ? 32767 : (v < -32768 ? -32768 : v); }
+
+// Quantiser parameters of one QP: level = ((|x| << shift) + offset) >> p,
+// then * m >> 32 (division by levelScale), capped at 32767, sign restored.
+struct HQuant {
+  int shift, p;
+  uint32_t offset, m;
+};
+
+__device__ __forceinline__ HQuant hquant(int q, int shift, int round_q12) {
+  HQuant h;
+  h.shift = shift;
+  h.p = q / 6 + 4;
+  const uint32_t d = (uint32_t)kHLevelScale[q % 6];
+  h.offset = (uint32_t)((((uint64_t)d << h.p) * (uint64_t)round_q12) / 12u);
+  h.m = (uint32_t)((((uint64_t)1 << 32) + d - 1) / d);
+  return h;
+}
+
+__device__ __forceinline__ int16_t hquant_level(int x, const HQuant& h) {
+  const uint32_t mag = (uint32_t)(x < 0 ? -x : x);
+  const uint32_t t = ((mag << h.shift) + h.offset) >> h.p;
+  uint32_t l = (uint32_t)(((uint64_t)t * h.m) >> 32);
+  if (l > 32767u) l = 32767u;
+  return (int16_t)(x < 0 ? -(int)l : (int)l);
+}
+
+// Dequantisation, flat scaling list (8.6.3): level * levelScale << (q/6+4),
+// rounded and shifted down by bd_shift, saturated to int16.
+__device__ __forceinline__ int hdequant(int c, int q, int bd_shift) {
+  const int a = q / 6 + 4, ls = kHLevelScale[q % 6];
+  const int prod = c * ls;
+  int v;
+  if (a >= bd_shift) v = (int)((uint32_t)prod << (a - bd_shift));
+  else v = (prod + (1 << (bd_shift - a - 1))) >> (bd_shift - a);
+  return sat16(v);
+}
+
+// ---- 4x4 -------------------------------------------------------------------
+__global__ void hevc_tq4_kernel(const int16_t* __restrict__ res, int16_t* __restrict__ out, int n, int q, int use_dst,
+                                int round_q12, int s1, int qshift) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const int16_t(*M)[4] = use_dst ? kHDst4 : kHDct4;
+  int x[16];
+  const int4* src = reinterpret_cast<const int4*>(res + (size_t)b * 16);
+  const int4 v0 = src[0], v1 = src[1];
+  const int w[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    x[2 * i] = (int)(int16_t)(w[i] & 0xffff);
+    x[2 * i + 1] = (int)(int16_t)((uint32_t)w[i] >> 16);
+  }
+  // an all-zero block gives all-zero levels whatever the rounding offset
+  // (with a full-step offset the quantiser alone would give 1s)
+  if (!(v0.x | v0.y | v0.z | v0.w | v1.x | v1.y | v1.z | v1.w)) {
+    int4* dst = reinterpret_cast<int4*>(out + (size_t)b * 16);
+    dst[0] = dst[1] = make_int4(0, 0, 0, 0);
+    return;
+  }
+  int t[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      int s = 0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) s += M[i][r] * x[r * 4 + c];
+      t[i][c] = sat16((s + (1 << (s1 - 1))) >> s1);
+    }
+  const HQuant h = hquant(q, qshift, round_q12);
+  __align__(16) int16_t o[16];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int s = 0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) s += M[j][c] * t[i][c];
+      o[i * 4 + j] = hquant_level(sat16((s + 128) >> 8), h);
+    }
+  int4* dst = reinterpret_cast<int4*>(out + (size_t)b * 16);
+  dst[0] = *reinterpret_cast<const int4*>(&o[0]);
+  dst[1] = *reinterpret_cast<const int4*>(&o[8]);
+}
+
+__global__ void hevc_dqit4_kernel(const int16_t* __restrict__ coeff, int16_t* __restrict__ out, int n, int q,
+                                  int use_dst, int bd_shift, int s2) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const int16_t(*M)[4] = use_dst ? kHDst4 : kHDct4;
+  const int4* src = reinterpret_cast<const int4*>(coeff + (size_t)b * 16);
+  const int4 v0 = src[0], v1 = src[1];
+  const int w[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+  int d[16];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    d[2 * i] = hdequant((int)(int16_t)(w[i] & 0xffff), q, bd_shift);
+    d[2 * i + 1] = hdequant((int)(int16_t)((uint32_t)w[i] >> 16), q, bd_shift);
+  }
+  int g[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      int s = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s += M[k][r] * d[k * 4 + c];
+      g[r][c] = sat16((s + 64) >> 7);
+    }
+  __align__(16) int16_t o[16];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      int s = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s += M[k][c] * g[r][k];
+      o[r * 4 + c] = (int16_t)sat16((s + (1 << (s2 - 1))) >> s2);
+    }
+  int4* dst = reinterpret_cast<int4*>(out + (size_t)b * 16);
+  dst[0] = *reinterpret_cast<const int4*>(&o[0]);
+  dst[1] = *reinterpret_cast<const int4*>(&o[8]);
+}
+
+// ---- 8x8 -------------------------------------------------------------------
+__global__ void __launch_bounds__(128) hevc_tq8_kernel(const int16_t* __restrict__ res, int16_t* __restrict__ out,
+                                                       int n, int q, int round_q12, int s1, int qshift) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  int x[64];
+  const int4* src = reinterpret_cast<const int4*>(res + (size_t)b * 64);
+  int any = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int4 v = src[i];
+    any |= v.x | v.y | v.z | v.w;
+    const int w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      x[8 * i + 2 * k] = (int)(int16_t)(w[k] & 0xffff);
+      x[8 * i + 2 * k + 1] = (int)(int16_t)((uint32_t)w[k] >> 16);
+    }
+  }
+  if (!any) {  // as for 4x4: an all-zero block gives all-zero levels
+    int4* dst = reinterpret_cast<int4*>(out + (size_t)b * 64);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) dst[i] = make_int4(0, 0, 0, 0);
+    return;
+  }
+  int t[64];  // t[i*8+c]: column c, frequency i
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      int s = 0;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) s += kHDct8[i][r] * x[r * 8 + c];
+      t[i * 8 + c] = sat16((s + (1 << (s1 - 1))) >> s1);
+    }
+  const HQuant h = hquant(q, qshift, round_q12);
+  int4* dst = reinterpret_cast<int4*>(out + (size_t)b * 64);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    __align__(16) int16_t o[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      int s = 0;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) s += kHDct8[j][c] * t[i * 8 + c];
+      o[j] = hquant_level(sat16((s + 256) >> 9), h);
+    }
+    dst[i] = *reinterpret_cast<const int4*>(o);
+  }
+}
+
+__global__ void __launch_bounds__(128) hevc_dqit8_kernel(const int16_t* __restrict__ coeff, int16_t* __restrict__ out,
+                                                         int n, int q, int bd_shift, int s2) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  int d[64];
+  const int4* src = reinterpret_cast<const int4*>(coeff + (size_t)b * 64);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int4 v = src[i];
+    const int w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      d[8 * i + 2 * k] = hdequant((int)(int16_t)(w[k] & 0xffff), q, bd_shift);
+      d[8 * i + 2 * k + 1] = hdequant((int)(int16_t)((uint32_t)w[k] >> 16), q, bd_shift);
+    }
+  }
+  int g[64];  // g[r*8+c]
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      int s = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) s += kHDct8[k][r] * d[k * 8 + c];
+      g[r * 8 + c] = sat16((s + 64) >> 7);
+    }
+  int4* dst = reinterpret_cast<int4*>(out + (size_t)b * 64);
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    __align__(16) int16_t o[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      int s = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) s += kHDct8[k][c] * g[r * 8 + k];
+      o[c] = (int16_t)sat16((s + (1 << (s2 - 1))) >> s2);
+    }
+    dst[r] = *reinterpret_cast<const int4*>(o);
+  }
+}
+
+// ---- half-sample planes ----------------------------------------------------
+// Output tile of 32 columns x 8 rows per 256-thread block. Plane coordinates
+// (r, c) are picture coordinates + margin; every reference read is clamped to
+// the picture (the reference's edge extension). With Y(k) = clampY(r - M - 3 + k)
+// and X(k) = clampX(c - M - 3 + k):
+//   I  = ref[clampY(r - M)][clampX(c - M)]
+//   H  = clip((sum_k tap[k] * ref[clampY(r - M)][X(k)] + 32) >> 6)
+//   V  = clip((sum_k tap[k] * ref[Y(k)][clampX(c - M)] + 32) >> 6)
+//   HV = clip((sum_k tap[k] * T(Y(k)) + 2048) >> 12),  T(y) = sum_j tap[j] * ref[y][X(j)]
+constexpr int kHpTileW = 32, kHpTileH = 8;
+
+__global__ void __launch_bounds__(256) hevc_hpel_kernel(const uint8_t* __restrict__ ref, int pitch, int w, int h,
+                                                        int M, uint8_t* __restrict__ pI, uint8_t* __restrict__ pH,
+                                                        uint8_t* __restrict__ pV, uint8_t* __restrict__ pHV,
+                                                        int opitch, int rows, int cols) {
+  __shared__ uint8_t src[kHpTileH + 7][kHpTileW + 8];
+  __shared__ int32_t tsum[kHpTileH + 7][kHpTileW];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int c0 = blockIdx.x * kHpTileW, r0 = blockIdx.y * kHpTileH;
+  // source rows r0-M-3 .. r0-M+kHpTileH+3, columns c0-M-3 .. c0-M+kHpTileW+4
+  for (int i = threadIdx.x; i < (kHpTileH + 7) * (kHpTileW + 8); i += 256) {
+    const int sr = i / (kHpTileW + 8), sc = i - sr * (kHpTileW + 8);
+    const int y = clampi(r0 - M - 3 + sr, 0, h - 1), x = clampi(c0 - M - 3 + sc, 0, w - 1);
+    src[sr][sc] = ref[(size_t)y * pitch + x];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < (kHpTileH + 7) * kHpTileW; i += 256) {
+    const int sr = i / kHpTileW, sc = i - sr * kHpTileW;
+    const uint8_t* p = &src[sr][sc];
+    tsum[sr][sc] = -p[0] + 4 * p[1] - 11 * p[2] + 40 * p[3] + 40 * p[4] - 11 * p[5] + 4 * p[6] - p[7];
+  }
+  __syncthreads();
+  const int r = r0 + ty, c = c0 + tx;
+  if (r >= rows || c >= cols) return;
+  const int sr = ty + 3, sc = tx + 3;  // the sample (r - M, c - M) in the staged tile
+  const size_t o = (size_t)r * opitch + c;
+  pI[o] = src[sr][sc];
+  pH[o] = (uint8_t)clip1((tsum[sr][tx] + 32) >> 6);
+  const int v = -src[ty][sc] + 4 * src[ty + 1][sc] - 11 * src[ty + 2][sc] + 40 * src[ty + 3][sc] +
+                40 * src[ty + 4][sc] - 11 * src[ty + 5][sc] + 4 * src[ty + 6][sc] - src[ty + 7][sc];
+  pV[o] = (uint8_t)clip1((v + 32) >> 6);
+  const int hv = -tsum[ty][tx] + 4 * tsum[ty + 1][tx] - 11 * tsum[ty + 2][tx] + 40 * tsum[ty + 3][tx] +
+                 40 * tsum[ty + 4][tx] - 11 * tsum[ty + 5][tx] + 4 * tsum[ty + 6][tx] - tsum[ty + 7][tx];
+  pHV[o] = (uint8_t)clip1((hv + 2048) >> 12);
+}
+
+bool aligned16(const void* p) { return (((uintptr_t)p) & 15) == 0; }
+int hclamp(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+}  // namespace b200enc
+
+using namespace b200enc;
+
+extern "C" {
+
+int b200enc_hevc_transform_quant_4x4(const int16_t* residual, int16_t* coeff, int n, int qp, int use_dst,
+                                     int round_q12, int bit_depth, void* stream) {
+  if (!residual || !coeff || n < 0 || (bit_depth != 8 && bit_depth != 10)) return -1;
+  if (!aligned16(residual) || !aligned16(coeff) || round_q12 < 0 || round_q12 > 12) return -1;
+  if (n == 0) return 0;
+  const int q = bit_depth == 8 ? hclamp(qp, 0, 51) : hclamp(qp, 0, 63);
+  hevc_tq4_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(residual, coeff, n, q, use_dst ? 1 : 0,
+                                                                       round_q12, bit_depth == 8 ? 1 : 3,
+                                                                       bit_depth == 8 ? 5 : 7);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_hevc_dequant_itransform_4x4(const int16_t* coeff, int16_t* residual, int n, int qp, int use_dst,
+                                        int bit_depth, void* stream) {
+  if (!residual || !coeff || n < 0 || (bit_depth != 8 && bit_depth != 10)) return -1;
+  if (!aligned16(residual) || !aligned16(coeff)) return -1;
+  // the reference clamps the 10-bit Qp' but takes the 8-bit QP as given
+  if (bit_depth == 8 && (qp < 0 || qp > 51)) return -1;
+  if (n == 0) return 0;
+  const int q = bit_depth == 8 ? qp : hclamp(qp, 0, 63);
+  hevc_dqit4_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(coeff, residual, n, q, use_dst ? 1 : 0,
+                                                                         bit_depth == 8 ? 5 : 7,
+                                                                         bit_depth == 8 ? 12 : 10);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_hevc_transform_quant_8x8(const int16_t* residual, int16_t* coeff, int n, int qp, int bit_depth,
+                                     int round_q12, void* stream) {
+  if (!residual || !coeff || n < 0 || (bit_depth != 8 && bit_depth != 10)) return -1;
+  if (!aligned16(residual) || !aligned16(coeff) || round_q12 < 0 || round_q12 > 12) return -1;
+  if (n == 0) return 0;
+  hevc_tq8_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(residual, coeff, n, hclamp(qp, 0, 63),
+                                                                       round_q12, 3 + bit_depth - 9, bit_depth - 2);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_hevc_dequant_itransform_8x8(const int16_t* coeff, int16_t* residual, int n, int qp, int bit_depth,
+                                        void* stream) {
+  if (!residual || !coeff || n < 0 || (bit_depth != 8 && bit_depth != 10)) return -1;
+  if (!aligned16(residual) || !aligned16(coeff)) return -1;
+  if (n == 0) return 0;
+  hevc_dqit8_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(coeff, residual, n, hclamp(qp, 0, 63),
+                                                                         bit_depth - 2, 20 - bit_depth);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_hevc_build_hpel(const uint8_t* recon, int pitch, int w, int h, int margin, uint8_t* plane_i,
+                            uint8_t* plane_h, uint8_t* plane_v, uint8_t* plane_hv, int plane_pitch, void* stream) {
+  if (!recon || !plane_i || !plane_h || !plane_v || !plane_hv || w <= 0 || h <= 0) return -1;
+  if (margin < 0 || margin > 256 || pitch < w) return -1;
+  const int rows = h + 2 * margin, cols = w + 2 * margin;
+  if (plane_pitch < cols) return -1;
+  dim3 grid((cols + kHpTileW - 1) / kHpTileW, (rows + kHpTileH - 1) / kHpTileH);
+  hevc_hpel_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(recon, pitch, w, h, margin, plane_i, plane_h, plane_v,
+                                                           plane_hv, plane_pitch, rows, cols);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+}  // extern "C"

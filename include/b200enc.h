@@ -222,6 +222,37 @@ int b200enc_proposal_me(void *h, const uint8_t *cur_y, int cur_pitch, const uint
 /* Device pointer and size of an internal tensor (index list in proposal.cu). */
 int b200enc_proposal_tensor(void *h, int which, void **ptr, size_t *bytes);
 
+/* ---- HEVC encoder primitives ----------------------------------------------
+ * Batched versions of the per-block routines the reference's HEVC host
+ * encoder calls in its RD loop; arrays are device memory, 16-byte aligned,
+ * blocks stored row-major back to back (16 or 64 int16 each). Results equal
+ * the reference's compiled (SSE2) routines bit for bit. */
+/* Forward 4x4 DCT-II (use_dst 0) or DST-VII (use_dst 1) + quantisation of n
+ * residual blocks; replaces hevc_transform_quant_4x4 (8-bit, QP clamped to
+ * 0..51) and hevc_transform_quant_4x4_10 (10-bit, Qp' clamped to 0..63),
+ * approach1-compute-encoder/src/hevc_intra.c:468, :565. round_q12 in 0..12. */
+int b200enc_hevc_transform_quant_4x4(const int16_t *residual, int16_t *coeff, int n, int qp, int use_dst,
+                                     int round_q12, int bit_depth, void *stream);
+/* Dequantisation + inverse 4x4; replaces hevc_dequant_itransform_4x4 and
+ * _4x4_10 (hevc_intra.c:484, :586). 8-bit QP must be 0..51. */
+int b200enc_hevc_dequant_itransform_4x4(const int16_t *coeff, int16_t *residual, int n, int qp, int use_dst,
+                                        int bit_depth, void *stream);
+/* Forward 8x8 DCT-II + quantisation (Qp' clamped to 0..63); replaces
+ * hevc_transform_quant_8x8 (hevc_intra.c:720). */
+int b200enc_hevc_transform_quant_8x8(const int16_t *residual, int16_t *coeff, int n, int qp, int bit_depth,
+                                     int round_q12, void *stream);
+/* Dequantisation + inverse 8x8; replaces hevc_dequant_itransform_8x8
+ * (hevc_intra.c:761). */
+int b200enc_hevc_dequant_itransform_8x8(const int16_t *coeff, int16_t *residual, int n, int qp, int bit_depth,
+                                        void *stream);
+/* The motion search's sample planes of an 8-bit reconstruction (w x h,
+ * pitch): whole-sample I and half-sample H, V, HV (8-tap -1 4 -11 40 40 -11
+ * 4 -1), each (h + 2*margin) x (w + 2*margin) with plane_pitch, picture
+ * edges extended; replaces build_hpel / hpel_pass,
+ * approach1-compute-encoder/src/hevc_enc_template.c:219-400 (margin 16 there). */
+int b200enc_hevc_build_hpel(const uint8_t *recon, int pitch, int w, int h, int margin, uint8_t *plane_i,
+                            uint8_t *plane_h, uint8_t *plane_v, uint8_t *plane_hv, int plane_pitch, void *stream);
+
 /* Reads the error word a wavefront launch left in its scratch (synchronises
  * `stream`): 0 = fine, 1 = a bounded wait gave up (the frame's output is
  * incomplete and must not be used), -1 = the read failed. */
