@@ -24,7 +24,7 @@ EXPORTS = [
     "b200enc_proposal_train_step", "b200enc_proposal_me", "b200enc_proposal_tensor", "b200enc_proposal_load",
     "b200enc_ctx_set_me", "b200enc_ctx_me_stats",
     "b200enc_hevc_transform_quant_4x4", "b200enc_hevc_dequant_itransform_4x4", "b200enc_hevc_transform_quant_8x8",
-    "b200enc_hevc_dequant_itransform_8x8", "b200enc_hevc_build_hpel",
+    "b200enc_hevc_dequant_itransform_8x8", "b200enc_hevc_build_hpel", "b200enc_hevc_motion_search",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
     "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",
@@ -109,6 +109,7 @@ def load_library(path=LIB_PATH):
     lib.b200enc_hevc_transform_quant_8x8.argtypes = [_vp, _vp, _i, _i, _i, _i, _vp]
     lib.b200enc_hevc_dequant_itransform_8x8.argtypes = [_vp, _vp, _i, _i, _i, _vp]
     lib.b200enc_hevc_build_hpel.argtypes = [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp]
+    lib.b200enc_hevc_motion_search.argtypes = [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _i, _vp, _vp]
     lib.b200enc_ctx_set_me.argtypes = [ctypes.POINTER(GpuContext), _i, ctypes.c_char_p, ctypes.c_float]
     return lib
 
@@ -288,6 +289,24 @@ def hevc_build_hpel(recon, w, h, margin, planes, stream=None):
     _check(lib().b200enc_hevc_build_hpel(_p(recon), recon.stride(0), w, h, margin, _p(planes[0]), _p(planes[1]),
                                          _p(planes[2]), _p(planes[3]), planes.stride(1), _stream(stream)),
            "hevc_build_hpel")
+
+
+# b200enc_hevc_me_job_t / b200enc_hevc_me_result_t as numpy structured dtypes
+import numpy as _np  # noqa: E402
+HEVC_ME_JOB = _np.dtype([("cu_x", "<i4"), ("cu_y", "<i4"), ("mvp", "<i2", (2, 2)), ("starts", "<i2", (16, 2)),
+                         ("n_starts", "<i4"), ("lambda_q8", "<i4")])
+HEVC_ME_RESULT = _np.dtype([("mv", "<i2", (2,)), ("mvp_idx", "<i4"), ("cost_q8", "<i8"), ("sad", "<u4"),
+                            ("pad", "<u4")])
+
+
+def hevc_motion_search(src, w, h, planes, margin, qpel, jobs, results, stream=None):
+    """src: uint8 device tensor [>=h][pitch]; planes as hevc_build_hpel;
+    jobs / results: uint8 device tensors holding HEVC_ME_JOB / HEVC_ME_RESULT
+    records."""
+    n = jobs.numel() // HEVC_ME_JOB.itemsize
+    _check(lib().b200enc_hevc_motion_search(_p(src), src.stride(0), w, h, _p(planes[0]), _p(planes[1]),
+                                            _p(planes[2]), _p(planes[3]), planes.stride(1), margin, int(qpel),
+                                            _p(jobs), n, _p(results), _stream(stream)), "hevc_motion_search")
 
 
 def wavefront_status(scr, stream=None):

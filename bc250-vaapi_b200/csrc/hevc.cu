@@ -292,6 +292,142 @@ __global__ void __launch_bounds__(256) hevc_hpel_kernel(const uint8_t* __restric
   pHV[o] = (uint8_t)clip1((hv + 2048) >> 12);
 }
 
+// ---- 8x8 CU motion search -------------------------------------------------
+// One warp per CU job, the reference's walk (hevc_enc_template.c:958-1043)
+// step for step: every lane follows the same (uniform) control flow and the
+// SADs are warp reductions, lane l scoring row l/4, columns 2(l%4), +1.
+struct HevcSearch {
+  const uint8_t* src;
+  int src_pitch, w, h, M, qpel;
+  const uint8_t* plane[4];
+  int ppitch;
+};
+
+__device__ __forceinline__ int hevc_mvd_bits(int d) {
+  const unsigned a = (unsigned)(d < 0 ? -d : d);
+  if (a == 0) return 1;
+  if (a == 1) return 3;
+  return 3 + 2 * (31 - __clz((int)((a - 2) / 2 + 1))) + 2;
+}
+
+// SAD of the CU against the search planes at absolute quarter-sample
+// position (qx, qy) (search_sad, hevc_enc_template.c:463): positions are
+// clamped to the planes' margin; even/even reads one half-grid block, a
+// position odd in x, y or both averages (rounded) the two blocks beside it.
+__device__ __forceinline__ uint32_t hevc_search_sad(const HevcSearch& S, int cu_x, int cu_y, int qx, int qy,
+                                                    int lane) {
+  const int lo = -(S.M - 2) * 4;
+  const int hx = (S.w - 8 + S.M - 2) * 4, hy = (S.h - 8 + S.M - 2) * 4;
+  qx = qx < lo ? lo : (qx > hx ? hx : qx);
+  qy = qy < lo ? lo : (qy > hy ? hy : qy);
+  const int r = lane >> 2, c = (lane & 3) * 2;
+  auto sample = [&](int bqx, int bqy, int dc) -> int {
+    const int ph = ((bqx & 2) ? 1 : 0) + ((bqy & 2) ? 2 : 0);
+    const int x = (bqx >> 2) + S.M + c + dc, y = (bqy >> 2) + S.M + r;
+    return S.plane[ph][(size_t)y * S.ppitch + x];
+  };
+  uint32_t sad = 0;
+#pragma unroll
+  for (int dc = 0; dc < 2; ++dc) {
+    int v;
+    if (!(qx & 1) && !(qy & 1)) v = sample(qx, qy, dc);
+    else if ((qx & 1) && (qy & 1)) v = (sample(qx - 1, qy - 1, dc) + sample(qx + 1, qy + 1, dc) + 1) >> 1;
+    else if (qx & 1) v = (sample(qx - 1, qy, dc) + sample(qx + 1, qy, dc) + 1) >> 1;
+    else v = (sample(qx, qy - 1, dc) + sample(qx, qy + 1, dc) + 1) >> 1;
+    const int sv = S.src[(size_t)(cu_y + r) * S.src_pitch + cu_x + c + dc];
+    sad += (uint32_t)abs(sv - v);
+  }
+  return __reduce_add_sync(0xffffffffu, sad);
+}
+
+__global__ void __launch_bounds__(128) hevc_me_kernel(HevcSearch S, const b200enc_hevc_me_job_t* __restrict__ jobs,
+                                                      int n, b200enc_hevc_me_result_t* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (j >= n) return;
+  const b200enc_hevc_me_job_t job = jobs[j];
+  const int cu_x = job.cu_x, cu_y = job.cu_y;
+  if (cu_x < 0 || cu_y < 0 || cu_x > S.w - 8 || cu_y > S.h - 8) {  // not a CU of this picture
+    if (lane == 0) {
+      b200enc_hevc_me_result_t r{};
+      r.sad = 0xffffffffu;
+      r.cost_q8 = -1;
+      out[j] = r;
+    }
+    return;
+  }
+  const int min_dx = -cu_x - 8, max_dx = S.w - cu_x, min_dy = -cu_y - 8, max_dy = S.h - cu_y;
+  const int range = 64, qx0 = cu_x * 4, qy0 = cu_y * 4;
+  auto mv_bits = [&](int qx, int qy) -> int {
+    const int b0 = hevc_mvd_bits(qx - job.mvp[0].x) + hevc_mvd_bits(qy - job.mvp[0].y);
+    const int b1 = hevc_mvd_bits(qx - job.mvp[1].x) + hevc_mvd_bits(qy - job.mvp[1].y);
+    return b0 <= b1 ? b0 : b1;
+  };
+  auto cost = [&](int qx, int qy, uint32_t sad) -> long long {
+    return (long long)sad * 256 + (long long)job.lambda_q8 * mv_bits(qx, qy);
+  };
+  int bx = 0, by = 0;
+  long long best = 0x7fffffffffffffffll;
+  uint32_t best_sad = 0;
+  int seen_x[16], seen_y[16], n_seen = 0;
+  const int ns = job.n_starts < 0 ? 0 : (job.n_starts > 16 ? 16 : job.n_starts);
+  for (int i = 0; i < ns; ++i) {
+    int dx = (job.starts[i].x + 2) >> 2, dy = (job.starts[i].y + 2) >> 2;
+    dx = dx < min_dx ? min_dx : (dx > max_dx ? max_dx : dx);
+    dy = dy < min_dy ? min_dy : (dy > max_dy ? max_dy : dy);
+    bool dup = false;
+    for (int k = 0; k < n_seen && !dup; ++k) dup = seen_x[k] == dx && seen_y[k] == dy;
+    if (dup) continue;
+    seen_x[n_seen] = dx;
+    seen_y[n_seen++] = dy;
+    const uint32_t sd = hevc_search_sad(S, cu_x, cu_y, qx0 + dx * 4, qy0 + dy * 4, lane);
+    const long long c = cost(dx * 4, dy * 4, sd);
+    if (c < best) { best = c; best_sad = sd; bx = dx; by = dy; }
+  }
+  const int cx0 = bx, cy0 = by;
+  int back = -1;
+  for (int step = 0; step < 32; ++step) {
+    const int ddx[4] = {-1, 1, 0, 0}, ddy[4] = {0, 0, -1, 1};
+    int nbx = bx, nby = by, nk = -1;
+    for (int k = 0; k < 4; ++k) {
+      if (k == back) continue;
+      const int dx = bx + ddx[k], dy = by + ddy[k];
+      if (dx < min_dx || dx > max_dx || dy < min_dy || dy > max_dy) continue;
+      if (dx < cx0 - range || dx > cx0 + range || dy < cy0 - range || dy > cy0 + range) continue;
+      const uint32_t sd = hevc_search_sad(S, cu_x, cu_y, qx0 + dx * 4, qy0 + dy * 4, lane);
+      const long long c = cost(dx * 4, dy * 4, sd);
+      if (c < best) { best = c; best_sad = sd; nbx = dx; nby = dy; nk = k; }
+    }
+    if (nbx == bx && nby == by) break;
+    bx = nbx;
+    by = nby;
+    back = nk ^ 1;
+  }
+  int mx = bx * 4, my = by * 4;
+  for (int st = 2; st >= (S.qpel ? 1 : 2); st >>= 1) {
+    const int ox[8] = {-1, 0, 1, -1, 1, -1, 0, 1}, oy[8] = {-1, -1, -1, 0, 0, 1, 1, 1};
+    const int c0x = mx, c0y = my;
+    for (int k = 0; k < 8; ++k) {
+      const int tx = c0x + ox[k] * st, ty = c0y + oy[k] * st;
+      const uint32_t sd = hevc_search_sad(S, cu_x, cu_y, qx0 + tx, qy0 + ty, lane);
+      const long long c = cost(tx, ty, sd);
+      if (c < best) { best = c; best_sad = sd; mx = tx; my = ty; }
+    }
+  }
+  if (lane == 0) {
+    const int b0 = hevc_mvd_bits(mx - job.mvp[0].x) + hevc_mvd_bits(my - job.mvp[0].y);
+    const int b1 = hevc_mvd_bits(mx - job.mvp[1].x) + hevc_mvd_bits(my - job.mvp[1].y);
+    b200enc_hevc_me_result_t r;
+    r.mv.x = (int16_t)mx;
+    r.mv.y = (int16_t)my;
+    r.mvp_idx = b1 < b0 ? 1 : 0;
+    r.cost_q8 = best;
+    r.sad = best_sad;
+    r.pad = 0;
+    out[j] = r;
+  }
+}
+
 bool aligned16(const void* p) { return (((uintptr_t)p) & 15) == 0; }
 int hclamp(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -356,6 +492,18 @@ int b200enc_hevc_build_hpel(const uint8_t* recon, int pitch, int w, int h, int m
   dim3 grid((cols + kHpTileW - 1) / kHpTileW, (rows + kHpTileH - 1) / kHpTileH);
   hevc_hpel_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(recon, pitch, w, h, margin, plane_i, plane_h, plane_v,
                                                            plane_hv, plane_pitch, rows, cols);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_hevc_motion_search(const uint8_t* src_y, int src_pitch, int w, int h, const uint8_t* plane_i,
+                               const uint8_t* plane_h, const uint8_t* plane_v, const uint8_t* plane_hv, int plane_pitch,
+                               int margin, int qpel, const b200enc_hevc_me_job_t* jobs, int n,
+                               b200enc_hevc_me_result_t* results, void* stream) {
+  if (!src_y || !plane_i || !plane_h || !plane_v || !plane_hv || !jobs || !results || n < 0) return -1;
+  if (w < 8 || h < 8 || margin < 10 || plane_pitch < w + 2 * margin || src_pitch < w) return -1;
+  if (n == 0) return 0;
+  HevcSearch S{src_y, src_pitch, w, h, margin, qpel ? 1 : 0, {plane_i, plane_h, plane_v, plane_hv}, plane_pitch};
+  hevc_me_kernel<<<(n + 3) / 4, 128, 0, (cudaStream_t)stream>>>(S, jobs, n, results);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -253,6 +253,38 @@ int b200enc_hevc_dequant_itransform_8x8(const int16_t *coeff, int16_t *residual,
 int b200enc_hevc_build_hpel(const uint8_t *recon, int pitch, int w, int h, int margin, uint8_t *plane_i,
                             uint8_t *plane_h, uint8_t *plane_v, uint8_t *plane_hv, int plane_pitch, void *stream);
 
+/* Motion search of 8x8 CUs against the planes of b200enc_hevc_build_hpel
+ * (8-bit), one job per CU: the reference's motion_search
+ * (approach1-compute-encoder/src/hevc_enc_template.c:958-1043, with
+ * search_sad :463) step for step: every starting point at the nearest whole
+ * sample, a downhill walk (at most 32 steps, within +-64 of the best start,
+ * at most 8 samples past the picture), then half- and (qpel != 0)
+ * quarter-sample refinement; cost = SAD * 256 + lambda_q8 * the MVD bits to
+ * the cheaper predictor. The CU must lie inside the w x h picture (cu_x <=
+ * w-8, cu_y <= h-8; a job outside gets sad 0xffffffff and cost -1);
+ * margin >= 10 (16 in the reference). Jobs and results are device arrays. */
+typedef struct {
+    int16_t x, y; /* quarter samples */
+} b200enc_hevc_mv_t;
+typedef struct {
+    int32_t cu_x, cu_y;             /* luma position of the CU */
+    b200enc_hevc_mv_t mvp[2];        /* the two AMVP predictors */
+    b200enc_hevc_mv_t starts[16];    /* starting points */
+    int32_t n_starts;                /* 0..16 */
+    int32_t lambda_q8;
+} b200enc_hevc_me_job_t;
+typedef struct {
+    b200enc_hevc_mv_t mv;
+    int32_t mvp_idx;                 /* the cheaper predictor */
+    int64_t cost_q8;
+    uint32_t sad;
+    uint32_t pad;
+} b200enc_hevc_me_result_t;
+int b200enc_hevc_motion_search(const uint8_t *src_y, int src_pitch, int w, int h, const uint8_t *plane_i,
+                               const uint8_t *plane_h, const uint8_t *plane_v, const uint8_t *plane_hv,
+                               int plane_pitch, int margin, int qpel, const b200enc_hevc_me_job_t *jobs, int n,
+                               b200enc_hevc_me_result_t *results, void *stream);
+
 /* Reads the error word a wavefront launch left in its scratch (synchronises
  * `stream`): 0 = fine, 1 = a bounded wait gave up (the frame's output is
  * incomplete and must not be used), -1 = the read failed. */

@@ -53,3 +53,31 @@ int refshim_hevc_build_hpel(const uint8_t *recon, int w, int h, uint8_t *planes[
     free(enc.hpel_tmp);
     return HPEL_MARGIN;
 }
+
+/* motion_search (hevc_enc_template.c:958) of the 8-bit encoder for one 8x8
+ * CU: the search planes as build_hpel leaves them (pitch w + 2*16), the
+ * source picture (pitch w), quarter-sample refinement on or off. Writes the
+ * vector, the predictor index, the cost (q8) and the SAD. */
+void refshim_hevc_motion_search(uint8_t *planes[4], const uint8_t *src, int w, int h, int qpel, int cu_x, int cu_y,
+                                const int16_t mvp[4], const int16_t *starts, int n_starts, int lambda_q8,
+                                int16_t mv_out[2], int *mvp_idx, int64_t *cost_q8, uint32_t *sad)
+{
+    struct hevc_encoder enc;
+    memset(&enc, 0, sizeof(enc));
+    enc.coded_width = (uint32_t)w;
+    enc.coded_height = (uint32_t)h;
+    enc.bit_depth = 8;
+    enc.hpel_stride = w + 2 * HPEL_MARGIN;
+    for (int i = 0; i < 4; i++) enc.hpel[i] = planes[i];
+    enc.src_y = (void *)src;
+    enc.qpel = qpel != 0;
+    hevc_mv_t p[2] = {{mvp[0], mvp[1]}, {mvp[2], mvp[3]}};
+    hevc_mv_t st[16];
+    for (int i = 0; i < n_starts && i < 16; i++) {
+        st[i].x = starts[2 * i];
+        st[i].y = starts[2 * i + 1];
+    }
+    hevc_mv_t m = motion_search_8(&enc, cu_x, cu_y, p, st, n_starts, lambda_q8, mvp_idx, cost_q8, sad);
+    mv_out[0] = m.x;
+    mv_out[1] = m.y;
+}

@@ -7,7 +7,10 @@ encoder's static build_hpel exposed by oracle/hevc_shim.c), bit for bit:
   reference clamps), every rounding offset class, zero blocks, and extreme
   inputs that drive the int16 saturation of both transform passes;
 * the motion search's whole- and half-sample planes (margin 16) on frames
-  from 16x16 to 1920x1088.
+  from 16x16 to 1920x1088;
+* the 8x8 CU motion search (starting points, downhill walk, half/quarter
+  refinement, MVD-bit cost): vector, predictor index, cost and SAD of every
+  CU of a frame.
 """
 import ctypes
 import os
@@ -156,3 +159,61 @@ def test_rejects_bad_arguments(gpu):
     assert L.b200enc_hevc_transform_quant_4x4(gpu._p(x), gpu._p(x), 4, 27, 0, 13, 8, None) == -1  # rounding
     assert L.b200enc_hevc_dequant_itransform_4x4(gpu._p(x), gpu._p(x), 4, 52, 0, 8, None) == -1  # 8-bit QP
     assert L.b200enc_hevc_transform_quant_4x4(gpu._p(x), gpu._p(x), 0, 27, 0, 4, 8, None) == 0   # empty batch
+
+
+@needs_ref
+@pytest.mark.parametrize("w,h,qpel,seed", [(320, 192, 1, 1), (320, 192, 0, 2), (200, 120, 1, 3), (64, 64, 1, 4)])
+def test_motion_search(gpu, w, h, qpel, seed):
+    """Every 8x8 CU of a frame, with predictors and starting points spread
+    from the true motion to far outside the picture."""
+    import torch
+    from b200enc import synth
+    L = _ref()
+    L.refshim_hevc_motion_search.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    seq = synth.Sequence(w, h, seed=seed, pan=True)
+    ref = np.ascontiguousarray(seq.frame(0)[0])
+    src = np.ascontiguousarray(seq.frame(1)[0])
+    M = 16
+    rows, cols = h + 2 * M, w + 2 * M
+    planes_h = [np.zeros((rows, cols), np.uint8) for _ in range(4)]
+    ptrs = (ctypes.c_void_p * 4)(*[p.ctypes.data for p in planes_h])
+    L.refshim_hevc_build_hpel(ref.ctypes.data, w, h, ptrs)
+    rs = np.random.Generator(np.random.PCG64(seed))
+    cus = [(x, y) for y in range(0, h - 7, 8) for x in range(0, w - 7, 8)]
+    jobs = np.zeros(len(cus) + 2, gpu.HEVC_ME_JOB)
+    for j, (x, y) in enumerate(cus):
+        jobs[j]["cu_x"], jobs[j]["cu_y"] = x, y
+        jobs[j]["mvp"] = rs.integers(-40, 41, (2, 2))
+        ns = int(rs.integers(0, 17))
+        st = rs.integers(-40, 41, (16, 2))
+        st[::5] = rs.integers(-600, 601, (4, 2))[: len(st[::5])]  # far away: clamped to the margin
+        jobs[j]["starts"] = st
+        jobs[j]["n_starts"] = ns
+        jobs[j]["lambda_q8"] = int(rs.integers(0, 4000))
+    jobs[-2]["cu_x"], jobs[-2]["cu_y"] = w - 4, 0     # outside: rejected in the kernel
+    jobs[-1]["cu_x"], jobs[-1]["cu_y"] = 0, h
+    src_d = torch.from_numpy(src).cuda()
+    ppitch = (cols + 127) // 128 * 128
+    planes = torch.zeros((4, rows, ppitch), dtype=torch.uint8, device="cuda")
+    for k in range(4):
+        planes[k, :, :cols] = torch.from_numpy(planes_h[k])
+    jobs_d = torch.from_numpy(jobs.view(np.uint8)).cuda()
+    res_d = torch.zeros(len(jobs) * gpu.HEVC_ME_RESULT.itemsize, dtype=torch.uint8, device="cuda")
+    gpu.hevc_motion_search(src_d, w, h, planes, M, qpel, jobs_d, res_d)
+    torch.cuda.synchronize()
+    got = res_d.cpu().numpy().view(gpu.HEVC_ME_RESULT)
+    for j, (x, y) in enumerate(cus):
+        mv = np.zeros(2, np.int16)
+        idx, cost, sad = ctypes.c_int(), ctypes.c_int64(), ctypes.c_uint32()
+        mvp = np.ascontiguousarray(jobs[j]["mvp"].reshape(-1))
+        st = np.ascontiguousarray(jobs[j]["starts"].reshape(-1))
+        L.refshim_hevc_motion_search(ptrs, src.ctypes.data, w, h, qpel, x, y, mvp.ctypes.data, st.ctypes.data,
+                                     int(jobs[j]["n_starts"]), int(jobs[j]["lambda_q8"]), mv.ctypes.data,
+                                     ctypes.byref(idx), ctypes.byref(cost), ctypes.byref(sad))
+        g = got[j]
+        assert (tuple(g["mv"]), int(g["mvp_idx"]), int(g["cost_q8"]), int(g["sad"])) == \
+            (tuple(mv), idx.value, cost.value, sad.value), f"CU ({x},{y})"
+    assert (got[-2]["sad"], got[-1]["sad"]) == (0xFFFFFFFF, 0xFFFFFFFF)
