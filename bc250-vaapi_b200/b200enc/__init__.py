@@ -25,6 +25,7 @@ EXPORTS = [
     "b200enc_ctx_set_me", "b200enc_ctx_me_stats",
     "b200enc_hevc_transform_quant_4x4", "b200enc_hevc_dequant_itransform_4x4", "b200enc_hevc_transform_quant_8x8",
     "b200enc_hevc_dequant_itransform_8x8", "b200enc_hevc_build_hpel", "b200enc_hevc_motion_search",
+    "b200enc_hevc_choose_luma_mode",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
     "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",
@@ -110,6 +111,7 @@ def load_library(path=LIB_PATH):
     lib.b200enc_hevc_dequant_itransform_8x8.argtypes = [_vp, _vp, _i, _i, _i, _vp]
     lib.b200enc_hevc_build_hpel.argtypes = [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp]
     lib.b200enc_hevc_motion_search.argtypes = [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _i, _vp, _vp]
+    lib.b200enc_hevc_choose_luma_mode.argtypes = [_vp, _i, _vp, _i, _i, _i, _vp, _i, _vp, _vp, _vp]
     lib.b200enc_ctx_set_me.argtypes = [ctypes.POINTER(GpuContext), _i, ctypes.c_char_p, ctypes.c_float]
     return lib
 
@@ -307,6 +309,14 @@ def hevc_motion_search(src, w, h, planes, margin, qpel, jobs, results, stream=No
     _check(lib().b200enc_hevc_motion_search(_p(src), src.stride(0), w, h, _p(planes[0]), _p(planes[1]),
                                             _p(planes[2]), _p(planes[3]), planes.stride(1), margin, int(qpel),
                                             _p(jobs), n, _p(results), _stream(stream)), "hevc_motion_search")
+
+
+def hevc_choose_luma_mode(src, recon, width, height, jobs, modes, preds, stream=None):
+    """src, recon: uint8 device tensors (pitch = stride(0)); jobs: int32
+    device tensor [n][3] (x0, y0, y_min); modes: int32 [n]; preds: uint8 [n][16]."""
+    _check(lib().b200enc_hevc_choose_luma_mode(_p(src), src.stride(0), _p(recon), recon.stride(0), width, height,
+                                               _p(jobs), jobs.shape[0], _p(modes), _p(preds), _stream(stream)),
+           "hevc_choose_luma_mode")
 
 
 def wavefront_status(scr, stream=None):

@@ -428,6 +428,143 @@ __global__ void __launch_bounds__(128) hevc_me_kernel(HevcSearch S, const b200en
   }
 }
 
+// ---- intra 4x4 luma mode choice ----------------------------------------------
+// hevc_intra_template.c:20-260 (gather_neighbors, predict_from_refs,
+// hevc_choose_luma_mode) with hevc_intra.c's z-scan availability: a
+// neighbour is available iff it is inside the picture, at or below the
+// slice's first row, and earlier in the encoder's fixed coding order (CTU
+// 16x16 raster, CU 8x8 z-order, PU 4x4 z-order).
+__device__ __forceinline__ long long hz_rank(int x, int y, int width) {
+  const int width_ctu = (width + 15) >> 4;
+  const int rx = x & 15, ry = y & 15;
+  long long rank = ((long long)(y >> 4) * width_ctu + (x >> 4)) * 4 + ((ry >> 3) * 2 + (rx >> 3));
+  return rank * 4 + (((ry & 7) >> 2) * 2 + ((rx & 7) >> 2));
+}
+__device__ __forceinline__ bool hz_avail(int nx, int ny, int width, int height, int y_min, long long cur) {
+  if (nx < 0 || ny < y_min || nx >= width || ny >= height) return false;
+  return hz_rank(nx, ny, width) < cur;
+}
+
+constexpr int kHModePlanar = 0, kHModeDc = 1, kHModeHor = 10, kHModeVer = 26;
+
+__device__ __forceinline__ void hpredict(const int* left, const int* top, int corner, int mode, int* pred) {
+  if (mode == kHModePlanar) {
+#pragma unroll
+    for (int y = 0; y < 4; ++y)
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+        pred[y * 4 + x] = ((3 - x) * left[y] + (x + 1) * top[4] + (3 - y) * top[x] + (y + 1) * left[4] + 4) >> 3;
+  } else if (mode == kHModeDc) {
+    const int dc = (left[0] + left[1] + left[2] + left[3] + top[0] + top[1] + top[2] + top[3] + 4) >> 3;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) pred[i] = dc;
+    pred[0] = (left[0] + 2 * dc + top[0] + 2) >> 2;
+#pragma unroll
+    for (int x = 1; x < 4; ++x) pred[x] = (top[x] + 3 * dc + 2) >> 2;
+#pragma unroll
+    for (int y = 1; y < 4; ++y) pred[y * 4] = (left[y] + 3 * dc + 2) >> 2;
+  } else if (mode == kHModeHor) {
+#pragma unroll
+    for (int y = 0; y < 4; ++y)
+#pragma unroll
+      for (int x = 0; x < 4; ++x) pred[y * 4 + x] = left[y];
+#pragma unroll
+    for (int x = 0; x < 4; ++x) pred[x] = clip1(left[0] + ((top[x] - corner) >> 1));
+  } else {
+#pragma unroll
+    for (int y = 0; y < 4; ++y)
+#pragma unroll
+      for (int x = 0; x < 4; ++x) pred[y * 4 + x] = top[x];
+#pragma unroll
+    for (int y = 0; y < 4; ++y) pred[y * 4] = clip1(top[0] + ((left[y] - corner) >> 1));
+  }
+}
+
+__global__ void hevc_intra4_kernel(const uint8_t* __restrict__ src, int src_pitch, const uint8_t* __restrict__ rec,
+                                   int rec_pitch, int width, int height, const int* __restrict__ jobs, int n,
+                                   int* __restrict__ modes, uint8_t* __restrict__ preds) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int x0 = jobs[3 * j], y0 = jobs[3 * j + 1], y_min = jobs[3 * j + 2];
+  if (x0 < 0 || y0 < 0 || x0 + 4 > width || y0 + 4 > height || (x0 & 3) || (y0 & 3)) {
+    modes[j] = -1;  // not a 4x4 PU of this picture
+    return;
+  }
+  const long long cur = hz_rank(x0, y0, width);
+  const bool a_left = hz_avail(x0 - 1, y0, width, height, y_min, cur);
+  const bool a_top = hz_avail(x0, y0 - 1, width, height, y_min, cur);
+  const bool a_corner = hz_avail(x0 - 1, y0 - 1, width, height, y_min, cur);
+  const bool a_tr = hz_avail(x0 + 4, y0 - 1, width, height, y_min, cur);
+  // the substitution scan over p[-1][3..0], p[-1][-1], p[0..4][-1]
+  int sv[10];
+  bool sa[10];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    sa[i] = a_left;
+    sv[i] = a_left ? rec[(size_t)(y0 + 3 - i) * rec_pitch + x0 - 1] : 0;
+  }
+  sa[4] = a_corner;
+  sv[4] = a_corner ? rec[(size_t)(y0 - 1) * rec_pitch + x0 - 1] : 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    sa[5 + i] = a_top;
+    sv[5 + i] = a_top ? rec[(size_t)(y0 - 1) * rec_pitch + x0 + i] : 0;
+  }
+  sa[9] = a_tr;
+  sv[9] = a_tr ? rec[(size_t)(y0 - 1) * rec_pitch + x0 + 4] : 0;
+  int first = -1;
+#pragma unroll
+  for (int i = 9; i >= 0; --i)
+    if (sa[i]) first = i;
+  if (first < 0) {
+#pragma unroll
+    for (int i = 0; i < 10; ++i) sv[i] = 128;
+  } else {
+    const int f = sv[first];
+#pragma unroll
+    for (int i = 0; i < 10; ++i)
+      if (i < first) sv[i] = f;
+#pragma unroll
+    for (int i = 1; i < 10; ++i)
+      if (i > first && !sa[i]) sv[i] = sv[i - 1];
+  }
+  int left[5], top[5];
+  left[3] = sv[0]; left[2] = sv[1]; left[1] = sv[2]; left[0] = sv[3];
+  const int corner = sv[4];
+  top[0] = sv[5]; top[1] = sv[6]; top[2] = sv[7]; top[3] = sv[8]; top[4] = sv[9];
+  left[4] = hz_avail(x0 - 1, y0 + 4, width, height, y_min, cur) ? rec[(size_t)(y0 + 4) * rec_pitch + x0 - 1]
+                                                                : left[3];
+  int s[16];
+#pragma unroll
+  for (int y = 0; y < 4; ++y)
+#pragma unroll
+    for (int x = 0; x < 4; ++x) s[y * 4 + x] = src[(size_t)(y0 + y) * src_pitch + x0 + x];
+  const int order[4] = {kHModePlanar, kHModeDc, kHModeHor, kHModeVer};
+  int best_mode = -1, best_sad = 0;
+  int best_pred[16];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    int pr[16];
+    hpredict(left, top, corner, order[m], pr);
+    int sad = 0;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) sad += abs(s[i] - pr[i]);
+    if (m == 0 || sad < best_sad) {
+      best_sad = sad;
+      best_mode = order[m];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) best_pred[i] = pr[i];
+    }
+  }
+  modes[j] = best_mode;
+  uint32_t w4[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+    w4[r] = (uint32_t)best_pred[4 * r] | ((uint32_t)best_pred[4 * r + 1] << 8) |
+            ((uint32_t)best_pred[4 * r + 2] << 16) | ((uint32_t)best_pred[4 * r + 3] << 24);
+  *reinterpret_cast<uint4*>(preds + (size_t)j * 16) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+}
+
 bool aligned16(const void* p) { return (((uintptr_t)p) & 15) == 0; }
 int hclamp(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -504,6 +641,17 @@ int b200enc_hevc_motion_search(const uint8_t* src_y, int src_pitch, int w, int h
   if (n == 0) return 0;
   HevcSearch S{src_y, src_pitch, w, h, margin, qpel ? 1 : 0, {plane_i, plane_h, plane_v, plane_hv}, plane_pitch};
   hevc_me_kernel<<<(n + 3) / 4, 128, 0, (cudaStream_t)stream>>>(S, jobs, n, results);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_hevc_choose_luma_mode(const uint8_t* src_y, int src_pitch, const uint8_t* recon_y, int recon_pitch,
+                                  int width, int height, const int* jobs, int n, int* modes, uint8_t* preds,
+                                  void* stream) {
+  if (!src_y || !recon_y || !jobs || !modes || !preds || n < 0 || width < 4 || height < 4) return -1;
+  if (!aligned16(preds) || src_pitch < width || recon_pitch < width) return -1;
+  if (n == 0) return 0;
+  hevc_intra4_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(src_y, src_pitch, recon_y, recon_pitch, width,
+                                                                         height, jobs, n, modes, preds);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

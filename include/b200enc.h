@@ -285,6 +285,18 @@ int b200enc_hevc_motion_search(const uint8_t *src_y, int src_pitch, int w, int h
                                int plane_pitch, int margin, int qpel, const b200enc_hevc_me_job_t *jobs, int n,
                                b200enc_hevc_me_result_t *results, void *stream);
 
+/* Intra 4x4 luma mode choice of n PUs whose neighbours are already final in
+ * recon_y (8-bit): jobs = n x {x0, y0, y_min} (PU position, multiple of 4;
+ * first picture row of its slice). For each PU the reference's
+ * hevc_choose_luma_mode (approach1-compute-encoder/src/hevc_intra_template.c
+ * :177, neighbours :26-117 with the z-scan availability of hevc_intra.c:95-120):
+ * Planar, DC, horizontal, vertical by SAD, first best kept; modes[j] = the
+ * mode (0, 1, 10, 26), -1 for a position that is not a PU of the picture;
+ * preds = n x 16 predicted samples (16-byte aligned). */
+int b200enc_hevc_choose_luma_mode(const uint8_t *src_y, int src_pitch, const uint8_t *recon_y, int recon_pitch,
+                                  int width, int height, const int *jobs, int n, int *modes, uint8_t *preds,
+                                  void *stream);
+
 /* Reads the error word a wavefront launch left in its scratch (synchronises
  * `stream`): 0 = fine, 1 = a bounded wait gave up (the frame's output is
  * incomplete and must not be used), -1 = the read failed. */

@@ -10,7 +10,9 @@ encoder's static build_hpel exposed by oracle/hevc_shim.c), bit for bit:
   from 16x16 to 1920x1088;
 * the 8x8 CU motion search (starting points, downhill walk, half/quarter
   refinement, MVD-bit cost): vector, predictor index, cost and SAD of every
-  CU of a frame.
+  CU of a frame;
+* the intra 4x4 luma mode choice (mode and prediction) of PUs across picture
+  edges, z-order availability and slice starts.
 """
 import ctypes
 import os
@@ -217,3 +219,37 @@ def test_motion_search(gpu, w, h, qpel, seed):
         assert (tuple(g["mv"]), int(g["mvp_idx"]), int(g["cost_q8"]), int(g["sad"])) == \
             (tuple(mv), idx.value, cost.value, sad.value), f"CU ({x},{y})"
     assert (got[-2]["sad"], got[-1]["sad"]) == (0xFFFFFFFF, 0xFFFFFFFF)
+
+
+@needs_ref
+@pytest.mark.parametrize("w,h,slices", [(64, 48, [0]), (200, 120, [0, 48]), (1920, 1088, [0, 272, 544, 816])])
+def test_choose_luma_mode(gpu, w, h, slices):
+    """Every 4x4 PU of a picture against a fixed reconstruction, including
+    picture edges, CTU/CU/PU z-order availability and slice starts."""
+    import torch
+    L = _ref()
+    L.hevc_choose_luma_mode.restype = ctypes.c_int
+    L.hevc_choose_luma_mode.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    rs = np.random.Generator(np.random.PCG64(w * h))
+    src = np.clip(128 + 50 * rs.standard_normal((h, w)), 0, 255).astype(np.uint8)
+    rec = np.clip(src.astype(int) + rs.integers(-6, 7, (h, w)), 0, 255).astype(np.uint8)
+    rec[h // 3: h // 3 + 8] = 255  # strong edges exercise the clipped H/V edge filters
+    pus = [(x, y) for y in range(0, h, 4) for x in range(0, w, 4)]
+    if w > 256:
+        pus = pus[:: 7]
+    jobs = np.array([(x, y, max(sy for sy in slices if sy <= y)) for x, y in pus] + [(w - 2, 0, 0), (0, h, 0)],
+                    np.int32)
+    modes = torch.full((len(jobs),), -5, dtype=torch.int32, device="cuda")
+    preds = torch.zeros((len(jobs), 16), dtype=torch.uint8, device="cuda")
+    gpu.hevc_choose_luma_mode(torch.from_numpy(src).cuda(), torch.from_numpy(rec).cuda(), w, h,
+                              torch.from_numpy(jobs).cuda(), modes, preds)
+    torch.cuda.synchronize()
+    gm, gp = modes.cpu().numpy(), preds.cpu().numpy()
+    for j, (x, y, ym) in enumerate(jobs[:-2]):
+        pred = np.zeros(16, np.uint8)
+        m = L.hevc_choose_luma_mode(int(ym), src.ctypes.data, rec.ctypes.data, w, w, h, int(x), int(y),
+                                    pred.ctypes.data)
+        assert gm[j] == m, f"PU ({x},{y}) mode"
+        np.testing.assert_array_equal(gp[j], pred, err_msg=f"PU ({x},{y}) prediction")
+    assert gm[-2] == -1 and gm[-1] == -1
