@@ -18,13 +18,15 @@
 //   * a CTA owns a group of R consecutive macroblock rows (taken by ticket,
 //     so groups are only owned by running CTAs and waits cannot deadlock);
 //     R luma warps + R chroma warps, one warp per row and plane kind;
-//   * the group's rows (plus a 4-row / 2-row halo above) live in shared
-//     memory for the whole frame: one bulk load, one bulk store at the end;
+//   * the group's rows (plus a 4-row / 2-row halo above) pass through a
+//     ring of 16 macroblock columns in shared memory (42 KB per CTA at
+//     4 rows, whatever the picture width), so deblocking CTAs leave room on
+//     their SMs for other streams' kernels;
 //   * inside a CTA a row waits on its upper neighbour through a shared-memory
 //     progress word; only the group's first row waits on global memory;
-//   * two publisher warps (luma, chroma) follow the group's last row through
-//     its shared progress word and publish its final macroblocks in batches
-//     (their bottom 4 luma / 2 chroma sample rows, one fence, a release
+//   * two IO warps (luma, chroma) load the ring's columns ahead of the first
+//     row and, once the group's last row is done with a column, write it
+//     back and release it to the next group in batches (one fence, a release
 //     store), so no row warp ever waits on a device-scope fence;
 //   * boundary strengths of the whole group are computed up front.
 // Waits are bounded; on timeout a CTA records the error and leaves, and
@@ -151,13 +153,18 @@ __device__ __forceinline__ void chroma_regs(int p1, int& p0, int& q0, int q1, in
 
 __device__ __forceinline__ int tc0_for(int bs, int t1, int t2, int t3) { return bs == 1 ? t1 : (bs == 2 ? t2 : t3); }
 
-// Shared-memory plan of one CTA (dynamic shared memory):
-//   luma image  : (16R + 4) rows x sp bytes, row 0 = picture row 16*y0 - 4
-//   chroma image: (8R + 2) rows x sp bytes (NV12), row 0 = picture row 8*y0 - 2
+// Shared-memory plan of one CTA (dynamic shared memory). The group's rows
+// are held as a ring of kDbRing macroblock columns (column mx in slot
+// mx % kDbRing), not the whole picture width:
+//   luma ring   : (16R + 4) rows x sp bytes, row 0 = picture row 16*y0 - 4
+//   chroma ring : (8R + 2) rows x sp bytes (NV12), row 0 = picture row 8*y0 - 2
 //   bS          : R x mbw x 32 bytes ([dir][edge][segment] per macroblock)
-//   progress    : 2R words (luma rows, then chroma rows)
-// sp = 16*mbw + 4: a 4-byte skew per row keeps the 16 lanes that walk 16
+//   progress    : 2R words (luma rows, then chroma rows), then 2 words of
+//                 loaded columns (luma, chroma)
+// sp = 16*kDbRing + 4: a 4-byte skew per row keeps the 16 lanes that walk 16
 // consecutive rows of one column on 16 different banks.
+constexpr int kDbRing = 16;
+
 struct DbPlan {
   int R, sp;
   size_t luma_off, chroma_off, bs_off, prog_off, bytes;
@@ -166,12 +173,12 @@ struct DbPlan {
 __host__ __device__ inline DbPlan db_plan(int mbw, int R) {
   DbPlan p;
   p.R = R;
-  p.sp = 16 * mbw + 4;
+  p.sp = 16 * kDbRing + 4;
   p.luma_off = 0;
   p.chroma_off = p.luma_off + (size_t)(16 * R + 4) * p.sp;
   p.bs_off = p.chroma_off + (size_t)(8 * R + 2) * p.sp;
   p.prog_off = (p.bs_off + (size_t)R * mbw * 32 + 15) & ~(size_t)15;
-  p.bytes = p.prog_off + 2 * R * sizeof(uint32_t);
+  p.bytes = p.prog_off + (2 * R + 2) * sizeof(uint32_t);
   return p;
 }
 
@@ -224,7 +231,8 @@ __global__ void __launch_bounds__(320) deblock_kernel(int mbw, int mbh, int R, i
   const int al = kAlpha[qp], be = kBeta[qp], alc = kAlpha[qpc], bec = kBeta[qpc];
   const int tcl1 = kTc0[qp][0], tcl2 = kTc0[qp][1], tcl3 = kTc0[qp][2];
   const int tcc1 = kTc0[qpc][0], tcc2 = kTc0[qpc][1], tcc3 = kTc0[qpc][2];
-  const int W16 = 16 * mbw;
+
+  auto scol = [](int mx) { return 16 * (mx & (kDbRing - 1)); };  // byte offset of MB column mx in a ring row
 
   for (;;) {
     if (tid == 0) {
@@ -237,23 +245,8 @@ __global__ void __launch_bounds__(320) deblock_kernel(int mbw, int mbh, int R, i
     const int rows = min(R, mbh - y0);
     const bool has_next = y0 + rows < mbh;
 
-    // ---- prologue: own rows into shared memory, progress, bS ----------
-    for (int i = tid; i < 2 * R; i += nthr) prog[i] = 0u;
-    {
-      const int wpr = W16 / 16;  // uint4 per picture row
-      for (int i = tid; i < 16 * rows * wpr; i += nthr) {
-        const int r = i / wpr, c = i - r * wpr;
-        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(rec_y + (size_t)(16 * y0 + r) * rec_pitch) + c);
-        uint32_t* d = reinterpret_cast<uint32_t*>(ly + (size_t)(4 + r) * P.sp + 16 * c);
-        d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-      }
-      for (int i = tid; i < 8 * rows * wpr; i += nthr) {
-        const int r = i / wpr, c = i - r * wpr;
-        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(rec_uv + (size_t)(8 * y0 + r) * rec_pitch) + c);
-        uint32_t* d = reinterpret_cast<uint32_t*>(cy + (size_t)(2 + r) * P.sp + 16 * c);
-        d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-      }
-    }
+    // ---- prologue: progress words and the group's boundary strengths -----
+    for (int i = tid; i < 2 * R + 2; i += nthr) prog[i] = 0u;
     for (int i = tid; i < rows * mbw * 32; i += nthr) {
       // clause 8.7.2.1 for this encoder's macroblock kinds
       const int k = i & 3, e = (i >> 2) & 3, dir = (i >> 4) & 1, m = i >> 5;
@@ -283,77 +276,105 @@ __global__ void __launch_bounds__(320) deblock_kernel(int mbw, int mbh, int R, i
     const int wr = is_luma ? warp : warp - R;  // row within the group
     const int y = y0 + wr;
     if (warp >= 2 * R) {
-      // ---- publisher: luma (warp 2R) or chroma (warp 2R+1) -------------------
-      const bool pl_luma = warp == 2 * R;
-      const int last = rows - 1, yl = y0 + last;
-      const volatile uint32_t* lp = prog + (pl_luma ? 0 : R) + last;
-      uint32_t* gflag = (pl_luma ? gprog_luma : gprog_chroma) + yl;
-      uint32_t published = 0;
-      while (has_next && published < (uint32_t)mbw) {
+      // ---- IO warp: luma (warp 2R) or chroma (warp 2R+1) ---------------------
+      // Loads the group's macroblock columns into the ring ahead of its first
+      // row; once the group's last row has finished macroblock c+1 (its left
+      // edge was the last change to column c), writes column c back (the
+      // halo rows above the group, modified by the first row's top edges,
+      // included) and releases column c to the next group.
+      const bool io_luma = warp == 2 * R;
+      const int halo = io_luma ? 4 : 2, nrows = io_luma ? 16 * rows : 8 * rows;
+      uint8_t* base = io_luma ? ly : cy;
+      uint8_t* gplane = io_luma ? rec_y : rec_uv;
+      const int grow0 = io_luma ? 16 * y0 : 8 * y0;  // picture row of ring row `halo`
+      volatile uint32_t* loaded_prog = prog + 2 * R + (io_luma ? 0 : 1);
+      const volatile uint32_t* last_prog = prog + (io_luma ? 0 : R) + (rows - 1);
+      uint32_t* gflag = (io_luma ? gprog_luma : gprog_chroma) + (y0 + rows - 1);
+      const int wb0 = y0 > 0 ? 1 : halo, wb1 = halo + nrows;  // ring rows written back
+      int loaded = 0, evicted = 0;
+      while (evicted < mbw) {
+        bool did = false;
+        while (loaded < mbw && loaded - evicted < kDbRing) {
+          for (int r = lane; r < nrows; r += 32) {  // one 16-byte row segment per lane
+            const uint4 v = __ldcg(reinterpret_cast<const uint4*>(gplane + (size_t)(grow0 + r) * rec_pitch + 16 * loaded));
+            uint32_t* d = reinterpret_cast<uint32_t*>(base + (size_t)(halo + r) * P.sp + scol(loaded));
+            d[0] = v.x;
+            d[1] = v.y;
+            d[2] = v.z;
+            d[3] = v.w;
+          }
+          ++loaded;
+          did = true;
+          __threadfence_block();
+          __syncwarp();
+          if (lane == 0) *loaded_prog = (uint32_t)loaded;
+        }
+        // columns [0, d) are final (one read, broadcast: the word keeps moving)
+        uint32_t d = 0;
+        if (lane == 0) d = *last_prog;
+        d = __shfl_sync(0xffffffffu, d, 0);
+        if ((int)d > evicted) {
+          __threadfence_block();
+          for (int c = evicted; c < (int)d; ++c)
+            for (int rr = wb0 + lane; rr < wb1; rr += 32) {
+              const uint32_t* s4 = reinterpret_cast<const uint32_t*>(base + (size_t)rr * P.sp + scol(c));
+              __stcg(reinterpret_cast<uint4*>(gplane + (size_t)(grow0 + rr - halo) * rec_pitch + 16 * c),
+                     make_uint4(s4[0], s4[1], s4[2], s4[3]));
+            }
+          if (has_next) __threadfence();
+          __syncwarp();
+          if (has_next && lane == 0) store_release(gflag, d);
+          evicted = (int)d;
+          continue;
+        }
+        if (did) continue;
+        // nothing to load or write back: wait for the last row to move
         bool ok = true;
-        if (lane == 0) ok = wait_shared(lp, sc, published + 1, max_wait, (uint32_t)(yl * mbw + (int)published));
+        if (lane == 0) ok = wait_shared(last_prog, sc, (uint32_t)evicted + 1, max_wait,
+                                        (uint32_t)((y0 + rows - 1) * mbw + evicted));
         ok = __shfl_sync(0xffffffffu, ok, 0);
         if (!ok) {
           s_abort = 1;
           break;
         }
-        __threadfence_block();
-        // one read, broadcast: the last row keeps advancing the word, and the
-        // loop below must stay uniform across the warp
-        uint32_t done = 0;
-        if (lane == 0) done = *lp;
-        done = __shfl_sync(0xffffffffu, done, 0);
-        for (int bx = (int)published; bx < (int)done; ++bx) {
-          if (pl_luma) {
-            if (lane < 16) {
-              const int r = lane >> 2, w = lane & 3;
-              __stcg(reinterpret_cast<uint32_t*>(rec_y + (size_t)(16 * yl + 12 + r) * rec_pitch + 16 * bx + 4 * w),
-                     *reinterpret_cast<const uint32_t*>(ly + (size_t)(4 + 16 * last + 12 + r) * P.sp + 16 * bx + 4 * w));
-            }
-          } else if (lane < 8) {
-            const int r = lane >> 2, w = lane & 3;
-            __stcg(reinterpret_cast<uint32_t*>(rec_uv + (size_t)(8 * yl + 6 + r) * rec_pitch + 16 * bx + 4 * w),
-                   *reinterpret_cast<const uint32_t*>(cy + (size_t)(2 + 8 * last + 6 + r) * P.sp + 16 * bx + 4 * w));
-          }
-        }
-        __threadfence();
-        __syncwarp();
-        if (lane == 0) store_release(gflag, done);
-        published = done;
       }
     } else if (wr < rows) {
       const uint8_t* bsrow = bsm + (size_t)wr * mbw * 32;
       volatile uint32_t* my_prog = prog + (is_luma ? 0 : R) + wr;
       const volatile uint32_t* up_prog = prog + (is_luma ? 0 : R) + wr - 1;
+      const volatile uint32_t* loaded_prog = prog + 2 * R + (is_luma ? 0 : 1);
       uint32_t* gflag_up = (is_luma ? gprog_luma : gprog_chroma) + (y - 1);
       for (int mx = 0; mx < mbw; ++mx) {
         const uint32_t need = (uint32_t)(mx + 1);  // upper row: bottom samples of MB mx final
         bool ok = true;
-        if (y > 0) {
-          if (wr == 0) {
+        if (wr == 0) {
+          // the column in the ring, then (below the first group) the halo above
+          if (lane == 0) ok = wait_shared(loaded_prog, sc, need, max_wait, (uint32_t)(y * mbw + mx));
+          ok = __shfl_sync(0xffffffffu, ok, 0);
+          __threadfence_block();
+          if (ok && y > 0) {
             if (lane == 0) ok = wait_global(sc, gflag_up, need, max_wait, (uint32_t)(y * mbw + mx));
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (ok) {
-              // halo above: 4 luma / 2 chroma sample rows of this column
               if (is_luma) {
                 if (lane < 16) {
                   const int r = lane >> 2, w = lane & 3;
                   const uint32_t v = __ldcg(reinterpret_cast<const uint32_t*>(
                       rec_y + (size_t)(16 * y - 4 + r) * rec_pitch + 16 * mx + 4 * w));
-                  *reinterpret_cast<uint32_t*>(ly + (size_t)r * P.sp + 16 * mx + 4 * w) = v;
+                  *reinterpret_cast<uint32_t*>(ly + (size_t)r * P.sp + scol(mx) + 4 * w) = v;
                 }
               } else if (lane < 8) {
                 const int r = lane >> 2, w = lane & 3;
                 const uint32_t v = __ldcg(reinterpret_cast<const uint32_t*>(
                     rec_uv + (size_t)(8 * y - 2 + r) * rec_pitch + 16 * mx + 4 * w));
-                *reinterpret_cast<uint32_t*>(cy + (size_t)r * P.sp + 16 * mx + 4 * w) = v;
+                *reinterpret_cast<uint32_t*>(cy + (size_t)r * P.sp + scol(mx) + 4 * w) = v;
               }
             }
-          } else {
-            if (lane == 0) ok = wait_shared(up_prog, sc, need, max_wait, (uint32_t)(y * mbw + mx));
-            ok = __shfl_sync(0xffffffffu, ok, 0);
-            __threadfence_block();
           }
+        } else {
+          if (lane == 0) ok = wait_shared(up_prog, sc, need, max_wait, (uint32_t)(y * mbw + mx));
+          ok = __shfl_sync(0xffffffffu, ok, 0);
+          __threadfence_block();
         }
         if (!ok) {
           s_abort = 1;
@@ -365,10 +386,11 @@ __global__ void __launch_bounds__(320) deblock_kernel(int mbw, int mbh, int R, i
           if (al && be && lane < 16) {
             // vertical edges: this lane's sample row, 20 samples from p3 of
             // the left edge to q3 of the last internal edge, in registers
-            uint8_t* row = ly + (size_t)(4 + 16 * wr + lane) * P.sp + 16 * mx;
+            uint8_t* rowb = ly + (size_t)(4 + 16 * wr + lane) * P.sp;
+            uint32_t* rw = reinterpret_cast<uint32_t*>(rowb + scol(mx));
+            uint32_t* lw = reinterpret_cast<uint32_t*>(rowb + scol(mx - 1) + 12);
             int v[20];
-            const uint32_t* rw = reinterpret_cast<const uint32_t*>(row);
-            const uint32_t w0 = mx > 0 ? rw[-1] : 0u;
+            const uint32_t w0 = mx > 0 ? *lw : 0u;
             const uint32_t w1 = rw[0], w2 = rw[1], w3 = rw[2], w4 = rw[3];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
@@ -391,17 +413,16 @@ __global__ void __launch_bounds__(320) deblock_kernel(int mbw, int mbh, int R, i
             for (int k = 0; k < 5; ++k)
               o[k] = (uint32_t)v[4 * k] | ((uint32_t)v[4 * k + 1] << 8) | ((uint32_t)v[4 * k + 2] << 16) |
                      ((uint32_t)v[4 * k + 3] << 24);
-            uint32_t* ww = reinterpret_cast<uint32_t*>(row);
-            if (mx > 0) ww[-1] = o[0];
-            ww[0] = o[1];
-            ww[1] = o[2];
-            ww[2] = o[3];
-            ww[3] = o[4];
+            if (mx > 0) *lw = o[0];
+            rw[0] = o[1];
+            rw[1] = o[2];
+            rw[2] = o[3];
+            rw[3] = o[4];
           }
           __syncwarp();
           if (al && be && lane < 16) {
             // horizontal edges: this lane's sample column, rows -4..15
-            uint8_t* col = ly + (size_t)(16 * wr) * P.sp + 16 * mx + lane;
+            uint8_t* col = ly + (size_t)(16 * wr) * P.sp + scol(mx) + lane;
             int v[20];
 #pragma unroll
             for (int r = 0; r < 20; ++r) v[r] = col[(size_t)r * P.sp];
@@ -421,10 +442,12 @@ __global__ void __launch_bounds__(320) deblock_kernel(int mbw, int mbh, int R, i
             // vertical edges of one chroma plane's sample row: chroma
             // samples 8mx-2 .. 8mx+7 (every other byte of the NV12 row)
             const int pl = lane >> 3, i = lane & 7;
-            uint8_t* row = cy + (size_t)(2 + 8 * wr + i) * P.sp + 16 * mx + pl;
+            uint8_t* rowb = cy + (size_t)(2 + 8 * wr + i) * P.sp;
+            uint8_t* row = rowb + scol(mx) + pl;
+            uint8_t* left = rowb + scol(mx - 1) + pl;
             int v[10];
-            v[0] = mx > 0 ? row[-4] : 0;
-            v[1] = mx > 0 ? row[-2] : 0;
+            v[0] = mx > 0 ? left[12] : 0;
+            v[1] = mx > 0 ? left[14] : 0;
 #pragma unroll
             for (int k = 2; k < 10; ++k) v[k] = row[2 * (k - 2)];
             const int seg = i >> 1;
@@ -434,14 +457,14 @@ __global__ void __launch_bounds__(320) deblock_kernel(int mbw, int mbh, int R, i
               const int j = 2 + 2 * e;
               chroma_regs(v[j - 2], v[j - 1], v[j], v[j + 1], b, alc, bec, tc0_for(b, tcc1, tcc2, tcc3));
             }
-            if (mx > 0) row[-2] = (uint8_t)v[1];
+            if (mx > 0) left[14] = (uint8_t)v[1];
 #pragma unroll
             for (int k = 2; k < 10; ++k) row[2 * (k - 2)] = (uint8_t)v[k];
           }
           __syncwarp();
           if (alc && bec && lane < 16) {
             const int pl = lane >> 3, i = lane & 7;
-            uint8_t* col = cy + (size_t)(8 * wr) * P.sp + 16 * mx + 2 * i + pl;
+            uint8_t* col = cy + (size_t)(8 * wr) * P.sp + scol(mx) + 2 * i + pl;
             int v[10];
 #pragma unroll
             for (int r = 0; r < 10; ++r) v[r] = col[(size_t)r * P.sp];
@@ -457,8 +480,8 @@ __global__ void __launch_bounds__(320) deblock_kernel(int mbw, int mbh, int R, i
           }
         }
         __syncwarp();
-        // Macroblock mx-1's bottom samples are final now (mx's left edge was
-        // its last change); all of them after the last macroblock.
+        // Macroblock mx-1's samples are final now (mx's left edge was its
+        // last change); all of them after the last macroblock.
         const uint32_t done = (mx == mbw - 1) ? (uint32_t)mbw : (uint32_t)mx;
         __threadfence_block();
         __syncwarp();
@@ -467,27 +490,6 @@ __global__ void __launch_bounds__(320) deblock_kernel(int mbw, int mbh, int R, i
     }
     __syncthreads();
     if (s_abort) return;
-
-    // ---- epilogue: write the group's final samples back ------------------
-    // Luma picture rows [16*y0-3, last], chroma [8*y0-1, last], where the
-    // last rows belong to the next group if there is one (it filters and
-    // writes the 3 luma / 1 chroma rows above its first edge itself).
-    {
-      const int wpr = W16 / 4;
-      const int l0 = y0 > 0 ? -3 : 0, l1 = 16 * rows - (has_next ? 3 : 0);
-      for (int i = tid; i < (l1 - l0) * wpr; i += nthr) {
-        const int r = l0 + i / wpr, c = i % wpr;
-        __stcg(reinterpret_cast<uint32_t*>(rec_y + (size_t)(16 * y0 + r) * rec_pitch) + c,
-               *reinterpret_cast<const uint32_t*>(ly + (size_t)(4 + r) * P.sp + 4 * c));
-      }
-      const int c0 = y0 > 0 ? -1 : 0, c1 = 8 * rows - (has_next ? 1 : 0);
-      for (int i = tid; i < (c1 - c0) * wpr; i += nthr) {
-        const int r = c0 + i / wpr, c = i % wpr;
-        __stcg(reinterpret_cast<uint32_t*>(rec_uv + (size_t)(8 * y0 + r) * rec_pitch) + c,
-               *reinterpret_cast<const uint32_t*>(cy + (size_t)(2 + r) * P.sp + 4 * c));
-      }
-    }
-    __syncthreads();
   }
 }
 
@@ -497,8 +499,9 @@ using namespace b200enc;
 
 static constexpr uint32_t kMaxWaitUsDb = 2000000u;  // 2 s
 
-// Rows per CTA: as many as fit in shared memory (one luma + one chroma warp
-// each, at most 8 rows = 512 threads... capped at 4 to keep 256 threads).
+// Rows per CTA: at most 4 (one luma + one chroma warp each, plus the two IO
+// warps: 320 threads). The ring must hold the 2*R columns a group's rows
+// span plus prefetch, so R stays well below kDbRing.
 static int db_rows_per_cta(int mbw, int mbh) {
   int dev = 0, maxsm = 0;
   cudaGetDevice(&dev);

@@ -274,6 +274,8 @@ def run_gpu(args):
             return float(tt.item())
         return ms
 
+    host_ms = {}
+
     def arm(mode, nstreams, steps, warmup, perf=False, clocks=False):
         """Encodes warmup + steps frames on each of the first nstreams
         contexts from the start of a GOP; returns (ms, launches, perf, clk)."""
@@ -308,9 +310,11 @@ def run_gpu(args):
         for st in streams[:nstreams]:
             st.wait_event(e0)
         launches = 0
+        h0 = time.perf_counter()
         for _ in range(steps):
             launches += one_step(t)
             t += 1
+        host_issue_s = time.perf_counter() - h0  # host time to enqueue the timed steps
         for st in streams[:nstreams]:
             ev = torch.cuda.Event()
             ev.record(st)
@@ -319,6 +323,7 @@ def run_gpu(args):
         barrier()
         c = clk.stop() if clk else None
         pf = (ctxs[0].perf_read(False), ctxs[0].perf_read(True)) if perf else None
+        host_ms[mode, nstreams] = 1000.0 * host_issue_s / steps
         return max_over_ranks(e0.elapsed_time(e1)), launches, pf, c
 
     K, Wm = args.steps, args.warmup
@@ -397,6 +402,8 @@ def run_gpu(args):
                        "parallelism": f"replicas x{ws} (independent streams per GPU)"},
             "plain": {"value": round(fps_plain, 2), "unit": "frames/s", "ms_per_step": round(ms_p / K, 4)},
             "speedup_vs_plain": round(fps / fps_plain, 3),
+            "host_issue_ms_per_step": {"learned": round(host_ms[1, S], 4), "plain": round(host_ms[0, S], 4),
+                                       "note": "host time to enqueue one step (all streams); compare ms_per_step"},
             "single_stream": {"learned_fps": round(k1 / (ms_l1 / 1000.0), 2),
                               "plain_fps": round(k1 / (ms_p1 / 1000.0), 2),
                               "learned_stage_ms_per_p_frame": {k2: round(v, 4) for k2, v in stage_ms.items()},
