@@ -25,7 +25,7 @@ EXPORTS = [
     "b200enc_ctx_set_me", "b200enc_ctx_me_stats",
     "b200enc_hevc_transform_quant_4x4", "b200enc_hevc_dequant_itransform_4x4", "b200enc_hevc_transform_quant_8x8",
     "b200enc_hevc_dequant_itransform_8x8", "b200enc_hevc_build_hpel", "b200enc_hevc_motion_search",
-    "b200enc_hevc_choose_luma_mode",
+    "b200enc_hevc_choose_luma_mode", "b200enc_hevc_deblock",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
     "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",
@@ -112,6 +112,7 @@ def load_library(path=LIB_PATH):
     lib.b200enc_hevc_build_hpel.argtypes = [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp]
     lib.b200enc_hevc_motion_search.argtypes = [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _i, _vp, _vp]
     lib.b200enc_hevc_choose_luma_mode.argtypes = [_vp, _i, _vp, _i, _i, _i, _vp, _i, _vp, _vp, _vp]
+    lib.b200enc_hevc_deblock.argtypes = [ctypes.POINTER(HevcDeblockParams), _vp]
     lib.b200enc_ctx_set_me.argtypes = [ctypes.POINTER(GpuContext), _i, ctypes.c_char_p, ctypes.c_float]
     return lib
 
@@ -317,6 +318,54 @@ def hevc_choose_luma_mode(src, recon, width, height, jobs, modes, preds, stream=
     _check(lib().b200enc_hevc_choose_luma_mode(_p(src), src.stride(0), _p(recon), recon.stride(0), width, height,
                                                _p(jobs), jobs.shape[0], _p(modes), _p(preds), _stream(stream)),
            "hevc_choose_luma_mode")
+
+
+# b200enc_hevc_mvf_t / b200enc_hevc_slice_filter_t records and the
+# b200enc_hevc_deblock_t parameter block
+HEVC_MVF = _np.dtype([("mv", "<i2", (2, 2)), ("ref_poc", "<i4", (2,)), ("pred_flag", "u1"), ("pad", "u1", (3,))])
+HEVC_SLICE_FILTER = _np.dtype([("beta_offset", "<i2"), ("tc_offset", "<i2"), ("disabled", "u1"),
+                               ("across_slices", "u1"), ("pad", "u1", (2,))])
+
+
+class HevcDeblockParams(ctypes.Structure):
+    _fields_ = [("plane", ctypes.c_void_p * 3), ("stride", ctypes.c_int * 3), ("width", ctypes.c_int),
+                ("height", ctypes.c_int), ("bit_depth_luma", ctypes.c_int), ("bit_depth_chroma", ctypes.c_int),
+                ("log2_ctb", ctypes.c_int), ("log2_min_cb", ctypes.c_int), ("edges", ctypes.c_void_p),
+                ("edges_stride", ctypes.c_int), ("mvf", ctypes.c_void_p), ("cbf", ctypes.c_void_p),
+                ("min_pu_width", ctypes.c_int), ("qp_y", ctypes.c_void_p), ("no_filter", ctypes.c_void_p),
+                ("slice_of_ctb", ctypes.c_void_p), ("slice_filter", ctypes.c_void_p),
+                ("n_slice_filter", ctypes.c_int), ("tile_of_ctb", ctypes.c_void_p),
+                ("loop_filter_across_tiles", ctypes.c_int), ("cb_qp_offset", ctypes.c_int),
+                ("cr_qp_offset", ctypes.c_int)]
+
+
+def hevc_deblock_params(ptr, planes, strides, width, height, bit_depth_luma, bit_depth_chroma, log2_ctb,
+                        log2_min_cb, edges, edges_stride, qp_y, mvf=None, cbf=None, min_pu_width=0,
+                        no_filter=None, slice_of_ctb=None, slice_filter=None, n_slice_filter=0, tile_of_ctb=None,
+                        loop_filter_across_tiles=True, cb_qp_offset=0, cr_qp_offset=0):
+    """The parameter block of b200enc_hevc_deblock; `ptr(x)` turns each
+    buffer (device tensor for the GPU, numpy array for the oracle) into an
+    address, None into NULL."""
+    a = lambda x: None if x is None else ptr(x)
+    q = HevcDeblockParams()
+    for c in range(3):
+        q.plane[c] = a(planes[c])
+        q.stride[c] = int(strides[c])
+    q.width, q.height = width, height
+    q.bit_depth_luma, q.bit_depth_chroma = bit_depth_luma, bit_depth_chroma
+    q.log2_ctb, q.log2_min_cb = log2_ctb, log2_min_cb
+    q.edges, q.edges_stride = a(edges), edges_stride
+    q.mvf, q.cbf, q.min_pu_width = a(mvf), a(cbf), min_pu_width
+    q.qp_y, q.no_filter = a(qp_y), a(no_filter)
+    q.slice_of_ctb, q.slice_filter, q.n_slice_filter = a(slice_of_ctb), a(slice_filter), n_slice_filter
+    q.tile_of_ctb, q.loop_filter_across_tiles = a(tile_of_ctb), int(loop_filter_across_tiles)
+    q.cb_qp_offset, q.cr_qp_offset = cb_qp_offset, cr_qp_offset
+    return q
+
+
+def hevc_deblock(params, stream=None):
+    """HEVC deblocking of one picture in place (device buffers in `params`)."""
+    _check(lib().b200enc_hevc_deblock(ctypes.byref(params), _stream(stream)), "hevc_deblock")
 
 
 def wavefront_status(scr, stream=None):

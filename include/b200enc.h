@@ -297,6 +297,54 @@ int b200enc_hevc_choose_luma_mode(const uint8_t *src_y, int src_pitch, const uin
                                   int width, int height, const int *jobs, int n, int *modes, uint8_t *preds,
                                   void *stream);
 
+/* HEVC deblocking (H.265 8.7.2) of one 4:2:0 picture, in place: every
+ * vertical edge of the picture, then every horizontal edge over what the
+ * vertical pass left. Replaces the deblocking stages of the reference's
+ * hevcd_loop_filters (approach1-compute-encoder/src/hevc_filter.c:449-490,
+ * stages 0 and 1 = deblock_row over one_direction,
+ * hevc_filter_template.c:48-420); SAO is not part of it. The maps are the
+ * decoder's (hevc_dec_internal.h:56-70, 133-148, 214-235), in device
+ * memory: */
+typedef struct {
+    int16_t mv[2][2];                /* [list][x, y], quarter samples */
+    int32_t ref_poc[2];              /* the picture each list points at */
+    uint8_t pred_flag;               /* 0 intra, 1 list 0, 2 list 1, 3 both */
+    uint8_t pad[3];
+} b200enc_hevc_mvf_t;                /* 20 bytes, one per 4x4 */
+typedef struct {
+    int16_t beta_offset, tc_offset;  /* slice_beta/tc_offset_div2 * 2 */
+    uint8_t disabled;                /* slice_deblocking_filter_disabled_flag */
+    uint8_t across_slices;           /* slice_loop_filter_across_slices_enabled_flag */
+    uint8_t pad[2];
+} b200enc_hevc_slice_filter_t;
+typedef struct {
+    void *plane[3];                  /* Y, Cb, Cr: uint8 at 8 bits, uint16 at 10 */
+    int stride[3];                   /* in samples */
+    int width, height;               /* luma samples, multiples of 8 and of the min CB */
+    int bit_depth_luma, bit_depth_chroma;  /* 8 or 10 (luma decides the sample type) */
+    int log2_ctb, log2_min_cb;
+    /* per 8x8 cell, edges_stride >= width/8 cells a row: bit 0 a block
+     * boundary on its left edge, bit 1 on its top edge, bit 2 / bit 3 that
+     * left / top edge is a transform block edge; cells at x >= width are
+     * not read */
+    const uint8_t *edges;
+    int edges_stride;
+    const b200enc_hevc_mvf_t *mvf;   /* per 4x4, min_pu_width a row; NULL: bS 2 on every edge */
+    const uint8_t *cbf;              /* per 4x4 (luma residual present), or NULL */
+    int min_pu_width;
+    const int8_t *qp_y;              /* QpY per min coding block, width >> log2_min_cb a row */
+    const uint8_t *no_filter;        /* per min coding block (lossless), or NULL */
+    const int32_t *slice_of_ctb;     /* per CTB in raster order, or NULL (all slice 0) */
+    const b200enc_hevc_slice_filter_t *slice_filter;  /* n_slice_filter entries; NULL filters nothing */
+    int n_slice_filter;
+    const int32_t *tile_of_ctb;      /* per CTB in raster order, or NULL (one tile) */
+    int loop_filter_across_tiles;
+    int cb_qp_offset, cr_qp_offset;  /* pps_cb/cr_qp_offset */
+} b200enc_hevc_deblock_t;
+/* The parameter block itself is host memory. Returns 0, or -1 for a
+ * parameter out of range or a launch failure. */
+int b200enc_hevc_deblock(const b200enc_hevc_deblock_t *p, void *stream);
+
 /* Reads the error word a wavefront launch left in its scratch (synchronises
  * `stream`): 0 = fine, 1 = a bounded wait gave up (the frame's output is
  * incomplete and must not be used), -1 = the read failed. */
