@@ -16,8 +16,9 @@
 // the 8-sample grid and a luma filter reads 4 and writes 3 samples either
 // side (chroma: 8 chroma samples apart, reads 2, writes 1), so no edge reads
 // or writes a sample another edge of the same pass writes. One thread per
-// 4-line segment filters in place in global memory - no tiles, no halos,
-// nothing shared between threads. (A single launch over tiles with halos
+// 4-line segment filters in place in global memory - no tiles, no halos -
+// one lane per line, the segment's four lanes sharing the decision through
+// warp shuffles. (A single launch over tiles with halos
 // would need the neighbours' samples as the vertical pass left them, which
 // an in-place neighbour may already have overwritten.) Consecutive threads
 // take consecutive segments along a row, so each warp reads and writes
@@ -61,26 +62,28 @@ __device__ __forceinline__ int hdb_ctb(const b200enc_hevc_deblock_t& p, int x, i
   return (y >> p.log2_ctb) * ctb_w + (x >> p.log2_ctb);
 }
 
-__device__ HdbEdge hdb_edge(const b200enc_hevc_deblock_t& p, int x, int y, bool vertical, int ctb_w) {
+__device__ __forceinline__ HdbEdge hdb_edge(const b200enc_hevc_deblock_t& p, int x, int y, bool vertical, int ctb_w) {
+  // Every map read is issued before any of them is looked at (one round
+  // trip instead of a chain); only the slice settings wait for the slice id.
+  const int xp = vertical ? x - 1 : x, yp = vertical ? y : y - 1;
+  const int cq = hdb_ctb(p, x, y, ctb_w), cp = hdb_ctb(p, xp, yp, ctb_w);
+  const int l = p.log2_min_cb, mcw = p.width >> l;
+  const int bq = (y >> l) * mcw + (x >> l), bp = (yp >> l) * mcw + (xp >> l);
+  const int tq = p.tile_of_ctb ? __ldg(p.tile_of_ctb + cq) : 0, tp = p.tile_of_ctb ? __ldg(p.tile_of_ctb + cp) : 0;
+  const int sq = p.slice_of_ctb ? __ldg(p.slice_of_ctb + cq) : 0, sp = p.slice_of_ctb ? __ldg(p.slice_of_ctb + cp) : 0;
+  const bool nq = p.no_filter && __ldg(p.no_filter + bq) != 0, np = p.no_filter && __ldg(p.no_filter + bp) != 0;
+  const int qq = __ldg(p.qp_y + bq), qp = __ldg(p.qp_y + bp);
   HdbEdge r;
   r.on = false;
-  const int xp = vertical ? x - 1 : x, yp = vertical ? y : y - 1;
-  if (p.tile_of_ctb && !p.loop_filter_across_tiles &&
-      __ldg(p.tile_of_ctb + hdb_ctb(p, xp, yp, ctb_w)) != __ldg(p.tile_of_ctb + hdb_ctb(p, x, y, ctb_w)))
-    return r;
-  const int sq = p.slice_of_ctb ? __ldg(p.slice_of_ctb + hdb_ctb(p, x, y, ctb_w)) : 0;
+  if (!p.loop_filter_across_tiles && tp != tq) return r;
   if (sq < 0 || !p.slice_filter || sq >= p.n_slice_filter) return r;
   const b200enc_hevc_slice_filter_t f = p.slice_filter[sq];
   if (f.disabled) return r;
-  if (!f.across_slices) {
-    const int sp = p.slice_of_ctb ? __ldg(p.slice_of_ctb + hdb_ctb(p, xp, yp, ctb_w)) : 0;
-    if (sp != sq) return r;
-  }
-  const int l = p.log2_min_cb, mcw = p.width >> l;
-  r.keep_p = p.no_filter && __ldg(p.no_filter + (yp >> l) * mcw + (xp >> l)) != 0;
-  r.keep_q = p.no_filter && __ldg(p.no_filter + (y >> l) * mcw + (x >> l)) != 0;
-  if (r.keep_p && r.keep_q) return r;
-  r.qp = ((int)__ldg(p.qp_y + (y >> l) * mcw + (x >> l)) + (int)__ldg(p.qp_y + (yp >> l) * mcw + (xp >> l)) + 1) >> 1;
+  if (!f.across_slices && sp != sq) return r;
+  r.keep_p = np;
+  r.keep_q = nq;
+  if (np && nq) return r;
+  r.qp = (qq + qp + 1) >> 1;
   r.beta = (int)kHdbBeta[hdb_clip(r.qp + f.beta_offset, 0, 51)] << (p.bit_depth_luma - 8);
   r.tc_offset = f.tc_offset;
   r.on = true;
@@ -141,78 +144,77 @@ __device__ int hdb_strength(const b200enc_hevc_deblock_t& p, int xp, int yp, int
   return (straight || swapped) ? 0 : 1;
 }
 
-// One 4-line luma segment in shared memory (clauses 8.7.2.5.3, 8.7.2.5.6,
-// 8.7.2.5.7; hevc_filter_template.c:48-140): `q` at q0 of the first line,
-// `fw` from p to q, `gl` from one line to the next.
+// One line of a 4-line luma segment (clauses 8.7.2.5.3, 8.7.2.5.6,
+// 8.7.2.5.7; hevc_filter_template.c:48-140). The four lanes 4k..4k+3 of a
+// warp hold the segment's four lines; the decisions read lines 0 and 3 only,
+// so those lanes' figures are shuffled to the other two. `q` points at this
+// line's q0 and `fw` steps from p to q. Every lane of the warp calls it
+// (the shuffles); `inside` says the segment lies in the picture (its
+// samples may be read), `act` that it is filtered.
 template <typename T>
-__device__ void hdb_luma(T* q, int fw, int gl, int beta, int tc, bool keep_p, bool keep_q, int maxv) {
-  auto P = [&](int k, int i) { return (int)q[i * gl - (k + 1) * fw]; };
-  auto Q = [&](int k, int i) { return (int)q[i * gl + k * fw]; };
-  const int dp0 = abs(P(2, 0) - 2 * P(1, 0) + P(0, 0)), dp3 = abs(P(2, 3) - 2 * P(1, 3) + P(0, 3));
-  const int dq0 = abs(Q(2, 0) - 2 * Q(1, 0) + Q(0, 0)), dq3 = abs(Q(2, 3) - 2 * Q(1, 3) + Q(0, 3));
+__device__ __forceinline__ void hdb_luma_line(T* q, int fw, bool inside, bool act, int beta, int tc, bool keep_p,
+                                              bool keep_q, int maxv) {
+  int p3 = 0, p2 = 0, p1 = 0, p0 = 0, q0 = 0, q1 = 0, q2 = 0, q3 = 0;
+  if (inside) {  // the samples of an edge position in the picture, whether or not it is filtered
+    p3 = q[-4 * fw];
+    p2 = q[-3 * fw];
+    p1 = q[-2 * fw];
+    p0 = q[-fw];
+    q0 = q[0];
+    q1 = q[fw];
+    q2 = q[2 * fw];
+    q3 = q[3 * fw];
+  }
+  const int dp = abs(p2 - 2 * p1 + p0), dq = abs(q2 - 2 * q1 + q0);
+  const int flat = abs(p3 - p0) + abs(q0 - q3), step = abs(p0 - q0);
+  const int l0 = (threadIdx.x & 31) & ~3, l3 = l0 + 3;
+  const int dp0 = __shfl_sync(0xffffffffu, dp, l0), dp3 = __shfl_sync(0xffffffffu, dp, l3);
+  const int dq0 = __shfl_sync(0xffffffffu, dq, l0), dq3 = __shfl_sync(0xffffffffu, dq, l3);
+  const int fl0 = __shfl_sync(0xffffffffu, flat, l0), fl3 = __shfl_sync(0xffffffffu, flat, l3);
+  const int st0 = __shfl_sync(0xffffffffu, step, l0), st3 = __shfl_sync(0xffffffffu, step, l3);
+  if (!act) return;
   const int dpq0 = dp0 + dq0, dpq3 = dp3 + dq3;
   if (dpq0 + dpq3 >= beta) return;
-  const int dp = dp0 + dp3, dq = dq0 + dq3;
   const int thr = (5 * tc + 1) >> 1;
-  bool strong = true;
-#pragma unroll
-  for (int i = 0; i < 4; i += 3) {
-    const int dpq = 2 * (i == 0 ? dpq0 : dpq3);
-    strong = strong && dpq < (beta >> 2) && abs(P(3, i) - P(0, i)) + abs(Q(0, i) - Q(3, i)) < (beta >> 3) &&
-             abs(P(0, i) - Q(0, i)) < thr;
-  }
+  const bool strong = 2 * dpq0 < (beta >> 2) && fl0 < (beta >> 3) && st0 < thr && 2 * dpq3 < (beta >> 2) &&
+                      fl3 < (beta >> 3) && st3 < thr;
   if (strong) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int p0 = P(0, i), p1 = P(1, i), p2 = P(2, i), p3 = P(3, i);
-      const int q0 = Q(0, i), q1 = Q(1, i), q2 = Q(2, i), q3 = Q(3, i);
-      T* l = q + i * gl;
-      if (!keep_p) {
-        l[-fw] = (T)hdb_clip((p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3, p0 - 2 * tc, p0 + 2 * tc);
-        l[-2 * fw] = (T)hdb_clip((p2 + p1 + p0 + q0 + 2) >> 2, p1 - 2 * tc, p1 + 2 * tc);
-        l[-3 * fw] = (T)hdb_clip((2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3, p2 - 2 * tc, p2 + 2 * tc);
-      }
-      if (!keep_q) {
-        l[0] = (T)hdb_clip((p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3, q0 - 2 * tc, q0 + 2 * tc);
-        l[fw] = (T)hdb_clip((p0 + q0 + q1 + q2 + 2) >> 2, q1 - 2 * tc, q1 + 2 * tc);
-        l[2 * fw] = (T)hdb_clip((p0 + q0 + q1 + 3 * q2 + 2 * q3 + 4) >> 3, q2 - 2 * tc, q2 + 2 * tc);
-      }
+    if (!keep_p) {
+      q[-fw] = (T)hdb_clip((p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3, p0 - 2 * tc, p0 + 2 * tc);
+      q[-2 * fw] = (T)hdb_clip((p2 + p1 + p0 + q0 + 2) >> 2, p1 - 2 * tc, p1 + 2 * tc);
+      q[-3 * fw] = (T)hdb_clip((2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3, p2 - 2 * tc, p2 + 2 * tc);
+    }
+    if (!keep_q) {
+      q[0] = (T)hdb_clip((p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3, q0 - 2 * tc, q0 + 2 * tc);
+      q[fw] = (T)hdb_clip((p0 + q0 + q1 + q2 + 2) >> 2, q1 - 2 * tc, q1 + 2 * tc);
+      q[2 * fw] = (T)hdb_clip((p0 + q0 + q1 + 3 * q2 + 2 * q3 + 4) >> 3, q2 - 2 * tc, q2 + 2 * tc);
     }
     return;
   }
-  const bool touch_p1 = dp < ((beta + (beta >> 1)) >> 3), touch_q1 = dq < ((beta + (beta >> 1)) >> 3);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int p0 = P(0, i), p1 = P(1, i), p2 = P(2, i);
-    const int q0 = Q(0, i), q1 = Q(1, i), q2 = Q(2, i);
-    int delta = (9 * (q0 - p0) - 3 * (q1 - p1) + 8) >> 4;
-    if (abs(delta) >= tc * 10) continue;
-    delta = hdb_clip(delta, -tc, tc);
-    T* l = q + i * gl;
-    if (!keep_p) l[-fw] = (T)hdb_clip(p0 + delta, 0, maxv);
-    if (!keep_q) l[0] = (T)hdb_clip(q0 - delta, 0, maxv);
-    if (touch_p1 && !keep_p) {
-      const int d1 = hdb_clip((((p2 + p0 + 1) >> 1) - p1 + delta) >> 1, -(tc >> 1), tc >> 1);
-      l[-2 * fw] = (T)hdb_clip(p1 + d1, 0, maxv);
-    }
-    if (touch_q1 && !keep_q) {
-      const int d1 = hdb_clip((((q2 + q0 + 1) >> 1) - q1 - delta) >> 1, -(tc >> 1), tc >> 1);
-      l[fw] = (T)hdb_clip(q1 + d1, 0, maxv);
-    }
+  int delta = (9 * (q0 - p0) - 3 * (q1 - p1) + 8) >> 4;
+  if (abs(delta) >= tc * 10) return;
+  delta = hdb_clip(delta, -tc, tc);
+  const int side = (beta + (beta >> 1)) >> 3;
+  if (!keep_p) {
+    q[-fw] = (T)hdb_clip(p0 + delta, 0, maxv);
+    if (dp0 + dp3 < side)
+      q[-2 * fw] = (T)hdb_clip(p1 + hdb_clip((((p2 + p0 + 1) >> 1) - p1 + delta) >> 1, -(tc >> 1), tc >> 1), 0, maxv);
+  }
+  if (!keep_q) {
+    q[0] = (T)hdb_clip(q0 - delta, 0, maxv);
+    if (dq0 + dq3 < side)
+      q[fw] = (T)hdb_clip(q1 + hdb_clip((((q2 + q0 + 1) >> 1) - q1 - delta) >> 1, -(tc >> 1), tc >> 1), 0, maxv);
   }
 }
 
-// One 4-line chroma segment (clause 8.7.2.5.5; hevc_filter_template.c:149-162).
+// One line of a chroma segment (clause 8.7.2.5.5; hevc_filter_template.c
+// :149-162): no decision, so nothing crosses lanes.
 template <typename T>
-__device__ void hdb_chroma(T* q, int fw, int gl, int tc, bool keep_p, bool keep_q, int maxv) {
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    T* l = q + i * gl;
-    const int p1 = l[-2 * fw], p0 = l[-fw], q0 = l[0], q1 = l[fw];
-    const int delta = hdb_clip((((q0 - p0) * 4) + p1 - q1 + 4) >> 3, -tc, tc);
-    if (!keep_p) l[-fw] = (T)hdb_clip(p0 + delta, 0, maxv);
-    if (!keep_q) l[0] = (T)hdb_clip(q0 - delta, 0, maxv);
-  }
+__device__ __forceinline__ void hdb_chroma_line(T* q, int fw, int tc, bool keep_p, bool keep_q, int maxv) {
+  const int p1 = q[-2 * fw], p0 = q[-fw], q0 = q[0], q1 = q[fw];
+  const int delta = hdb_clip((((q0 - p0) * 4) + p1 - q1 + 4) >> 3, -tc, tc);
+  if (!keep_p) q[-fw] = (T)hdb_clip(p0 + delta, 0, maxv);
+  if (!keep_q) q[0] = (T)hdb_clip(q0 - delta, 0, maxv);
 }
 
 // tC of one chroma plane, hevc_filter_template.c:176-181 and :322-329.
@@ -222,68 +224,82 @@ __device__ __forceinline__ int hdb_tc_chroma(const b200enc_hevc_deblock_t& p, co
   return (int)kHdbTc[hdb_clip(qpc + 2 + ed.tc_offset, 0, 53)] << (p.bit_depth_chroma - 8);
 }
 
-// Vertical edges: thread = (4-row segment, 8x8 cell column); chroma with the
-// first segment of a cell on the 16-sample grid (hevc_filter_template.c
-// :298-335).
+// Vertical edges: four lanes per (4-row segment, 8x8 cell column), one per
+// row; chroma with the first segment of a cell on the 16-sample grid, one
+// chroma row per lane (hevc_filter_template.c:298-335).
 template <typename T>
 __global__ void __launch_bounds__(kHdbThreads) hevc_deblock_v_kernel(const b200enc_hevc_deblock_t p) {
   const int ncx = p.width >> 3, nseg = p.height >> 2;
-  const int idx = blockIdx.x * kHdbThreads + threadIdx.x;
-  if (idx >= ncx * nseg) return;
-  const int seg = idx / ncx, cx = idx - seg * ncx;
-  if (cx == 0) return;  // the picture's left border is no edge
-  const int ex = cx << 3, sy = seg << 2;
-  const int e = __ldg(p.edges + (size_t)(sy >> 3) * p.edges_stride + cx);
-  if (!(e & 1)) return;
-  const int ctb_w = (p.width + (1 << p.log2_ctb) - 1) >> p.log2_ctb;
-  const HdbEdge ed = hdb_edge(p, ex, sy & ~7, true, ctb_w);
-  if (!ed.on) return;
-  const int bs = hdb_strength(p, ex - 1, sy, ex, sy, (e & 4) != 0);
-  if (!bs) return;
+  const int g = blockIdx.x * kHdbThreads + threadIdx.x, sid = g >> 2, line = g & 3;
+  int ex = 0, sy = 0, bs = 0;
+  bool inside = false;
+  HdbEdge ed;
+  ed.on = false;
+  if (sid < ncx * nseg) {
+    const int seg = sid / ncx, cx = sid - seg * ncx;
+    ex = cx << 3;
+    sy = seg << 2;
+    inside = cx > 0;
+    const int e = inside ? __ldg(p.edges + (size_t)(sy >> 3) * p.edges_stride + cx) : 0;
+    if (inside) {
+      const int ctb_w = (p.width + (1 << p.log2_ctb) - 1) >> p.log2_ctb;
+      ed = hdb_edge(p, ex, sy & ~7, true, ctb_w);
+      const int b = hdb_strength(p, ex - 1, sy, ex, sy, (e & 4) != 0);
+      bs = ((e & 1) && ed.on) ? b : 0;
+    }
+  }
   const int maxv = (int)(sizeof(T) == 1 ? 255 : 1023);
-  const int tc = (int)kHdbTc[hdb_clip(ed.qp + 2 * (bs - 1) + ed.tc_offset, 0, 53)] << (p.bit_depth_luma - 8);
+  const int tc = bs ? (int)kHdbTc[hdb_clip(ed.qp + 2 * (bs - 1) + ed.tc_offset, 0, 53)] << (p.bit_depth_luma - 8) : 0;
   T* Y = reinterpret_cast<T*>(p.plane[0]);
-  hdb_luma<T>(Y + (size_t)sy * p.stride[0] + ex, 1, p.stride[0], ed.beta, tc, ed.keep_p, ed.keep_q, maxv);
+  hdb_luma_line<T>(Y + (size_t)(sy + line) * p.stride[0] + ex, 1, inside, bs != 0, ed.beta, tc, ed.keep_p, ed.keep_q,
+                   maxv);
   if (bs != 2 || (ex & 15) || (sy & 7)) return;
 #pragma unroll
   for (int pl = 0; pl < 2; ++pl) {
     const int tcc = hdb_tc_chroma(p, ed, pl);
     if (!tcc) continue;
     T* C = reinterpret_cast<T*>(p.plane[1 + pl]);
-    hdb_chroma<T>(C + (size_t)(sy >> 1) * p.stride[1 + pl] + (ex >> 1), 1, p.stride[1 + pl], tcc, ed.keep_p,
-                  ed.keep_q, maxv);
+    hdb_chroma_line<T>(C + (size_t)((sy >> 1) + line) * p.stride[1 + pl] + (ex >> 1), 1, tcc, ed.keep_p, ed.keep_q,
+                       maxv);
   }
 }
 
-// Horizontal edges: thread = (8x8 cell row, 4-column segment); chroma with
-// the first segment of a cell on the 16-row grid.
+// Horizontal edges: four lanes per (8x8 cell row, 4-column segment), one
+// per column; chroma with the first segment of a cell on the 16-row grid.
 template <typename T>
 __global__ void __launch_bounds__(kHdbThreads) hevc_deblock_h_kernel(const b200enc_hevc_deblock_t p) {
   const int nsx = p.width >> 2, ncy = p.height >> 3;
-  const int idx = blockIdx.x * kHdbThreads + threadIdx.x;
-  if (idx >= nsx * ncy) return;
-  const int cy = idx / nsx, s = idx - cy * nsx;
-  if (cy == 0) return;  // nor is its top border
-  const int ey = cy << 3, sx = s << 2;
-  const int e = __ldg(p.edges + (size_t)cy * p.edges_stride + (sx >> 3));
-  if (!(e & 2)) return;
-  const int ctb_w = (p.width + (1 << p.log2_ctb) - 1) >> p.log2_ctb;
-  const HdbEdge ed = hdb_edge(p, sx & ~7, ey, false, ctb_w);
-  if (!ed.on) return;
-  const int bs = hdb_strength(p, sx, ey - 1, sx, ey, (e & 8) != 0);
-  if (!bs) return;
+  const int g = blockIdx.x * kHdbThreads + threadIdx.x, sid = g >> 2, line = g & 3;
+  int ey = 0, sx = 0, bs = 0;
+  bool inside = false;
+  HdbEdge ed;
+  ed.on = false;
+  if (sid < nsx * ncy) {
+    const int cy = sid / nsx, s = sid - cy * nsx;
+    ey = cy << 3;
+    sx = s << 2;
+    inside = cy > 0;
+    const int e = inside ? __ldg(p.edges + (size_t)cy * p.edges_stride + (sx >> 3)) : 0;
+    if (inside) {
+      const int ctb_w = (p.width + (1 << p.log2_ctb) - 1) >> p.log2_ctb;
+      ed = hdb_edge(p, sx & ~7, ey, false, ctb_w);
+      const int b = hdb_strength(p, sx, ey - 1, sx, ey, (e & 8) != 0);
+      bs = ((e & 2) && ed.on) ? b : 0;
+    }
+  }
   const int maxv = (int)(sizeof(T) == 1 ? 255 : 1023);
-  const int tc = (int)kHdbTc[hdb_clip(ed.qp + 2 * (bs - 1) + ed.tc_offset, 0, 53)] << (p.bit_depth_luma - 8);
+  const int tc = bs ? (int)kHdbTc[hdb_clip(ed.qp + 2 * (bs - 1) + ed.tc_offset, 0, 53)] << (p.bit_depth_luma - 8) : 0;
   T* Y = reinterpret_cast<T*>(p.plane[0]);
-  hdb_luma<T>(Y + (size_t)ey * p.stride[0] + sx, p.stride[0], 1, ed.beta, tc, ed.keep_p, ed.keep_q, maxv);
+  hdb_luma_line<T>(Y + (size_t)ey * p.stride[0] + sx + line, p.stride[0], inside, bs != 0, ed.beta, tc, ed.keep_p,
+                   ed.keep_q, maxv);
   if (bs != 2 || (ey & 15) || (sx & 7)) return;
 #pragma unroll
   for (int pl = 0; pl < 2; ++pl) {
     const int tcc = hdb_tc_chroma(p, ed, pl);
     if (!tcc) continue;
     T* C = reinterpret_cast<T*>(p.plane[1 + pl]);
-    hdb_chroma<T>(C + (size_t)(ey >> 1) * p.stride[1 + pl] + (sx >> 1), p.stride[1 + pl], 1, tcc, ed.keep_p,
-                  ed.keep_q, maxv);
+    hdb_chroma_line<T>(C + (size_t)(ey >> 1) * p.stride[1 + pl] + (sx >> 1) + line, p.stride[1 + pl], tcc, ed.keep_p,
+                       ed.keep_q, maxv);
   }
 }
 
@@ -305,7 +321,7 @@ extern "C" int b200enc_hevc_deblock(const b200enc_hevc_deblock_t* p, void* strea
   if ((q.mvf || q.cbf) && q.min_pu_width < q.width / 4) return -1;
   if (((uintptr_t)q.mvf & 3) || ((uintptr_t)q.slice_filter & 3)) return -1;
   if (q.slice_filter && q.n_slice_filter <= 0) return -1;
-  const int nv = (q.width >> 3) * (q.height >> 2), nh = (q.width >> 2) * (q.height >> 3);
+  const int nv = 4 * (q.width >> 3) * (q.height >> 2), nh = 4 * (q.width >> 2) * (q.height >> 3);  // lanes
   const cudaStream_t st = (cudaStream_t)stream;
   if (q.bit_depth_luma == 8) {
     hevc_deblock_v_kernel<uint8_t><<<(nv + kHdbThreads - 1) / kHdbThreads, kHdbThreads, 0, st>>>(q);
