@@ -436,6 +436,62 @@ def run_gpu(args):
         pg.destroy_process_group()
 
 
+def run_hevc_deblock(args):
+    """HEVC deblocking (b200enc_hevc_deblock) on seeded synthetic pictures:
+    1080p 8-bit and 2160p 10-bit, enough resident copies to exceed L2, timed
+    with CUDA events over `steps` passes; the reference decoder's filter
+    (oracle/_ref/libhevcfilt.so) timed on the host threads beside it. Prints
+    one JSON line per picture format."""
+    import numpy as np
+    import torch
+    import b200enc
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import hevc_db_inputs as hdi
+    hbm_peak, peak_kind = measured_peaks()
+    fmts = (("1080p_8bit", dict(seed=11, width=1920, height=1080, bit_depth=8, log2_ctb=6, log2_min_cb=3), 48),
+            ("2160p_10bit", dict(seed=16, width=3840, height=2160, bit_depth=10, log2_ctb=6, log2_min_cb=3, slices=4),
+             12))
+    dev = lambda a: None if a is None else torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).reshape(-1).copy()).cuda()
+    for name, kw, npic in fmts:
+        case = hdi.make_case(**kw)
+        maps = {k: dev(case[k]) for k in ("edges", "mvf", "cbf", "qp_y", "no_filter", "slice_of_ctb", "tile_of_ctb")}
+        sfd = dev(case["slice_filter"])
+        pics = [[dev(p) for p in case["planes"]] for _ in range(npic)]
+        qs = []
+        for pl in pics:
+            q = hdi.params(b200enc, dict(case, **maps), lambda t: t.data_ptr(), planes=pl, slice_filter=None)
+            q.slice_filter, q.n_slice_filter = sfd.data_ptr(), len(case["slice_filter"])
+            qs.append(q)
+        for q in qs[:args.warmup]:
+            b200enc.hevc_deblock(q)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(args.steps):
+            b200enc.hevc_deblock(qs[k % npic])
+        e1.record()
+        torch.cuda.synchronize()
+        us = e0.elapsed_time(e1) * 1e3 / args.steps
+        bps = 1 if kw["bit_depth"] == 8 else 2
+        traffic = 4 * kw["width"] * kw["height"] * 1.5 * bps   # two passes, each reads and writes the picture
+        line = {"metric": "HEVC deblocking pictures/s", "workload": name, "value": round(1e6 / us, 1),
+                "unit": "pictures/s", "us_per_picture": round(us, 2), "steps": args.steps, "warmup": args.warmup,
+                "launches_per_picture": 2, "resident_pictures": npic,
+                "roofline": {"bound": "hbm", "achieved": round(traffic / (us * 1e-6) / 1e9, 1),
+                             "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
+                             "frac": round(traffic / (us * 1e-6) / 1e9 / hbm_peak, 4),
+                             "traffic_model_bytes": traffic}}
+        if not args.no_cpu_baseline and os.path.exists(hdi.FILT_SO):
+            t0, n = time.perf_counter(), 0
+            while time.perf_counter() - t0 < 3.0:
+                hdi.reference(b200enc, case)
+                n += 1
+            ms = (time.perf_counter() - t0) / n * 1e3
+            line["cpu_baseline"] = {"value": round(1e3 / ms, 1), "unit": "pictures/s", "cores": os.cpu_count(),
+                                    "kind": "reference", "sample": f"{n} pictures through hevcd_loop_filters"}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -445,10 +501,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--streams", type=int, default=8)
     ap.add_argument("--conf", type=float, default=0.9)
+    ap.add_argument("--hevc-deblock", action="store_true",
+                    help="time b200enc_hevc_deblock instead of the H.264 encode (own JSON lines)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.hevc_deblock:
+        run_hevc_deblock(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)
