@@ -296,7 +296,7 @@ __global__ void deblock_kernel(int mbw, int mbh, int R, int qp, int is_intra,
           s_abort = 1;
           break;
         }
-        __nanosleep(32);
+        __nanosleep(128);  // off the rows' critical path: poll gently
       }
     } else if (warp >= 2 * R) {
       // ---- IO warp: luma (2R) or chroma (2R+1) -------------------------------
@@ -376,7 +376,7 @@ __global__ void deblock_kernel(int mbw, int mbh, int R, int qp, int is_intra,
           s_abort = 1;
           break;
         }
-        __nanosleep(32);
+        __nanosleep(128);
       }
     } else if (wr < rows) {
       const uint8_t* bsrow = bsm + (size_t)wr * mbw * 32;

@@ -2,7 +2,7 @@
 // persistent kernel on the tcgen05 tensor cores, with the candidate
 // selection fused into its last epilogue.
 //
-// One CTA per SM (192 KB of shared memory), 16 warps, looping over tiles of
+// One CTA per SM (168 KB of shared memory), 16 warps, looping over tiles of
 // 16 MBs. The BF16 weights of all six layers are staged once per CTA as
 // UMMA B operands. Per tile every layer is a handful of M=128 MMAs into
 // TMEM, issued by one thread and committed to an mbarrier; the epilogue
@@ -42,8 +42,7 @@ struct NetSmem {
   // activations as A operands (canonical, 128-row tiles)
   alignas(128) uint16_t x0[8][128 * 16];  // also a4 [128 x 128] once c1 has consumed it
   alignas(128) uint16_t a2[2][128 * 128];  // also hd [128 x 64] once c2 has consumed it
-  alignas(128) uint16_t a3[128 * 128];
-  alignas(128) uint16_t f[128 * 96];
+  alignas(128) uint16_t a3[128 * 128];  // also f [128 x 96] once c3 has consumed it
   float b1[32], b2[32], b3[32], b4[32], bf1[64], bf2[16];
   uint64_t bar;
   uint32_t tmem;
@@ -130,12 +129,13 @@ __global__ void __launch_bounds__(kNetThreads, 1) lp_net_kernel(int mbs, LpBuf b
   uint32_t phase = 0;
   constexpr uint64_t kWaitNs = 2000000000ull;
 
-  const uint32_t a_x0 = smem_u32(s.x0), a_a2 = smem_u32(s.a2), a_a3 = smem_u32(s.a3), a_f = smem_u32(s.f);
+  const uint32_t a_x0 = smem_u32(s.x0), a_a2 = smem_u32(s.a2), a_a3 = smem_u32(s.a3);
   const uint32_t a_w1 = smem_u32(s.w1), a_w2 = smem_u32(s.w2), a_w3 = smem_u32(s.w3), a_w4 = smem_u32(s.w4);
   const uint32_t a_wf1 = smem_u32(s.wf1), a_wf2 = smem_u32(s.wf2);
   uint16_t* a4 = &s.x0[0][0];
   uint16_t* hd = &s.a2[0][0];
-  const uint32_t a_a4 = a_x0, a_hd = a_a2;
+  uint16_t* fin = s.a3;  // fc1 input: c4 outputs (columns 0..31) + side features (32..95)
+  const uint32_t a_a4 = a_x0, a_hd = a_a2, a_f = a_a3;
 
   // one layer: issue, commit, wait (all threads); false if the wait gave up
   auto sync_mma = [&]() -> bool {
@@ -184,7 +184,8 @@ __global__ void __launch_bounds__(kNetThreads, 1) lp_net_kernel(int mbs, LpBuf b
       *reinterpret_cast<uint4*>(t + canon_off(R & 127, 0, 128)) = pre_x[i];
       *reinterpret_cast<uint4*>(t + canon_off(R & 127, 8, 128)) = make_uint4(0, 0, 0, 0);
     }
-    if (tid < 128) *reinterpret_cast<uint4*>(s.f + canon_off(tid >> 3, 32 + (tid & 7) * 8, 128)) = pre_f;
+    // the side features wait in registers until c3 has freed a3
+    const uint4 cur_f = pre_f;
     if (tile + (int)gridDim.x < ntiles) prefetch(tile + gridDim.x);
     fence_async_smem();
     tc_fence_before();
@@ -255,12 +256,13 @@ __global__ void __launch_bounds__(kNetThreads, 1) lp_net_kernel(int mbs, LpBuf b
       umma_commit(&s.bar);
     }
     if (!sync_mma()) break;
+    if (tid < 128) *reinterpret_cast<uint4*>(fin + canon_off(tid >> 3, 32 + (tid & 7) * 8, 128)) = cur_f;
     if (quad == 0 && wq < 2) {  // rows 0..15, two halves of the 32 channels
       uint32_t v[16];
       tmem_row16(tmem, 0, 16 * wq, v);
       if (lane < 16) {
-        store8_relu(s.f + canon_off(lane, 16 * wq, 128), &v[0], s.b4 + 16 * wq);
-        store8_relu(s.f + canon_off(lane, 16 * wq + 8, 128), &v[8], s.b4 + 16 * wq + 8);
+        store8_relu(fin + canon_off(lane, 16 * wq, 128), &v[0], s.b4 + 16 * wq);
+        store8_relu(fin + canon_off(lane, 16 * wq + 8, 128), &v[8], s.b4 + 16 * wq + 8);
       }
     }
     publish();
