@@ -470,7 +470,7 @@ class Context:
     def stream(self):
         return self.L.b200enc_ctx_stream(ctypes.byref(self.ctx))
 
-    ME_PLAIN, ME_LEARNED, ME_CANDIDATES = 0, 1, 2
+    ME_PLAIN, ME_LEARNED, ME_CANDIDATES, ME_LEARNED_FP8 = 0, 1, 2, 3
 
     def set_me(self, mode, weights=None, conf=0.9):
         """Motion estimation form of P frames (plain / learned / candidates)."""

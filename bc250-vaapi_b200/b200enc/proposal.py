@@ -179,12 +179,12 @@ class Proposal:
         from . import _stream
         self._ck(self._lib.b200enc_proposal_train_step(self.h, mbs, lr, step, _stream(stream)), "train_step")
 
-    NETWORK, CANDIDATES = 1, 2
+    NETWORK, CANDIDATES, NETWORK_FP8 = 1, 2, 3
 
     def me(self, cur, ref, W, H, RW, RH, prev_mv, rng, lam, zero_thresh, param, mv_out, mode=1, stream=None):
         """Learned-form ME of one frame: mode NETWORK (param = confidence
-        threshold) or CANDIDATES (no network; param = fallback cost per pel,
-        < 0 never)."""
+        threshold), NETWORK_FP8 (the same with FP8 inference) or CANDIDATES
+        (no network; param = fallback cost per pel, < 0 never)."""
         from . import _p, _stream
         self._ck(self._lib.b200enc_proposal_me(self.h, cur.yp(), cur.pitch, ref.yp(), ref.pitch, W, H, RW, RH,
                                                _p(prev_mv) if prev_mv is not None else None, rng, lam, zero_thresh,

@@ -66,7 +66,7 @@ struct Impl {
   // parameters
   int range = 16, lambda = -1, zero_thresh = 512, clamp_coded = 1, deblock = -1;
   int intra_flags = B200ENC_INTRA_CORNER_CHECK;
-  // learned proposal (me_mode 1: network, 2: candidates only)
+  // learned proposal (me_mode 1: network, 2: candidates only, 3: network in FP8)
   int me_mode = 0;
   float conf = 0.9f;
   std::string weights;
@@ -381,6 +381,7 @@ int bc250_gpu_init(bc250_gpu_context_t* ctx) {
   const char* me = getenv("B200ENC_ME");
   if (me && strcmp(me, "learned") == 0) m->me_mode = 1;
   if (me && strcmp(me, "candidates") == 0) m->me_mode = 2;
+  if (me && strcmp(me, "learned_fp8") == 0) m->me_mode = 3;
   const char* wp = getenv("B200ENC_PROPOSAL_WEIGHTS");
   if (wp && *wp) m->weights = wp;
   const char* cf = getenv("B200ENC_PROPOSAL_CONF");
@@ -695,7 +696,7 @@ int b200enc_ctx_configure(gpu_context_t* ctx, int search_range, int lambda, int 
 
 int b200enc_ctx_set_me(gpu_context_t* ctx, int mode, const char* weights, float conf) {
   Impl* m = impl_of(ctx);
-  if (!m || mode < 0 || mode > 2) return -1;
+  if (!m || mode < 0 || mode > 3) return -1;
   cudaStreamSynchronize(m->stream);
   m->me_mode = mode;
   m->weights = weights ? weights : "";
@@ -706,7 +707,7 @@ int b200enc_ctx_set_me(gpu_context_t* ctx, int mode, const char* weights, float 
     m->prop_mbs = 0;
   }
   if (mode != 0 && m->mbw > 0) return ensure_proposal(m);
-  if (mode == 1 && m->mbw == 0) {  // check the checkpoint now, before the first frame
+  if ((mode == 1 || mode == 3) && m->mbw == 0) {  // check the checkpoint now, before the first frame
     void* probe = b200enc_proposal_create(1);
     if (!probe) return -1;
     const int rc = b200enc_proposal_load(probe, (m->weights.empty() ? default_weights() : m->weights).c_str());

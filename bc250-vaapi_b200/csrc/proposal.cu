@@ -731,7 +731,7 @@ int b200enc_proposal_me(void* h, const uint8_t* cur_y, int cur_pitch, const uint
                         int H, int RW, int RH, const void* prev_mv, int range, int lambda, int zero_thresh, int mode,
                         float param, void* mv_out, void* stream) {
   Proposal* P = static_cast<Proposal*>(h);
-  if (!P || !mv_out || (mode != 1 && mode != 2)) return -1;
+  if (!P || !mv_out || (mode < 1 || mode > 3)) return -1;
   if (!prev_mv)  // no motion history: the plain search
     return b200enc_me_full_search(cur_y, cur_pitch, ref_y, ref_pitch, W, H, RW, RH, range, lambda, zero_thresh,
                                   mv_out, stream);
@@ -745,6 +745,8 @@ int b200enc_proposal_me(void* h, const uint8_t* cur_y, int cur_pitch, const uint
   cudaStream_t st = (cudaStream_t)stream;
   if (mode == 1) {
     if (lp_net_launch(mbs, P->b, P->wb, P->params, param, lambda, (MV*)mv_out, P->err, st) != 0) return -1;
+  } else if (mode == 3) {
+    if (lp_net8_launch(mbs, P->b, P->params, param, lambda, (MV*)mv_out, P->err, st) != 0) return -1;
   } else {
     lp_select_kernel<<<(mbs + 127) / 128, 128, 0, st>>>(mbs, P->b, mode, param, lambda, (MV*)mv_out);
   }

@@ -119,5 +119,9 @@ __device__ __forceinline__ void lp_select_one(int mb, int mbs, const LpBuf& b, i
 // every MB into b.logits, selection as lp_select_one(mode 1, conf).
 int lp_net_launch(int mbs, const LpBuf& b, const __nv_bfloat16* wb, const float* params, float conf, int lambda,
                   MV* mv_out, uint32_t* err, cudaStream_t st);
+// The same in FP8 E4M3 (proposal_infer8.cu), weights quantised from the FP32
+// master parameters in each CTA.
+int lp_net8_launch(int mbs, const LpBuf& b, const float* params, float conf, int lambda, MV* mv_out, uint32_t* err,
+                   cudaStream_t st);
 
 }  // namespace b200enc

@@ -67,11 +67,6 @@ __device__ __forceinline__ void store8_relu(uint16_t* dst, const uint32_t* acc, 
   *reinterpret_cast<uint4*>(dst) = v;
 }
 
-// 16 channels of TMEM row (lane) 32*quad + lane, columns col .. col+15.
-__device__ __forceinline__ void tmem_row16(uint32_t tmem, int quad, int col, uint32_t (&v)[16]) {
-  tmem_ld16(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)col, v);
-  tmem_wait_ld();
-}
 
 // Writes channels ch0 .. ch0+15 of conv output row R into the next layer's
 // operand tile set `dst` (128-row tiles of K=128): row R/4, K offset

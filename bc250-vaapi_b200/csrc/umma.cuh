@@ -1,7 +1,7 @@
 // umma.cuh - tcgen05 (5th-generation tensor core) building blocks for sm_100a:
 // shared-memory matrix descriptors in the canonical K-major no-swizzle layout,
-// the kind::f16 instruction descriptor, MMA issue/commit, bounded mbarrier
-// waits and TMEM loads.
+// the kind::f16 (BF16) and kind::f8f6f4 (E4M3) instruction descriptors, MMA
+// issue/commit, bounded mbarrier waits and TMEM loads.
 //
 // Canonical K-major no-swizzle layout of an operand tile of `rows` rows
 // (rows a multiple of 8): core matrices of 8 rows x 16 bytes (8 BF16), rows
@@ -59,6 +59,38 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t
       : "memory");
 }
 
+// The same layout for 8-bit operands (FP8 E4M3): a core matrix row is 16
+// bytes = 16 elements, so K chunks are 16 elements wide:
+//   element (r, k) at byte ((k/16) * rows/8 + r/8) * 128 + (r%8) * 16 + k%16.
+__host__ __device__ constexpr int canon_off8(int r, int k, int rows) {
+  return ((k >> 4) * (rows >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (k & 15);
+}
+
+// Descriptor of the 32-wide K step (one kind::f8f6f4 MMA) starting at
+// element k0 (a multiple of 16) of an 8-bit canonical tile.
+__device__ __forceinline__ uint64_t canon_desc8(uint32_t base, int rows, int k0) {
+  return umma_desc(base + (uint32_t)((k0 >> 4) * (rows >> 3) * 128), (uint32_t)rows * 16u, 128u);
+}
+
+// Instruction descriptor of kind::f8f6f4: D F32, A and B E4M3 (format 0),
+// both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_e4m3(int M, int N) {
+  return (1u << 4)                        // c_format F32
+         | (0u << 7)                      // a_format E4M3
+         | (0u << 10)                     // b_format E4M3
+         | ((uint32_t)(N >> 3) << 17)     // n_dim
+         | ((uint32_t)(M >> 4) << 24);    // m_dim
+}
+
+__device__ __forceinline__ void umma_f8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
@@ -95,6 +127,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// 16 accumulator columns of TMEM lane 32*quad + lane (a warp reads its own
+// lane quadrant), columns col .. col+15; waits for the load.
+__device__ __forceinline__ void tmem_row16(uint32_t tmem, int quad, int col, uint32_t (&v)[16]) {
+  tmem_ld16(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)col, v);
+  tmem_wait_ld();
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }

@@ -329,11 +329,13 @@ def run_gpu(args):
     K, Wm = args.steps, args.warmup
     ms_l, launches, _, clk = arm(1, S, K, Wm, clocks=True)
     ms_p, _, _, _ = arm(0, S, K, Wm)
+    ms_8, _, _, _ = arm(3, S, K, Wm)  # the learned form with the network's inference in FP8
     k1 = max(K, 2 * GOP)
     ms_l1, _, perf_l1, _ = arm(1, 1, k1, Wm, perf=True)
     ms_p1, _, perf_p1, _ = arm(0, 1, k1, Wm, perf=True)
     fps = ws * S * K / (ms_l / 1000.0)
     fps_plain = ws * S * K / (ms_p / 1000.0)
+    fps_fp8 = ws * S * K / (ms_8 / 1000.0)
     me_counts = ctxs[0].me_stats()
 
     # ---- e2e through the reference boundary, host buffers -----------------
@@ -402,6 +404,10 @@ def run_gpu(args):
                        "parallelism": f"replicas x{ws} (independent streams per GPU)"},
             "plain": {"value": round(fps_plain, 2), "unit": "frames/s", "ms_per_step": round(ms_p / K, 4)},
             "speedup_vs_plain": round(fps / fps_plain, 3),
+            "learned_fp8": {"value": round(fps_fp8, 2), "unit": "frames/s", "ms_per_step": round(ms_8 / K, 4),
+                            "speedup_vs_plain": round(fps_fp8 / fps_plain, 3),
+                            "note": "network inference in FP8 E4M3 (b200enc_ctx_set_me mode 3); BD-rate "
+                                    "recorded for the BF16 form"},
             "host_issue_ms_per_step": {"learned": round(host_ms[1, S], 4), "plain": round(host_ms[0, S], 4),
                                        "note": "host time to enqueue one step (all streams); compare ms_per_step"},
             "single_stream": {"learned_fps": round(k1 / (ms_l1 / 1000.0), 2),

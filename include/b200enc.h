@@ -215,7 +215,10 @@ int b200enc_proposal_train_step(void *h, int mbs, float lr, int step, void *stre
  * candidates and MBs whose top-4 probability is under `param` fall back to
  * the full search. mode 2, the baseline the network is measured against:
  * the 4 distinct candidates of lowest exact cost, falling back when that
- * cost exceeds param * 256 (param < 0: never). */
+ * cost exceeds param * 256 (param < 0: never). mode 3: mode 1 with the
+ * network run in FP8 E4M3 on the tensor cores (per-channel weight scales,
+ * per-tile activation scales; the BF16-trained parameters are quantised on
+ * the fly). */
 int b200enc_proposal_me(void *h, const uint8_t *cur_y, int cur_pitch, const uint8_t *ref_y, int ref_pitch,
                         int W, int H, int RW, int RH, const void *prev_mv, int range, int lambda,
                         int zero_thresh, int mode, float param, void *mv_out, void *stream);

@@ -195,9 +195,10 @@ int b200enc_ctx_encode_device(gpu_context_t *ctx, const uint8_t *y, const uint8_
  * checkpoint `weights` (NULL: the packaged proposal_h264.b2pn next to the
  * library's b200enc package) and confidence threshold conf, 2 = the same
  * candidate search without the network, falling back when the best
- * candidate's cost per pel exceeds conf (conf < 0: never). The first P frame
+ * candidate's cost per pel exceeds conf (conf < 0: never), 3 = mode 1 with
+ * the network's inference in FP8 E4M3. The first P frame
  * after an I frame, and any P frame without a previous MV field, uses the
- * full search. Env: B200ENC_ME=learned|candidates, B200ENC_PROPOSAL_WEIGHTS,
+ * full search. Env: B200ENC_ME=learned|candidates|learned_fp8, B200ENC_PROPOSAL_WEIGHTS,
  * B200ENC_PROPOSAL_CONF. Returns -2 if the checkpoint is missing or bad. */
 int b200enc_ctx_set_me(gpu_context_t *ctx, int mode, const char *weights, float conf);
 /* Learned-form counters of the last P frame: MBs re-scored from the network's

@@ -74,6 +74,82 @@ def forward(params, x0, side, exact=False):
     return logits, acts
 
 
+FP8_MAX = np.float32(448.0)
+NET8_TILE = 16
+
+
+def e4m3(x):
+    """Round float32 values to FP8 E4M3 (the 'fn' variant: largest finite
+    448, no infinities), nearest with ties to even, saturating at +-448;
+    returns float32. torch's float8_e4m3fn conversion does the rounding."""
+    import torch
+    t = torch.from_numpy(np.clip(np.ascontiguousarray(x, np.float32), -FP8_MAX, FP8_MAX))
+    return t.to(torch.float8_e4m3fn).to(torch.float32).numpy()
+
+
+def _e4m3_scale(amax):
+    """(multiplier that quantises, multiplier that undoes it) of a maximum."""
+    amax = np.float32(amax)
+    if amax > 0:
+        return np.float32(FP8_MAX / amax), np.float32(amax / FP8_MAX)
+    return np.float32(1.0), np.float32(1.0)
+
+
+def quantize_weights_fp8(params):
+    """Per-output-channel E4M3 weights of every layer: [(W8, s_w, b)], W8
+    holding the E4M3 values as float32 (csrc/proposal_infer8.cu stage_w8)."""
+    out = []
+    for W, b in unpack(np.asarray(params, np.float32)):
+        W = W.astype(np.float32)
+        amax = np.abs(W).max(axis=1).astype(np.float32)
+        safe = np.where(amax > 0, amax, np.float32(1)).astype(np.float32)
+        inv = np.where(amax > 0, FP8_MAX / safe, np.float32(1)).astype(np.float32)
+        sw = np.where(amax > 0, safe / FP8_MAX, np.float32(1)).astype(np.float32)
+        out.append((e4m3(W * inv[:, None]), sw, b.astype(np.float32)))
+    return out
+
+
+def _fma32(acc, sc, b):
+    """float32(acc * sc + b) with one rounding (fmaf), via float64."""
+    return (acc.astype(np.float64) * sc.astype(np.float64) + b.astype(np.float64)).astype(np.float32)
+
+
+def forward_fp8(params, x0, side):
+    """The FP8 inference form (csrc/proposal_infer8.cu): per 16-MB tile, the
+    network input, each hidden output after bias and ReLU, and the fc1 input
+    (c4 output with the side features) are quantised to E4M3 with one scale
+    per tile (amax / 448); weights with one scale per output channel; E4M3
+    products accumulate in FP32 (here FP64, then rounded); each epilogue is
+    fma(acc, s_in * s_w, b). A last partial tile is padded with zero MBs, as
+    the kernel does. Returns logits [B][16] (float32)."""
+    Q = quantize_weights_fp8(params)
+    B = side.shape[0]
+    T = NET8_TILE
+    logits = np.zeros((B, N_OUT), np.float32)
+    for t0 in range(0, B, T):
+        n = min(T, B - t0)
+        x = np.zeros((T * 64, 8), np.float32)
+        x[:n * 64] = x0[t0 * 64:(t0 + n) * 64]
+        sd = np.zeros((T, 64), np.float32)
+        sd[:n] = side[t0:t0 + n]
+        inv, s = _e4m3_scale(np.abs(x).max())
+        a8 = e4m3(x * inv)
+        for l in range(5):
+            W8, sw, b = Q[l]
+            acc = (a8.astype(np.float64) @ W8.astype(np.float64).T).astype(np.float32)
+            y = np.maximum(_fma32(acc, (s * sw).astype(np.float32), b), np.float32(0))
+            if l < 3:
+                y = y.reshape(-1, 128)
+            elif l == 3:
+                y = np.concatenate([y, sd], axis=1)
+            inv, s = _e4m3_scale(np.abs(y).max())
+            a8 = e4m3(y * inv)
+        W8, sw, b = Q[5]
+        acc = (a8.astype(np.float64) @ W8.astype(np.float64).T).astype(np.float32)
+        logits[t0:t0 + n] = _fma32(acc, (s * sw).astype(np.float32), b)[:n]
+    return logits
+
+
 def _masked_softmax(z, dup):
     valid = np.ones_like(z[:, :N_CLASSES], bool)
     valid[:, :N_CAND] = ((dup[:, None] >> np.arange(N_CAND)[None, :]) & 1) == 0

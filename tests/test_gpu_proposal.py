@@ -210,7 +210,7 @@ def test_training_reduces_loss(gpu):
     assert hist[-1] < 0.6 * hist[0], hist[::10]
 
 
-def _learned_case(gpu, seed, conf, params_seed):
+def _learned_case(gpu, seed, conf, params_seed, mode=1):
     import torch
     from b200enc import proposal as pp
     W, H, R, lam = 320, 192, 32, 5
@@ -224,7 +224,7 @@ def _learned_case(gpu, seed, conf, params_seed):
     gpu.me_full_search_ex(nv[2], nv[1], W, H, CW, CH, R, lam, 512, full, flags=gpu.ME_LOG_INTEGER)
     P = pp.Proposal(mbs, _random_params(params_seed))
     out = torch.full((mbs, 4), -7, dtype=torch.int32, device="cuda")
-    P.me(nv[2], nv[1], W, H, CW, CH, prev, R, lam, 512, conf, out, mode=pp.Proposal.NETWORK)
+    P.me(nv[2], nv[1], W, H, CW, CH, prev, R, lam, 512, conf, out, mode=mode)
     torch.cuda.synchronize()
     return P, mbs, out.cpu().numpy(), full.cpu().numpy(), fr, (W, H, CW, CH, R, lam)
 
@@ -236,11 +236,14 @@ def test_learned_me_all_fallback_equals_full_search(gpu):
     np.testing.assert_array_equal(got[:, :3], full[:, :3])
 
 
-@pytest.mark.parametrize("seed,params_seed,conf", [(22, 2, 0.0), (23, 5, 0.0), (24, 6, 0.6)])
-def test_learned_me_rescoring_exact(gpu, oracle_mod, seed, params_seed, conf):
+@pytest.mark.parametrize("seed,params_seed,conf,mode", [(22, 2, 0.0, 1), (23, 5, 0.0, 1), (24, 6, 0.6, 1),
+                                                         (25, 2, 0.0, 3), (26, 6, 0.6, 3)])
+def test_learned_me_rescoring_exact(gpu, oracle_mod, seed, params_seed, conf, mode):
+    """mode 1: BF16 inference; mode 3: FP8 inference. Whatever the network
+    selects, the re-scoring and fallbacks are exact."""
     import torch
     from b200enc import proposal as pp
-    P, mbs, got, full, fr, (W, H, CW, CH, R, lam) = _learned_case(gpu, seed, conf, params_seed)
+    P, mbs, got, full, fr, (W, H, CW, CH, R, lam) = _learned_case(gpu, seed, conf, params_seed, mode)
     state = P.tensor(pp.T_STATE, torch.int32, (mbs,)).cpu().numpy().view(np.uint32)
     sel = P.tensor(pp.T_SEL, torch.int32, (mbs,)).cpu().numpy().view(np.uint32)
     cand = _decode_cand(P.tensor(pp.T_CAND, torch.int32, (mbs, 10)).cpu().numpy())
@@ -312,3 +315,54 @@ def test_fused_network_matches_layer_by_layer(gpu, W, H, seed):
     live = (state & 3) == 0  # the fused kernel computes every MB; early-outs are selected without logits
     assert live.sum() > 0
     np.testing.assert_array_equal(fused, layered)
+
+
+@pytest.mark.parametrize("W,H,seed,packaged", [(320, 192, 41, False), (200, 120, 42, True), (1920, 1080, 43, True)])
+def test_fp8_network_matches_oracle(gpu, W, H, seed, packaged):
+    """The FP8 inference kernel (E4M3 operands, per-channel weight scales,
+    per-16-MB-tile activation scales, FP32 accumulation) against the
+    oracle's forward_fp8 on the GPU's own network inputs. Tolerance: an
+    activation that sits on an E4M3 rounding boundary may round the other
+    way when the FP32 accumulation order differs, and that one step then
+    moves the MB's logits visibly; so the typical logit must agree to
+    1e-4 of the logit spread (median), at most 2 % of MBs may differ by
+    more than 2 % of the spread, and the top-1 class must agree on >= 98 %
+    of MBs. Covers a partial last tile (200x120: 104 MBs) and the packaged
+    parameters (whose logits span ~30-50; on the CPU oracle their FP8 top-1
+    agrees with BF16's on 98-99 % of MBs). Also: on the GPU the FP8 top-1
+    class agrees with the BF16 network's on >= 90 % of live MBs."""
+    import torch
+    from b200enc import proposal as pp
+    CW, CH = gpu.coded(W, H)
+    mbs = (CW // 16) * (CH // 16)
+    fr = _frames(W, H, 3, seed)
+    nv = [gpu.NV12.from_host(y, uv) for y, uv in fr]
+    prev = torch.zeros((mbs, 4), dtype=torch.int32, device="cuda")
+    gpu.me_full_search_ex(nv[1], nv[0], W, H, CW, CH, 32, 5, 512, prev)
+    P = pp.Proposal(mbs)
+    if packaged and os.path.exists(pp.DEFAULT_WEIGHTS):
+        P.load(pp.DEFAULT_WEIGHTS)
+    else:
+        P.set_params(_random_params(11))
+    out = torch.zeros((mbs, 4), dtype=torch.int32, device="cuda")
+    P.me(nv[2], nv[1], W, H, CW, CH, prev, 32, 5, 512, 0.9, out, mode=pp.Proposal.NETWORK_FP8)
+    torch.cuda.synchronize()
+    assert int(P.tensor(pp.T_ERR, torch.int32, (1,)).cpu()[0]) == 0
+    got = P.tensor(pp.T_LOGITS, torch.float32, (mbs, 16)).cpu().numpy().copy()
+    state = P.tensor(pp.T_STATE, torch.int32, (mbs,)).cpu().numpy().view(np.uint32)
+    x0 = P.tensor(pp.T_X0, pp._BF16, (mbs * 64, 8)).float().cpu().numpy()
+    side = P.tensor(pp.T_F, pp._BF16, (mbs, 96)).float().cpu().numpy()[:, 32:]
+    want = pr.forward_fp8(P.get_params(), x0, side)
+    live = (state & 3) == 0  # early-outs are selected without logits
+    assert live.sum() > 0
+    d = np.abs(got[live] - want[live])
+    spread = float(np.abs(want[live]).max())
+    far = (d.max(axis=1) > 0.02 * spread).mean()
+    top1 = (got[live, :11].argmax(1) == want[live, :11].argmax(1)).mean()
+    assert np.median(d) <= 1e-4 * spread + 1e-6 and far <= 0.02 and top1 >= 0.98, \
+        (float(np.median(d)), float(d.max()), spread, float(far), float(top1))
+    P.me(nv[2], nv[1], W, H, CW, CH, prev, 32, 5, 512, 0.9, out, mode=pp.Proposal.NETWORK)
+    torch.cuda.synchronize()
+    bf = P.tensor(pp.T_LOGITS, torch.float32, (mbs, 16)).cpu().numpy()
+    agree = (bf[live, :11].argmax(1) == got[live, :11].argmax(1)).mean()
+    assert agree >= 0.9, agree

@@ -133,3 +133,23 @@ def test_prepare_oracle_candidates_and_features():
     assert d["cand_sad"][4, 0] == 0
     dn = pr.prepare(cur, ref, W, H, W, H, None, 16, 512)
     assert (dn["state"] & 2).all() and (dn["side"][:, 63] == 1).all()
+
+
+def test_fp8_oracle_rounding_and_closeness():
+    """E4M3 known answers (nearest-even, saturation at 448, subnormals down to
+    2^-9) and the FP8 forward against the BF16 forward on random
+    parameters: same top-1 class on >= 95 % of MBs, logits within 10 % of
+    their spread."""
+    v = np.array([0.5, 448.0, 500.0, -1000.0, 0.3, 1e-4, 0.0017578125, 17.0, 19.0], np.float32)
+    np.testing.assert_array_equal(pr.e4m3(v), np.array([0.5, 448, 448, -448, 0.3125, 0, 2.0 ** -9, 16, 20],
+                                                       np.float32))
+    rs = np.random.default_rng(3)
+    p = (rs.standard_normal(sum(i * o + o for i, o in pr.LAYERS)) * 0.1).astype(np.float32)
+    B = 40  # 3 tiles, the last one partial
+    x0 = rs.standard_normal((B * 64, 8)).astype(np.float32)
+    side = (rs.standard_normal((B, 64)) * 0.5).astype(np.float32)
+    lb, _ = pr.forward(p, x0, side)
+    l8 = pr.forward_fp8(p, x0, side)
+    spread = np.abs(lb).max()
+    assert np.abs(lb - l8).max() <= 0.1 * spread
+    assert (lb[:, :11].argmax(1) == l8[:, :11].argmax(1)).mean() >= 0.95
