@@ -115,6 +115,62 @@ __device__ __forceinline__ void lp_select_one(int mb, int mbs, const LpBuf& b, i
   }
 }
 
+// lp_select_one in mode 1 for the MBs mb0 .. mb0+nmb-1 of a network tile,
+// lane i taking MB mb0+i (nmb <= 32), called by all 32 lanes of a warp.
+// `st` is the lane's MB state word (read ahead by the caller). The same
+// selection; the list appends are aggregated to one atomic per list per
+// warp (the order inside a list is not meaningful).
+__device__ __forceinline__ void lp_select_warp(int mb0, int nmb, int mbs, const LpBuf& b, float param,
+                                               const float* logits, uint32_t st, MV* __restrict__ mv_out) {
+  const int lane = threadIdx.x & 31;
+  const bool act = lane < nmb;
+  const int mb = mb0 + lane;
+  const bool early = act && (st & kStEarly);
+  bool fall = false;
+  if (act && !early) {
+    uint32_t sel = 0xffffffffu;
+    if (st & kStNoHist) {
+      fall = true;
+    } else {
+      const uint32_t dup = (st >> 8) & 0x3ffu;
+      float p[kClasses];
+      masked_softmax(logits, dup, p);
+      b.p_norez[mb] = 1.f / (1.f + expf(-logits[11]));
+      uint32_t chosen = dup;
+      float conf = 0.f;
+      for (int k = 0; k < 4; ++k) {
+        int best = -1;
+        for (int c = 0; c < kCand; ++c)
+          if (!((chosen >> c) & 1u) && (best < 0 || p[c] > p[best])) best = c;
+        if (best < 0) break;
+        chosen |= 1u << best;
+        conf += p[best];
+        sel = (sel & ~(0xffu << (8 * k))) | ((uint32_t)best << (8 * k));
+      }
+      fall = conf < param;
+    }
+    b.sel[mb] = sel;
+  }
+  if (early) {
+    mv_out[mb] = MV{0, 0, b.cand_sad[mb * kCand + 9], 0u};
+    b.sel[mb] = 0xffffffffu;
+  }
+  const bool learn = act && !early && !fall;
+  const uint32_t m_early = __ballot_sync(0xffffffffu, early), m_fall = __ballot_sync(0xffffffffu, fall),
+                 m_learn = __ballot_sync(0xffffffffu, learn);
+  int base_f = 0, base_l = 0;
+  if (lane == 0) {
+    if (m_early) atomicAdd(&b.counters[3], __popc(m_early));
+    if (m_fall) base_f = atomicAdd(&b.counters[1], __popc(m_fall));
+    if (m_learn) base_l = atomicAdd(&b.counters[0], __popc(m_learn));
+  }
+  base_f = __shfl_sync(0xffffffffu, base_f, 0);
+  base_l = __shfl_sync(0xffffffffu, base_l, 0);
+  const uint32_t below = (1u << lane) - 1u;
+  if (fall) b.lists[mbs + base_f + __popc(m_fall & below)] = mb;
+  if (learn) b.lists[base_l + __popc(m_learn & below)] = mb;
+}
+
 // The fused inference network + selection (proposal_infer.cu): logits of
 // every MB into b.logits, selection as lp_select_one(mode 1, conf).
 int lp_net_launch(int mbs, const LpBuf& b, const __nv_bfloat16* wb, const float* params, float conf, int lambda,

@@ -153,6 +153,7 @@ __global__ void __launch_bounds__(kNetThreads, 1) lp_net_kernel(int mbs, LpBuf b
   // chunks of side features (threads 0..127).
   constexpr int kRowsPerThread = kNetTileMbs * 64 / kNetThreads;
   uint4 pre_x[kRowsPerThread], pre_f = make_uint4(0, 0, 0, 0);
+  uint32_t pre_st = 0u;  // warp 0: the MB state words the selection reads
   auto prefetch = [&](int tile) {
     const int mb0 = tile * kNetTileMbs, nmb = min(kNetTileMbs, mbs - mb0);
 #pragma unroll
@@ -161,6 +162,7 @@ __global__ void __launch_bounds__(kNetThreads, 1) lp_net_kernel(int mbs, LpBuf b
       pre_x[i] = (R >> 6) < nmb ? *reinterpret_cast<const uint4*>(b.x0 + ((size_t)mb0 * 64 + R) * 8)
                                 : make_uint4(0, 0, 0, 0);
     }
+    if (warp == 0) pre_st = lane < nmb ? b.state[mb0 + lane] : 0u;
     if (tid < 128) {
       const int m = tid >> 3, c8 = tid & 7;
       pre_f = m < nmb ? *reinterpret_cast<const uint4*>(b.f + (size_t)(mb0 + m) * kFIn + 32 + c8 * 8)
@@ -171,6 +173,7 @@ __global__ void __launch_bounds__(kNetThreads, 1) lp_net_kernel(int mbs, LpBuf b
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int mb0 = tile * kNetTileMbs;
     const int nmb = min(kNetTileMbs, mbs - mb0);
+    const uint32_t cur_st = pre_st;
     // ---- inputs: network rows (both K chunks) and side features ---------
 #pragma unroll
     for (int i = 0; i < kRowsPerThread; ++i) {
@@ -296,16 +299,15 @@ __global__ void __launch_bounds__(kNetThreads, 1) lp_net_kernel(int mbs, LpBuf b
       uint32_t v[16];
       tmem_ld16(tmem, v);
       tmem_wait_ld();
-      if (lane < nmb) {
-        const int mb = mb0 + lane;
-        float z[kOut];
+      float z[kOut];
 #pragma unroll
-        for (int j = 0; j < kOut; ++j) z[j] = __uint_as_float(v[j]) + s.bf2[j];
-        float4* lo = reinterpret_cast<float4*>(b.logits + (size_t)mb * kOut);
+      for (int j = 0; j < kOut; ++j) z[j] = __uint_as_float(v[j]) + s.bf2[j];
+      if (lane < nmb) {
+        float4* lo = reinterpret_cast<float4*>(b.logits + (size_t)(mb0 + lane) * kOut);
 #pragma unroll
         for (int j = 0; j < 4; ++j) lo[j] = make_float4(z[4 * j], z[4 * j + 1], z[4 * j + 2], z[4 * j + 3]);
-        lp_select_one(mb, mbs, b, 1, param, lambda, z, mv_out);
       }
+      lp_select_warp(mb0, nmb, mbs, b, param, z, cur_st, mv_out);
     }
     publish();
   }
