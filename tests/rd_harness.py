@@ -16,7 +16,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ENC_SO = os.path.join(ROOT, "oracle", "_ref", "libh264enc_b200.so")
 
-PLAIN, LEARNED, CANDIDATES = 0, 1, 2
+PLAIN, LEARNED, CANDIDATES, LEARNED_FP8 = 0, 1, 2, 3
 
 
 def available():
