@@ -420,6 +420,8 @@ struct Proposal {
   int max_mbs = 0;
   float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
   __nv_bfloat16* wb = nullptr;
+  uint8_t* w8 = nullptr;  // FP8 weights + scales (lp_net8_launch), rebuilt when w8_stale
+  bool w8_stale = true;
   LpBuf b{};
   uint32_t* err = nullptr;
   // the fallback full search runs on a side stream, concurrently with the
@@ -453,7 +455,7 @@ struct Proposal {
     max_mbs = mbs;
     const size_t B = (size_t)mbs;
     return alloc(&params, kParams) && alloc(&grads, kParams) && alloc(&adam_m, kParams) && alloc(&adam_v, kParams) &&
-           alloc(&wb, kParams) && alloc(&b.x0, B * 64 * 8) && alloc(&b.y1, B * 64 * 32) && alloc(&b.y2, B * 16 * 32) &&
+           alloc(&wb, kParams) && alloc(&w8, kNet8PackBytes) && alloc(&b.x0, B * 64 * 8) && alloc(&b.y1, B * 64 * 32) && alloc(&b.y2, B * 16 * 32) &&
            alloc(&b.y3, B * 4 * 32) && alloc(&b.f, B * kFIn) && alloc(&b.h, B * 64) && alloc(&b.logits, B * kOut) &&
            alloc(&b.cand, B * kCand) && alloc(&b.cand_sad, B * kCand) && alloc(&b.state, B) && alloc(&b.sel, B) &&
            alloc(&b.p_norez, B) && alloc(&b.lists, 2 * B) && alloc(&b.counters, 8) && alloc(&err, 1) &&
@@ -633,6 +635,7 @@ int b200enc_proposal_set_params(void* h, const float* host_params, int n) {
   Proposal* P = static_cast<Proposal*>(h);
   if (!P || !host_params || n != kParams) return -1;
   if (cudaMemcpy(P->params, host_params, kParams * 4, cudaMemcpyHostToDevice) != cudaSuccess) return -1;
+  P->w8_stale = true;
   lp_to_bf16_kernel<<<(kParams + 255) / 256, 256>>>(kParams, P->params, P->wb);
   return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1;
 }
@@ -716,6 +719,7 @@ int b200enc_proposal_adam(void* h, float lr, float beta1, float beta2, float eps
   if (!P || step < 1) return -1;
   const double c1 = 1.0 - std::pow((double)beta1, step), c2 = 1.0 - std::pow((double)beta2, step);
   const float lr_t = (float)(lr * std::sqrt(c2) / c1);
+  P->w8_stale = true;
   lp_adam_kernel<<<(kParams + 255) / 256, 256, 0, (cudaStream_t)stream>>>(kParams, P->params, P->grads, P->adam_m,
                                                                          P->adam_v, P->wb, lr_t, beta1, beta2, eps);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
@@ -746,7 +750,8 @@ int b200enc_proposal_me(void* h, const uint8_t* cur_y, int cur_pitch, const uint
   if (mode == 1) {
     if (lp_net_launch(mbs, P->b, P->wb, P->params, param, lambda, (MV*)mv_out, P->err, st) != 0) return -1;
   } else if (mode == 3) {
-    if (lp_net8_launch(mbs, P->b, P->params, param, lambda, (MV*)mv_out, P->err, st) != 0) return -1;
+    if (lp_net8_launch(mbs, P->b, P->params, P->w8, &P->w8_stale, param, lambda, (MV*)mv_out, P->err, st) != 0)
+      return -1;
   } else {
     lp_select_kernel<<<(mbs + 127) / 128, 128, 0, st>>>(mbs, P->b, mode, param, lambda, (MV*)mv_out);
   }

@@ -175,9 +175,11 @@ __device__ __forceinline__ void lp_select_warp(int mb0, int nmb, int mbs, const 
 // every MB into b.logits, selection as lp_select_one(mode 1, conf).
 int lp_net_launch(int mbs, const LpBuf& b, const __nv_bfloat16* wb, const float* params, float conf, int lambda,
                   MV* mv_out, uint32_t* err, cudaStream_t st);
-// The same in FP8 E4M3 (proposal_infer8.cu), weights quantised from the FP32
-// master parameters in each CTA.
-int lp_net8_launch(int mbs, const LpBuf& b, const float* params, float conf, int lambda, MV* mv_out, uint32_t* err,
-                   cudaStream_t st);
+// The same in FP8 E4M3 (proposal_infer8.cu). `w8` (kNet8PackBytes) holds the
+// E4M3 weights and their scales, quantised from the FP32 master parameters
+// on `st` first when *stale (then cleared).
+constexpr int kNet8PackBytes = 20480 + 6 * 64 * 4;
+int lp_net8_launch(int mbs, const LpBuf& b, const float* params, uint8_t* w8, bool* stale, float conf, int lambda,
+                   MV* mv_out, uint32_t* err, cudaStream_t st);
 
 }  // namespace b200enc

@@ -7,8 +7,9 @@
 // Quantisation (the CPU oracle, oracle/proposal_ref.py forward_fp8, follows
 // the same arithmetic step for step):
 //   * weights: one scale per output channel, s_w = amax_k |W[n][k]| / 448,
-//     W8 = E4M3(W * (448 / amax)), from the FP32 master parameters, in each
-//     CTA's prologue (so a parameter update needs no cached copy);
+//     W8 = E4M3(W * (448 / amax)), from the FP32 master parameters, by a
+//     one-CTA pass whenever they have changed (the runtime marks the pack
+//     stale on set_params and on each Adam step); each CTA copies the pack;
 //   * activations: one scale per 16-MB tile and layer input, s = amax / 448
 //     over the tile, A8 = E4M3(A * (448 / amax)) - the network input, each
 //     hidden layer's output after bias and ReLU, and the fc1 input (the c4
@@ -20,12 +21,15 @@
 // Shape of the work as in proposal_infer.cu (Morton conv rows, 2x2 stride-2
 // convs as plain GEMMs), with 8-bit operands: one MMA consumes K = 32, the
 // canonical layout's core-matrix rows hold 16 elements, and the operand
-// tiles take half the shared memory (~100 KB per CTA instead of 168 KB).
+// tiles take half the shared memory (~105 KB per CTA instead of 168 KB), so
+// two CTAs share an SM.
 // Each hidden epilogue makes two passes over TMEM: the first finds the
 // tile's maximum (warp max, one shared atomic per warp), a barrier
 // publishes it, the second quantises and stores - so no thread holds its
 // values across the barrier.
 #include <cuda_fp8.h>
+
+#include <cstddef>
 
 #include "me_common.cuh"
 #include "proposal.cuh"
@@ -34,7 +38,11 @@
 namespace b200enc {
 
 constexpr int kNet8TileMbs = 16;
-constexpr int kNet8Threads = 512;
+// 8 warps (two per TMEM lane quadrant) and ~105 KB of shared memory: two
+// CTAs fit on an SM (registers, shared memory and TMEM's 512 columns), so
+// one CTA's epilogues run while the other waits on its MMAs.
+constexpr int kNet8Threads = 256;
+constexpr int kNet8Wpq = kNet8Threads / 128;  // warps per TMEM lane quadrant
 
 struct Net8Smem {
   // weights as B operands (8-bit canonical, rows = N)
@@ -121,24 +129,49 @@ __device__ __forceinline__ float max16(const float (&y)[16]) {
   return m;
 }
 
+// The weight pack in global memory: the six E4M3 tiles in Net8Smem's order
+// (w1 .. wf2, contiguous) and the per-channel scales.
+struct W8Pack {
+  uint8_t w[20480];
+  float sw[6][64];
+};
+static_assert(sizeof(W8Pack) == kNet8PackBytes, "weight pack");
+static_assert(offsetof(Net8Smem, w2) == 1024 && offsetof(Net8Smem, w3) == 5120 && offsetof(Net8Smem, w4) == 9216 &&
+                  offsetof(Net8Smem, wf1) == 13312 && offsetof(Net8Smem, wf2) == 19456 &&
+                  offsetof(Net8Smem, x0) == 20480,
+              "the weight tiles are contiguous at the start of Net8Smem");
+
+// Quantises the FP32 parameters into the pack (one CTA; once per parameter
+// change).
+__global__ void __launch_bounds__(kNet8Threads) lp_quant8_kernel(const float* __restrict__ params, uint8_t* w8) {
+  W8Pack& pk = *reinterpret_cast<W8Pack*>(w8);
+  stage_w8(params + layer_woff(0), 32, 8, 32, pk.w + 0, pk.sw[0]);
+  stage_w8(params + layer_woff(1), 32, 128, 128, pk.w + 1024, pk.sw[1]);
+  stage_w8(params + layer_woff(2), 32, 128, 128, pk.w + 5120, pk.sw[2]);
+  stage_w8(params + layer_woff(3), 32, 128, 128, pk.w + 9216, pk.sw[3]);
+  stage_w8(params + layer_woff(4), 64, 96, 96, pk.w + 13312, pk.sw[4]);
+  stage_w8(params + layer_woff(5), 16, 64, 64, pk.w + 19456, pk.sw[5]);
+}
+
 __device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
 __device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
 
-__global__ void __launch_bounds__(kNet8Threads, 1) lp_net8_kernel(int mbs, LpBuf b, const float* __restrict__ params,
-                                                         float param, int lambda, MV* __restrict__ mv_out,
-                                                         uint32_t* __restrict__ err) {
+__global__ void __launch_bounds__(kNet8Threads, 2) lp_net8_kernel(int mbs, LpBuf b, const float* __restrict__ params,
+                                                         const uint8_t* __restrict__ w8, float param, int lambda,
+                                                         MV* __restrict__ mv_out, uint32_t* __restrict__ err) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
   Net8Smem& s = *reinterpret_cast<Net8Smem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int quad = warp & 3, wq = warp >> 2;  // TMEM lane quadrant, warp index within it (0..3)
+  const int quad = warp & 3, wq = warp >> 2;  // TMEM lane quadrant, warp index within it
 
-  // ---- E4M3 weights with per-channel scales, biases, once per CTA ---------
-  stage_w8(params + layer_woff(0), 32, 8, 32, s.w1, s.sw[0]);
-  stage_w8(params + layer_woff(1), 32, 128, 128, s.w2, s.sw[1]);
-  stage_w8(params + layer_woff(2), 32, 128, 128, s.w3, s.sw[2]);
-  stage_w8(params + layer_woff(3), 32, 128, 128, s.w4, s.sw[3]);
-  stage_w8(params + layer_woff(4), 64, 96, 96, s.wf1, s.sw[4]);
-  stage_w8(params + layer_woff(5), 16, 64, 64, s.wf2, s.sw[5]);
+  // ---- E4M3 weights with per-channel scales (the pack), biases, once per CTA
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(w8);
+    uint4* dst = reinterpret_cast<uint4*>(s.w1);
+    for (int i = tid; i < 20480 / 16; i += kNet8Threads) dst[i] = src[i];
+    const float* sws = reinterpret_cast<const W8Pack*>(w8)->sw[0];
+    for (int i = tid; i < 6 * 64; i += kNet8Threads) (&s.sw[0][0])[i] = sws[i];
+  }
   if (tid < 32) {
     s.b1[tid] = params[layer_boff(0) + tid];
     s.b2[tid] = params[layer_boff(1) + tid];
@@ -262,7 +295,7 @@ __global__ void __launch_bounds__(kNet8Threads, 1) lp_net8_kernel(int mbs, LpBuf
     if (!sync_mma()) break;
     {  // pass 1: the tile's maximum (8 tiles x 2 channel halves per quadrant, 4 warps each)
       float m = 0.f;
-      for (int job = wq; job < 16; job += 4) {
+      for (int job = wq; job < 16; job += kNet8Wpq) {
         const int t = job >> 1, h = job & 1;
         uint32_t v[16];
         float y[16];
@@ -275,7 +308,7 @@ __global__ void __launch_bounds__(kNet8Threads, 1) lp_net8_kernel(int mbs, LpBuf
     __syncthreads();
     float inv1, s1;
     scale_of(1, inv1, s1);
-    for (int job = wq; job < 16; job += 4) {  // pass 2: E4M3 conv rows -> a2 (row R/4, K (R%4)*32 + ch)
+    for (int job = wq; job < 16; job += kNet8Wpq) {  // pass 2: E4M3 conv rows -> a2 (row R/4, K (R%4)*32 + ch)
       const int t = job >> 1, h = job & 1;
       uint32_t v[16];
       float y[16];
@@ -297,18 +330,23 @@ __global__ void __launch_bounds__(kNet8Threads, 1) lp_net8_kernel(int mbs, LpBuf
       umma_commit(&s.bar);
     }
     if (!sync_mma()) break;
-    const int t2 = wq >> 1, h2 = wq & 1;  // one (tile, half) job per warp
-    {
-      uint32_t v[16];
-      float y[16];
-      tmem_row16(tmem, quad, 32 * t2 + 16 * h2, v);
-      epi16(v, s1, s.sw[1] + 16 * h2, s.b2 + 16 * h2, y);
-      warp_amax(&s.amax[2], max16(y));
+    {  // 2 tiles x 2 halves per quadrant
+      float m = 0.f;
+      for (int job = wq; job < 4; job += kNet8Wpq) {
+        const int t2 = job >> 1, h2 = job & 1;
+        uint32_t v[16];
+        float y[16];
+        tmem_row16(tmem, quad, 32 * t2 + 16 * h2, v);
+        epi16(v, s1, s.sw[1] + 16 * h2, s.b2 + 16 * h2, y);
+        m = fmaxf(m, max16(y));
+      }
+      warp_amax(&s.amax[2], m);
     }
     __syncthreads();
     float inv2, s2;
     scale_of(2, inv2, s2);
-    {
+    for (int job = wq; job < 4; job += kNet8Wpq) {
+      const int t2 = job >> 1, h2 = job & 1;
       uint32_t v[16];
       float y[16];
       tmem_row16(tmem, quad, 32 * t2 + 16 * h2, v);
@@ -413,23 +451,28 @@ __global__ void __launch_bounds__(kNet8Threads, 1) lp_net8_kernel(int mbs, LpBuf
       umma_commit(&s.bar);
     }
     if (!sync_mma()) break;
-    if (quad == 0) {  // rows 0..15, 64 channels: 16 per warp of quadrant 0
-      uint32_t v[16];
-      float y[16];
-      tmem_row16(tmem, 0, 16 * wq, v);
-      epi16(v, s4, s.sw[4] + 16 * wq, s.bf1 + 16 * wq, y);
-      warp_amax(&s.amax[5], lane < 16 ? max16(y) : 0.f);
+    if (quad == 0) {  // rows 0..15, 64 channels in blocks of 16 over quadrant 0's warps
+      float m = 0.f;
+      for (int blk = wq; blk < 4; blk += kNet8Wpq) {
+        uint32_t v[16];
+        float y[16];
+        tmem_row16(tmem, 0, 16 * blk, v);
+        epi16(v, s4, s.sw[4] + 16 * blk, s.bf1 + 16 * blk, y);
+        if (lane < 16) m = fmaxf(m, max16(y));
+      }
+      warp_amax(&s.amax[5], m);
     }
     __syncthreads();
     float inv5, s5;
     scale_of(5, inv5, s5);
-    if (quad == 0) {
-      uint32_t v[16];
-      float y[16];
-      tmem_row16(tmem, 0, 16 * wq, v);
-      epi16(v, s4, s.sw[4] + 16 * wq, s.bf1 + 16 * wq, y);
-      if (lane < 16) store16_e4m3(hd + canon_off8(lane, 16 * wq, 128), y, inv5);
-    }
+    if (quad == 0)
+      for (int blk = wq; blk < 4; blk += kNet8Wpq) {
+        uint32_t v[16];
+        float y[16];
+        tmem_row16(tmem, 0, 16 * blk, v);
+        epi16(v, s4, s.sw[4] + 16 * blk, s.bf1 + 16 * blk, y);
+        if (lane < 16) store16_e4m3(hd + canon_off8(lane, 16 * blk, 128), y, inv5);
+      }
     publish();
 
     // ---- fc2 (K 64, N 16) -> logits -> selection ------------------------------
@@ -465,8 +508,13 @@ __global__ void __launch_bounds__(kNet8Threads, 1) lp_net8_kernel(int mbs, LpBuf
   if (warp == 0) tmem_dealloc(tmem, 256);
 }
 
-int lp_net8_launch(int mbs, const LpBuf& b, const float* params, float conf, int lambda, MV* mv_out, uint32_t* err,
-                   cudaStream_t st) {
+int lp_net8_launch(int mbs, const LpBuf& b, const float* params, uint8_t* w8, bool* stale, float conf, int lambda,
+                   MV* mv_out, uint32_t* err, cudaStream_t st) {
+  if (*stale) {
+    lp_quant8_kernel<<<1, kNet8Threads, 0, st>>>(params, w8);
+    if (cudaGetLastError() != cudaSuccess) return -1;
+    *stale = false;
+  }
   static_assert(sizeof(Net8Smem) <= 227 * 1024, "FP8 network exceeds shared memory");
   const int smem = (int)sizeof(Net8Smem);
   if (cudaFuncSetAttribute(lp_net8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
@@ -475,7 +523,8 @@ int lp_net8_launch(int mbs, const LpBuf& b, const float* params, float conf, int
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int ntiles = (mbs + kNet8TileMbs - 1) / kNet8TileMbs;
-  lp_net8_kernel<<<std::min(ntiles, sms), kNet8Threads, smem, st>>>(mbs, b, params, conf, lambda, mv_out, err);
+  lp_net8_kernel<<<std::min(ntiles, 2 * sms), kNet8Threads, smem, st>>>(mbs, b, params, w8, conf, lambda, mv_out,
+                                                                       err);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
