@@ -89,7 +89,8 @@ __global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restric
   __syncthreads();
 
   // exact SAD at each candidate: one (candidate, row) per task, 4 byte-SIMD
-  // words off 5 aligned (clamped) loads of the reference row
+  // words off 5 aligned (clamped) loads of the reference row; a candidate's
+  // 16 row tasks are one aligned half-warp, summed by shuffles
   for (int task = tid; task < kCand * 16; task += 64) {
     const int c = task >> 4, r = task & 15;
     const int x0 = X + scx[c], xa = x0 & ~3, shft = (x0 - xa) * 8;
@@ -104,7 +105,9 @@ __global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restric
       sad = sad4_acc(rv, scw[r * 4 + i], sad);
       if (c == 0) rfw[r * 4 + i] = rv;
     }
-    atomicAdd(&ssad[c], sad);
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) sad += __shfl_xor_sync(0xffffffffu, sad, o);
+    if (r == 0) ssad[c] = sad;
   }
   // block gradients: sum |horizontal| and |vertical| neighbour differences
   {
