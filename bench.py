@@ -24,7 +24,8 @@ every P frame. Both are timed in the same run, and again with one stream
   e2e    the learned form through the reference boundary (per stream
          gpu_compute_upload_nv12 from pinned host memory,
          begin/dispatch/end_picture; then sync_slot and a host read of the
-         staged outputs), S streams.
+         staged outputs), S streams, double-buffered over the boundary's two
+         staging slots (step k+1 is submitted before step k is read back).
   bd_rate the learned form's BD-rate against the plain form (bits from the
          reference's host encoder, CABAC, QP 22/27/32/37, 60 1080p frames),
          measured on a B200 with tests/rd_report.py and recorded in
@@ -365,7 +366,11 @@ def run_gpu(args):
     for c in ctxs:
         c.set_me(LEARNED, conf=args.conf)
 
-    def e2e_step(k):
+    # Double-buffered, as the boundary's two staging slots allow: step k+1 is
+    # uploaded and submitted before step k's staged results are read, so each
+    # stream's copies overlap its (and the other streams') compute. Every
+    # step's upload and result read lie inside the timed region.
+    def e2e_submit(k):
         slots = []
         for s, c in enumerate(ctxs):
             py, puv = pinned[s][k % NP]
@@ -375,22 +380,31 @@ def run_gpu(args):
                                              b200enc.ctypes.c_void_p(puv.data_ptr()), W, W, H)
             assert rc == 0
             slots.append(c.encode(img, W, H, QP, (k % GOP) == 0, 1, 0, None))
+        return slots
+
+    def e2e_collect(slots):
         acc = 0
         for c, slot in zip(ctxs, slots):
             assert c.sync(slot) == 0
             acc += int(c.staging(slot)["nz"][0, 0])  # a host read of each step's result
         return acc
 
-    k = 0
-    for _ in range(Wm):
-        e2e_step(k)
-        k += 1
+    def e2e_run(k, n):
+        pending = None
+        for _ in range(n):
+            cur = e2e_submit(k)
+            if pending is not None:
+                e2e_collect(pending)
+            pending = cur
+            k += 1
+        e2e_collect(pending)
+        return k
+
+    k = e2e_run(0, Wm)
     barrier()
     s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s0.record(control)
-    for _ in range(K):
-        e2e_step(k)
-        k += 1
+    k = e2e_run(k, K)
     s1.record(control)
     barrier()
     e2e_fps = ws * S * K / (max_over_ranks(s0.elapsed_time(s1)) / 1000.0)
