@@ -202,8 +202,11 @@ def run_reference(args):
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 / fps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
             "data": "synthetic (seeded generator, 1080p NV12)", "impl": "reference",
-            "config": {"workload": WORKLOAD, "width": W, "height": H, "qp": QP, "search_range": RANGE,
-                       "gop": GOP, "deblock": True},
+            "config": {"workload": f"{WORKLOAD}_x{args.streams}_streams", "streams_per_gpu": args.streams,
+                       "width": W, "height": H, "qp": QP, "search_range": RANGE, "lambda": LAMBDA, "gop": GOP,
+                       "deblock": True, "recon_clamp": "coded",
+                       "parallelism": "the host's threads on one stream's frames at a time (frames/s does not "
+                                      "depend on how many streams share the host)"},
             "cpu_baseline": {"value": round(fps, 4), "unit": "frames/s", "cores": info["cores"],
                              "kind": info["kind"], "sample": info["sample"]},
             "e2e": {"value": round(fps, 4), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
