@@ -8,13 +8,17 @@
 // edges then horizontal per macroblock, luma and chroma, bS 0-4 with the
 // strong filter.
 //
-// Raster order matters only between macroblocks whose sample footprints
-// overlap: (x-1,y), (x-1,y-1), (x,y-1) and (x+1,y-1) before (x,y). So rows
-// run as a wavefront with a 2-macroblock skew. Luma and chroma never share a
-// sample, so they are two independent wavefronts.
+// Raster order matters only between filtering steps whose sample footprints
+// overlap. The vertical edges of (x,y) read and write only rows of
+// macroblock row y, which no step of row y-1 touches; they follow the
+// horizontal edges of (x-1,y). The horizontal edges of (x,y) read and change
+// the bottom rows of (x,y-1), final once the vertical edges of (x+1,y-1)
+// (the last step to change its right columns) are done. So rows run as a
+// wavefront with a skew of one macroblock step. Luma and chroma never share
+// a sample, so they are two independent wavefronts.
 //
-// Layout for latency (the wavefront is latency-bound: ~mbw + 2*mbh
-// dependent macroblock steps per frame):
+// Layout for latency (the wavefront is latency-bound: ~mbw + mbh dependent
+// macroblock steps per frame):
 //   * a CTA owns a group of R consecutive macroblock rows (taken by ticket,
 //     so groups are only owned by running CTAs and waits cannot deadlock);
 //     R luma warps + R chroma warps, one warp per row and plane kind;
@@ -154,7 +158,10 @@ __host__ __device__ inline DbPlan db_plan(int mbw, int R) {
 
 // Bounded wait on a shared progress word: give up after max_wait_us
 // microseconds of %globaltimer, or as soon as another CTA has recorded an
-// error.
+// error. Called by all 32 lanes of a warp: each poll is one broadcast
+// shared load and the lanes stay converged. (Lane 0 spinning alone while the
+// other lanes waited at a shuffle for its result measured ~2000 cycles more
+// per wait, even when the word was already there.)
 __device__ __forceinline__ bool wait_shared(const volatile uint32_t* flag, const Scratch& sc, uint32_t need,
                                             uint32_t max_wait_us, uint32_t where) {
   const uint64_t t0 = global_ns(), budget = (uint64_t)max_wait_us * 1000u;
@@ -382,21 +389,20 @@ __global__ void deblock_kernel(int mbw, int mbh, int R, int qp, int is_intra,
       const uint8_t* bsrow = bsm + (size_t)wr * mbw * 32;
       volatile uint32_t* my_prog = prog + (is_luma ? 0 : R) + wr;
       const volatile uint32_t* up_prog = prog + (is_luma ? 0 : R) + wr - 1;
+      const volatile uint32_t* loaded_prog = prog + 2 * R + (is_luma ? 0 : 1);
       const volatile uint32_t* ready_prog = prog + 2 * R + (is_luma ? 2 : 3);
       for (int mx = 0; mx < mbw; ++mx) {
-        const uint32_t need = (uint32_t)(mx + 1);  // upper row: bottom samples of MB mx final
+        const uint32_t need = (uint32_t)(mx + 1);
         bool ok = true;
-        // The first row waits for its columns (and their halo) in the ring,
-        // every other row for the row above. Two call sites on purpose: one
-        // wait on a pointer selected between the two words measured 40%
-        // slower per macroblock over the whole row loop.
+        // Vertical edges read and write only this row's own sample rows, so
+        // they need nothing from the row above, only the columns staged in
+        // the ring: the first row waits for them; every other row is behind
+        // the row above (which waited) except at its first macroblock.
         if (wr == 0) {
-          if (lane == 0) ok = wait_shared(ready_prog, sc, need, max_wait, (uint32_t)(y * mbw + mx));
-          ok = __shfl_sync(0xffffffffu, ok, 0);
+          ok = wait_shared(loaded_prog, sc, need, max_wait, (uint32_t)(y * mbw + mx));
           __threadfence_block();
-        } else {
-          if (lane == 0) ok = wait_shared(up_prog, sc, need, max_wait, (uint32_t)(y * mbw + mx));
-          ok = __shfl_sync(0xffffffffu, ok, 0);
+        } else if (mx == 0) {
+          ok = wait_shared(loaded_prog, sc, 1u, max_wait, (uint32_t)(y * mbw));
           __threadfence_block();
         }
         if (!ok) {
@@ -444,26 +450,6 @@ __global__ void deblock_kernel(int mbw, int mbh, int R, int qp, int is_intra,
             rw[2] = o[3];
             rw[3] = o[4];
           }
-          __syncwarp();
-          if (al && be && lane < 16) {
-            // horizontal edges: this lane's sample column, rows -4..15
-            uint8_t* col = ly + (size_t)(16 * wr) * P.sp + scol(mx) + lane;
-            int v[20];
-#pragma unroll
-            for (int r = 0; r < 20; ++r) v[r] = col[(size_t)r * P.sp];
-            const int seg = lane >> 2;
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const int b = bs[16 + e * 4 + seg];
-              const int i = 4 + 4 * e;
-              if (is_intra && e == 0)
-                luma_strong(v[i - 4], v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], v[i + 3], b, al, be);
-              else
-                luma_normal(v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], b, al, be, tc0_for(b, tcl1, tcl2, tcl3));
-            }
-#pragma unroll
-            for (int r = 1; r < 19; ++r) col[(size_t)r * P.sp] = (uint8_t)v[r];
-          }
         } else {
           if (alc && bec && lane < 16) {
             // vertical edges of one chroma plane's sample row: chroma
@@ -491,7 +477,52 @@ __global__ void deblock_kernel(int mbw, int mbh, int R, int qp, int is_intra,
 #pragma unroll
             for (int k = 2; k < 10; ++k) row[2 * (k - 2)] = (uint8_t)v[k];
           }
+        }
+        __syncwarp();
+        // Macroblock mx-1's samples are final for this row now (the left
+        // edge of mx was their last change).
+        if (mx > 0) {
+          __threadfence_block();
           __syncwarp();
+          if (lane == 0) *my_prog = (uint32_t)mx;
+        }
+        // Horizontal edges of mx read and change the bottom rows of the
+        // macroblock above, which are final once the row above has filtered
+        // the vertical edges of mx+1: a skew of one macroblock step per row.
+        // The first row waits for the halo rows above the group instead.
+        if (wr == 0) {
+          ok = wait_shared(ready_prog, sc, need, max_wait, (uint32_t)(y * mbw + mx));
+          __threadfence_block();
+        } else {
+          ok = wait_shared(up_prog, sc, need, max_wait, (uint32_t)(y * mbw + mx));
+          __threadfence_block();
+        }
+        if (!ok) {
+          s_abort = 1;
+          break;
+        }
+        __syncwarp();
+        if (is_luma) {
+          if (al && be && lane < 16) {
+            // horizontal edges: this lane's sample column, rows -4..15
+            uint8_t* col = ly + (size_t)(16 * wr) * P.sp + scol(mx) + lane;
+            int v[20];
+#pragma unroll
+            for (int r = 0; r < 20; ++r) v[r] = col[(size_t)r * P.sp];
+            const int seg = lane >> 2;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int b = bs[16 + e * 4 + seg];
+              const int i = 4 + 4 * e;
+              if (is_intra && e == 0)
+                luma_strong(v[i - 4], v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], v[i + 3], b, al, be);
+              else
+                luma_normal(v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], b, al, be, tc0_for(b, tcl1, tcl2, tcl3));
+            }
+#pragma unroll
+            for (int r = 1; r < 19; ++r) col[(size_t)r * P.sp] = (uint8_t)v[r];
+          }
+        } else {
           if (alc && bec && lane < 16) {
             const int pl = lane >> 3, i = lane & 7;
             uint8_t* col = cy + (size_t)(8 * wr) * P.sp + scol(mx) + 2 * i + pl;
@@ -512,13 +543,12 @@ __global__ void deblock_kernel(int mbw, int mbh, int R, int qp, int is_intra,
             for (int r = 1; r < 9; ++r) col[(size_t)r * P.sp] = (uint8_t)v[r];
           }
         }
-        __syncwarp();
-        // Macroblock mx-1's samples are final now (mx's left edge was its
-        // last change); all of them after the last macroblock.
-        const uint32_t done = (mx == mbw - 1) ? (uint32_t)mbw : (uint32_t)mx;
-        __threadfence_block();
-        __syncwarp();
-        if (lane == 0) *my_prog = done;
+        if (mx == mbw - 1) {  // all of the row's macroblocks are final
+          __syncwarp();
+          __threadfence_block();
+          __syncwarp();
+          if (lane == 0) *my_prog = (uint32_t)mbw;
+        }
       }
     }
     __syncthreads();
