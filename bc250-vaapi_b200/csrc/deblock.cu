@@ -308,10 +308,12 @@ __global__ void deblock_kernel(int mbw, int mbh, int R, int qp, int is_intra,
     } else if (warp >= 2 * R) {
       // ---- IO warp: luma (2R) or chroma (2R+1) -------------------------------
       // Loads the group's macroblock columns into the ring ahead of its first
-      // row; once the group's last row has finished macroblock c+1 (its left
-      // edge was the last change to column c), writes column c back (the
-      // halo rows above the group, modified by the first row's top edges,
-      // included) and releases column c to the next group.
+      // row; once the group's last row has filtered the vertical edges of
+      // macroblock c+1 (the last change to column c), writes column c back
+      // (the halo rows above the group, modified by the first row's top
+      // edges, included) and releases column c to the next group. Releases
+      // come before loads, and only the rows the next group reads are
+      // written ahead of the release's fence.
       const bool io_luma = warp == 2 * R;
       const int halo = io_luma ? 4 : 2, nrows = io_luma ? 16 * rows : 8 * rows;
       uint8_t* base = io_luma ? ly : cy;
@@ -326,38 +328,52 @@ __global__ void deblock_kernel(int mbw, int mbh, int R, int qp, int is_intra,
       uint64_t t_idle = 0;
       while (evicted < mbw) {
         bool did = false;
-        while (loaded < mbw && loaded - evicted < kDbRing) {
+        // Releases first: they gate the next group. Columns [0, d) are
+        // final (one read, broadcast: the word keeps moving).
+        uint32_t d = *last_prog;
+        if ((int)d > evicted) {
+          __threadfence_block();
+          const int nc = (int)d - evicted;
+          if (has_next) {
+            // the group's last `halo` rows, which the next group reads as
+            // its halo, then the release; only these stores wait on the fence
+            for (int t = lane; t < nc * halo; t += 32) {
+              const int c = evicted + t / halo, rr = wb1 - halo + t % halo;
+              const uint32_t* s4 = reinterpret_cast<const uint32_t*>(base + (size_t)rr * P.sp + scol(c));
+              __stcg(reinterpret_cast<uint4*>(gplane + (size_t)(grow0 + rr - halo) * rec_pitch + 16 * c),
+                     make_uint4(s4[0], s4[1], s4[2], s4[3]));
+            }
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) store_release(gflag, d);
+          }
+          // the other rows (the next group writes its halo rows back itself,
+          // so they are not written again here)
+          const int wbe = has_next ? wb1 - halo : wb1;
+          for (int c = evicted; c < (int)d; ++c)
+            for (int rr = wb0 + lane; rr < wbe; rr += 32) {
+              const uint32_t* s4 = reinterpret_cast<const uint32_t*>(base + (size_t)rr * P.sp + scol(c));
+              __stcg(reinterpret_cast<uint4*>(gplane + (size_t)(grow0 + rr - halo) * rec_pitch + 16 * c),
+                     make_uint4(s4[0], s4[1], s4[2], s4[3]));
+            }
+          evicted = (int)d;
+          did = true;
+        }
+        // then at most two columns of loads before looking for releases again
+        for (int n = 0; n < 2 && loaded < mbw && loaded - evicted < kDbRing; ++n) {
           for (int r = lane; r < nrows; r += 32) {  // one 16-byte row segment per lane
             const uint4 v = __ldcg(reinterpret_cast<const uint4*>(gplane + (size_t)(grow0 + r) * rec_pitch + 16 * loaded));
-            uint32_t* d = reinterpret_cast<uint32_t*>(base + (size_t)(halo + r) * P.sp + scol(loaded));
-            d[0] = v.x;
-            d[1] = v.y;
-            d[2] = v.z;
-            d[3] = v.w;
+            uint32_t* w = reinterpret_cast<uint32_t*>(base + (size_t)(halo + r) * P.sp + scol(loaded));
+            w[0] = v.x;
+            w[1] = v.y;
+            w[2] = v.z;
+            w[3] = v.w;
           }
           ++loaded;
           did = true;
           __threadfence_block();
           __syncwarp();
           if (lane == 0) *loaded_prog = (uint32_t)loaded;
-        }
-        // columns [0, d) are final (one read, broadcast: the word keeps moving)
-        uint32_t d = 0;
-        if (lane == 0) d = *last_prog;
-        d = __shfl_sync(0xffffffffu, d, 0);
-        if ((int)d > evicted) {
-          __threadfence_block();
-          for (int c = evicted; c < (int)d; ++c)
-            for (int rr = wb0 + lane; rr < wb1; rr += 32) {
-              const uint32_t* s4 = reinterpret_cast<const uint32_t*>(base + (size_t)rr * P.sp + scol(c));
-              __stcg(reinterpret_cast<uint4*>(gplane + (size_t)(grow0 + rr - halo) * rec_pitch + 16 * c),
-                     make_uint4(s4[0], s4[1], s4[2], s4[3]));
-            }
-          if (has_next) __threadfence();
-          __syncwarp();
-          if (has_next && lane == 0) store_release(gflag, d);
-          evicted = (int)d;
-          did = true;
         }
         if (did) {
           idle = 0;
