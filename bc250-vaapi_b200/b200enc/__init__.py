@@ -156,12 +156,12 @@ class NV12:
         self.uv = self.buf[self.CH:]
 
     @classmethod
-    def from_host(cls, y, uv, device="cuda"):
+    def from_host(cls, y, uv, device="cuda", pitch=None):
         """y: [H, W] uint8, uv: [H/2, W] uint8 (numpy); pads by edge replication."""
         import numpy as np
         import torch
         H, W = y.shape
-        f = cls(W, H, device)
+        f = cls(W, H, device, pitch)
         yp = np.pad(y, ((0, f.CH - H), (0, f.pitch - W)), mode="edge")
         uvp = np.pad(uv, ((0, f.CH // 2 - H // 2), (0, f.pitch - W)), mode="edge")
         f.y.copy_(torch.from_numpy(yp))

@@ -45,6 +45,13 @@ namespace b200enc {
 // Preparation: candidates, their SADs, the network input and side features.
 // 64 threads per MB.
 // ---------------------------------------------------------------------------
+// Word i (0..7) of an 8-word register window, by selects (no local memory).
+__device__ __forceinline__ uint32_t pick8(const uint32_t (&w)[8], int i) {
+  const uint32_t lo = (i & 2) ? ((i & 1) ? w[3] : w[2]) : ((i & 1) ? w[1] : w[0]);
+  const uint32_t hi = (i & 2) ? ((i & 1) ? w[7] : w[6]) : ((i & 1) ? w[5] : w[4]);
+  return (i & 4) ? hi : lo;
+}
+
 __global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restrict__ cur, int cur_pitch,
                                                         const uint8_t* __restrict__ ref, int ref_pitch, Geo g,
                                                         const MV* __restrict__ prev, int R, int zero_thresh,
@@ -88,26 +95,52 @@ __global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restric
   }
   __syncthreads();
 
-  // exact SAD at each candidate: one (candidate, row) per task, 4 byte-SIMD
-  // words off 5 aligned (clamped) loads of the reference row; a candidate's
-  // 16 row tasks are one aligned half-warp, summed by shuffles
-  for (int task = tid; task < kCand * 16; task += 64) {
-    const int c = task >> 4, r = task & 15;
-    const int x0 = X + scx[c], xa = x0 & ~3, shft = (x0 - xa) * 8;
-    const uint8_t* rp = ref + (size_t)clampi(Y + r + scy[c], 0, g.RH - 1) * ref_pitch;
-    uint32_t w[5];
+  // exact SAD at each candidate: one warp per candidate, two lanes per
+  // reference row (lane pair h = 0, 1 scores the row's bytes 8h .. 8h+7),
+  // summed over the warp by shuffles. Where the plane's base and pitch are
+  // 16-byte aligned and the row's 32-byte aligned window lies inside the
+  // picture, each lane loads one 16-byte half of the window and the pair
+  // swaps halves: one load instruction covers 16 rows, where five word loads
+  // per row touched ~5x the L1 wavefronts. Other rows take clamped word
+  // loads (the same bytes).
+  {
+    const bool vec = ((ref_pitch & 15) == 0) && ((reinterpret_cast<uintptr_t>(ref) & 15) == 0);
+    const int r = lane >> 1, h = lane & 1;
+    for (int c = warp; c < kCand; c += 2) {
+      const int x0 = X + scx[c];
+      const uint8_t* rp = ref + (size_t)clampi(Y + r + scy[c], 0, g.RH - 1) * ref_pitch;
+      const int x16 = x0 & ~15;
+      uint32_t w0, w1, w2;  // the words at (x0 & ~3) + 8h + 0, 4, 8
+      int shft;
+      if (vec && x16 >= 0 && x16 + 32 <= g.RW) {  // warp-uniform
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(rp + x16 + 16 * h));
+        const uint32_t o0 = __shfl_xor_sync(0xffffffffu, v.x, 1), o1 = __shfl_xor_sync(0xffffffffu, v.y, 1);
+        const uint32_t o2 = __shfl_xor_sync(0xffffffffu, v.z, 1), o3 = __shfl_xor_sync(0xffffffffu, v.w, 1);
+        const uint32_t win[8] = {h ? o0 : v.x, h ? o1 : v.y, h ? o2 : v.z, h ? o3 : v.w,
+                                 h ? v.x : o0, h ? v.y : o1, h ? v.z : o2, h ? v.w : o3};
+        const int q = ((x0 - x16) >> 2) + 2 * h;  // 0..5
+        w0 = pick8(win, q);
+        w1 = pick8(win, q + 1);
+        w2 = pick8(win, q + 2);
+        shft = (x0 & 3) * 8;
+      } else {
+        const int xa = x0 & ~3;
+        w0 = load_word_clamped(rp, xa + 8 * h, g.RW);
+        w1 = load_word_clamped(rp, xa + 8 * h + 4, g.RW);
+        w2 = load_word_clamped(rp, xa + 8 * h + 8, g.RW);
+        shft = (x0 - xa) * 8;
+      }
+      const uint32_t rv0 = __funnelshift_r(w0, w1, shft), rv1 = __funnelshift_r(w1, w2, shft);
+      uint32_t sad = sad4_acc(rv0, scw[r * 4 + 2 * h], 0u);
+      sad = sad4_acc(rv1, scw[r * 4 + 2 * h + 1], sad);
+      if (c == 0) {
+        rfw[r * 4 + 2 * h] = rv0;
+        rfw[r * 4 + 2 * h + 1] = rv1;
+      }
 #pragma unroll
-    for (int i = 0; i < 5; ++i) w[i] = load_word_clamped(rp, xa + 4 * i, g.RW);
-    uint32_t sad = 0;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const uint32_t rv = __funnelshift_r(w[i], w[i + 1], shft);
-      sad = sad4_acc(rv, scw[r * 4 + i], sad);
-      if (c == 0) rfw[r * 4 + i] = rv;
+      for (int o = 16; o > 0; o >>= 1) sad += __shfl_xor_sync(0xffffffffu, sad, o);
+      if (lane == 0) ssad[c] = sad;
     }
-#pragma unroll
-    for (int o = 8; o > 0; o >>= 1) sad += __shfl_xor_sync(0xffffffffu, sad, o);
-    if (r == 0) ssad[c] = sad;
   }
   // block gradients: sum |horizontal| and |vertical| neighbour differences
   {

@@ -57,14 +57,14 @@ def _random_params(seed):
     return p
 
 
-def _prepared(gpu, W, H, R, prev_kind, coded, seed):
+def _prepared(gpu, W, H, R, prev_kind, coded, seed, pitch=None):
     import torch
     from b200enc import proposal
     (y0, uv0), (y1, uv1) = _frames(W, H, 2, seed)
     CW, CH = gpu.coded(W, H)
     RW, RH = (CW, CH) if coded else (W, H)
-    ref = gpu.NV12.from_host(y0, uv0)
-    cur = gpu.NV12.from_host(y1, uv1)
+    ref = gpu.NV12.from_host(y0, uv0, pitch=pitch)
+    cur = gpu.NV12.from_host(y1, uv1, pitch=pitch)
     mbs = (CW // 16) * (CH // 16)
     rs = np.random.Generator(np.random.PCG64(seed + 1))
     prev = None
@@ -89,10 +89,14 @@ def _prepared(gpu, W, H, R, prev_kind, coded, seed):
 @pytest.mark.parametrize("R", [16, 32])
 @pytest.mark.parametrize("prev_kind", ["random", None])
 @pytest.mark.parametrize("coded", [True, False])
-def test_prepare_bit_exact(gpu, W, H, R, prev_kind, coded):
+@pytest.mark.parametrize("pitch_pad", [None, 4])
+def test_prepare_bit_exact(gpu, W, H, R, prev_kind, coded, pitch_pad):
+    """pitch_pad 4: a plane pitch that is a multiple of 4 but not of 16 (the
+    word-load path of the candidate SADs); None: the 128-byte pitch."""
     import torch
     from b200enc import proposal as pp
-    P, want, mbs, _ = _prepared(gpu, W, H, R, prev_kind, coded, seed=W + R)
+    pitch = None if pitch_pad is None else gpu.coded(W, H)[0] + pitch_pad
+    P, want, mbs, _ = _prepared(gpu, W, H, R, prev_kind, coded, seed=W + R, pitch=pitch)
     got_cand = _decode_cand(P.tensor(pp.T_CAND, torch.int32, (mbs, 10)).cpu().numpy())
     np.testing.assert_array_equal(got_cand, want["cand"])
     np.testing.assert_array_equal(P.tensor(pp.T_CAND_SAD, torch.int32, (mbs, 10)).cpu().numpy().view(np.uint32),
