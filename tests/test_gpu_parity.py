@@ -127,6 +127,19 @@ def test_i_frame(gpu, oracle_mod, W, H, num_slices, qp, coded_clamp, corner_chec
 @pytest.mark.parametrize("qp", [15, 24, 33, 45, 51])
 @pytest.mark.parametrize("intra", [0, 1])
 def test_deblock(gpu, oracle_mod, mbw, mbh, qp, intra):
+    _deblock_case(gpu, oracle_mod, mbw, mbh, qp, intra)
+
+
+@pytest.mark.parametrize("mbw,mbh,ctas", [(120, 68, 1), (120, 68, 3), (13, 9, 1), (13, 9, 2)])
+@pytest.mark.parametrize("intra", [0, 1])
+def test_deblock_fewer_ctas_than_groups(gpu, oracle_mod, mbw, mbh, ctas, intra):
+    """CTAs that take several row groups by ticket (the ring and progress
+    words reset between groups; 13 x 9 ends on a one-row group) filter
+    exactly as one CTA per group."""
+    _deblock_case(gpu, oracle_mod, mbw, mbh, 33, intra, ctas)
+
+
+def _deblock_case(gpu, oracle_mod, mbw, mbh, qp, intra, ctas=0):
     import torch
     rs = np.random.Generator(np.random.PCG64(mbw * 1000 + mbh * 10 + qp + intra))
     CW, CH = mbw * 16, mbh * 16
@@ -138,7 +151,8 @@ def test_deblock(gpu, oracle_mod, mbw, mbh, qp, intra):
     mvh[:, :2] = rs.integers(-9, 10, (mbs, 2))
     rec = gpu.NV12.from_host(y, uv)
     scr = gpu.scratch(mbh)
-    gpu.deblock(mbw, mbh, qp, intra, torch.from_numpy(nz.view(np.int32)).cuda(), torch.from_numpy(mvh).cuda(), rec, scr)
+    gpu.deblock(mbw, mbh, qp, intra, torch.from_numpy(nz.view(np.int32)).cuda(), torch.from_numpy(mvh).cuda(), rec, scr,
+                ctas=ctas)
     assert gpu.wavefront_status(scr) == 0
     wy, wuv = y.copy(), uv.copy()
     oracle_mod.deblock(mbw, mbh, qp, intra, nz, mvh, wy, wuv)
