@@ -43,7 +43,7 @@ namespace b200enc {
 
 // ---------------------------------------------------------------------------
 // Preparation: candidates, their SADs, the network input and side features.
-// 64 threads per MB.
+// 64 threads (two warps) per MB.
 // ---------------------------------------------------------------------------
 // Word i (0..7) of an 8-word register window, by selects (no local memory).
 __device__ __forceinline__ uint32_t pick8(const uint32_t (&w)[8], int i) {
