@@ -61,10 +61,8 @@ D2H_PER_STEP = MBS * (768 + 96 + 4 + 16 + 96) + 8
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from b200enc import replicas
+    return replicas.dist_env()
 
 
 def measured_peaks():
@@ -262,19 +260,15 @@ def run_gpu(args):
     import torch
     import b200enc
 
+    from b200enc import replicas
+
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     os.environ["B200ENC_DEVICE"] = str(local)
-    pg = None
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-        pg = dist
+    group = replicas.Group("nccl", device="cuda")
 
     S = args.streams
-    host_frames = _frames_pool([rank * 1000 + s for s in range(S)], NFRAMES)
+    host_frames = _frames_pool(replicas.stream_seeds(rank, S), NFRAMES)
     dev = [[b200enc.NV12.from_host(y, uv) for (y, uv) in fr] for fr in host_frames]
     ctxs = []
     for s in range(S):
@@ -285,16 +279,10 @@ def run_gpu(args):
     control = torch.cuda.Stream()
 
     def barrier():
-        if pg:
-            pg.barrier()
-        torch.cuda.synchronize()
+        group.barrier(torch.cuda.synchronize)
 
     def max_over_ranks(ms):
-        if pg:
-            tt = torch.tensor([ms], device="cuda")
-            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-            return float(tt.item())
-        return ms
+        return group.max(ms)
 
     host_ms = {}
 
@@ -356,9 +344,9 @@ def run_gpu(args):
     ms_l1, _, perf_l1, _ = arm(LEARNED, 1, k1, Wm, perf=True)
     me_counts = ctxs[0].me_stats()  # the learned form's last P frame
     ms_p1, _, perf_p1, _ = arm(0, 1, k1, Wm, perf=True)
-    fps = ws * S * K / (ms_l / 1000.0)
-    fps_plain = ws * S * K / (ms_p / 1000.0)
-    fps_bf16 = ws * S * K / (ms_b / 1000.0)
+    fps = replicas.aggregate_rate(ws, S * K, ms_l)
+    fps_plain = replicas.aggregate_rate(ws, S * K, ms_p)
+    fps_bf16 = replicas.aggregate_rate(ws, S * K, ms_b)
 
     # ---- e2e through the reference boundary, host buffers -----------------
     NP = 30
@@ -410,7 +398,7 @@ def run_gpu(args):
     k = e2e_run(k, K)
     s1.record(control)
     barrier()
-    e2e_fps = ws * S * K / (max_over_ranks(s0.elapsed_time(s1)) / 1000.0)
+    e2e_fps = replicas.aggregate_rate(ws, S * K, max_over_ranks(s0.elapsed_time(s1)))
     for c, (img, mem) in zip(ctxs, imgs):
         c.destroy_image(img, mem)
 
@@ -471,9 +459,7 @@ def run_gpu(args):
         print(json.dumps(line), flush=True)
     for c in ctxs:
         c.close()
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    group.close()
 
 
 def run_hevc_deblock(args):
