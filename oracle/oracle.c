@@ -761,52 +761,68 @@ static int bs_of(int is_intra, int mb_edge, const uint32_t *nz, const orc_mv_t *
     return 0;
 }
 
+/* One filtering step of macroblock mb: its vertical edges (dir 0, left to
+ * right) or its horizontal edges (dir 1, top to bottom), luma and chroma
+ * (A1/src/h264_deblock.c:263-347). Uniform QP so qPav = QP. */
+static void deblock_step(int mbw, int qp, int is_intra, const uint32_t *nz, const orc_mv_t *mv, uint8_t *ry,
+                         uint8_t *ruv, int rp, int mb, int dir)
+{
+    const int qpc = orc_chroma_qp(qp);
+    const int a = ALPHA[qp], b = BETA[qp], ac = ALPHA[qpc], bc = BETA[qpc];
+    const int my = mb / mbw, mx = mb % mbw;
+    uint8_t *py = ry + (size_t)my * 16 * rp + mx * 16;
+    uint8_t *pc = ruv + (size_t)my * 8 * rp + mx * 16;
+    for (int e = 0; e < 4; e++) {
+        if (e == 0 && (dir == 0 ? mx == 0 : my == 0)) continue;
+        int mbp = e ? mb : (dir == 0 ? mb - 1 : mb - mbw);
+        for (int k = 0; k < 4; k++) {
+            int bq = dir == 0 ? k * 4 + e : e * 4 + k;
+            int bp = e ? (dir == 0 ? bq - 1 : bq - 4) : (dir == 0 ? k * 4 + 3 : 12 + k);
+            int bs = bs_of(is_intra, e == 0, nz, mv, mbp, bp, mb, bq);
+            if (!bs) continue;
+            if (a && b) {
+                int tc0 = bs < 4 ? TC0[qp][bs - 1] : 0;
+                for (int i = 0; i < 4; i++) {
+                    uint8_t *q = dir == 0 ? py + (size_t)(k * 4 + i) * rp + e * 4
+                                          : py + (size_t)(e * 4) * rp + k * 4 + i;
+                    filt_luma(q, dir == 0 ? 1 : rp, bs, a, b, tc0);
+                }
+            }
+            if ((e == 0 || e == 2) && ac && bc) {
+                int tc0 = bs < 4 ? TC0[qpc][bs - 1] : 0;
+                for (int pl = 0; pl < 2; pl++)
+                    for (int i = 0; i < 2; i++) {
+                        uint8_t *q = dir == 0 ? pc + (size_t)(k * 2 + i) * rp + 2 * (e * 2) + pl
+                                              : pc + (size_t)(e * 2) * rp + 2 * (k * 2 + i) + pl;
+                        filt_chroma(q, dir == 0 ? 2 : rp, bs, ac, bc, tc0);
+                    }
+            }
+        }
+    }
+}
+
 void orc_deblock_frame(int mbw, int mbh, int qp, int is_intra, const uint32_t *nz, const orc_mv_t *mv,
                        uint8_t *ry, uint8_t *ruv, int rp)
 {
     /* Macroblocks in raster order; per macroblock the vertical edges left
      * to right, then the horizontal edges top to bottom (clause 8.7,
-     * A1/src/h264_deblock.c:263-347). Uniform QP so qPav = QP. */
-    const int qpc = orc_chroma_qp(qp);
-    const int a = ALPHA[qp], b = BETA[qp], ac = ALPHA[qpc], bc = BETA[qpc];
-    if (!a || !b) {
-        /* luma untouched; chroma alpha/beta are never larger at QPc <= QP */
-        if (!ac || !bc) return;
+     * A1/src/h264_deblock.c:263-347). */
+    for (int mb = 0; mb < mbw * mbh; mb++) {
+        deblock_step(mbw, qp, is_intra, nz, mv, ry, ruv, rp, mb, 0);
+        deblock_step(mbw, qp, is_intra, nz, mv, ry, ruv, rp, mb, 1);
     }
-    for (int my = 0; my < mbh; my++)
-        for (int mx = 0; mx < mbw; mx++) {
-            const int mb = my * mbw + mx;
-            uint8_t *py = ry + (size_t)my * 16 * rp + mx * 16;
-            uint8_t *pc = ruv + (size_t)my * 8 * rp + mx * 16;
-            for (int dir = 0; dir < 2; dir++)
-                for (int e = 0; e < 4; e++) {
-                    if (e == 0 && (dir == 0 ? mx == 0 : my == 0)) continue;
-                    int mbp = e ? mb : (dir == 0 ? mb - 1 : mb - mbw);
-                    for (int k = 0; k < 4; k++) {
-                        int bq = dir == 0 ? k * 4 + e : e * 4 + k;
-                        int bp = e ? (dir == 0 ? bq - 1 : bq - 4) : (dir == 0 ? k * 4 + 3 : 12 + k);
-                        int bs = bs_of(is_intra, e == 0, nz, mv, mbp, bp, mb, bq);
-                        if (!bs) continue;
-                        if (a && b) {
-                            int tc0 = bs < 4 ? TC0[qp][bs - 1] : 0;
-                            for (int i = 0; i < 4; i++) {
-                                uint8_t *q = dir == 0 ? py + (size_t)(k * 4 + i) * rp + e * 4
-                                                      : py + (size_t)(e * 4) * rp + k * 4 + i;
-                                filt_luma(q, dir == 0 ? 1 : rp, bs, a, b, tc0);
-                            }
-                        }
-                        if ((e == 0 || e == 2) && ac && bc) {
-                            int tc0 = bs < 4 ? TC0[qpc][bs - 1] : 0;
-                            for (int pl = 0; pl < 2; pl++)
-                                for (int i = 0; i < 2; i++) {
-                                    uint8_t *q = dir == 0 ? pc + (size_t)(k * 2 + i) * rp + 2 * (e * 2) + pl
-                                                          : pc + (size_t)(e * 2) * rp + 2 * (k * 2 + i) + pl;
-                                    filt_chroma(q, dir == 0 ? 2 : rp, bs, ac, bc, tc0);
-                                }
-                        }
-                    }
-                }
-        }
+}
+
+int orc_deblock_steps(int mbw, int mbh, int qp, int is_intra, const uint32_t *nz, const orc_mv_t *mv, uint8_t *ry,
+                      uint8_t *ruv, int rp, const int32_t *steps, int nsteps)
+{
+    /* The same steps in the caller's order: steps[i] = 2 * mb + dir. */
+    for (int i = 0; i < nsteps; i++) {
+        const int mb = steps[i] >> 1, dir = steps[i] & 1;
+        if (steps[i] < 0 || mb >= mbw * mbh) return -1;
+        deblock_step(mbw, qp, is_intra, nz, mv, ry, ruv, rp, mb, dir);
+    }
+    return 0;
 }
 
 /* ------------------------------------------------------------ one frame */

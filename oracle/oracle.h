@@ -123,6 +123,16 @@ void orc_deblock_frame(int mbw, int mbh, int qp, int is_intra,
                        const uint32_t *nz, const orc_mv_t *mv,
                        uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch);
 
+/* The same filtering as steps applied in a caller-given order, steps[i] =
+ * 2 * mb + dir (dir 0: the macroblock's vertical edges, 1: its horizontal
+ * edges); orc_deblock_frame is the raster order 0, 1, 2, 3, ... Returns -1
+ * for a step outside the picture. For checking that a parallel schedule
+ * keeps the raster order's result. */
+int orc_deblock_steps(int mbw, int mbh, int qp, int is_intra,
+                      const uint32_t *nz, const orc_mv_t *mv,
+                      uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch,
+                      const int32_t *steps, int nsteps);
+
 /* One whole frame of the hot path: ME (P only) -> P or I chain -> deblock. */
 void orc_encode_frame(const orc_frame_t *f, const orc_me_params_t *p, int is_intra, int deblock,
                       const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,

@@ -134,6 +134,16 @@ def deblock(mbw, mbh, qp, is_intra, nz, mv, rec_y, rec_uv):
                             _p(np.ascontiguousarray(mv, np.int32)), _p(rec_y), _p(rec_uv), rec_y.shape[1])
 
 
+def deblock_steps(mbw, mbh, qp, is_intra, nz, mv, rec_y, rec_uv, steps):
+    """The deblocking steps (2 * mb + dir) in the given order (oracle.h)."""
+    st = np.ascontiguousarray(steps, np.int32)
+    rc = lib().orc_deblock_steps(mbw, mbh, qp, int(is_intra), _p(np.ascontiguousarray(nz, np.uint32)),
+                                 _p(np.ascontiguousarray(mv, np.int32)), _p(rec_y), _p(rec_uv), rec_y.shape[1],
+                                 _p(st), len(st))
+    if rc != 0:
+        raise ValueError("deblocking step outside the picture")
+
+
 def encode_frame(f, rng, lam, zero_thresh, is_intra, do_deblock, cur_y, cur_uv, ref_y, ref_uv, rec_y, rec_uv):
     o = alloc_outputs(f.mbw * f.mbh)
     lib().orc_encode_frame(ctypes.byref(f), ctypes.byref(MeParams(rng, lam, zero_thresh)), int(is_intra),
