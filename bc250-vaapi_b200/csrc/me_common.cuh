@@ -176,7 +176,7 @@ __device__ __forceinline__ uint32_t qpel_refine(RefineShared& rf, G8F G8, const 
 // which vavgu4 forms for 4 pels at once, and vabsdiff4 accumulates the SAD.
 // Results are identical to qpel_refine.
 struct RefineSimd {
-  int32_t hr[23][18];
+  int16_t hr[23][18];  // 6-tap sums of 8-bit samples: -2550 .. 10710
   alignas(4) uint8_t pl[3][18][20];  // b, h, j at [ry+1][rx+1], ry, rx in -1..16
 };
 

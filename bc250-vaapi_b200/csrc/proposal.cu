@@ -235,9 +235,13 @@ __global__ void lp_select_kernel(int mbs, LpBuf b, int mode, float param, int la
 // Candidate k's patch covers rows cy-5 .. cy+21 and 32 bytes from
 // xa = (X+cx-5) & ~3: the +-2 search window plus the refine's -3..+19 reach
 // around any winner inside that window, so the refine reads no global memory.
-constexpr int kPatchRows = 27, kPatchWords = 8;
+// Rows are kPatchStride = 9 words apart (8 used) and candidates 244 words
+// (20 mod 32): the 25 offsets of two candidates that a warp scores at once
+// then read 32 different banks, where 8-word rows put offsets 0 and 4 rows
+// apart, and the next candidate, on the same banks.
+constexpr int kPatchRows = 27, kPatchWords = 8, kPatchStride = 9;
 struct RescoreWarp {
-  uint32_t patch[4][kPatchRows][kPatchWords];
+  uint32_t patch[4][kPatchRows * kPatchStride + 1];
   uint32_t cur[64];
   int ccx[4], ccy[4];
   RefineSimd rf;
@@ -289,7 +293,7 @@ __global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restri
       const int r = rem / kPatchWords, w = rem - r * kPatchWords;
       const int xa = (X + sh.ccx[k] - 5) & ~3;
       const uint8_t* rp = ref + (size_t)clampi(Y + sh.ccy[k] - 5 + r, 0, g.RH - 1) * ref_pitch;
-      sh.patch[k][r][w] = load_word_clamped(rp, xa + 4 * w, g.RW);
+      sh.patch[k][r * kPatchStride + w] = load_word_clamped(rp, xa + 4 * w, g.RW);
     }
     __syncwarp();
 
@@ -305,7 +309,7 @@ __global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restri
       uint32_t sad = 0;
 #pragma unroll 4
       for (int r = 0; r < 16; ++r) {
-        const uint32_t* rw = sh.patch[k][oy + 3 + r] + w0;
+        const uint32_t* rw = sh.patch[k] + (oy + 3 + r) * kPatchStride + w0;
         const uint32_t a0 = rw[0], a1 = rw[1], a2 = rw[2], a3 = rw[3], a4 = rw[4];
         sad = sad4_acc(__funnelshift_r(a0, a1, shft), sh.cur[r * 4 + 0], sad);
         sad = sad4_acc(__funnelshift_r(a1, a2, shft), sh.cur[r * 4 + 1], sad);
@@ -325,11 +329,11 @@ __global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restri
     int kw = 0;
     for (int k = nk - 1; k >= 0; --k)
       if (abs(mx - sh.ccx[k]) <= 2 && abs(my - sh.ccy[k]) <= 2) kw = k;
-    const uint8_t* pb8 = reinterpret_cast<const uint8_t*>(&sh.patch[kw][0][0]);
+    const uint8_t* pb8 = reinterpret_cast<const uint8_t*>(&sh.patch[kw][0]);
     const int row0 = my - (sh.ccy[kw] - 5), col0 = (X + mx) - ((X + sh.ccx[kw] - 5) & ~3);
     int qx, qy;
     const uint32_t bsad =
-        qpel_refine_warp_simd(sh.rf, pb8, kPatchWords * 4, row0, col0, sh.cur, int_sad, &qx, &qy);
+        qpel_refine_warp_simd(sh.rf, pb8, kPatchStride * 4, row0, col0, sh.cur, int_sad, &qx, &qy);
     if (lane == 0) mv_out[mb] = MV{4 * mx + qx, 4 * my + qy, bsad, 0u};
     __syncwarp();  // the warp's shared memory is restaged for its next MB
   }
