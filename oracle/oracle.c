@@ -528,159 +528,179 @@ void orc_p_frame(const orc_frame_t *f,
 
 /* ------------------------------------------------------- I-frame chain */
 
+/* One macroblock of the I frame (A1/shaders/intra_wavefront.comp:398-756):
+ * the I16x16 decision from the reconstructed left, top and top-left
+ * neighbours, the chain, and its reconstruction into rec. */
+static void i_mb(const orc_frame_t *f, const uint8_t *cur_y, const uint8_t *cur_uv, int cp, orc_out_t *out,
+                 uint8_t *rec_y, uint8_t *rec_uv, int rp, int mbx, int mby)
+{
+    const int qp = f->qp, qpc = orc_chroma_qp(qp);
+    const uint32_t total = (uint32_t)(f->mbw * f->mbh);
+    const int rmx = f->RW - 1, rmy = f->RH - 1, cmx = f->RW / 2 - 1, cmy = f->RH / 2 - 1;
+    const int mb = mby * f->mbw + mbx, X = mbx * 16, Y = mby * 16, Xc = X / 2, Yc = Y / 2;
+    const uint32_t sl = orc_slice_of((uint32_t)mb, total, (uint32_t)f->num_slices);
+    const int top_exists = mby > 0, left_exists = mbx > 0;
+    const int top_av = top_exists && orc_slice_of((uint32_t)(mb - f->mbw), total, (uint32_t)f->num_slices) == sl;
+    const int left_av = left_exists && orc_slice_of((uint32_t)(mb - 1), total, (uint32_t)f->num_slices) == sl;
+    const int plane_av = top_av && left_av &&
+        (!(f->flags & ORC_INTRA_CORNER_CHECK) ||
+         orc_slice_of((uint32_t)(mb - f->mbw - 1), total, (uint32_t)f->num_slices) == sl);
+    int top[16], left[16], corner;
+    for (int i = 0; i < 16; i++) {
+        top[i] = top_exists ? rec_y[(size_t)clampi(Y - 1, 0, rmy) * rp + clampi(X + i, 0, rmx)] : 128;
+        left[i] = left_exists ? rec_y[(size_t)clampi(Y + i, 0, rmy) * rp + clampi(X - 1, 0, rmx)] : 128;
+    }
+    corner = (top_exists && left_exists) ? rec_y[(size_t)clampi(Y - 1, 0, rmy) * rp + clampi(X - 1, 0, rmx)] : 128;
+    int st = 0, sl_ = 0;
+    for (int i = 0; i < 16; i++) { st += top[i]; sl_ += left[i]; }
+    int dcv;
+    if (top_av && left_av) dcv = (st + sl_ + 16) >> 5;
+    else if (top_av) dcv = (st + 8) >> 4;
+    else if (left_av) dcv = (sl_ + 8) >> 4;
+    else dcv = 128;
+    int pa = 0, pb = 0, pc = 0;
+    if (plane_av) {
+        int Hs = 0, Vs = 0;
+        for (int k = 0; k < 8; k++) {
+            int l = (6 - k >= 0) ? top[6 - k] : corner;
+            Hs += (k + 1) * (top[8 + k] - l);
+            int a = (6 - k >= 0) ? left[6 - k] : corner;
+            Vs += (k + 1) * (left[8 + k] - a);
+        }
+        pa = 16 * (left[15] + top[15]);
+        pb = (5 * Hs + 32) >> 6;
+        pc = (5 * Vs + 32) >> 6;
+    }
+    int src[256];
+    for (int y = 0; y < 16; y++)
+        for (int x = 0; x < 16; x++) src[y * 16 + x] = srcY(f, cur_y, cp, X + x, Y + y);
+    uint32_t sdc = 0, sv = 0, sh = 0, spl = 0;
+    for (int y = 0; y < 16; y++)
+        for (int x = 0; x < 16; x++) {
+            int s = src[y * 16 + x];
+            sdc += (uint32_t)iabs(s - dcv);
+            if (top_av) sv += (uint32_t)iabs(s - top[x]);
+            if (left_av) sh += (uint32_t)iabs(s - left[y]);
+            if (plane_av) spl += (uint32_t)iabs(s - clip1((pa + pb * (x - 7) + pc * (y - 7) + 16) >> 5));
+        }
+    uint32_t best = sdc;
+    int mode = 2;
+    if (top_av && sv < best) { best = sv; mode = 0; }
+    if (left_av && sh < best) { best = sh; mode = 1; }
+    if (plane_av && spl < best) { best = spl; mode = 3; }
+    out->pred_mode[mb] = (uint32_t)mode;
+    out->mv[mb].mvx = out->mv[mb].mvy = 0;
+    out->mv[mb].sad = out->mv[mb].pad = 0;
+
+    int res[24][16], pred[24][16], coef[24][16], lev[24][16];
+    for (int y = 0; y < 16; y++)
+        for (int x = 0; x < 16; x++) {
+            int pv;
+            if (mode == 0) pv = top[x];
+            else if (mode == 1) pv = left[y];
+            else if (mode == 3) pv = clip1((pa + pb * (x - 7) + pc * (y - 7) + 16) >> 5);
+            else pv = dcv;
+            int blk = (y >> 2) * 4 + (x >> 2), pos = (y & 3) * 4 + (x & 3);
+            pred[blk][pos] = pv;
+            res[blk][pos] = src[y * 16 + x] - pv;
+        }
+    int dcin[16];
+    for (int b = 0; b < 16; b++) {
+        uint32_t nz = 0;
+        orc_forward_4x4(res[b], coef[b]);
+        out->dc[(size_t)mb * 24 + b] = coef[b][0];
+        dcin[b] = coef[b][0];
+        lev[b][0] = 0;
+        out->levels[((size_t)mb * 24 + b) * 16] = 0;
+        for (int p = 1; p < 16; p++) {
+            lev[b][p] = orc_quant_ac(coef[b][p], p, qp, 1);
+            out->levels[((size_t)mb * 24 + b) * 16 + p] = (int16_t)clampi(lev[b][p], -32768, 32767);
+            if (lev[b][p]) nz |= 1u << p;
+        }
+        out->nz[(size_t)mb * 24 + b] = nz;
+    }
+    int raw[16], dl[16], fv[16];
+    orc_luma_dc_hadamard_fwd(dcin, raw);
+    for (int b = 0; b < 16; b++) dl[b] = orc_quantize_dc_luma(raw[b], qp);
+    orc_luma_dc_hadamard_inv(dl, fv);
+    for (int b = 0; b < 16; b++) {
+        int d[16], r[16], v[16];
+        d[0] = orc_dequant_dc_luma(fv[b], qp);
+        for (int p = 1; p < 16; p++) d[p] = orc_dequant_ac(lev[b][p], p, qp);
+        orc_inverse_4x4(d, r);
+        for (int p = 0; p < 16; p++) v[p] = clip1(pred[b][p] + r[p]);
+        store_rec_luma(f, rec_y, rp, X, Y, b, v);
+    }
+    /* Chroma: DC prediction from recon neighbours gated on slice
+     * availability (intra_wavefront.comp:601-642). */
+    for (int pl = 0; pl < 2; pl++) {
+        int tu[8], lu[8];
+        for (int i = 0; i < 8; i++) {
+            tu[i] = top_av ? rec_uv[(size_t)clampi(Yc - 1, 0, cmy) * rp + 2 * clampi(Xc + i, 0, cmx) + pl] : 128;
+            lu[i] = left_av ? rec_uv[(size_t)clampi(Yc + i, 0, cmy) * rp + 2 * clampi(Xc - 1, 0, cmx) + pl] : 128;
+        }
+        int t0 = tu[0] + tu[1] + tu[2] + tu[3], t1 = tu[4] + tu[5] + tu[6] + tu[7];
+        int l0 = lu[0] + lu[1] + lu[2] + lu[3], l1 = lu[4] + lu[5] + lu[6] + lu[7];
+        int dcp[4];
+        if (top_av && left_av) dcp[0] = (t0 + l0 + 4) >> 3;
+        else if (top_av) dcp[0] = (t0 + 2) >> 2;
+        else if (left_av) dcp[0] = (l0 + 2) >> 2;
+        else dcp[0] = 128;
+        if (top_av) dcp[1] = (t1 + 2) >> 2;
+        else if (left_av) dcp[1] = (l0 + 2) >> 2;
+        else dcp[1] = 128;
+        if (left_av) dcp[2] = (l1 + 2) >> 2;
+        else if (top_av) dcp[2] = (t0 + 2) >> 2;
+        else dcp[2] = 128;
+        if (top_av && left_av) dcp[3] = (t1 + l1 + 4) >> 3;
+        else if (top_av) dcp[3] = (t1 + 2) >> 2;
+        else if (left_av) dcp[3] = (l1 + 2) >> 2;
+        else dcp[3] = 128;
+        for (int sub = 0; sub < 4; sub++) {
+            int blk = 16 + 4 * pl + sub;
+            uint32_t nz = 0;
+            for (int pos = 0; pos < 16; pos++) {
+                int xo = (sub & 1) * 4 + (pos & 3), yo = (sub >> 1) * 4 + (pos >> 2);
+                pred[blk][pos] = dcp[sub];
+                res[blk][pos] = srcC(f, cur_uv, cp, pl, Xc + xo, Yc + yo) - dcp[sub];
+            }
+            orc_forward_4x4(res[blk], coef[blk]);
+            out->dc[(size_t)mb * 24 + blk] = coef[blk][0];
+            lev[blk][0] = 0;
+            out->levels[((size_t)mb * 24 + blk) * 16] = 0;
+            for (int p = 1; p < 16; p++) {
+                lev[blk][p] = orc_quant_ac(coef[blk][p], p, qpc, 1);
+                out->levels[((size_t)mb * 24 + blk) * 16 + p] = (int16_t)clampi(lev[blk][p], -32768, 32767);
+                if (lev[blk][p]) nz |= 1u << p;
+            }
+            out->nz[(size_t)mb * 24 + blk] = nz;
+        }
+    }
+    chroma_recon(f, qpc, coef, lev, pred, rec_uv, rp, Xc, Yc);
+}
+
 void orc_i_frame(const orc_frame_t *f,
                  const uint8_t *cur_y, const uint8_t *cur_uv, int cp,
                  orc_out_t *out, uint8_t *rec_y, uint8_t *rec_uv, int rp)
 {
-    /* A1/shaders/intra_wavefront.comp:398-756. Raster order visits every
-     * macroblock after its left, top and top-left neighbours, which is all
-     * the diagonal schedule (A1/src/gpu_compute.c:3238-3249) guarantees. */
-    const int qp = f->qp, qpc = orc_chroma_qp(qp);
-    const uint32_t total = (uint32_t)(f->mbw * f->mbh);
-    const int rmx = f->RW - 1, rmy = f->RH - 1, cmx = f->RW / 2 - 1, cmy = f->RH / 2 - 1;
+    /* Raster order visits every macroblock after its left, top and top-left
+     * neighbours, which is all the diagonal schedule
+     * (A1/src/gpu_compute.c:3238-3249) guarantees. */
     for (int mby = 0; mby < f->mbh; mby++)
-        for (int mbx = 0; mbx < f->mbw; mbx++) {
-            const int mb = mby * f->mbw + mbx, X = mbx * 16, Y = mby * 16, Xc = X / 2, Yc = Y / 2;
-            const uint32_t sl = orc_slice_of((uint32_t)mb, total, (uint32_t)f->num_slices);
-            const int top_exists = mby > 0, left_exists = mbx > 0;
-            const int top_av = top_exists && orc_slice_of((uint32_t)(mb - f->mbw), total, (uint32_t)f->num_slices) == sl;
-            const int left_av = left_exists && orc_slice_of((uint32_t)(mb - 1), total, (uint32_t)f->num_slices) == sl;
-            const int plane_av = top_av && left_av &&
-                (!(f->flags & ORC_INTRA_CORNER_CHECK) ||
-                 orc_slice_of((uint32_t)(mb - f->mbw - 1), total, (uint32_t)f->num_slices) == sl);
-            int top[16], left[16], corner;
-            for (int i = 0; i < 16; i++) {
-                top[i] = top_exists ? rec_y[(size_t)clampi(Y - 1, 0, rmy) * rp + clampi(X + i, 0, rmx)] : 128;
-                left[i] = left_exists ? rec_y[(size_t)clampi(Y + i, 0, rmy) * rp + clampi(X - 1, 0, rmx)] : 128;
-            }
-            corner = (top_exists && left_exists) ? rec_y[(size_t)clampi(Y - 1, 0, rmy) * rp + clampi(X - 1, 0, rmx)] : 128;
-            int st = 0, sl_ = 0;
-            for (int i = 0; i < 16; i++) { st += top[i]; sl_ += left[i]; }
-            int dcv;
-            if (top_av && left_av) dcv = (st + sl_ + 16) >> 5;
-            else if (top_av) dcv = (st + 8) >> 4;
-            else if (left_av) dcv = (sl_ + 8) >> 4;
-            else dcv = 128;
-            int pa = 0, pb = 0, pc = 0;
-            if (plane_av) {
-                int Hs = 0, Vs = 0;
-                for (int k = 0; k < 8; k++) {
-                    int l = (6 - k >= 0) ? top[6 - k] : corner;
-                    Hs += (k + 1) * (top[8 + k] - l);
-                    int a = (6 - k >= 0) ? left[6 - k] : corner;
-                    Vs += (k + 1) * (left[8 + k] - a);
-                }
-                pa = 16 * (left[15] + top[15]);
-                pb = (5 * Hs + 32) >> 6;
-                pc = (5 * Vs + 32) >> 6;
-            }
-            int src[256];
-            for (int y = 0; y < 16; y++)
-                for (int x = 0; x < 16; x++) src[y * 16 + x] = srcY(f, cur_y, cp, X + x, Y + y);
-            uint32_t sdc = 0, sv = 0, sh = 0, spl = 0;
-            for (int y = 0; y < 16; y++)
-                for (int x = 0; x < 16; x++) {
-                    int s = src[y * 16 + x];
-                    sdc += (uint32_t)iabs(s - dcv);
-                    if (top_av) sv += (uint32_t)iabs(s - top[x]);
-                    if (left_av) sh += (uint32_t)iabs(s - left[y]);
-                    if (plane_av) spl += (uint32_t)iabs(s - clip1((pa + pb * (x - 7) + pc * (y - 7) + 16) >> 5));
-                }
-            uint32_t best = sdc;
-            int mode = 2;
-            if (top_av && sv < best) { best = sv; mode = 0; }
-            if (left_av && sh < best) { best = sh; mode = 1; }
-            if (plane_av && spl < best) { best = spl; mode = 3; }
-            out->pred_mode[mb] = (uint32_t)mode;
-            out->mv[mb].mvx = out->mv[mb].mvy = 0;
-            out->mv[mb].sad = out->mv[mb].pad = 0;
+        for (int mbx = 0; mbx < f->mbw; mbx++) i_mb(f, cur_y, cur_uv, cp, out, rec_y, rec_uv, rp, mbx, mby);
+}
 
-            int res[24][16], pred[24][16], coef[24][16], lev[24][16];
-            for (int y = 0; y < 16; y++)
-                for (int x = 0; x < 16; x++) {
-                    int pv;
-                    if (mode == 0) pv = top[x];
-                    else if (mode == 1) pv = left[y];
-                    else if (mode == 3) pv = clip1((pa + pb * (x - 7) + pc * (y - 7) + 16) >> 5);
-                    else pv = dcv;
-                    int blk = (y >> 2) * 4 + (x >> 2), pos = (y & 3) * 4 + (x & 3);
-                    pred[blk][pos] = pv;
-                    res[blk][pos] = src[y * 16 + x] - pv;
-                }
-            int dcin[16];
-            for (int b = 0; b < 16; b++) {
-                uint32_t nz = 0;
-                orc_forward_4x4(res[b], coef[b]);
-                out->dc[(size_t)mb * 24 + b] = coef[b][0];
-                dcin[b] = coef[b][0];
-                lev[b][0] = 0;
-                out->levels[((size_t)mb * 24 + b) * 16] = 0;
-                for (int p = 1; p < 16; p++) {
-                    lev[b][p] = orc_quant_ac(coef[b][p], p, qp, 1);
-                    out->levels[((size_t)mb * 24 + b) * 16 + p] = (int16_t)clampi(lev[b][p], -32768, 32767);
-                    if (lev[b][p]) nz |= 1u << p;
-                }
-                out->nz[(size_t)mb * 24 + b] = nz;
-            }
-            int raw[16], dl[16], fv[16];
-            orc_luma_dc_hadamard_fwd(dcin, raw);
-            for (int b = 0; b < 16; b++) dl[b] = orc_quantize_dc_luma(raw[b], qp);
-            orc_luma_dc_hadamard_inv(dl, fv);
-            for (int b = 0; b < 16; b++) {
-                int d[16], r[16], v[16];
-                d[0] = orc_dequant_dc_luma(fv[b], qp);
-                for (int p = 1; p < 16; p++) d[p] = orc_dequant_ac(lev[b][p], p, qp);
-                orc_inverse_4x4(d, r);
-                for (int p = 0; p < 16; p++) v[p] = clip1(pred[b][p] + r[p]);
-                store_rec_luma(f, rec_y, rp, X, Y, b, v);
-            }
-            /* Chroma: DC prediction from recon neighbours gated on slice
-             * availability (intra_wavefront.comp:601-642). */
-            for (int pl = 0; pl < 2; pl++) {
-                int tu[8], lu[8];
-                for (int i = 0; i < 8; i++) {
-                    tu[i] = top_av ? rec_uv[(size_t)clampi(Yc - 1, 0, cmy) * rp + 2 * clampi(Xc + i, 0, cmx) + pl] : 128;
-                    lu[i] = left_av ? rec_uv[(size_t)clampi(Yc + i, 0, cmy) * rp + 2 * clampi(Xc - 1, 0, cmx) + pl] : 128;
-                }
-                int t0 = tu[0] + tu[1] + tu[2] + tu[3], t1 = tu[4] + tu[5] + tu[6] + tu[7];
-                int l0 = lu[0] + lu[1] + lu[2] + lu[3], l1 = lu[4] + lu[5] + lu[6] + lu[7];
-                int dcp[4];
-                if (top_av && left_av) dcp[0] = (t0 + l0 + 4) >> 3;
-                else if (top_av) dcp[0] = (t0 + 2) >> 2;
-                else if (left_av) dcp[0] = (l0 + 2) >> 2;
-                else dcp[0] = 128;
-                if (top_av) dcp[1] = (t1 + 2) >> 2;
-                else if (left_av) dcp[1] = (l0 + 2) >> 2;
-                else dcp[1] = 128;
-                if (left_av) dcp[2] = (l1 + 2) >> 2;
-                else if (top_av) dcp[2] = (t0 + 2) >> 2;
-                else dcp[2] = 128;
-                if (top_av && left_av) dcp[3] = (t1 + l1 + 4) >> 3;
-                else if (top_av) dcp[3] = (t1 + 2) >> 2;
-                else if (left_av) dcp[3] = (l1 + 2) >> 2;
-                else dcp[3] = 128;
-                for (int sub = 0; sub < 4; sub++) {
-                    int blk = 16 + 4 * pl + sub;
-                    uint32_t nz = 0;
-                    for (int pos = 0; pos < 16; pos++) {
-                        int xo = (sub & 1) * 4 + (pos & 3), yo = (sub >> 1) * 4 + (pos >> 2);
-                        pred[blk][pos] = dcp[sub];
-                        res[blk][pos] = srcC(f, cur_uv, cp, pl, Xc + xo, Yc + yo) - dcp[sub];
-                    }
-                    orc_forward_4x4(res[blk], coef[blk]);
-                    out->dc[(size_t)mb * 24 + blk] = coef[blk][0];
-                    lev[blk][0] = 0;
-                    out->levels[((size_t)mb * 24 + blk) * 16] = 0;
-                    for (int p = 1; p < 16; p++) {
-                        lev[blk][p] = orc_quant_ac(coef[blk][p], p, qpc, 1);
-                        out->levels[((size_t)mb * 24 + blk) * 16 + p] = (int16_t)clampi(lev[blk][p], -32768, 32767);
-                        if (lev[blk][p]) nz |= 1u << p;
-                    }
-                    out->nz[(size_t)mb * 24 + blk] = nz;
-                }
-            }
-            chroma_recon(f, qpc, coef, lev, pred, rec_uv, rp, Xc, Yc);
-        }
+int orc_i_frame_steps(const orc_frame_t *f,
+                      const uint8_t *cur_y, const uint8_t *cur_uv, int cp,
+                      orc_out_t *out, uint8_t *rec_y, uint8_t *rec_uv, int rp,
+                      const int32_t *order, int n)
+{
+    /* The same macroblocks in the caller's order (raster indices). */
+    for (int i = 0; i < n; i++) {
+        if (order[i] < 0 || order[i] >= f->mbw * f->mbh) return -1;
+        i_mb(f, cur_y, cur_uv, cp, out, rec_y, rec_uv, rp, order[i] % f->mbw, order[i] / f->mbw);
+    }
+    return 0;
 }
 
 /* --------------------------------------------------------------- deblock */

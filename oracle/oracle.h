@@ -115,6 +115,14 @@ void orc_i_frame(const orc_frame_t *f,
                  const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
                  orc_out_t *out, uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch);
 
+/* The same macroblocks in a caller-given order (raster indices); orc_i_frame
+ * is the raster order. Returns -1 for a macroblock outside the picture. For
+ * checking that a parallel schedule keeps the raster order's result. */
+int orc_i_frame_steps(const orc_frame_t *f,
+                      const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
+                      orc_out_t *out, uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch,
+                      const int32_t *order, int n);
+
 /* Spec deblocking (H.264 8.7) of the coded picture (16*mbw x 16*mbh) for
  * the macroblock kinds this encoder emits: all-intra (I16x16) frames or
  * all-inter (P16x16 / P_Skip, one reference) frames, uniform QP,

@@ -129,6 +129,17 @@ def i_frame(f, cur_y, cur_uv, rec_y, rec_uv):
     return o
 
 
+def i_frame_steps(f, cur_y, cur_uv, rec_y, rec_uv, order):
+    """The I frame's macroblocks in the given order of raster indices (oracle.h)."""
+    o = alloc_outputs(f.mbw * f.mbh)
+    st = np.ascontiguousarray(order, np.int32)
+    rc = lib().orc_i_frame_steps(ctypes.byref(f), _p(cur_y), _p(cur_uv), cur_y.shape[1], ctypes.byref(_out_struct(o)),
+                                 _p(rec_y), _p(rec_uv), rec_y.shape[1], _p(st), len(st))
+    if rc != 0:
+        raise ValueError("macroblock outside the picture")
+    return o
+
+
 def deblock(mbw, mbh, qp, is_intra, nz, mv, rec_y, rec_uv):
     lib().orc_deblock_frame(mbw, mbh, qp, int(is_intra), _p(np.ascontiguousarray(nz, np.uint32)),
                             _p(np.ascontiguousarray(mv, np.int32)), _p(rec_y), _p(rec_uv), rec_y.shape[1])
