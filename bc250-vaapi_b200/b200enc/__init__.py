@@ -478,6 +478,18 @@ class Context:
         if rc != 0:
             raise RuntimeError(f"b200enc_ctx_set_me failed (rc={rc})")
 
+    def mv_field(self):
+        """The latest frame's MV field from device memory, [mbs, 4] int32
+        (mvx, mvy in quarter pel, sad, pad), without staging."""
+        import numpy as np
+        import torch
+        mv = _vp()
+        _check(self.L.b200enc_ctx_device_outputs(ctypes.byref(self.ctx), None, None, None, None, ctypes.byref(mv)),
+               "b200enc_ctx_device_outputs")
+        mbs = ((self.ctx.frame_width + 15) // 16) * ((self.ctx.frame_height + 15) // 16)
+        torch.cuda.synchronize()
+        return device_view(mv.value, mbs * 16).cpu().numpy().view(np.int32).reshape(mbs, 4)
+
     def me_stats(self):
         """(learned, fallback, early-out) MB counts of the last P frame."""
         v = [ctypes.c_int() for _ in range(3)]

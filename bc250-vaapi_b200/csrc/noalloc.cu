@@ -11,6 +11,9 @@
 // start-up may not add allocations afterwards. This file gives them a
 // variant whose scratch lives in a fixed, file-scope device array that the
 // module brings with it, so the call itself allocates nothing.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cstdio>
 #include <mutex>
 
@@ -23,32 +26,73 @@ namespace {
 constexpr int kNoAllocMaxMbRows = 512;
 constexpr size_t kNoAllocScratchWords = 4 + 2 * (size_t)kNoAllocMaxMbRows;  // 4112 bytes
 
-// One copy per device that loads this library; it stays resident until the
-// process exits. Every call on a device shares it.
+// One copy per CUDA context that loads this library's module (the primary
+// context of each device, for ordinary runtime-API callers); it stays
+// resident until that context is destroyed. Every call in a context shares it.
 static __device__ __align__(256) uint32_t g_deblock_scratch[kNoAllocScratchWords];
 
-constexpr int kMaxDevices = 64;
+// Device addresses already looked up, keyed by the driver's context ID. The
+// ID is unique for the life of the process: a context created after
+// cudaDeviceReset, or a caller's own driver-API context on the same device,
+// gets a new ID and so a fresh lookup, never the address of a context that
+// is gone or belongs to someone else.
+constexpr int kCacheEntries = 16;
+struct CacheEntry {
+  unsigned long long ctx_id;
+  uint32_t* addr;
+};
 std::mutex g_mu;
-uint32_t* g_addr[kMaxDevices] = {};
+CacheEntry g_cache[kCacheEntries] = {};
+int g_cache_next = 0;
+PFN_cuCtxGetCurrent_v4000 g_ctx_current = nullptr;
+PFN_cuCtxGetId_v12000 g_ctx_id = nullptr;
 
-// Device address of the scratch on the current device. In host code the
-// array's name is only a host-side stand-in, so the address has to come from
-// cudaGetSymbolAddress, once per device, with that device current.
-uint32_t* scratch_on_current_device() {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_deblock_scratch);
-    if (e != cudaSuccess || !p) {
-      fprintf(stderr, "[b200enc] b200enc_deblock_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
-              cudaGetErrorString(e));
-      return nullptr;
-    }
-    g_addr[dev] = static_cast<uint32_t*>(p);
+// ID of the context current on this thread, 0 if none is (or the driver
+// entry points are unavailable).
+unsigned long long current_context_id() {
+  if (!g_ctx_current || !g_ctx_id) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess)
+      return 0;
+    g_ctx_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(f1);
+    g_ctx_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(f2);
   }
-  return g_addr[dev];
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (g_ctx_current(&c) != CUDA_SUCCESS || !c || g_ctx_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of the scratch in the current context. In host code the
+// array's name is only a host-side stand-in, so the address has to come from
+// cudaGetSymbolAddress, with the device current; it is looked up once per
+// context and cached under the context's ID.
+uint32_t* scratch_in_current_context() {
+  std::lock_guard<std::mutex> lock(g_mu);
+  unsigned long long id = current_context_id();
+  if (id != 0) {
+    for (const CacheEntry& e : g_cache)
+      if (e.ctx_id == id) return e.addr;
+  }
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_deblock_scratch);  // makes the primary context current if none is
+  if (e != cudaSuccess || !p) {
+    int dev = -1;
+    cudaGetDevice(&dev);
+    fprintf(stderr, "[b200enc] b200enc_deblock_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
+            cudaGetErrorString(e));
+    return nullptr;
+  }
+  if (id == 0) id = current_context_id();
+  if (id != 0) {
+    g_cache[g_cache_next] = CacheEntry{id, static_cast<uint32_t*>(p)};
+    g_cache_next = (g_cache_next + 1) % kCacheEntries;
+  }
+  return static_cast<uint32_t*>(p);
 }
 
 }  // namespace
@@ -65,7 +109,7 @@ extern "C" int b200enc_deblock_noalloc(int mbw, int mbh, int qp, int is_intra, c
   if (!nz || !mv || !rec_y || !rec_uv || mbw <= 0 || mbh <= 0 || qp < 0 || qp > 51) return -1;
   if ((rec_pitch & 15) || (((uintptr_t)rec_y) & 15) || (((uintptr_t)rec_uv) & 15) || rec_pitch < mbw * 16)
     return -1;
-  uint32_t* scratch = scratch_on_current_device();
+  uint32_t* scratch = scratch_in_current_context();
   if (!scratch) return -1;
   // The array keeps whatever the previous call left: the ticket, error and
   // progress words this frame uses must start at zero.

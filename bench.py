@@ -4,17 +4,19 @@ learned-proposal form against the plain full-search form.
 
 Workload: S concurrent streams (default 8, one context and CUDA stream each)
 of 1920x1080 8-bit NV12, IPPP with an IDR every 60 frames, QP 27 (a point of
-the 22/27/32/37 sweep), search range 32, lambda 5, spec deblocking on. A step
-is one frame of every stream through ME -> P chain (or intra wavefront) ->
-deblock. Each stream cycles 60 seeded synthetic frames resident in HBM
-(S x 187 MB, far larger than L2). The learned form (value) ranks candidates
-with the packaged network - trained in BF16, run in FP8 E4M3 on the tensor
-cores - and re-scores the top 4 exactly, falling back to the full search
-under the confidence threshold; the first P frame of each GOP has no motion
-history and takes the full search. The plain form is the full search on
-every P frame. Both are timed in the same run, and again with one stream
-(single_stream); the learned form with BF16 inference is timed beside them
-(learned_bf16).
+the 22/27/32/37 sweep), search range 32, lambda 5, spec deblocking on. Stream
+s runs its GOP s*60/S frames ahead of stream 0, as independent encoders do,
+so every timed window holds I frames at the GOP's rate (one per stream per 60
+frames) whatever the step count. A step is one frame of every stream through
+ME -> P chain (or intra wavefront) -> deblock. Each stream cycles 60 seeded
+synthetic frames resident in HBM (S x 187 MB, far larger than L2). The
+learned form (value) ranks candidates with the packaged network - trained in
+BF16, run in FP8 E4M3 on the tensor cores - and re-scores the top 4 exactly,
+falling back to the full search under the confidence threshold; the first P
+frame after each IDR has no motion history and takes the full search. The
+plain form is the full search on every P frame. Both are timed in the same
+run, and again with one stream (single_stream); the learned form with BF16
+inference is timed beside them (learned_bf16).
 
   value  learned-form frames/s summed over the S streams and over ranks,
          device-timed with CUDA events (start event on a control stream that
@@ -26,22 +28,30 @@ every P frame. Both are timed in the same run, and again with one stream
          begin/dispatch/end_picture; then sync_slot and a host read of the
          staged outputs), S streams, double-buffered over the boundary's two
          staging slots (step k+1 is submitted before step k is read back).
+  full_encode  the rate an application sees: S streams, one host thread
+         each, through the reference's unchanged host encoder
+         (h264_encoder_encode_frame_ext in oracle/_ref/libh264enc_b200.so:
+         upload, the GPU hot path, CAVLC or CABAC slices on the host cores),
+         wall clock over the timed frames.
+  me_int the plain full search's integer rate (abs-diffs/s) on one stream.
   bd_rate the learned form's BD-rate against the plain form (bits from the
          reference's host encoder, CABAC, QP 22/27/32/37, 60 1080p frames),
          measured on a B200 with tests/rd_report.py and recorded in
-         profiles/rd_h264_1080p_learned_vs_plain.json.
+         profiles/rd_h264_1080p_learned_fp8_vs_plain.json.
 
 `--impl reference` times the reference's CPU implementation of the same
-frame (the plain form; the reference has no learned form) on the host cores
+frames (the plain form; the reference has no learned form) on the host cores
 (oracle/_ref: the reference's AVX2 SAD in the exhaustive search, its C
-deblocking filter; the P chain from the CPU restatement), each step a
-bounded sample of one frame.
+deblocking filter; the P chain with the frame's own full-search MVs and the
+I frame from the CPU restatement), each step a bounded sample of a GOP's
+frame mix.
 """
 import argparse
 import json
 import os
 import subprocess
 import sys
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -51,18 +61,37 @@ W, H, QP, RANGE, LAMBDA, GOP, NFRAMES = 1920, 1080, 27, 32, 5, 60, 60
 MBW, MBH = (W + 15) // 16, (H + 15) // 16
 MBS = MBW * MBH
 WORKLOAD = "h264_1080p_ippp_fullsearch_r32"
+METRIC = "1080p encode fps, learned-proposal form (vs plain full-search form)"
 # Algorithmic bytes per macroblock of each stage (per launch = x MBS):
 #   ME: current + reference luma once (2 B/px) + the 16-byte MV
 #   P chain: src YUV 1.5 + ref YUV 1.5 + levels 3.0 + nz 0.375 + dc 0.375 + recon 1.5 B/px
+#   intra: the P chain's bytes without the reference (6.75 B/px)
 #   deblock: recon read+write 3.0 + nz 0.375 + MV 0.0625 B/px
-ALGO_BYTES_PER_MB = {"me": 2 * 256 + 16, "chain": 8.25 * 256, "deblock": 3.4375 * 256}
+ALGO_BYTES_PER_MB = {"me": 2 * 256 + 16, "chain": 8.25 * 256, "intra": 6.75 * 256, "deblock": 3.4375 * 256}
+# Integer ME work per searched MB: (2R+1)^2 candidates x 256 abs-diffs + 16 sub-pel candidates x 256
+ME_ABSDIFF_PER_MB = (2 * RANGE + 1) ** 2 * 256 + 16 * 256
 H2D_PER_STEP = W * H * 3 // 2
 D2H_PER_STEP = MBS * (768 + 96 + 4 + 16 + 96) + 8
+ENC_SO = os.path.join(ROOT, "oracle", "_ref", "libh264enc_b200.so")
 
 
 def dist_env():
     from b200enc import replicas
     return replicas.dist_env()
+
+
+def gop_phase(s, S):
+    """GOP offset of stream s among S: the streams' IDRs are spread evenly."""
+    return (s * GOP) // max(1, S)
+
+
+def bench_config(S, conf):
+    """The workload's configuration, printed identically by both arms."""
+    return {"workload": f"{WORKLOAD}_x{S}_streams", "streams_per_gpu": S, "width": W, "height": H, "qp": QP,
+            "search_range": RANGE, "lambda": LAMBDA, "gop": GOP, "gop_phase": "stream s: s*gop/streams",
+            "deblock": True, "recon_clamp": "coded", "proposal_conf": conf,
+            "l2": f"each stream cycles {NFRAMES} resident frames ({S * NFRAMES * W * H * 3 // 2 >> 20} MiB > L2)",
+            "parallelism": "independent streams (one context each); replicas across GPUs"}
 
 
 def measured_peaks():
@@ -132,19 +161,36 @@ def make_frames(seed_stream, n):
 # ----------------------------------------------------------------- CPU arm
 
 def cpu_reference_frame_time(frames, budget_s=15.0, threads=None):
-    """Seconds one 1080p P frame takes on the host cores through the
-    reference's CPU code, measured on a bounded sample and scaled by the
-    macroblock rows processed. Returns (seconds_per_frame, info)."""
+    """Seconds one 1080p frame of the GOP's mix (59 P frames, 1 I frame)
+    takes on the host cores through the reference's CPU code. The P frame's
+    full search is timed on a bounded sample of macroblock rows and scaled;
+    its P chain runs with the frame's own full-search MVs (every sub-pel
+    phase the search picks), macroblocks in parallel; deblocking is the
+    reference's filter as shipped (one thread); the I frame is the
+    restatement's intra wavefront in raster order (one thread: its
+    macroblocks depend on one another). Returns (seconds_per_frame, info)."""
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     oracle.build()
     threads = threads or os.cpu_count()
+    oracle.set_threads(threads)
     (y0, uv0), (y1, uv1) = frames[0], frames[1]
     CW, CH = MBW * 16, MBH * 16
-    ry = np.pad(y0, ((0, CH - H), (0, 0)), mode="edge")
-    ruv = np.pad(uv0, ((0, CH // 2 - H // 2), (0, 0)), mode="edge")
     kind = "reference" if oracle.ref_available() else "port"
+    f = oracle.frame(W, H, QP)
+    # the reference picture: frame 0 intra-coded and deblocked
+    ry = np.zeros((CH, CW), np.uint8)
+    ruv = np.zeros((CH // 2, CW), np.uint8)
+    t0 = time.perf_counter()
+    oi = oracle.i_frame(f, y0, uv0, ry, ruv)
+    t_intra = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    if kind == "reference":
+        oracle.ref_deblock(MBW, MBH, QP, 1, oi["nz"], oi["mv"], ry, ruv)
+    else:
+        oracle.deblock(MBW, MBH, QP, 1, oi["nz"], oi["mv"], ry, ruv)
+    t_db_i = time.perf_counter() - t0
     # ME integer search: rows sampled until ~half the budget is spent
     t0 = time.perf_counter()
     rows = 0
@@ -154,13 +200,12 @@ def cpu_reference_frame_time(frames, budget_s=15.0, threads=None):
         if kind == "reference":
             oracle.ref_full_search_int(y1, W, H, ry, CW, CH, RANGE, LAMBDA, r0, r1, threads)
         else:
-            f = oracle.frame(W, 16 * (r1 - r0), QP)
-            oracle.me_frame(f, np.ascontiguousarray(y1[16 * r0:16 * r1]), ry, RANGE, LAMBDA)
+            fr = oracle.frame(W, 16 * (r1 - r0), QP)
+            oracle.me_frame(fr, np.ascontiguousarray(y1[16 * r0:16 * r1]), ry[16 * r0:], RANGE, LAMBDA)
         rows = r1
     t_me = (time.perf_counter() - t0) / rows * MBH
-    # P chain (CPU restatement, one thread) and deblocking over the full frame
-    f = oracle.frame(W, H, QP)
-    mv = np.zeros((MBS, 4), np.int32)
+    # the frame's own MVs (full search + sub-pel refine), not timed here
+    mv = oracle.me_frame(f, y1, ry, RANGE, LAMBDA)
     rec_y = np.zeros((CH, CW), np.uint8)
     rec_uv = np.zeros((CH // 2, CW), np.uint8)
     t1 = time.perf_counter()
@@ -172,13 +217,16 @@ def cpu_reference_frame_time(frames, budget_s=15.0, threads=None):
     else:
         oracle.deblock(MBW, MBH, QP, 0, o["nz"], o["mv"], rec_y, rec_uv)
     t_db = time.perf_counter() - t2
-    sample = (f"one 1080p P frame: full search +-{RANGE} on {rows}/{MBH} MB rows "
+    t_p = t_me + t_chain + t_db
+    t_i = t_intra + t_db_i
+    sample = (f"1080p GOP mix (59 P + 1 I per 60 frames). P frame: full search +-{RANGE} on {rows}/{MBH} MB rows "
               f"({'reference cpu_simd_sad_16x16 AVX2' if kind == 'reference' else 'CPU restatement'}, "
-              f"{threads} threads) scaled to {MBH} rows; P chain (CPU restatement, 1 thread) and "
-              f"{'reference h264d_deblock_picture' if kind == 'reference' else 'restated deblocking'} (1 thread) "
-              f"on the whole frame")
-    return t_me + t_chain + t_db, dict(kind=kind, cores=threads, sample=sample,
-                                       stage_s=dict(me=t_me, chain=t_chain, deblock=t_db))
+              f"{threads} threads) scaled to {MBH} rows; P chain (CPU restatement, {threads} threads, the frame's "
+              f"own full-search MVs); {'reference h264d_deblock_picture' if kind == 'reference' else 'restated deblocking'}"
+              f" (1 thread). I frame: intra wavefront restatement (1 thread) + the same deblocking")
+    return ((GOP - 1) * t_p + t_i) / GOP, dict(kind=kind, cores=threads, sample=sample,
+                                               stage_s=dict(me=t_me, chain=t_chain, deblock=t_db, intra=t_intra,
+                                                            deblock_intra=t_db_i))
 
 
 def run_reference(args):
@@ -195,18 +243,16 @@ def run_reference(args):
         t, info = cpu_reference_frame_time(frames, budget_s=budget)
         times.append(t)
     fps = len(times) / sum(times)
-    line = {"metric": "1080p encode fps, learned-proposal form (vs plain full-search form)", "value": round(fps, 4),
-            "unit": "frames/s",
+    line = {"metric": METRIC, "value": round(fps, 4), "unit": "frames/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 / fps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
-            "data": "synthetic (seeded generator, 1080p NV12)", "impl": "reference",
-            "config": {"workload": f"{WORKLOAD}_x{args.streams}_streams", "streams_per_gpu": args.streams,
-                       "width": W, "height": H, "qp": QP, "search_range": RANGE, "lambda": LAMBDA, "gop": GOP,
-                       "deblock": True, "recon_clamp": "coded",
-                       "parallelism": "the host's threads on one stream's frames at a time (frames/s does not "
-                                      "depend on how many streams share the host)"},
+            "data": "synthetic (seeded generator: gradients, sigma-8 texture, 6 moving rectangles, pan, noise patch)",
+            "impl": "reference", "config": bench_config(args.streams, args.conf),
             "cpu_baseline": {"value": round(fps, 4), "unit": "frames/s", "cores": info["cores"],
-                             "kind": info["kind"], "sample": info["sample"]},
+                             "kind": info["kind"], "sample": info["sample"],
+                             "parallelism": "the host's threads on one stream's frames at a time (frames/s does not "
+                                            "depend on how many streams share the host)",
+                             "stage_s": {k: round(v, 4) for k, v in info["stage_s"].items()}},
             "e2e": {"value": round(fps, 4), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -255,6 +301,125 @@ LEARNED = 3
 LAUNCHES = {"i": 2, "p_full": 3, "p_learned": 12}
 
 
+class GopSchedule:
+    """Frame kinds of S streams with spread GOP phases. Each arm starts every
+    stream with an IDR (a warm-up step), then stream s follows its phase:
+    intra when (t + phase_s) % GOP == 0. A P frame is learned when its stream
+    has a P frame since the last IDR (the motion history the candidates come
+    from)."""
+
+    def __init__(self, S):
+        self.S = S
+        self.phase = [gop_phase(s, S) for s in range(S)]
+        self.since_i = [0] * S
+
+    def kind(self, s, t, learned):
+        """'i', 'p_full' or 'p_learned' for stream s at step t (advances)."""
+        if t == 0 or (t + self.phase[s]) % GOP == 0:
+            self.since_i[s] = 0
+            return "i"
+        self.since_i[s] += 1
+        return "p_learned" if (learned and self.since_i[s] >= 2) else "p_full"
+
+
+def full_encode(args, host_frames, S, steps, warmup, profile, me):
+    """Frames/s of S streams through the reference's host encoder
+    (h264_encoder_encode_frame_ext), one host thread per stream: pinned
+    upload, the GPU hot path, the host's CAVLC (profile 66) or CABAC (77)
+    slices. Wall clock over `steps` frames per stream, all streams at once;
+    stream s first encodes gop_phase(s) + warmup frames so the IDRs spread."""
+    import ctypes
+    import numpy as np
+    import torch
+    import b200enc
+    if not os.path.exists(ENC_SO):
+        return {"unavailable": "oracle/_ref/libh264enc_b200.so not built"}
+    os.environ.update({"BC250_FORCE_QP": str(QP), "BC250_FORCE_TIER": "0", "BC250_SLICES_PER_FRAME": "4",
+                       "BC250_FORCE_SLICES": "0", "BC250_THREADS": "4", "B200ENC_SEARCH_RANGE": str(RANGE),
+                       "B200ENC_ME": me})
+    enc = ctypes.CDLL(ENC_SO)
+    L = b200enc.lib()
+    enc.h264_encoder_create.restype = ctypes.c_void_p
+    enc.h264_encoder_create.argtypes = [ctypes.POINTER(b200enc.GpuContext), ctypes.c_uint32, ctypes.c_uint32,
+                                        ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int]
+    enc.h264_encoder_encode_frame_ext.argtypes = [ctypes.c_void_p, ctypes.POINTER(b200enc.GpuContext),
+                                                  b200enc.GpuImage, b200enc.GpuMemory, ctypes.c_void_p,
+                                                  ctypes.c_size_t]
+    NP = 30
+    pinned = [[(torch.from_numpy(np.ascontiguousarray(y)).pin_memory(),
+                torch.from_numpy(np.ascontiguousarray(uv)).pin_memory()) for (y, uv) in fr[:NP]]
+              for fr in host_frames[:S]]
+    ctxs, encs, imgs, outs = [], [], [], []
+    for s in range(S):
+        c = b200enc.GpuContext()
+        assert enc.bc250_gpu_init(ctypes.byref(c)) == 0
+        e = enc.h264_encoder_create(ctypes.byref(c), W, H, 30, 8_000_000, profile)
+        assert e
+        enc.h264_encoder_set_gop_size(ctypes.c_void_p(e), ctypes.c_uint32(GOP))
+        img, mem = b200enc.GpuImage(), b200enc.GpuMemory()
+        assert L.gpu_compute_create_image(ctypes.byref(c), W, H, 0, ctypes.byref(img), ctypes.byref(mem)) == 0
+        ctxs.append(c)
+        encs.append(e)
+        imgs.append((img, mem))
+        outs.append(np.zeros(W * H * 4, np.uint8))
+    bits = [0] * S
+    errors = []
+    gate = threading.Barrier(S + 1)
+
+    def one(s, k):
+        py, puv = pinned[s][k % NP]
+        img, mem = imgs[s]
+        c = ctypes.byref(ctxs[s])
+        if L.gpu_compute_upload_nv12(c, ctypes.byref(img), mem, ctypes.c_void_p(py.data_ptr()), W,
+                                     ctypes.c_void_p(puv.data_ptr()), W, W, H) != 0:
+            raise RuntimeError("upload failed")
+        n = enc.h264_encoder_encode_frame_ext(ctypes.c_void_p(encs[s]), c, img, mem,
+                                              ctypes.c_void_p(outs[s].ctypes.data), outs[s].nbytes)
+        if n <= 0:
+            raise RuntimeError(f"encoder returned {n}")
+        return n
+
+    def worker(s):
+        try:
+            k = 0
+            for _ in range(gop_phase(s, S) + warmup):
+                one(s, k)
+                k += 1
+            gate.wait()
+            for _ in range(steps):
+                bits[s] += 8 * one(s, k)
+                k += 1
+            gate.wait()
+        except Exception as exc:  # noqa: BLE001 - reported in the JSON line
+            errors.append(repr(exc))
+            gate.abort()
+
+    th = [threading.Thread(target=worker, args=(s,)) for s in range(S)]
+    for t in th:
+        t.start()
+    try:
+        gate.wait()
+        t0 = time.perf_counter()
+        gate.wait()
+        wall = time.perf_counter() - t0
+    except threading.BrokenBarrierError:
+        wall = None
+    for t in th:
+        t.join()
+    for s in range(S):
+        enc.h264_encoder_destroy(ctypes.c_void_p(encs[s]))
+        L.gpu_compute_destroy_image(ctypes.byref(ctxs[s]), *imgs[s])
+        L.bc250_gpu_destroy(ctypes.byref(ctxs[s]))
+    for k in ("B200ENC_ME", "B200ENC_SEARCH_RANGE"):
+        os.environ.pop(k, None)
+    if errors or not wall:
+        return {"unavailable": "; ".join(errors) or "no timing"}
+    return {"value": round(S * steps / wall, 2), "unit": "frames/s", "streams": S, "frames_per_stream": steps,
+            "entropy": "CAVLC" if profile == 66 else "CABAC", "slices_per_frame": 4, "host_threads_per_stream": 4,
+            "host_cores": os.cpu_count(), "mbit_per_frame": round(sum(bits) / (S * steps) / 1e6, 4),
+            "timing": "wall clock, upload + encode_frame_ext per frame, all streams in parallel threads"}
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -285,30 +450,31 @@ def run_gpu(args):
         return group.max(ms)
 
     host_ms = {}
+    frame_kinds = {}
 
     def arm(mode, nstreams, steps, warmup, perf=False, clocks=False):
         """Encodes warmup + steps frames on each of the first nstreams
-        contexts from the start of a GOP; returns (ms, launches, perf, clk)."""
+        contexts (the first warm-up step an IDR on every stream, then the
+        streams' GOP phases); returns (ms, launches, perf, clk)."""
         for c in ctxs[:nstreams]:
             c.set_me(mode, conf=args.conf)
             c.perf(False)
-        t = 0
+        sched = GopSchedule(nstreams)
+        kinds = {"i": 0, "p_full": 0, "p_learned": 0}
 
-        def one_step(t):
+        def one_step(t, count):
             n = 0
-            intra = (t % GOP) == 0
             for s in range(nstreams):
-                ctxs[s].encode_device(dev[s][t % NFRAMES], W, H, QP, intra, 1, False)
-            if intra:
-                n = LAUNCHES["i"]
-            elif mode == 0 or (t % GOP) == 1:
-                n = LAUNCHES["p_full"]
-            else:
-                n = LAUNCHES["p_learned"]
-            return n * nstreams
+                k = sched.kind(s, t, mode != 0)
+                ctxs[s].encode_device(dev[s][t % NFRAMES], W, H, QP, k == "i", 1, False)
+                n += LAUNCHES[k]
+                if count:
+                    kinds[k] += 1
+            return n
 
+        t = 0
         for _ in range(warmup):
-            one_step(t)
+            one_step(t, False)
             t += 1
         barrier()
         if perf:
@@ -322,7 +488,7 @@ def run_gpu(args):
         launches = 0
         h0 = time.perf_counter()
         for _ in range(steps):
-            launches += one_step(t)
+            launches += one_step(t, True)
             t += 1
         host_issue_s = time.perf_counter() - h0  # host time to enqueue the timed steps
         for st in streams[:nstreams]:
@@ -334,6 +500,7 @@ def run_gpu(args):
         c = clk.stop() if clk else None
         pf = (ctxs[0].perf_read(False), ctxs[0].perf_read(True)) if perf else None
         host_ms[mode, nstreams] = 1000.0 * host_issue_s / steps
+        frame_kinds[mode, nstreams] = kinds
         return max_over_ranks(e0.elapsed_time(e1)), launches, pf, c
 
     K, Wm = args.steps, args.warmup
@@ -344,6 +511,8 @@ def run_gpu(args):
     ms_l1, _, perf_l1, _ = arm(LEARNED, 1, k1, Wm, perf=True)
     me_counts = ctxs[0].me_stats()  # the learned form's last P frame
     ms_p1, _, perf_p1, _ = arm(0, 1, k1, Wm, perf=True)
+    mvf = ctxs[0].mv_field()  # the plain form's last P frame: early-outs are MV 0 with SAD <= 512
+    searched = int(MBS - np.count_nonzero((mvf[:, 0] == 0) & (mvf[:, 1] == 0) & (mvf[:, 2].view(np.uint32) <= 512)))
     fps = replicas.aggregate_rate(ws, S * K, ms_l)
     fps_plain = replicas.aggregate_rate(ws, S * K, ms_p)
     fps_bf16 = replicas.aggregate_rate(ws, S * K, ms_b)
@@ -356,6 +525,7 @@ def run_gpu(args):
     imgs = [c.create_image(W, H) for c in ctxs]
     for c in ctxs:
         c.set_me(LEARNED, conf=args.conf)
+    esched = GopSchedule(S)
 
     # Double-buffered, as the boundary's two staging slots allow: step k+1 is
     # uploaded and submitted before step k's staged results are read, so each
@@ -370,7 +540,7 @@ def run_gpu(args):
                                              b200enc.ctypes.c_void_p(py.data_ptr()), W,
                                              b200enc.ctypes.c_void_p(puv.data_ptr()), W, W, H)
             assert rc == 0
-            slots.append(c.encode(img, W, H, QP, (k % GOP) == 0, 1, 0, None))
+            slots.append(c.encode(img, W, H, QP, esched.kind(s, k, True) == "i", 1, 0, None))
         return slots
 
     def e2e_collect(slots):
@@ -401,46 +571,61 @@ def run_gpu(args):
     e2e_fps = replicas.aggregate_rate(ws, S * K, max_over_ranks(s0.elapsed_time(s1)))
     for c, (img, mem) in zip(ctxs, imgs):
         c.destroy_image(img, mem)
+    for c in ctxs:
+        c.close()
+
+    # ---- full encode through the reference host encoder ---------------------
+    fe = {}
+    if not args.no_full_encode:
+        fe["learned_cavlc"] = full_encode(args, host_frames, S, K, Wm, 66, "learned_fp8")
+        fe["learned_cabac"] = full_encode(args, host_frames, S, K, Wm, 77, "learned_fp8")
+        fe["plain_cavlc"] = full_encode(args, host_frames, S, K, Wm, 66, "full")
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
         pp1, pi1 = perf_l1
         nP = max(1, pp1["frames"])
         stage_ms = {k2: pp1[k2] / nP for k2 in ("me", "chain", "deblock", "staging")}
+        nI = max(1, pi1["frames"])
+        intra_ms = {"intra": pi1["chain"] / nI, "deblock": pi1["deblock"] / nI}
         plain_stage_ms = {k2: perf_p1[0][k2] / max(1, perf_p1[0]["frames"]) for k2 in ("me", "chain", "deblock")}
         dom = max(("me", "chain", "deblock"), key=lambda k2: stage_ms[k2])
         algo = ALGO_BYTES_PER_MB[dom] * MBS
         ach = algo / (stage_ms[dom] / 1000.0) / 1e9
         tr = traffic_from_profiles(dom)
         pipe_bytes = (ALGO_BYTES_PER_MB["me"] + ALGO_BYTES_PER_MB["chain"] + ALGO_BYTES_PER_MB["deblock"]) * MBS
+        me_abs = ME_ABSDIFF_PER_MB * searched
         line = {
-            "metric": "1080p encode fps, learned-proposal form (vs plain full-search form)", "value": round(fps, 2),
+            "metric": METRIC, "value": round(fps, 2),
             "unit": "frames/s", "n_gpus": ws, "steps": K, "warmup": Wm,
             "ms_per_step": round(ms_l / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u8/int32 (integer path), fp8 e4m3 (proposal network inference; trained in bf16)",
             "data": "synthetic (seeded generator: gradients, sigma-8 texture, 6 moving rectangles, pan, noise patch)",
-            "config": {"workload": f"{WORKLOAD}_x{S}_streams", "streams_per_gpu": S, "width": W, "height": H,
-                       "qp": QP, "search_range": RANGE, "lambda": LAMBDA, "gop": GOP, "deblock": True,
-                       "recon_clamp": "coded", "proposal_conf": args.conf,
-                       "l2": f"each stream cycles {NFRAMES} resident frames ({S * NFRAMES * W * H * 3 // 2 >> 20} MiB "
-                             "> L2)",
-                       "parallelism": f"replicas x{ws} (independent streams per GPU)"},
-            "plain": {"value": round(fps_plain, 2), "unit": "frames/s", "ms_per_step": round(ms_p / K, 4)},
+            "config": bench_config(S, args.conf),
+            "timed_frames": frame_kinds[LEARNED, S],
+            "plain": {"value": round(fps_plain, 2), "unit": "frames/s", "ms_per_step": round(ms_p / K, 4),
+                      "timed_frames": frame_kinds[0, S]},
             "speedup_vs_plain": round(fps / fps_plain, 3),
             "learned_bf16": {"value": round(fps_bf16, 2), "unit": "frames/s", "ms_per_step": round(ms_b / K, 4),
                              "speedup_vs_plain": round(fps_bf16 / fps_plain, 3),
                              "note": "the same learned form with the network's inference in BF16 (set_me mode 1)"},
-            "host_issue_ms_per_step": {"learned": round(host_ms[1, S], 4), "plain": round(host_ms[0, S], 4),
+            "host_issue_ms_per_step": {"learned": round(host_ms[LEARNED, S], 4), "plain": round(host_ms[0, S], 4),
                                        "note": "host time to enqueue one step (all streams); compare ms_per_step"},
             "single_stream": {"learned_fps": round(k1 / (ms_l1 / 1000.0), 2),
-                              "plain_fps": round(k1 / (ms_p1 / 1000.0), 2),
+                              "plain_fps": round(k1 / (ms_p1 / 1000.0), 2), "frames": k1,
                               "learned_stage_ms_per_p_frame": {k2: round(v, 4) for k2, v in stage_ms.items()},
                               "plain_stage_ms_per_p_frame": {k2: round(v, 4) for k2, v in plain_stage_ms.items()},
+                              "stage_ms_per_i_frame": {k2: round(v, 4) for k2, v in intra_ms.items()},
                               "last_p_frame_mbs": dict(zip(("learned", "fallback", "early"), me_counts))},
+            "me_int": {"value": round(me_abs / (plain_stage_ms["me"] / 1000.0), 1), "unit": "abs-diff/s",
+                       "searched_mbs": searched,
+                       "note": f"plain full search, one stream: ({2 * RANGE + 1}^2 + 16) x 256 abs-diffs per searched "
+                               "MB (zero-MV early-outs of the last P frame excluded) / ME stage time"},
             "bd_rate": rd_record(),
             "gpu_launches": launches,
             "e2e": {"value": round(e2e_fps, 2), "unit": "frames/s", "h2d_bytes_per_step": S * H2D_PER_STEP,
                     "d2h_bytes_per_step": S * D2H_PER_STEP},
+            "full_encode": fe or None,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(ach / peak, 5), "peak_kind": peak_kind,
                          "traffic": (round(tr * MBS) if tr is not None else None),
@@ -457,8 +642,6 @@ def run_gpu(args):
                                     "kind": info["kind"], "sample": info["sample"],
                                     "stage_s": {k2: round(v, 4) for k2, v in info["stage_s"].items()}}
         print(json.dumps(line), flush=True)
-    for c in ctxs:
-        c.close()
     group.close()
 
 
@@ -525,6 +708,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-full-encode", action="store_true", help="skip the full-encode figure (host entropy coding)")
     ap.add_argument("--streams", type=int, default=8)
     ap.add_argument("--conf", type=float, default=0.9)
     ap.add_argument("--hevc-deblock", action="store_true",

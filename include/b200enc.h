@@ -143,8 +143,10 @@ int b200enc_deblock_launch(int mbw, int mbh, int qp, int is_intra, const uint32_
  * the caller still passes the planes, nz and MVs.
  *   - Limit: mbh <= 512 macroblock rows (frames up to 8192 lines); larger
  *     frames return -2 with a message on stderr. Bad arguments return -1.
- *   - The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress, with that device current); make that first call
+ *   - The first call in each CUDA context (the device's primary context for
+ *     runtime-API callers; a new one after cudaDeviceReset) looks up the
+ *     array's device address (cudaGetSymbolAddress, with that device
+ *     current) and caches it under the context's ID; make that first call
  *     before any stream capture.
  *   - Every call on a device shares the one array and zeroes the part it
  *     uses on `stream` before launching: calls whose work overlaps on the GPU

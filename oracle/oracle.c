@@ -11,6 +11,8 @@
  */
 #include "oracle.h"
 
+#include <omp.h>
+#include <stddef.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -368,6 +370,31 @@ uint32_t orc_me_rect_key(const orc_frame_t *f, const orc_me_params_t *p, const u
     return best_key;
 }
 
+/* Edge-replicated copy of the reference luma: sample (x, y) of the copy at
+ * pad[(y + P) * pp + x + P] equals refY(ref, rp, RW, RH, x, y) for every x in
+ * [-P, RW+P), y in [-P, RH+P), so the search reads it without clamps. */
+static uint8_t *pad_ref(const orc_frame_t *f, const uint8_t *ref_y, int rp, int P, int *pp)
+{
+    const int pw = f->RW + 2 * P, ph = f->RH + 2 * P;
+    uint8_t *pad = (uint8_t *)malloc((size_t)pw * ph);
+    if (!pad) return NULL;
+    for (int y = 0; y < ph; y++)
+        for (int x = 0; x < pw; x++) pad[(size_t)y * pw + x] = (uint8_t)refY(ref_y, rp, f->RW, f->RH, x - P, y - P);
+    *pp = pw;
+    return pad;
+}
+
+/* SAD of the 16x16 block cur (contiguous rows) against r (pitch rp). */
+static inline uint32_t sad16_u8(const uint8_t *cur, const uint8_t *r, int rp)
+{
+    uint32_t s = 0;
+    for (int y = 0; y < 16; y++) {
+        const uint8_t *a = cur + 16 * y, *b = r + (size_t)y * rp;
+        for (int x = 0; x < 16; x++) s += (uint32_t)iabs((int)a[x] - (int)b[x]);
+    }
+    return s;
+}
+
 void orc_me_frame(const orc_frame_t *f, const orc_me_params_t *p,
                   const uint8_t *cur_y, int cp, const uint8_t *ref_y, int rp, orc_mv_t *mv)
 {
@@ -381,18 +408,25 @@ void orc_me_frame(const orc_frame_t *f, const orc_me_params_t *p,
      *   3. Eight half-pel offsets around the winner, exact 6-tap SAD, strict
      *      improvement over the winner's integer SAD, in :395-398 order.
      *   4. Eight quarter-pel offsets around that, same rule (:435-438).
+     * Reference samples are read clamped to (RW, RH) (refY); steps 1-2 read
+     * them from an edge-replicated copy, which holds the same values, and the
+     * macroblock rows run in parallel (each MB is independent).
      */
-    const int R = p->range, side = 2 * R + 1;
-    int cur[256];
-    for (int mby = 0; mby < f->mbh; mby++)
+    const int R = p->range, side = 2 * R + 1, P = R + 16;
+    int pp = 0;
+    uint8_t *pad = pad_ref(f, ref_y, rp, P, &pp);
+    if (!pad) return;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int mby = 0; mby < f->mbh; mby++) {
+        int cur[256];
+        uint8_t cur8[256];
         for (int mbx = 0; mbx < f->mbw; mbx++) {
             const int X = mbx * 16, Y = mby * 16;
             orc_mv_t *o = &mv[mby * f->mbw + mbx];
             load_cur_mb(f, cur_y, cp, mbx, mby, cur);
-            uint32_t sad0 = 0;
-            for (int y = 0; y < 16; y++)
-                for (int x = 0; x < 16; x++)
-                    sad0 += (uint32_t)iabs(cur[y * 16 + x] - refY(ref_y, rp, f->RW, f->RH, X + x, Y + y));
+            for (int i = 0; i < 256; i++) cur8[i] = (uint8_t)cur[i];
+            const uint8_t *at = pad + (size_t)(Y + P) * pp + (X + P);
+            const uint32_t sad0 = sad16_u8(cur8, at, pp);
             if (p->zero_thresh >= 0 && sad0 <= (uint32_t)p->zero_thresh) {
                 o->mvx = o->mvy = 0;
                 o->sad = sad0;
@@ -402,10 +436,7 @@ void orc_me_frame(const orc_frame_t *f, const orc_me_params_t *p,
             uint32_t best_key = 0xffffffffu, best_sad = 0;
             for (int dy = -R; dy <= R; dy++)
                 for (int dx = -R; dx <= R; dx++) {
-                    uint32_t s = 0;
-                    for (int y = 0; y < 16; y++)
-                        for (int x = 0; x < 16; x++)
-                            s += (uint32_t)iabs(cur[y * 16 + x] - refY(ref_y, rp, f->RW, f->RH, X + x + dx, Y + y + dy));
+                    const uint32_t s = sad16_u8(cur8, at + (ptrdiff_t)dy * pp + dx, pp);
                     uint32_t cost = s + (uint32_t)p->lambda * (uint32_t)(iabs(dx) + iabs(dy));
                     uint32_t key = (cost << 14) | (uint32_t)((dy + R) * side + (dx + R));
                     if (key < best_key) { best_key = key; best_sad = s; }
@@ -413,6 +444,8 @@ void orc_me_frame(const orc_frame_t *f, const orc_me_params_t *p,
             int idx = (int)(best_key & 0x3fff);
             orc_me_refine(f, cur_y, cp, ref_y, rp, mbx, mby, idx % side - R, idx / side - R, best_sad, o);
         }
+    }
+    free(pad);
 }
 
 /* ------------------------------------------------------- P-frame chain */
@@ -480,7 +513,10 @@ void orc_p_frame(const orc_frame_t *f,
     /* A1/shaders/residual_predict.comp:417-434 (luma MC), :576-635 (chroma
      * MC), dct_transform.comp:75-98, quantize.comp:189-225 (inter f = 1/6),
      * reconstruct.comp:318-442 (P luma has no DC split, :358-363). */
+    /* Macroblocks are independent (each reads the reference and writes only
+     * its own outputs and reconstruction): the rows run in parallel. */
     const int qp = f->qp, qpc = orc_chroma_qp(qp);
+#pragma omp parallel for schedule(dynamic, 1)
     for (int mby = 0; mby < f->mbh; mby++)
         for (int mbx = 0; mbx < f->mbw; mbx++) {
             const int mb = mby * f->mbw + mbx, X = mbx * 16, Y = mby * 16, Xc = X / 2, Yc = Y / 2;
@@ -861,4 +897,10 @@ void orc_encode_frame(const orc_frame_t *f, const orc_me_params_t *p, int is_int
         orc_p_frame(f, cur_y, cur_uv, cp, ref_y, ref_uv, rfp, out->mv, out, rec_y, rec_uv, rp);
     }
     if (deblock) orc_deblock_frame(f->mbw, f->mbh, f->qp, is_intra, out->nz, out->mv, rec_y, rec_uv, rp);
+}
+
+/* Threads the parallel loops above may use (OpenMP); 0 leaves the default. */
+void orc_set_threads(int n)
+{
+    if (n > 0) omp_set_num_threads(n);
 }

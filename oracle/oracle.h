@@ -147,7 +147,11 @@ void orc_encode_frame(const orc_frame_t *f, const orc_me_params_t *p, int is_int
                       const uint8_t *ref_y, const uint8_t *ref_uv, int ref_pitch,
                       orc_out_t *out, uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch);
 
+/* Threads for the oracle's parallel loops (full search, P chain). */
+void orc_set_threads(int n);
+
 #ifdef __cplusplus
 }
 #endif
+
 #endif

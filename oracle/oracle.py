@@ -38,7 +38,7 @@ class Out(ctypes.Structure):
 
 def build():
     """Compiles liboracle.so and, where the reference sources exist, _ref/."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    subprocess.run([os.path.join(HERE, "build.sh")], check=True)
 
 
 _lib = None
@@ -138,6 +138,11 @@ def i_frame_steps(f, cur_y, cur_uv, rec_y, rec_uv, order):
     if rc != 0:
         raise ValueError("macroblock outside the picture")
     return o
+
+
+def set_threads(n):
+    """Threads of the oracle's parallel loops (full search, P chain)."""
+    lib().orc_set_threads(int(n))
 
 
 def deblock(mbw, mbh, qp, is_intra, nz, mv, rec_y, rec_uv):

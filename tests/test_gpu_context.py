@@ -12,15 +12,17 @@ def _pad(a, rows, cols):
 
 
 def _run(gpu, oracle_mod, W, H, frames, qp, rng, me_mode=0, deblock=1, num_slices=1, coded_clamp=True,
-         gop=None, cpu_mv_frames=()):
+         gop=None, cpu_mv_frames=(), seq=None, lam=None):
     from b200enc import synth
-    seq = synth.Sequence(W, H, seed=11, pan=W >= 640, noise_patch=W >= 1280)
+    if seq is None:
+        seq = synth.Sequence(W, H, seed=11, pan=W >= 640, noise_patch=W >= 1280)
     ctx = gpu.Context()
-    ctx.configure(search_range=rng, coded_clamp=coded_clamp, deblock=deblock)
+    ctx.configure(search_range=rng, lam=-1 if lam is None else lam, coded_clamp=coded_clamp, deblock=deblock)
     img, mem = ctx.create_image(W, H)
     CW, CH = gpu.coded(W, H)
     f = oracle_mod.frame(W, H, qp, num_slices=num_slices, coded_clamp=coded_clamp)
-    lam = 8 if me_mode == 1 else 5
+    if lam is None:
+        lam = 8 if me_mode == 1 else 5
     ref_y = ref_uv = None
     for t in range(frames):
         y, uv = seq.frame(t)
@@ -72,3 +74,83 @@ def test_cpu_mvs_replace_me(gpu, oracle_mod):
 
 def test_ippp_1080p(gpu, oracle_mod):
     _run(gpu, oracle_mod, 1920, 1080, 3, 27, 16)
+
+
+# ---- the benchmarked configuration and the workload configurations -------
+# bench.py times 1920x1080 IPPP at search range 32, lambda 5, spec deblocking
+# on, reads clamped at the coded size, at QP 27 (a point of the 22/27/32/37
+# sweep of the 1080p workload), on the seeded 1080p generator (pan + noise
+# patch). These run that exact frame sequence through gpu_compute_* and
+# compare every staged output and the reconstruction with the oracle's.
+
+@pytest.mark.parametrize("qp", [22, 27, 32, 37])
+def test_bench_config_1080p_r32_sequence(gpu, oracle_mod, qp):
+    from b200enc import synth
+    _run(gpu, oracle_mod, 1920, 1080, 8, qp, 32, lam=5, seq=synth.workload("h264_1080p", seed=0, stream=qp))
+
+
+def test_bench_config_1080p_r32_gop_refresh(gpu, oracle_mod):
+    """An IDR refresh inside the sequence (I P P P I P P), as the timed region
+    of the bench holds one per stream and GOP."""
+    from b200enc import synth
+    _run(gpu, oracle_mod, 1920, 1080, 7, 27, 32, lam=5, gop=4, seq=synth.workload("h264_1080p", seed=0, stream=0))
+
+
+def test_workload_640x480_30_frames(gpu, oracle_mod):
+    """The 640x480 workload at its stated length: 30 frames IPPP, QP 26,
+    search range 16 with the quarter-pel refine."""
+    from b200enc import synth
+    _run(gpu, oracle_mod, 640, 480, 30, 26, 16, lam=5, seq=synth.workload("h264_640x480", seed=0, stream=0))
+
+
+@pytest.mark.parametrize("mode", [3, 1])
+def test_learned_form_bench_config_chain_exact(gpu, oracle_mod, mode):
+    """The learned form (mode 3: network in FP8, the bench's headline form;
+    mode 1: BF16) at the bench configuration. Its motion vectors differ from
+    the full search's by design (that difference is the BD-rate test's
+    subject); everything after motion estimation must not: given the MVs the
+    learned form chose, the levels, DC, nonzero masks, prediction modes and
+    the deblocked reconstruction equal the oracle's P chain and deblocking
+    bit for bit, frame after frame, each frame predicted from the previous
+    reconstruction."""
+    from b200enc import synth
+    W, H, qp, R = 1920, 1080, 27, 32
+    seq = synth.workload("h264_1080p", seed=0, stream=5)
+    ctx = gpu.Context()
+    ctx.configure(search_range=R, lam=5, zero_thresh=512, coded_clamp=True, deblock=1)
+    ctx.set_me(mode)
+    img, mem = ctx.create_image(W, H)
+    CW, CH = gpu.coded(W, H)
+    f = oracle_mod.frame(W, H, qp)
+    ref_y = ref_uv = None
+    learned_frames = 0
+    for t in range(8):
+        y, uv = seq.frame(t)
+        intra = t == 0
+        ctx.upload(img, mem, y, uv)
+        slot = ctx.encode(img, W, H, qp, intra)
+        assert ctx.sync(slot) == 0
+        got = ctx.staging(slot)
+        rec_y = np.zeros((CH, CW), np.uint8)
+        rec_uv = np.zeros((CH // 2, CW), np.uint8)
+        if intra:
+            ref_y, ref_uv = _pad(y, CH, CW), _pad(uv, CH // 2, CW)
+            want = oracle_mod.encode_frame(f, R, 5, 512, True, 1, y, uv, ref_y, ref_uv, rec_y, rec_uv)
+            np.testing.assert_array_equal(got["mv"], want["mv"], err_msg=f"frame {t} mv")
+        else:
+            mvs = np.ascontiguousarray(got["mv"]).astype(np.int32).reshape(-1, 4)
+            want = oracle_mod.p_frame(f, y, uv, ref_y, ref_uv, mvs, rec_y, rec_uv)
+            oracle_mod.deblock(f.mbw, f.mbh, qp, 0, want["nz"], want["mv"], rec_y, rec_uv)
+            if t >= 2:
+                learned, fallback, early = ctx.me_stats()
+                assert learned > 0, f"frame {t}: no macroblock took the learned path"
+                learned_frames += 1
+        for k in ("levels", "dc", "nz", "pred_mode"):
+            np.testing.assert_array_equal(got[k], want[k], err_msg=f"frame {t} {k}")
+        gy, guv = ctx.recon_host()
+        np.testing.assert_array_equal(gy, rec_y, err_msg=f"frame {t} recon Y")
+        np.testing.assert_array_equal(guv, rec_uv, err_msg=f"frame {t} recon UV")
+        ref_y, ref_uv = rec_y, rec_uv
+    assert learned_frames == 6
+    ctx.destroy_image(img, mem)
+    ctx.close()

@@ -24,12 +24,14 @@ ENC_SO = os.path.join(ROOT, "oracle", "_ref", "libh264enc_b200.so")
 DEC = os.path.join(ROOT, "oracle", "_ref", "h264dec")
 
 
-def _encode(gpu, W, H, frames, qp, profile, slices, gop, tmp_path, seed=3):
+def _encode(gpu, W, H, frames, qp, profile, slices, gop, tmp_path, seed=3, search_range=16, me="full", seq=None):
     from b200enc import synth
     os.environ["BC250_FORCE_QP"] = str(qp)
     os.environ["BC250_FORCE_TIER"] = "0"
     os.environ["BC250_SLICES_PER_FRAME"] = str(slices)
     os.environ["BC250_FORCE_SLICES"] = "0"
+    os.environ["B200ENC_SEARCH_RANGE"] = str(search_range)  # read by bc250_gpu_init
+    os.environ["B200ENC_ME"] = me
     enc = ctypes.CDLL(ENC_SO)
     L = gpu.lib()
     ctx = gpu.GpuContext()
@@ -44,7 +46,8 @@ def _encode(gpu, W, H, frames, qp, profile, slices, gop, tmp_path, seed=3):
                                                   gpu.GpuMemory, ctypes.c_void_p, ctypes.c_size_t]
     img, mem = gpu.GpuImage(), gpu.GpuMemory()
     assert L.gpu_compute_create_image(ctypes.byref(ctx), W, H, 0, ctypes.byref(img), ctypes.byref(mem)) == 0
-    seq = synth.Sequence(W, H, seed=seed, pan=True)
+    if seq is None:
+        seq = synth.Sequence(W, H, seed=seed, pan=True)
     out = np.zeros(W * H * 4, np.uint8)
     stream, recons = bytearray(), []
     for t in range(frames):
@@ -96,6 +99,33 @@ def _decode(path, W, H, n):
 def test_reference_encoder_roundtrip(gpu, tmp_path, W, H, qp, profile, slices, gop, frames):
     path, recons = _encode(gpu, W, H, frames, qp, profile, slices, gop, tmp_path)
     dec = _decode(path, W, H, frames)
+    for t, ((ry, ruv), (dy, du, dv)) in enumerate(zip(recons, dec)):
+        np.testing.assert_array_equal(dy, ry, err_msg=f"frame {t}: decoded luma != GPU reconstruction")
+        np.testing.assert_array_equal(du, ruv[:, 0::2], err_msg=f"frame {t}: decoded Cb != GPU reconstruction")
+        np.testing.assert_array_equal(dv, ruv[:, 1::2], err_msg=f"frame {t}: decoded Cr != GPU reconstruction")
+
+
+@pytest.mark.skipif(not (os.path.exists(ENC_SO) and os.path.exists(DEC)), reason="reference integration not built")
+@pytest.mark.parametrize("qp,profile,me", [
+    (27, 66, "full"),          # Baseline (CAVLC), the bench's QP
+    (27, 77, "full"),          # Main (CABAC)
+    (22, 77, "learned_fp8"),   # the learned form (network in FP8), CABAC
+    (37, 66, "learned_fp8"),   # the learned form, CAVLC, coarse QP
+])
+def test_reference_encoder_roundtrip_1080p_r32(gpu, tmp_path, qp, profile, me):
+    """1920x1080 at the bench's search range 32 on the bench's generator:
+    the reference host encoder's stream, decoded by the reference decoder,
+    equals the GPU's reconstruction in every frame (I plus 7 P frames, the
+    learned form's candidates taking over from the third frame)."""
+    from b200enc import synth
+    W, H, n = 1920, 1080, 8
+    seq = synth.workload("h264_1080p", seed=0, stream=qp)
+    try:
+        path, recons = _encode(gpu, W, H, n, qp, profile, 1, 60, tmp_path, search_range=32, me=me, seq=seq)
+    finally:
+        os.environ.pop("B200ENC_ME", None)
+        os.environ.pop("B200ENC_SEARCH_RANGE", None)
+    dec = _decode(path, W, H, n)
     for t, ((ry, ruv), (dy, du, dv)) in enumerate(zip(recons, dec)):
         np.testing.assert_array_equal(dy, ry, err_msg=f"frame {t}: decoded luma != GPU reconstruction")
         np.testing.assert_array_equal(du, ruv[:, 0::2], err_msg=f"frame {t}: decoded Cb != GPU reconstruction")
