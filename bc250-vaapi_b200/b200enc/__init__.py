@@ -25,7 +25,8 @@ EXPORTS = [
     "b200enc_ctx_set_me", "b200enc_ctx_me_stats",
     "b200enc_hevc_transform_quant_4x4", "b200enc_hevc_dequant_itransform_4x4", "b200enc_hevc_transform_quant_8x8",
     "b200enc_hevc_dequant_itransform_8x8", "b200enc_hevc_build_hpel", "b200enc_hevc_motion_search",
-    "b200enc_hevc_choose_luma_mode", "b200enc_hevc_deblock",
+    "b200enc_hevc_choose_luma_mode", "b200enc_hevc_deblock", "b200enc_hevc_build_hpel_10",
+    "b200enc_hevc_motion_search_10", "b200enc_hevc_choose_luma_mode_10",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
     "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",
@@ -112,6 +113,10 @@ def load_library(path=LIB_PATH):
     lib.b200enc_hevc_build_hpel.argtypes = [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp]
     lib.b200enc_hevc_motion_search.argtypes = [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _i, _vp, _vp]
     lib.b200enc_hevc_choose_luma_mode.argtypes = [_vp, _i, _vp, _i, _i, _i, _vp, _i, _vp, _vp, _vp]
+    lib.b200enc_hevc_build_hpel_10.argtypes = [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp]
+    lib.b200enc_hevc_motion_search_10.argtypes = [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _i, _vp,
+                                                  _vp]
+    lib.b200enc_hevc_choose_luma_mode_10.argtypes = [_vp, _i, _vp, _i, _i, _i, _vp, _i, _vp, _vp, _vp]
     lib.b200enc_hevc_deblock.argtypes = [ctypes.POINTER(HevcDeblockParams), _vp]
     lib.b200enc_ctx_set_me.argtypes = [ctypes.POINTER(GpuContext), _i, ctypes.c_char_p, ctypes.c_float]
     return lib
@@ -286,12 +291,23 @@ def hevc_dequant_itransform_8x8(coeff, residual, qp, bit_depth=8, stream=None):
                                                      _stream(stream)), "hevc_dequant_itransform_8x8")
 
 
+def _ten_bit(t):
+    import torch
+    if t.dtype == torch.uint8:
+        return False
+    if t.dtype in (torch.int16, torch.uint16):
+        return True
+    raise TypeError(f"samples must be uint8 (8-bit) or 16-bit words (10-bit), not {t.dtype}")
+
+
 def hevc_build_hpel(recon, w, h, margin, planes, stream=None):
-    """recon: uint8 device tensor [>=h][pitch]; planes: uint8 device tensor
-    [4][h + 2*margin][pitch >= w + 2*margin] (I, H, V, HV)."""
-    _check(lib().b200enc_hevc_build_hpel(_p(recon), recon.stride(0), w, h, margin, _p(planes[0]), _p(planes[1]),
-                                         _p(planes[2]), _p(planes[3]), planes.stride(1), _stream(stream)),
-           "hevc_build_hpel")
+    """recon: device tensor [>=h][pitch], uint8 (8-bit) or int16/uint16
+    words holding 10-bit samples; planes: device tensor of the same type
+    [4][h + 2*margin][pitch >= w + 2*margin] (I, H, V, HV). Pitches are in
+    samples."""
+    fn = "b200enc_hevc_build_hpel_10" if _ten_bit(recon) else "b200enc_hevc_build_hpel"
+    _check(getattr(lib(), fn)(_p(recon), recon.stride(0), w, h, margin, _p(planes[0]), _p(planes[1]),
+                              _p(planes[2]), _p(planes[3]), planes.stride(1), _stream(stream)), fn)
 
 
 # b200enc_hevc_me_job_t / b200enc_hevc_me_result_t as numpy structured dtypes
@@ -307,17 +323,20 @@ def hevc_motion_search(src, w, h, planes, margin, qpel, jobs, results, stream=No
     jobs / results: uint8 device tensors holding HEVC_ME_JOB / HEVC_ME_RESULT
     records."""
     n = jobs.numel() // HEVC_ME_JOB.itemsize
-    _check(lib().b200enc_hevc_motion_search(_p(src), src.stride(0), w, h, _p(planes[0]), _p(planes[1]),
-                                            _p(planes[2]), _p(planes[3]), planes.stride(1), margin, int(qpel),
-                                            _p(jobs), n, _p(results), _stream(stream)), "hevc_motion_search")
+    fn = "b200enc_hevc_motion_search_10" if _ten_bit(src) else "b200enc_hevc_motion_search"
+    _check(getattr(lib(), fn)(_p(src), src.stride(0), w, h, _p(planes[0]), _p(planes[1]), _p(planes[2]),
+                              _p(planes[3]), planes.stride(1), margin, int(qpel), _p(jobs), n, _p(results),
+                              _stream(stream)), fn)
 
 
 def hevc_choose_luma_mode(src, recon, width, height, jobs, modes, preds, stream=None):
-    """src, recon: uint8 device tensors (pitch = stride(0)); jobs: int32
-    device tensor [n][3] (x0, y0, y_min); modes: int32 [n]; preds: uint8 [n][16]."""
-    _check(lib().b200enc_hevc_choose_luma_mode(_p(src), src.stride(0), _p(recon), recon.stride(0), width, height,
-                                               _p(jobs), jobs.shape[0], _p(modes), _p(preds), _stream(stream)),
-           "hevc_choose_luma_mode")
+    """src, recon: uint8 device tensors, or 16-bit words holding 10-bit
+    samples (pitch = stride(0), in samples); jobs: int32 device tensor
+    [n][3] (x0, y0, y_min); modes: int32 [n]; preds: [n][16] of the sample
+    type."""
+    fn = "b200enc_hevc_choose_luma_mode_10" if _ten_bit(src) else "b200enc_hevc_choose_luma_mode"
+    _check(getattr(lib(), fn)(_p(src), src.stride(0), _p(recon), recon.stride(0), width, height, _p(jobs),
+                              jobs.shape[0], _p(modes), _p(preds), _stream(stream)), fn)
 
 
 # b200enc_hevc_mvf_t / b200enc_hevc_slice_filter_t records and the

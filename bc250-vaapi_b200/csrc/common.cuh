@@ -139,44 +139,45 @@ __device__ __forceinline__ uint32_t slice_of(uint32_t mb, uint32_t total, uint32
 // ---------------------------------------------------------------------------
 // Quad (4-lane) transform block pipeline.
 //
-// Lane `r` of a quad owns row r of one 4x4 block. `sm` is that block's
-// 16-int shared scratch (raster). Functions leave results in registers;
-// callers fence with __syncwarp (every quad of a block sits in one warp).
+// Lane `r` of a quad (lanes 4q .. 4q+3 of a warp) owns row r of one 4x4
+// block. Rows become columns by a register transpose over the quad (two
+// shuffle stages), so no shared memory and no barrier is involved; every lane
+// of the warp must call these together.
 // ---------------------------------------------------------------------------
+
+// 4x4 transpose across the quad: on entry lane r holds row r (x[i] = M[r][i]),
+// on return column r (x[i] = M[i][r]). Stage 1 swaps the off-diagonal 2x2
+// blocks between lanes r and r^2, stage 2 the off-diagonal elements of each
+// 2x2 block between lanes r and r^1.
+__device__ __forceinline__ void quad_transpose(int x[4], int r) {
+  const unsigned full = 0xffffffffu;
+  const bool hi = (r & 2) != 0;
+  int s0 = hi ? x[0] : x[2], s1 = hi ? x[1] : x[3];
+  s0 = __shfl_xor_sync(full, s0, 2);
+  s1 = __shfl_xor_sync(full, s1, 2);
+  if (hi) { x[0] = s0; x[1] = s1; } else { x[2] = s0; x[3] = s1; }
+  const bool odd = (r & 1) != 0;
+  int t0 = odd ? x[0] : x[1], t1 = odd ? x[2] : x[3];
+  t0 = __shfl_xor_sync(full, t0, 1);
+  t1 = __shfl_xor_sync(full, t1, 1);
+  if (odd) { x[0] = t0; x[2] = t1; } else { x[1] = t0; x[3] = t1; }
+}
 
 // Forward 4x4 of the residual row x[0..3] held by lane r. Returns column r
 // of the coefficients: c[i] = coef[i][r]. Rows then columns, like
 // dct_transform.comp; the forward transform is exact so order is moot.
-__device__ __forceinline__ void quad_forward(int x[4], int r, int* sm) {
+__device__ __forceinline__ void quad_forward(int x[4], int r) {
   fwd4(x[0], x[1], x[2], x[3]);
-  sm[4 * r + 0] = x[0];
-  sm[4 * r + 1] = x[1];
-  sm[4 * r + 2] = x[2];
-  sm[4 * r + 3] = x[3];
-  __syncwarp();
-  x[0] = sm[r];
-  x[1] = sm[4 + r];
-  x[2] = sm[8 + r];
-  x[3] = sm[12 + r];
-  __syncwarp();
+  quad_transpose(x, r);
   fwd4(x[0], x[1], x[2], x[3]);
 }
 
 // Inverse 4x4 of the dequantized row d[0..3] (lane r holds row r, +32 already
 // on d[0][0]); returns column r of the residual: out[i] = res[i][r]
 // (reconstruct.comp:162-177: rows first, then columns, >>6).
-__device__ __forceinline__ void quad_inverse(int d[4], int r, int* sm) {
+__device__ __forceinline__ void quad_inverse(int d[4], int r) {
   inv4(d[0], d[1], d[2], d[3]);
-  sm[4 * r + 0] = d[0];
-  sm[4 * r + 1] = d[1];
-  sm[4 * r + 2] = d[2];
-  sm[4 * r + 3] = d[3];
-  __syncwarp();
-  d[0] = sm[r];
-  d[1] = sm[4 + r];
-  d[2] = sm[8 + r];
-  d[3] = sm[12 + r];
-  __syncwarp();
+  quad_transpose(d, r);
   inv4(d[0], d[1], d[2], d[3]);
   d[0] >>= 6;
   d[1] >>= 6;

@@ -4,6 +4,13 @@
 //       search (approach1-compute-encoder/src/hevc_enc_template.c:312-400,
 //       build_hpel / hpel_pass): the whole-sample plane and the H, V and HV
 //       planes of the 8-tap filter -1 4 -11 40 40 -11 4 -1, with a margin;
+//   H2  8x8 CU motion search on those planes (search_sad :463, motion_search
+//       :958);
+//   H3  4x4 intra luma mode choice (hevc_intra_template.c:177);
+//   H1-H3 at 8 bits and at 10 (Main10): the reference builds its template
+//       twice (encoder_h265.c:1220-1227, hevc_intra.c), changing only the
+//       sample type, the clip value, the no-neighbour fill and the search
+//       SAD's scaling to eight-bit units;
 //   H4  forward transform + quantisation of 4x4 (DCT-II or DST-VII) and 8x8
 //       (DCT-II) residual blocks at 8 or 10 bits (hevc_intra.c:468, :565, :720);
 //   H5  dequantisation + inverse transform of the same blocks
@@ -257,11 +264,14 @@ __global__ void __launch_bounds__(128) hevc_dqit8_kernel(const int16_t* __restri
 //   HV = clip((sum_k tap[k] * T(Y(k)) + 2048) >> 12),  T(y) = sum_j tap[j] * ref[y][X(j)]
 constexpr int kHpTileW = 32, kHpTileH = 8;
 
-__global__ void __launch_bounds__(256) hevc_hpel_kernel(const uint8_t* __restrict__ ref, int pitch, int w, int h,
-                                                        int M, uint8_t* __restrict__ pI, uint8_t* __restrict__ pH,
-                                                        uint8_t* __restrict__ pV, uint8_t* __restrict__ pHV,
-                                                        int opitch, int rows, int cols) {
-  __shared__ uint8_t src[kHpTileH + 7][kHpTileW + 8];
+// P: the sample type (uint8_t at 8 bits, uint16_t at 10); maxv the largest
+// sample value, (1 << BitDepth) - 1 (hevc_enc_template.c:23-25).
+template <typename P>
+__global__ void __launch_bounds__(256) hevc_hpel_kernel(const P* __restrict__ ref, int pitch, int w, int h, int M,
+                                                        P* __restrict__ pI, P* __restrict__ pH, P* __restrict__ pV,
+                                                        P* __restrict__ pHV, int opitch, int rows, int cols,
+                                                        int maxv) {
+  __shared__ P src[kHpTileH + 7][kHpTileW + 8];
   __shared__ int32_t tsum[kHpTileH + 7][kHpTileW];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int c0 = blockIdx.x * kHpTileW, r0 = blockIdx.y * kHpTileH;
@@ -274,7 +284,7 @@ __global__ void __launch_bounds__(256) hevc_hpel_kernel(const uint8_t* __restric
   __syncthreads();
   for (int i = threadIdx.x; i < (kHpTileH + 7) * kHpTileW; i += 256) {
     const int sr = i / kHpTileW, sc = i - sr * kHpTileW;
-    const uint8_t* p = &src[sr][sc];
+    const P* p = &src[sr][sc];
     tsum[sr][sc] = -p[0] + 4 * p[1] - 11 * p[2] + 40 * p[3] + 40 * p[4] - 11 * p[5] + 4 * p[6] - p[7];
   }
   __syncthreads();
@@ -283,24 +293,27 @@ __global__ void __launch_bounds__(256) hevc_hpel_kernel(const uint8_t* __restric
   const int sr = ty + 3, sc = tx + 3;  // the sample (r - M, c - M) in the staged tile
   const size_t o = (size_t)r * opitch + c;
   pI[o] = src[sr][sc];
-  pH[o] = (uint8_t)clip1((tsum[sr][tx] + 32) >> 6);
+  pH[o] = (P)clampi((tsum[sr][tx] + 32) >> 6, 0, maxv);
   const int v = -src[ty][sc] + 4 * src[ty + 1][sc] - 11 * src[ty + 2][sc] + 40 * src[ty + 3][sc] +
                 40 * src[ty + 4][sc] - 11 * src[ty + 5][sc] + 4 * src[ty + 6][sc] - src[ty + 7][sc];
-  pV[o] = (uint8_t)clip1((v + 32) >> 6);
+  pV[o] = (P)clampi((v + 32) >> 6, 0, maxv);
   const int hv = -tsum[ty][tx] + 4 * tsum[ty + 1][tx] - 11 * tsum[ty + 2][tx] + 40 * tsum[ty + 3][tx] +
                  40 * tsum[ty + 4][tx] - 11 * tsum[ty + 5][tx] + 4 * tsum[ty + 6][tx] - tsum[ty + 7][tx];
-  pHV[o] = (uint8_t)clip1((hv + 2048) >> 12);
+  pHV[o] = (P)clampi((hv + 2048) >> 12, 0, maxv);
 }
 
 // ---- 8x8 CU motion search -------------------------------------------------
 // One warp per CU job, the reference's walk (hevc_enc_template.c:958-1043)
 // step for step: every lane follows the same (uniform) control flow and the
 // SADs are warp reductions, lane l scoring row l/4, columns 2(l%4), +1.
+// Strides in samples. sad_shift brings a SAD back to eight-bit units (0 at
+// eight bits, 2 at ten: hevc_enc_template.c:484).
+template <typename P>
 struct HevcSearch {
-  const uint8_t* src;
+  const P* src;
   int src_pitch, w, h, M, qpel;
-  const uint8_t* plane[4];
-  int ppitch;
+  const P* plane[4];
+  int ppitch, sad_shift;
 };
 
 __device__ __forceinline__ int hevc_mvd_bits(int d) {
@@ -314,7 +327,8 @@ __device__ __forceinline__ int hevc_mvd_bits(int d) {
 // position (qx, qy) (search_sad, hevc_enc_template.c:463): positions are
 // clamped to the planes' margin; even/even reads one half-grid block, a
 // position odd in x, y or both averages (rounded) the two blocks beside it.
-__device__ __forceinline__ uint32_t hevc_search_sad(const HevcSearch& S, int cu_x, int cu_y, int qx, int qy,
+template <typename P>
+__device__ __forceinline__ uint32_t hevc_search_sad(const HevcSearch<P>& S, int cu_x, int cu_y, int qx, int qy,
                                                     int lane) {
   const int lo = -(S.M - 2) * 4;
   const int hx = (S.w - 8 + S.M - 2) * 4, hy = (S.h - 8 + S.M - 2) * 4;
@@ -337,10 +351,11 @@ __device__ __forceinline__ uint32_t hevc_search_sad(const HevcSearch& S, int cu_
     const int sv = S.src[(size_t)(cu_y + r) * S.src_pitch + cu_x + c + dc];
     sad += (uint32_t)abs(sv - v);
   }
-  return __reduce_add_sync(0xffffffffu, sad);
+  return __reduce_add_sync(0xffffffffu, sad) >> S.sad_shift;
 }
 
-__global__ void __launch_bounds__(128) hevc_me_kernel(HevcSearch S, const b200enc_hevc_me_job_t* __restrict__ jobs,
+template <typename P>
+__global__ void __launch_bounds__(128) hevc_me_kernel(HevcSearch<P> S, const b200enc_hevc_me_job_t* __restrict__ jobs,
                                                       int n, b200enc_hevc_me_result_t* __restrict__ out) {
   const int lane = threadIdx.x & 31;
   const int j = blockIdx.x * 4 + (threadIdx.x >> 5);
@@ -447,7 +462,7 @@ __device__ __forceinline__ bool hz_avail(int nx, int ny, int width, int height, 
 
 constexpr int kHModePlanar = 0, kHModeDc = 1, kHModeHor = 10, kHModeVer = 26;
 
-__device__ __forceinline__ void hpredict(const int* left, const int* top, int corner, int mode, int* pred) {
+__device__ __forceinline__ void hpredict(const int* left, const int* top, int corner, int mode, int maxv, int* pred) {
   if (mode == kHModePlanar) {
 #pragma unroll
     for (int y = 0; y < 4; ++y)
@@ -469,20 +484,23 @@ __device__ __forceinline__ void hpredict(const int* left, const int* top, int co
 #pragma unroll
       for (int x = 0; x < 4; ++x) pred[y * 4 + x] = left[y];
 #pragma unroll
-    for (int x = 0; x < 4; ++x) pred[x] = clip1(left[0] + ((top[x] - corner) >> 1));
+    for (int x = 0; x < 4; ++x) pred[x] = clampi(left[0] + ((top[x] - corner) >> 1), 0, maxv);
   } else {
 #pragma unroll
     for (int y = 0; y < 4; ++y)
 #pragma unroll
       for (int x = 0; x < 4; ++x) pred[y * 4 + x] = top[x];
 #pragma unroll
-    for (int y = 0; y < 4; ++y) pred[y * 4] = clip1(top[0] + ((left[y] - corner) >> 1));
+    for (int y = 0; y < 4; ++y) pred[y * 4] = clampi(top[0] + ((left[y] - corner) >> 1), 0, maxv);
   }
 }
 
-__global__ void hevc_intra4_kernel(const uint8_t* __restrict__ src, int src_pitch, const uint8_t* __restrict__ rec,
+// P: the sample type; bd the bit depth (8 or 10). Pitches in samples.
+template <typename P>
+__global__ void hevc_intra4_kernel(const P* __restrict__ src, int src_pitch, const P* __restrict__ rec,
                                    int rec_pitch, int width, int height, const int* __restrict__ jobs, int n,
-                                   int* __restrict__ modes, uint8_t* __restrict__ preds) {
+                                   int* __restrict__ modes, P* __restrict__ preds, int bd) {
+  const int maxv = (1 << bd) - 1;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const int x0 = jobs[3 * j], y0 = jobs[3 * j + 1], y_min = jobs[3 * j + 2];
@@ -518,7 +536,7 @@ __global__ void hevc_intra4_kernel(const uint8_t* __restrict__ src, int src_pitc
     if (sa[i]) first = i;
   if (first < 0) {
 #pragma unroll
-    for (int i = 0; i < 10; ++i) sv[i] = 128;
+    for (int i = 0; i < 10; ++i) sv[i] = 1 << (bd - 1);  // 128 at eight bits, 512 at ten
   } else {
     const int f = sv[first];
 #pragma unroll
@@ -545,7 +563,7 @@ __global__ void hevc_intra4_kernel(const uint8_t* __restrict__ src, int src_pitc
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
     int pr[16];
-    hpredict(left, top, corner, order[m], pr);
+    hpredict(left, top, corner, order[m], maxv, pr);
     int sad = 0;
 #pragma unroll
     for (int i = 0; i < 16; ++i) sad += abs(s[i] - pr[i]);
@@ -557,12 +575,21 @@ __global__ void hevc_intra4_kernel(const uint8_t* __restrict__ src, int src_pitc
     }
   }
   modes[j] = best_mode;
-  uint32_t w4[4];
+  if (sizeof(P) == 1) {
+    uint32_t w4[4];
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
-    w4[r] = (uint32_t)best_pred[4 * r] | ((uint32_t)best_pred[4 * r + 1] << 8) |
-            ((uint32_t)best_pred[4 * r + 2] << 16) | ((uint32_t)best_pred[4 * r + 3] << 24);
-  *reinterpret_cast<uint4*>(preds + (size_t)j * 16) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+    for (int r = 0; r < 4; ++r)
+      w4[r] = (uint32_t)best_pred[4 * r] | ((uint32_t)best_pred[4 * r + 1] << 8) |
+              ((uint32_t)best_pred[4 * r + 2] << 16) | ((uint32_t)best_pred[4 * r + 3] << 24);
+    *reinterpret_cast<uint4*>(preds + (size_t)j * 16) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+  } else {
+    uint32_t w8[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) w8[k] = (uint32_t)best_pred[2 * k] | ((uint32_t)best_pred[2 * k + 1] << 16);
+    uint4* o = reinterpret_cast<uint4*>(preds + (size_t)j * 16);
+    o[0] = make_uint4(w8[0], w8[1], w8[2], w8[3]);
+    o[1] = make_uint4(w8[4], w8[5], w8[6], w8[7]);
+  }
 }
 
 bool aligned16(const void* p) { return (((uintptr_t)p) & 15) == 0; }
@@ -627,8 +654,22 @@ int b200enc_hevc_build_hpel(const uint8_t* recon, int pitch, int w, int h, int m
   const int rows = h + 2 * margin, cols = w + 2 * margin;
   if (plane_pitch < cols) return -1;
   dim3 grid((cols + kHpTileW - 1) / kHpTileW, (rows + kHpTileH - 1) / kHpTileH);
-  hevc_hpel_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(recon, pitch, w, h, margin, plane_i, plane_h, plane_v,
-                                                           plane_hv, plane_pitch, rows, cols);
+  hevc_hpel_kernel<uint8_t><<<grid, 256, 0, (cudaStream_t)stream>>>(recon, pitch, w, h, margin, plane_i, plane_h,
+                                                                    plane_v, plane_hv, plane_pitch, rows, cols, 255);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_hevc_build_hpel_10(const uint16_t* recon, int pitch, int w, int h, int margin, uint16_t* plane_i,
+                               uint16_t* plane_h, uint16_t* plane_v, uint16_t* plane_hv, int plane_pitch,
+                               void* stream) {
+  if (!recon || !plane_i || !plane_h || !plane_v || !plane_hv || w <= 0 || h <= 0) return -1;
+  if (margin < 0 || margin > 256 || pitch < w) return -1;
+  const int rows = h + 2 * margin, cols = w + 2 * margin;
+  if (plane_pitch < cols) return -1;
+  dim3 grid((cols + kHpTileW - 1) / kHpTileW, (rows + kHpTileH - 1) / kHpTileH);
+  hevc_hpel_kernel<uint16_t><<<grid, 256, 0, (cudaStream_t)stream>>>(recon, pitch, w, h, margin, plane_i, plane_h,
+                                                                     plane_v, plane_hv, plane_pitch, rows, cols,
+                                                                     1023);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -639,8 +680,22 @@ int b200enc_hevc_motion_search(const uint8_t* src_y, int src_pitch, int w, int h
   if (!src_y || !plane_i || !plane_h || !plane_v || !plane_hv || !jobs || !results || n < 0) return -1;
   if (w < 8 || h < 8 || margin < 10 || plane_pitch < w + 2 * margin || src_pitch < w) return -1;
   if (n == 0) return 0;
-  HevcSearch S{src_y, src_pitch, w, h, margin, qpel ? 1 : 0, {plane_i, plane_h, plane_v, plane_hv}, plane_pitch};
-  hevc_me_kernel<<<(n + 3) / 4, 128, 0, (cudaStream_t)stream>>>(S, jobs, n, results);
+  HevcSearch<uint8_t> S{src_y, src_pitch, w, h, margin, qpel ? 1 : 0, {plane_i, plane_h, plane_v, plane_hv},
+                        plane_pitch, 0};
+  hevc_me_kernel<uint8_t><<<(n + 3) / 4, 128, 0, (cudaStream_t)stream>>>(S, jobs, n, results);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_hevc_motion_search_10(const uint16_t* src_y, int src_pitch, int w, int h, const uint16_t* plane_i,
+                                  const uint16_t* plane_h, const uint16_t* plane_v, const uint16_t* plane_hv,
+                                  int plane_pitch, int margin, int qpel, const b200enc_hevc_me_job_t* jobs, int n,
+                                  b200enc_hevc_me_result_t* results, void* stream) {
+  if (!src_y || !plane_i || !plane_h || !plane_v || !plane_hv || !jobs || !results || n < 0) return -1;
+  if (w < 8 || h < 8 || margin < 10 || plane_pitch < w + 2 * margin || src_pitch < w) return -1;
+  if (n == 0) return 0;
+  HevcSearch<uint16_t> S{src_y, src_pitch, w, h, margin, qpel ? 1 : 0, {plane_i, plane_h, plane_v, plane_hv},
+                         plane_pitch, 2};
+  hevc_me_kernel<uint16_t><<<(n + 3) / 4, 128, 0, (cudaStream_t)stream>>>(S, jobs, n, results);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -650,8 +705,19 @@ int b200enc_hevc_choose_luma_mode(const uint8_t* src_y, int src_pitch, const uin
   if (!src_y || !recon_y || !jobs || !modes || !preds || n < 0 || width < 4 || height < 4) return -1;
   if (!aligned16(preds) || src_pitch < width || recon_pitch < width) return -1;
   if (n == 0) return 0;
-  hevc_intra4_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(src_y, src_pitch, recon_y, recon_pitch, width,
-                                                                         height, jobs, n, modes, preds);
+  hevc_intra4_kernel<uint8_t><<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+      src_y, src_pitch, recon_y, recon_pitch, width, height, jobs, n, modes, preds, 8);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int b200enc_hevc_choose_luma_mode_10(const uint16_t* src_y, int src_pitch, const uint16_t* recon_y, int recon_pitch,
+                                     int width, int height, const int* jobs, int n, int* modes, uint16_t* preds,
+                                     void* stream) {
+  if (!src_y || !recon_y || !jobs || !modes || !preds || n < 0 || width < 4 || height < 4) return -1;
+  if (!aligned16(preds) || src_pitch < width || recon_pitch < width) return -1;
+  if (n == 0) return 0;
+  hevc_intra4_kernel<uint16_t><<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+      src_y, src_pitch, recon_y, recon_pitch, width, height, jobs, n, modes, preds, 10);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -31,7 +31,6 @@ struct IShared {
   int16_t src[16][16];
   int16_t srcc[2][8][8];
   int16_t pred[24][16];
-  int32_t tsm[24][16];
   alignas(16) int16_t lev[24][16];
   int32_t ldc[16];     // pre-quant luma DC coefficients (block raster)
   int32_t ldl[16];     // quantized luma DC (natural order)
@@ -245,7 +244,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
 #pragma unroll
         for (int i = 0; i < 4; ++i) x[i] = s.srcc[pl][4 * (sub >> 1) + r][4 * (sub & 1) + i] - s.pred[b][4 * r + i];
       }
-      quad_forward(x, r, s.tsm[b]);  // x[i] = coef[i][r]
+      quad_forward(x, r);  // x[i] = coef[i][r]
       uint32_t nz = 0;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
@@ -301,7 +300,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
 #pragma unroll
       for (int i = 0; i < 4; ++i) d[i] = dequant_ac(s.lev[b][4 * r + i], 4 * r + i, q);
       if (r == 0) d[0] = (luma ? s.ldcval[b] : s.cdcval[b - 16]) + 32;
-      quad_inverse(d, r, s.tsm[b]);
+      quad_inverse(d, r);
       if (luma) {
         const int bx = b & 3, by = b >> 2;
 #pragma unroll

@@ -17,11 +17,17 @@
 namespace b200enc {
 
 struct PShared {
-  uint8_t lp[21][24];      // luma reference patch, origin (ix0-2, iy0-2)
-  uint8_t cp[9][20];       // chroma reference patch (NV12 pairs), 9 x 9
+  // Reference and source rows staged as 16-byte units. The luma patch row r
+  // holds reference row iy0-2+r from column lxa (16-aligned) on; the patch
+  // origin (ix0-2, iy0-2) is at byte lo of row 0. The chroma patch (NV12
+  // pairs) starts at byte cxa (16-aligned); chroma sample (ixc, iyc) is at
+  // byte co of row 0.
+  alignas(16) uint8_t lp[21][48];
+  alignas(16) uint8_t cp[9][32];
+  alignas(16) uint8_t src[16][16];   // current luma
+  alignas(16) uint8_t srcc[8][16];   // current chroma (NV12 pairs)
   int16_t pred[24][16];    // prediction per block, raster within block
   int16_t res[24][16];     // residual
-  int32_t tsm[24][16];     // transpose scratch per block
   alignas(16) int16_t lev[24][16];  // quantized levels (for the coalesced store)
   int32_t cdc[8];          // pre-quant chroma DC coefficients
   int32_t dcval[8];        // dequantized chroma DC per chroma block
@@ -29,33 +35,37 @@ struct PShared {
   alignas(16) uint8_t ruv[8][16];  // reconstructed chroma (NV12)
 };
 
-__device__ __forceinline__ int hraw_p(const uint8_t (*lp)[24], int x, int y) {
-  // horizontal 6-tap centred between integer columns x and x+1 of row y
-  const uint8_t* r = lp[y + 2];
+// Horizontal / vertical 6-tap raw sums on a staged patch `p` (row pitch ps)
+// whose element (0, 0) is reference sample (ix0-2, iy0-2).
+__device__ __forceinline__ int hraw_p(const uint8_t* p, int ps, int x, int y) {
+  // centred between integer columns x and x+1 of row y
+  const uint8_t* r = p + (y + 2) * ps;
   return r[x] - 5 * r[x + 1] + 20 * r[x + 2] + 20 * r[x + 3] - 5 * r[x + 4] + r[x + 5];
 }
-__device__ __forceinline__ int vraw_p(const uint8_t (*lp)[24], int x, int y) {
-  return lp[y][x + 2] - 5 * lp[y + 1][x + 2] + 20 * lp[y + 2][x + 2] + 20 * lp[y + 3][x + 2] -
-         5 * lp[y + 4][x + 2] + lp[y + 5][x + 2];
+__device__ __forceinline__ int vraw_p(const uint8_t* p, int ps, int x, int y) {
+  const uint8_t* c = p + x + 2;
+  return c[y * ps] - 5 * c[(y + 1) * ps] + 20 * c[(y + 2) * ps] + 20 * c[(y + 3) * ps] - 5 * c[(y + 4) * ps] +
+         c[(y + 5) * ps];
 }
 
 // Luma quarter-pel sample (residual_predict.comp:263-298) for block-relative
 // pixel (x, y) whose integer anchor is patch (x+2, y+2).
-__device__ __forceinline__ int mc_luma(const uint8_t (*lp)[24], int x, int y, int fx, int fy) {
-  const int G = lp[y + 2][x + 2];
+__device__ __forceinline__ int mc_luma(const uint8_t* p, int ps, int x, int y, int fx, int fy) {
+  auto at = [&](int xx, int yy) { return (int)p[yy * ps + xx]; };
+  const int G = at(x + 2, y + 2);
   if (!(fx | fy)) return G;
   const int phase = fy * 4 + fx;
-  auto B = [&](int xx, int yy) { return clip1((hraw_p(lp, xx, yy) + 16) >> 5); };
-  auto Hh = [&](int xx, int yy) { return clip1((vraw_p(lp, xx, yy) + 16) >> 5); };
+  auto B = [&](int xx, int yy) { return clip1((hraw_p(p, ps, xx, yy) + 16) >> 5); };
+  auto Hh = [&](int xx, int yy) { return clip1((vraw_p(p, ps, xx, yy) + 16) >> 5); };
   auto J = [&]() {
-    const int j1 = hraw_p(lp, x, y - 2) - 5 * hraw_p(lp, x, y - 1) + 20 * hraw_p(lp, x, y) +
-                   20 * hraw_p(lp, x, y + 1) - 5 * hraw_p(lp, x, y + 2) + hraw_p(lp, x, y + 3);
+    const int j1 = hraw_p(p, ps, x, y - 2) - 5 * hraw_p(p, ps, x, y - 1) + 20 * hraw_p(p, ps, x, y) +
+                   20 * hraw_p(p, ps, x, y + 1) - 5 * hraw_p(p, ps, x, y + 2) + hraw_p(p, ps, x, y + 3);
     return clip1((j1 + 512) >> 10);
   };
   switch (phase) {
     case 1: return (G + B(x, y) + 1) >> 1;
     case 2: return B(x, y);
-    case 3: return (B(x, y) + lp[y + 2][x + 3] + 1) >> 1;
+    case 3: return (B(x, y) + at(x + 3, y + 2) + 1) >> 1;
     case 4: return (G + Hh(x, y) + 1) >> 1;
     case 5: return (B(x, y) + Hh(x, y) + 1) >> 1;
     case 6: return (B(x, y) + J() + 1) >> 1;
@@ -64,14 +74,33 @@ __device__ __forceinline__ int mc_luma(const uint8_t (*lp)[24], int x, int y, in
     case 9: return (Hh(x, y) + J() + 1) >> 1;
     case 10: return J();
     case 11: return (J() + Hh(x + 1, y) + 1) >> 1;
-    case 12: return (Hh(x, y) + lp[y + 3][x + 2] + 1) >> 1;
+    case 12: return (Hh(x, y) + at(x + 2, y + 3) + 1) >> 1;
     case 13: return (Hh(x, y) + B(x, y + 1) + 1) >> 1;
     case 14: return (J() + B(x, y + 1) + 1) >> 1;
     default: return (Hh(x + 1, y) + B(x, y + 1) + 1) >> 1;
   }
 }
 
-__global__ void __launch_bounds__(96) p_mb_kernel(const uint8_t* __restrict__ cur_y, const uint8_t* __restrict__ cur_uv,
+// Stages sixteen bytes of a row, `gx` 16-aligned, into `dst` (shared,
+// 16-aligned): one vector load where the bytes lie inside [0, lim) of a row
+// whose base is 16-byte aligned (`vec`), else byte loads of the clamped
+// columns. `pair` selects NV12 chroma clamping: byte b of the row is
+// component b&1 of sample clamp(b>>1, 0, lim/2-1).
+__device__ __forceinline__ void stage16_clamped(uint8_t* dst, const uint8_t* row, int gx, int lim, bool vec,
+                                                bool pair) {
+  if (vec && gx >= 0 && gx + 16 <= lim) {
+    *reinterpret_cast<uint4*>(dst) = __ldg(reinterpret_cast<const uint4*>(row + gx));
+    return;
+  }
+#pragma unroll 1
+  for (int j = 0; j < 16; ++j) {
+    const int b = gx + j;
+    const int c = pair ? 2 * clampi(b >> 1, 0, (lim >> 1) - 1) + (b & 1) : clampi(b, 0, lim - 1);
+    dst[j] = __ldg(row + c);
+  }
+}
+
+__global__ void __launch_bounds__(96, 16) p_mb_kernel(const uint8_t* __restrict__ cur_y, const uint8_t* __restrict__ cur_uv,
                                                   int cur_pitch, const uint8_t* __restrict__ ref_y,
                                                   const uint8_t* __restrict__ ref_uv, int ref_pitch, Geo g, int qp,
                                                   const MV* __restrict__ mvs, int16_t* __restrict__ levels,
@@ -87,35 +116,55 @@ __global__ void __launch_bounds__(96) p_mb_kernel(const uint8_t* __restrict__ cu
   const int ixc = Xc + (mv.mvx >> 3), iyc = Yc + (mv.mvy >> 3), fxc = mv.mvx & 7, fyc = mv.mvy & 7;
   const int cmx = g.RW / 2 - 1, cmy = g.RH / 2 - 1;
 
-  // ---- stage reference patches (clamped) --------------------------------
-  for (int i = tid; i < 21 * 21; i += 96) {
-    const int py = i / 21, px = i - py * 21;
-    s.lp[py][px] = __ldg(ref_y + (size_t)clampi(iy0 - 2 + py, 0, g.RH - 1) * ref_pitch + clampi(ix0 - 2 + px, 0, g.RW - 1));
-  }
-  for (int i = tid; i < 9 * 9; i += 96) {
-    const int py = i / 9, px = i - py * 9;
-    const uint16_t v = __ldg(reinterpret_cast<const uint16_t*>(ref_uv + (size_t)clampi(iyc + py, 0, cmy) * ref_pitch +
-                                                               2 * clampi(ixc + px, 0, cmx)));
-    s.cp[py][2 * px] = (uint8_t)(v & 0xff);
-    s.cp[py][2 * px + 1] = (uint8_t)(v >> 8);
+  // ---- stage reference patches and the source (16-byte units) -----------
+  // Units: 0..62 luma patch (21 rows x 3), 63..80 chroma patch (9 x 2),
+  // 81..96 source luma rows, 97..104 source chroma rows. Reads clamp to
+  // (RW, RH) for the reference and (W, H) for the source, per sample, as the
+  // byte-wise reference stages do; the vector path is taken where no clamp
+  // applies.
+  const int lxa = (ix0 - 2) & ~15, lo = (ix0 - 2) - lxa;
+  const int cxa = (2 * ixc) & ~15, co = 2 * ixc - cxa;
+  const bool rvec = ((ref_pitch & 15) == 0) && ((reinterpret_cast<uintptr_t>(ref_y) & 15) == 0) &&
+                    ((reinterpret_cast<uintptr_t>(ref_uv) & 15) == 0);
+  const bool cvec = ((cur_pitch & 15) == 0) && ((reinterpret_cast<uintptr_t>(cur_y) & 15) == 0) &&
+                    ((reinterpret_cast<uintptr_t>(cur_uv) & 15) == 0);
+  for (int u = tid; u < 105; u += 96) {
+    if (u < 63) {
+      const int r = u / 3, q = u - 3 * r;
+      const uint8_t* row = ref_y + (size_t)clampi(iy0 - 2 + r, 0, g.RH - 1) * ref_pitch;
+      stage16_clamped(&s.lp[r][16 * q], row, lxa + 16 * q, g.RW, rvec, false);
+    } else if (u < 81) {
+      const int r = (u - 63) >> 1, q = (u - 63) & 1;
+      const uint8_t* row = ref_uv + (size_t)clampi(iyc + r, 0, cmy) * ref_pitch;
+      stage16_clamped(&s.cp[r][16 * q], row, cxa + 16 * q, 2 * (g.RW / 2), rvec, true);
+    } else if (u < 97) {
+      const int r = u - 81;
+      const uint8_t* row = cur_y + (size_t)clampi(Y + r, 0, g.H - 1) * cur_pitch;
+      stage16_clamped(&s.src[r][0], row, X, g.W, cvec, false);
+    } else {
+      const int r = u - 97;
+      const uint8_t* row = cur_uv + (size_t)clampi(Yc + r, 0, g.H / 2 - 1) * cur_pitch;
+      stage16_clamped(&s.srcc[r][0], row, 2 * Xc, 2 * (g.W / 2), cvec, true);
+    }
   }
   __syncthreads();
 
   // ---- prediction + residual --------------------------------------------
+  const uint8_t* lpp = &s.lp[0][lo];
   for (int i = tid; i < 256; i += 96) {
     const int x = i & 15, y = i >> 4;
-    const int pv = mc_luma(s.lp, x, y, fx, fy);
-    const int src = __ldg(cur_y + (size_t)clampi(Y + y, 0, g.H - 1) * cur_pitch + clampi(X + x, 0, g.W - 1));
+    const int pv = mc_luma(lpp, 48, x, y, fx, fy);
+    const int src = s.src[y][x];
     const int blk = (y >> 2) * 4 + (x >> 2), pos = (y & 3) * 4 + (x & 3);
     s.pred[blk][pos] = (int16_t)pv;
     s.res[blk][pos] = (int16_t)(src - pv);
   }
   for (int i = tid; i < 128; i += 96) {
     const int pl = i >> 6, x = i & 7, y = (i >> 3) & 7;
-    const int A = s.cp[y][2 * x + pl], B = s.cp[y][2 * x + 2 + pl];
-    const int C = s.cp[y + 1][2 * x + pl], D = s.cp[y + 1][2 * x + 2 + pl];
+    const int A = s.cp[y][co + 2 * x + pl], B = s.cp[y][co + 2 * x + 2 + pl];
+    const int C = s.cp[y + 1][co + 2 * x + pl], D = s.cp[y + 1][co + 2 * x + 2 + pl];
     const int pv = ((8 - fxc) * (8 - fyc) * A + fxc * (8 - fyc) * B + (8 - fxc) * fyc * C + fxc * fyc * D + 32) >> 6;
-    const int src = __ldg(cur_uv + (size_t)clampi(Yc + y, 0, g.H / 2 - 1) * cur_pitch + 2 * clampi(Xc + x, 0, g.W / 2 - 1) + pl);
+    const int src = s.srcc[y][2 * x + pl];
     const int blk = 16 + 4 * pl + (y >> 2) * 2 + (x >> 2), pos = (y & 3) * 4 + (x & 3);
     s.pred[blk][pos] = (int16_t)pv;
     s.res[blk][pos] = (int16_t)(src - pv);
@@ -129,7 +178,7 @@ __global__ void __launch_bounds__(96) p_mb_kernel(const uint8_t* __restrict__ cu
   int x[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) x[i] = s.res[b][4 * r + i];
-  quad_forward(x, r, s.tsm[b]);  // x[i] = coef[i][r]
+  quad_forward(x, r);  // x[i] = coef[i][r]
   uint32_t nz = 0;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -168,7 +217,7 @@ __global__ void __launch_bounds__(96) p_mb_kernel(const uint8_t* __restrict__ cu
     if (!luma) d[0] = s.dcval[b - 16];
     d[0] += 32;
   }
-  quad_inverse(d, r, s.tsm[b]);  // d[i] = res[i][r]
+  quad_inverse(d, r);  // d[i] = res[i][r]
   if (luma) {
     const int bx = b & 3, by = b >> 2;
 #pragma unroll

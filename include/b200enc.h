@@ -257,6 +257,13 @@ int b200enc_hevc_dequant_itransform_8x8(const int16_t *coeff, int16_t *residual,
  * approach1-compute-encoder/src/hevc_enc_template.c:219-400 (margin 16 there). */
 int b200enc_hevc_build_hpel(const uint8_t *recon, int pitch, int w, int h, int margin, uint8_t *plane_i,
                             uint8_t *plane_h, uint8_t *plane_v, uint8_t *plane_hv, int plane_pitch, void *stream);
+/* The same planes of a 10-bit (Main10) reconstruction: samples 0..1023 in
+ * 16-bit words, pitches in samples, half-sample values clipped at 1023;
+ * replaces build_hpel_10, the BIT_DEPTH 10 instance of the same template
+ * (approach1-compute-encoder/src/encoder_h265.c:1220-1227, called at :1571). */
+int b200enc_hevc_build_hpel_10(const uint16_t *recon, int pitch, int w, int h, int margin, uint16_t *plane_i,
+                               uint16_t *plane_h, uint16_t *plane_v, uint16_t *plane_hv, int plane_pitch,
+                               void *stream);
 
 /* Motion search of 8x8 CUs against the planes of b200enc_hevc_build_hpel
  * (8-bit), one job per CU: the reference's motion_search
@@ -289,6 +296,14 @@ int b200enc_hevc_motion_search(const uint8_t *src_y, int src_pitch, int w, int h
                                const uint8_t *plane_h, const uint8_t *plane_v, const uint8_t *plane_hv,
                                int plane_pitch, int margin, int qpel, const b200enc_hevc_me_job_t *jobs, int n,
                                b200enc_hevc_me_result_t *results, void *stream);
+/* The same search on 10-bit (Main10) source and planes (16-bit words,
+ * pitches in samples); SADs are brought back to eight-bit units (>> 2)
+ * before they are costed, as motion_search_10 / search_sad_10 do
+ * (approach1-compute-encoder/src/hevc_enc_template.c:484). */
+int b200enc_hevc_motion_search_10(const uint16_t *src_y, int src_pitch, int w, int h, const uint16_t *plane_i,
+                                  const uint16_t *plane_h, const uint16_t *plane_v, const uint16_t *plane_hv,
+                                  int plane_pitch, int margin, int qpel, const b200enc_hevc_me_job_t *jobs, int n,
+                                  b200enc_hevc_me_result_t *results, void *stream);
 
 /* Intra 4x4 luma mode choice of n PUs whose neighbours are already final in
  * recon_y (8-bit): jobs = n x {x0, y0, y_min} (PU position, multiple of 4;
@@ -301,6 +316,13 @@ int b200enc_hevc_motion_search(const uint8_t *src_y, int src_pitch, int w, int h
 int b200enc_hevc_choose_luma_mode(const uint8_t *src_y, int src_pitch, const uint8_t *recon_y, int recon_pitch,
                                   int width, int height, const int *jobs, int n, int *modes, uint8_t *preds,
                                   void *stream);
+/* The same choice on 10-bit (Main10) samples (16-bit words, pitches in
+ * samples): no-neighbour fill 512, edge filters clipped at 1023; preds =
+ * n x 16 samples (16-byte aligned); replaces hevc_choose_luma_mode_10
+ * (approach1-compute-encoder/src/hevc_intra.h:152). */
+int b200enc_hevc_choose_luma_mode_10(const uint16_t *src_y, int src_pitch, const uint16_t *recon_y,
+                                     int recon_pitch, int width, int height, const int *jobs, int n, int *modes,
+                                     uint16_t *preds, void *stream);
 
 /* HEVC deblocking (H.265 8.7.2) of one 4:2:0 picture, in place: every
  * vertical edge of the picture, then every horizontal edge over what the

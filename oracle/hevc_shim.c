@@ -81,3 +81,49 @@ void refshim_hevc_motion_search(uint8_t *planes[4], const uint8_t *src, int w, i
     mv_out[0] = m.x;
     mv_out[1] = m.y;
 }
+
+/* build_hpel_10, the 10-bit (Main10) instance of the same template
+ * (encoder_h265.c:1220-1227): 16-bit samples, pitches in samples. */
+int refshim_hevc_build_hpel_10(const uint16_t *recon, int w, int h, uint16_t *planes[4])
+{
+    struct hevc_encoder enc;
+    memset(&enc, 0, sizeof(enc));
+    enc.coded_width = (uint32_t)w;
+    enc.coded_height = (uint32_t)h;
+    enc.bit_depth = 10;
+    enc.prev_recon_y = (void *)recon;
+    enc.hpel_stride = w + 2 * HPEL_MARGIN;
+    for (int i = 0; i < 4; i++) enc.hpel[i] = planes[i];
+    enc.hpel_tmp = malloc((size_t)enc.hpel_stride * (h + 2 * HPEL_MARGIN + 7) * sizeof(int32_t));
+    if (!enc.hpel_tmp) return -1;
+    enc.pool = NULL;
+    enc.threads = 1;
+    build_hpel_10(&enc);
+    free(enc.hpel_tmp);
+    return HPEL_MARGIN;
+}
+
+/* motion_search_10 for one 8x8 CU on 10-bit planes and source. */
+void refshim_hevc_motion_search_10(uint16_t *planes[4], const uint16_t *src, int w, int h, int qpel, int cu_x,
+                                   int cu_y, const int16_t mvp[4], const int16_t *starts, int n_starts,
+                                   int lambda_q8, int16_t mv_out[2], int *mvp_idx, int64_t *cost_q8, uint32_t *sad)
+{
+    struct hevc_encoder enc;
+    memset(&enc, 0, sizeof(enc));
+    enc.coded_width = (uint32_t)w;
+    enc.coded_height = (uint32_t)h;
+    enc.bit_depth = 10;
+    enc.hpel_stride = w + 2 * HPEL_MARGIN;
+    for (int i = 0; i < 4; i++) enc.hpel[i] = planes[i];
+    enc.src_y = (void *)src;
+    enc.qpel = qpel != 0;
+    hevc_mv_t p[2] = {{mvp[0], mvp[1]}, {mvp[2], mvp[3]}};
+    hevc_mv_t st[16];
+    for (int i = 0; i < n_starts && i < 16; i++) {
+        st[i].x = starts[2 * i];
+        st[i].y = starts[2 * i + 1];
+    }
+    hevc_mv_t m = motion_search_10(&enc, cu_x, cu_y, p, st, n_starts, lambda_q8, mvp_idx, cost_q8, sad);
+    mv_out[0] = m.x;
+    mv_out[1] = m.y;
+}
