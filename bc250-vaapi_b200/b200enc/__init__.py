@@ -27,6 +27,7 @@ EXPORTS = [
     "b200enc_hevc_dequant_itransform_8x8", "b200enc_hevc_build_hpel", "b200enc_hevc_motion_search",
     "b200enc_hevc_choose_luma_mode", "b200enc_hevc_deblock", "b200enc_hevc_build_hpel_10",
     "b200enc_hevc_motion_search_10", "b200enc_hevc_choose_luma_mode_10",
+    "b200enc_tune_set", "b200enc_tune_get", "b200enc_tune_name", "b200enc_tune_load",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
     "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",
@@ -42,7 +43,8 @@ EXPORTS = [
     "gpu_compute_get_dc_staging_data", "gpu_compute_get_pred_mode_staging_data",
     "gpu_compute_get_mv_staging_data", "gpu_compute_get_nz_staging_data", "gpu_compute_debug_dump_recon",
     "b200enc_ctx_configure", "b200enc_ctx_stream", "b200enc_ctx_recon", "b200enc_ctx_device_outputs",
-    "b200enc_ctx_encode_device", "b200enc_ctx_perf", "b200enc_ctx_perf_read",
+    "b200enc_ctx_encode_device", "b200enc_ctx_perf", "b200enc_ctx_perf_read", "b200enc_host_register",
+    "b200enc_host_unregister",
 ]
 
 _vp = ctypes.c_void_p
@@ -119,6 +121,13 @@ def load_library(path=LIB_PATH):
     lib.b200enc_hevc_choose_luma_mode_10.argtypes = [_vp, _i, _vp, _i, _i, _i, _vp, _i, _vp, _vp, _vp]
     lib.b200enc_hevc_deblock.argtypes = [ctypes.POINTER(HevcDeblockParams), _vp]
     lib.b200enc_ctx_set_me.argtypes = [ctypes.POINTER(GpuContext), _i, ctypes.c_char_p, ctypes.c_float]
+    lib.b200enc_host_register.argtypes = [ctypes.POINTER(GpuContext), _vp, ctypes.c_size_t]
+    lib.b200enc_host_unregister.argtypes = [ctypes.POINTER(GpuContext), _vp]
+    lib.b200enc_tune_set.argtypes = [_i, _i]
+    lib.b200enc_tune_get.argtypes = [_i]
+    lib.b200enc_tune_name.argtypes = [_i]
+    lib.b200enc_tune_name.restype = ctypes.c_char_p
+    lib.b200enc_tune_load.argtypes = [ctypes.c_char_p]
     return lib
 
 

@@ -6,3 +6,6 @@
 #include <cstdint>
 
 #include "../../include/b200enc.h"
+
+// Value of an autotuned launch parameter (B200ENC_TUNE_*), 0 = the default.
+int b200enc_tuned(int key);

@@ -578,15 +578,16 @@ using namespace b200enc;
 
 static constexpr uint32_t kMaxWaitUsDb = 2000000u;  // 2 s
 
-// Rows per CTA: at most 4 (one luma + one chroma warp each, plus two IO and
-// two halo warps: 384 threads). The ring must hold the 2*R columns a group's rows
+// Rows per CTA: 4 unless the autotuner chose otherwise (one luma + one
+// chroma warp each, plus two IO and two halo warps: 64R + 128 threads). The ring must hold the 2*R columns a group's rows
 // span plus prefetch, so R stays well below kDbRing.
 static int db_rows_per_cta(int mbw, int mbh) {
   int dev = 0, maxsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (maxsm <= 0) maxsm = 48 * 1024;
-  int R = 4;
+  const int tuned = b200enc_tuned(B200ENC_TUNE_DEBLOCK_ROWS);
+  int R = tuned > 0 ? tuned : 4;
   while (R > 1 && db_plan(mbw, R).bytes + 64 > (size_t)maxsm) --R;
   if (R > mbh) R = mbh;
   if (db_plan(mbw, R).bytes + 64 > (size_t)maxsm) return 0;

@@ -19,6 +19,7 @@
 #include <map>
 #include <string>
 #include <thread>
+#include <utility>
 
 #include "../../include/gpu_compute.h"
 #include "b200enc_internal.h"
@@ -76,6 +77,7 @@ struct Impl {
   bool mv_hist = false;  // d_mv holds the previous P frame's field
   bool last_learned = false;  // the last P frame ran b200enc_proposal_me
   std::map<void*, Shadow> shadows;
+  std::map<void*, size_t> registered;  // caller buffers this context page-locked
   // Per-stage timing (the reference's BC250_PERF_STATS timestamps,
   // gpu_compute.c:50-67): a ring of event sets, one per frame, folded into
   // running sums when completed.
@@ -298,9 +300,10 @@ int encode_frame(gpu_context_t* ctx, Impl* m, const uint8_t* y, const uint8_t* u
       if (m->me_mode != 0 && have_ref && m->mv_hist) {
         // the learned form fails loudly without its parameters
         if (ensure_proposal(m) != 0) return -1;
-        rc |= cudaMemcpyAsync(m->d_mv_prev, m->d_mv, mbs * 16, cudaMemcpyDeviceToDevice, m->stream) == cudaSuccess
-                  ? 0
-                  : -1;
+        // the previous frame's field becomes the history, the other buffer
+        // takes this frame's (work already enqueued on the stream that reads
+        // either buffer runs first)
+        std::swap(m->d_mv, m->d_mv_prev);
         rc |= b200enc_proposal_me(m->prop, y, src_pitch, ref_y, ref_pitch, W, H, ref_RW, ref_RH, m->d_mv_prev,
                                   m->range, lambda, m->zero_thresh, m->me_mode, m->conf, m->d_mv, m->stream);
         m->last_learned = true;
@@ -396,6 +399,7 @@ void bc250_gpu_destroy(bc250_gpu_context_t* ctx) {
   cudaStreamSynchronize(m->stream);
   free_frame_buffers(m);
   for (auto& kv : m->shadows) cudaFreeHost(kv.second.host);
+  for (auto& kv : m->registered) cudaHostUnregister(kv.first);
   for (Slot& s : m->slot) {
     cudaEventDestroy(s.start);
     cudaEventDestroy(s.done);
@@ -502,10 +506,12 @@ int gpu_compute_upload_nv12(gpu_context_t* ctx, gpu_image_t* image, gpu_memory_t
       cudaMemcpy2DAsync(image->uv_plane, image->pitch, uv_plane, uv_pitch, width, height / 2,
                         cudaMemcpyHostToDevice, m->stream) != cudaSuccess)
     return -1;
-  // Host buffers the caller may reuse on return: unless they are page-locked
-  // (then stream order is enough), wait for the copy.
-  cudaPointerAttributes a{};
-  if (cudaPointerGetAttributes(&a, y_plane) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+  // Host buffers the caller may reuse on return: unless both planes are
+  // page-locked (cudaMallocHost, or b200enc_host_register: then stream
+  // order is enough), wait for the copy.
+  cudaPointerAttributes a{}, b{};
+  if (cudaPointerGetAttributes(&a, y_plane) != cudaSuccess || a.type != cudaMemoryTypeHost ||
+      cudaPointerGetAttributes(&b, uv_plane) != cudaSuccess || b.type != cudaMemoryTypeHost) {
     cudaGetLastError();
     return cudaStreamSynchronize(m->stream) == cudaSuccess ? 0 : -1;
   }
@@ -764,6 +770,28 @@ int b200enc_ctx_encode_device(gpu_context_t* ctx, const uint8_t* y, const uint8_
   Impl* m = impl_of(ctx);
   if (!m || !y || !uv || (pitch & 3)) return -1;
   return encode_frame(ctx, m, y, uv, pitch, width, height, qp, is_intra, num_slices, 0, nullptr, stage_outputs != 0);
+}
+
+int b200enc_host_register(gpu_context_t* ctx, void* ptr, size_t bytes) {
+  Impl* m = impl_of(ctx);
+  if (!m || !ptr || bytes == 0 || m->registered.count(ptr)) return -1;
+  if (cudaHostRegister(ptr, bytes, cudaHostRegisterDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  m->registered[ptr] = bytes;
+  return 0;
+}
+
+int b200enc_host_unregister(gpu_context_t* ctx, void* ptr) {
+  Impl* m = impl_of(ctx);
+  if (!m || !ptr) return -1;
+  auto it = m->registered.find(ptr);
+  if (it == m->registered.end()) return -1;
+  // copies from the buffer may still be queued
+  cudaStreamSynchronize(m->stream);
+  m->registered.erase(it);
+  return cudaHostUnregister(ptr) == cudaSuccess ? 0 : -1;
 }
 
 int b200enc_ctx_perf(gpu_context_t* ctx, int enable) {

@@ -368,6 +368,7 @@ extern "C" int b200enc_i_frame_launch(const uint8_t* cur_y, const uint8_t* cur_u
                                       int rec_pitch, uint32_t* scratch, int ctas, uint32_t max_wait, int flags,
                                       void* stream) {
   Geo g{W, H, RW, RH, (W + 15) / 16, (H + 15) / 16};
+  if (ctas <= 0) ctas = b200enc_tuned(B200ENC_TUNE_INTRA_CTAS);
   if (ctas <= 0) ctas = g.mbh;
   if (ctas > g.mbh) ctas = g.mbh;
   i_frame_kernel<<<ctas, 96, 0, (cudaStream_t)stream>>>(cur_y, cur_uv, cur_pitch, g, qp, num_slices, levels, dc, nz,

@@ -190,8 +190,10 @@ extern "C" int b200enc_me_full_search_ex(const uint8_t* cur_y, int cur_pitch, co
   if (mb_list && (list_capacity <= 0 || list_capacity > g.mbw * g.mbh)) return -1;
   int sms = 148, dev = 0;
   if (mb_list && cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // list mode: a persistent grid of up to 8 CTAs per SM walks the list
-  dim3 grid = mb_list ? dim3(std::min(list_capacity, 8 * sms)) : dim3(g.mbw, g.mbh);
+  // list mode: a persistent grid of up to 8 CTAs per SM (or the tuned
+  // count) walks the list
+  const int per_sm = b200enc_tuned(B200ENC_TUNE_FALLBACK_CTAS_PER_SM) > 0 ? b200enc_tuned(B200ENC_TUNE_FALLBACK_CTAS_PER_SM) : 8;
+  dim3 grid = mb_list ? dim3(std::min(list_capacity, per_sm * sms)) : dim3(g.mbw, g.mbh);
   cudaStream_t st = (cudaStream_t)stream;
   const bool list = mb_list != nullptr;
   switch (range) {

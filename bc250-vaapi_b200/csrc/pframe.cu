@@ -100,16 +100,24 @@ __device__ __forceinline__ void stage16_clamped(uint8_t* dst, const uint8_t* row
   }
 }
 
-__global__ void __launch_bounds__(96, 16) p_mb_kernel(const uint8_t* __restrict__ cur_y, const uint8_t* __restrict__ cur_uv,
+// One CTA holds blockDim.y macroblocks of a row (the autotuner's tile
+// shape: 1, 2 or 4), 96 threads (three warps) each; a macroblock's shared
+// state is its slice of the dynamic shared memory.
+__global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict__ cur_y, const uint8_t* __restrict__ cur_uv,
                                                   int cur_pitch, const uint8_t* __restrict__ ref_y,
                                                   const uint8_t* __restrict__ ref_uv, int ref_pitch, Geo g, int qp,
                                                   const MV* __restrict__ mvs, int16_t* __restrict__ levels,
                                                   int32_t* __restrict__ dc, uint32_t* __restrict__ nzm,
                                                   uint32_t* __restrict__ pred_mode, uint8_t* __restrict__ rec_y,
                                                   uint8_t* __restrict__ rec_uv, int rec_pitch) {
-  __shared__ PShared s;
+  extern __shared__ __align__(16) uint8_t p_smem[];
+  PShared& s = reinterpret_cast<PShared*>(p_smem)[threadIdx.y];
   const int tid = threadIdx.x;
-  const int mbx = blockIdx.x, mby = blockIdx.y, mb = mby * g.mbw + mbx;
+  // a tile reaching past the right edge computes a copy of the last
+  // macroblock and stores nothing
+  const int mbx_t = blockIdx.x * blockDim.y + threadIdx.y;
+  const bool active = mbx_t < g.mbw;
+  const int mbx = active ? mbx_t : g.mbw - 1, mby = blockIdx.y, mb = mby * g.mbw + mbx;
   const int X = mbx * 16, Y = mby * 16, Xc = X >> 1, Yc = Y >> 1;
   const MV mv = mvs[mb];
   const int ix0 = X + (mv.mvx >> 2), iy0 = Y + (mv.mvy >> 2), fx = mv.mvx & 3, fy = mv.mvy & 3;
@@ -190,8 +198,10 @@ __global__ void __launch_bounds__(96, 16) p_mb_kernel(const uint8_t* __restrict_
   nz |= __shfl_xor_sync(0xffffffffu, nz, 1);
   nz |= __shfl_xor_sync(0xffffffffu, nz, 2);
   if (r == 0) {
-    nzm[(size_t)mb * 24 + b] = nz;
-    dc[(size_t)mb * 24 + b] = x[0];
+    if (active) {
+      nzm[(size_t)mb * 24 + b] = nz;
+      dc[(size_t)mb * 24 + b] = x[0];
+    }
     if (!luma) s.cdc[b - 16] = x[0];
   }
   __syncwarp();
@@ -231,6 +241,7 @@ __global__ void __launch_bounds__(96, 16) p_mb_kernel(const uint8_t* __restrict_
   __syncthreads();
 
   // ---- coalesced stores ---------------------------------------------------
+  if (!active) return;
   if (tid < 48) {
     reinterpret_cast<uint4*>(levels + (size_t)mb * 384)[tid] = reinterpret_cast<const uint4*>(&s.lev[0][0])[tid];
   } else if (tid < 64) {
@@ -276,8 +287,9 @@ extern "C" int b200enc_p_frame(const uint8_t* cur_y, const uint8_t* cur_uv, int 
     return -1;
   if ((ref_pitch & 1) || (((uintptr_t)ref_uv) & 1)) return -1;
   Geo g{W, H, RW, RH, (W + 15) / 16, (H + 15) / 16};
-  p_mb_kernel<<<dim3(g.mbw, g.mbh), 96, 0, (cudaStream_t)stream>>>(cur_y, cur_uv, cur_pitch, ref_y, ref_uv, ref_pitch,
-                                                                   g, qp, (const MV*)mv, levels, dc, nz, pred_mode,
-                                                                   rec_y, rec_uv, rec_pitch);
+  const int T = b200enc_tuned(B200ENC_TUNE_PCHAIN_MBS_PER_CTA) > 0 ? b200enc_tuned(B200ENC_TUNE_PCHAIN_MBS_PER_CTA) : 1;
+  p_mb_kernel<<<dim3((g.mbw + T - 1) / T, g.mbh), dim3(96, T), T * sizeof(PShared), (cudaStream_t)stream>>>(
+      cur_y, cur_uv, cur_pitch, ref_y, ref_uv, ref_pitch, g, qp, (const MV*)mv, levels, dc, nz, pred_mode, rec_y,
+      rec_uv, rec_pitch);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -801,7 +801,10 @@ int b200enc_proposal_me(void* h, const uint8_t* cur_y, int cur_pitch, const uint
   const int rc = b200enc_me_full_search_ex(cur_y, cur_pitch, ref_y, ref_pitch, W, H, RW, RH, range, lambda,
                                            zero_thresh, mv_out, P->b.lists + mbs, P->b.counters + 1, mbs, 0,
                                            (void*)P->side);
-  lp_rescore_kernel<<<std::max(1, std::min((mbs + 3) / 4, 148 * 8)), 128, 0, st>>>(
+  int sms = 148, dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int per_sm = b200enc_tuned(B200ENC_TUNE_RESCORE_CTAS_PER_SM) > 0 ? b200enc_tuned(B200ENC_TUNE_RESCORE_CTAS_PER_SM) : 8;
+  lp_rescore_kernel<<<std::max(1, std::min((mbs + 3) / 4, per_sm * sms)), 128, 0, st>>>(
       cur_y, cur_pitch, ref_y, ref_pitch, g, range, lambda, mbs, P->b, (MV*)mv_out);
   // join
   if (cudaEventRecord(P->ev_fb, P->side) != cudaSuccess || cudaStreamWaitEvent(st, P->ev_fb, 0) != cudaSuccess)

@@ -504,6 +504,14 @@ def run_gpu(args):
         return max_over_ranks(e0.elapsed_time(e1)), launches, pf, c
 
     K, Wm = args.steps, args.warmup
+    if args.profile_arm:
+        # one arm only, for a profiler's launch list; no JSON line
+        mode = {"learned": LEARNED, "plain": 0, "learned_bf16": 1}[args.profile_arm]
+        arm(mode, S, K, Wm)
+        for c in ctxs:
+            c.close()
+        group.close()
+        return
     ms_l, launches, _, clk = arm(LEARNED, S, K, Wm, clocks=True)
     ms_p, _, _, _ = arm(0, S, K, Wm)
     ms_b, _, _, _ = arm(1, S, K, Wm)  # the learned form with the network's inference in BF16
@@ -709,6 +717,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-full-encode", action="store_true", help="skip the full-encode figure (host entropy coding)")
+    ap.add_argument("--profile-arm", choices=["learned", "plain", "learned_bf16"], default=None,
+                    help="run only this S-stream arm (warm-up + steps) and print nothing: a profiler's launch list")
     ap.add_argument("--streams", type=int, default=8)
     ap.add_argument("--conf", type=float, default=0.9)
     ap.add_argument("--hevc-deblock", action="store_true",

@@ -158,6 +158,29 @@ int b200enc_deblock_noalloc(int mbw, int mbh, int qp, int is_intra,
                             const uint32_t *nz, const void *mv,
                             uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch, void *stream);
 
+/* Launch parameters picked by the autotuner (no reference counterpart: the
+ * reference's dispatch sizes are fixed in gpu_compute.c). Each changes how
+ * a kernel's work is laid out, never its results. 0 = the built-in default.
+ * The table is process-wide; B200ENC_TUNE_FILE (a file of "name value"
+ * lines, as b200enc_tune_name spells the names) is loaded before the first
+ * launch. */
+#define B200ENC_TUNE_DEBLOCK_ROWS 0         /* macroblock rows per deblocking CTA, 1..6 (default 4) */
+#define B200ENC_TUNE_PCHAIN_MBS_PER_CTA 1   /* macroblocks per P-chain CTA, 1, 2 or 4 (default 1) */
+#define B200ENC_TUNE_RESCORE_CTAS_PER_SM 2  /* learned re-scoring grid, CTAs per SM, 1..16 (default 8) */
+#define B200ENC_TUNE_FALLBACK_CTAS_PER_SM 3 /* fallback full-search grid, CTAs per SM, 1..16 (default 8) */
+#define B200ENC_TUNE_INTRA_CTAS 4           /* intra wavefront CTAs (rows in flight), >= 1 (default: one per row) */
+#define B200ENC_TUNE_COUNT 5
+/* Sets a knob (0 restores the default); -1 for an unknown key or a value
+ * out of range. */
+int b200enc_tune_set(int key, int value);
+/* Current value of a knob (0 = default), -1 for an unknown key. */
+int b200enc_tune_get(int key);
+/* The knob's name in tune files, NULL for an unknown key. */
+const char *b200enc_tune_name(int key);
+/* Loads "name value" lines; returns the number of knobs set, -1 if the file
+ * cannot be read. */
+int b200enc_tune_load(const char *path);
+
 /* BF16 GEMM on the tcgen05 tensor cores with FP32 accumulation in tensor
  * memory: C[m][n] (row pitch ldc floats) = epilogue(sum_k A(m,k) * B(n,k)),
  * where A(m,k) = A[m*a_rs + k*a_ks] and B(n,k) = B[n*b_rs + k*b_ks] (BF16,

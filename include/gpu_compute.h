@@ -215,6 +215,21 @@ int b200enc_ctx_perf(gpu_context_t *ctx, int enable);
 int b200enc_ctx_perf_read(gpu_context_t *ctx, int intra, double *me_ms, double *chain_ms,
                           double *deblock_ms, double *staging_ms, long *frames);
 
+/* Surface ingest without a staging copy. The reference uploads and downloads
+ * NV12 through host-visible Vulkan memory (gpu_compute.c:2551, :2699); here
+ * a caller's own frame buffers (a decoder's output pool, a capture ring) are
+ * page-locked once with b200enc_host_register, after which
+ * gpu_compute_upload_nv12 from them is one asynchronous DMA per plane on the
+ * context stream, ordered before the next dispatch, with no copy through a
+ * bounce buffer and no wait in the call (the caller must not rewrite the
+ * buffer until a frame submitted after the upload has been synced).
+ * Unregistered pageable buffers still work, synchronously. Registration is
+ * process-wide; b200enc_host_unregister (or bc250_gpu_destroy, for what this
+ * context registered) undoes it. 0 / -1 (already registered, or the driver
+ * refused). */
+int b200enc_host_register(gpu_context_t *ctx, void *ptr, size_t bytes);
+int b200enc_host_unregister(gpu_context_t *ctx, void *ptr);
+
 #ifdef __cplusplus
 }
 #endif

@@ -154,3 +154,51 @@ def test_learned_form_bench_config_chain_exact(gpu, oracle_mod, mode):
     assert learned_frames == 6
     ctx.destroy_image(img, mem)
     ctx.close()
+
+
+def test_registered_host_buffers_upload_without_staging(gpu, oracle_mod):
+    """A caller's own frame buffers, page-locked once with
+    b200enc_host_register, feed gpu_compute_upload_nv12 asynchronously; the
+    encode equals the oracle's as with any upload, and unregistering works
+    (and refuses a buffer that is not registered)."""
+    import ctypes
+    import torch
+    from b200enc import synth
+    W, H, qp = 640, 480, 28
+    seq = synth.workload("h264_640x480", seed=0, stream=9)
+    ctx = gpu.Context()
+    ctx.configure(search_range=16, coded_clamp=True, deblock=1)
+    img, mem = ctx.create_image(W, H)
+    CW, CH = gpu.coded(W, H)
+    f = oracle_mod.frame(W, H, qp)
+    pool = [np.zeros((H * 3 // 2, W), np.uint8) for _ in range(2)]  # the caller's frame pool
+    c = ctypes.byref(ctx.ctx)
+    for buf in pool:
+        assert ctx.L.b200enc_host_register(c, ctypes.c_void_p(buf.ctypes.data), buf.nbytes) == 0
+    assert ctx.L.b200enc_host_register(c, ctypes.c_void_p(pool[0].ctypes.data), pool[0].nbytes) == -1
+    ref_y = ref_uv = None
+    for t in range(4):
+        buf = pool[t % 2]
+        y, uv = seq.frame(t)
+        buf[:H], buf[H:] = y, uv
+        by, buv = buf[:H], buf[H:]
+        rc = ctx.L.gpu_compute_upload_nv12(c, ctypes.byref(img), mem, ctypes.c_void_p(by.ctypes.data), W,
+                                           ctypes.c_void_p(buv.ctypes.data), W, W, H)
+        assert rc == 0
+        slot = ctx.encode(img, W, H, qp, t == 0)
+        assert ctx.sync(slot) == 0
+        got = ctx.staging(slot)
+        rec_y = np.zeros((CH, CW), np.uint8)
+        rec_uv = np.zeros((CH // 2, CW), np.uint8)
+        if ref_y is None:
+            ref_y, ref_uv = _pad(y, CH, CW), _pad(uv, CH // 2, CW)
+        want = oracle_mod.encode_frame(f, 16, 5, 512, t == 0, 1, y, uv, ref_y, ref_uv, rec_y, rec_uv)
+        for k in ("levels", "dc", "nz", "pred_mode", "mv"):
+            np.testing.assert_array_equal(got[k], want[k], err_msg=f"frame {t} {k}")
+        ref_y, ref_uv = rec_y, rec_uv
+    for buf in pool:
+        assert ctx.L.b200enc_host_unregister(c, ctypes.c_void_p(buf.ctypes.data)) == 0
+    assert ctx.L.b200enc_host_unregister(c, ctypes.c_void_p(pool[0].ctypes.data)) == -1
+    torch.cuda.synchronize()
+    ctx.destroy_image(img, mem)
+    ctx.close()
