@@ -23,6 +23,9 @@ namespace b200enc {
 
 struct IShared {
   int top[16], left[16], corner;
+  alignas(16) uint8_t topv[16];    // row Y-1 from X (luma), raw
+  alignas(16) uint8_t topc[16];    // row Yc-1 from 2*Xc (NV12 pairs), raw
+  int prev_top15;                  // byte 15 of the previous MB's topv: the corner of this MB
   int tuv[2][8], luv[2][8];
   int sad[4][3];
   int mode, dcv, pa, pb, pc, top_av, left_av;
@@ -63,8 +66,9 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
   const bool luma = b < 16;
   const QP ql = make_qp(qp, true), qc = make_qp(chroma_qp(qp), true);
   const QP& q = luma ? ql : qc;
-  const uint32_t total = (uint32_t)(g.mbw * g.mbh);
   const int rmx = g.RW - 1, rmy = g.RH - 1, cmx = g.RW / 2 - 1, cmy = g.RH / 2 - 1;
+  const bool src_vec = ((cur_pitch & 3) == 0) && ((reinterpret_cast<uintptr_t>(cur_y) & 3) == 0) &&
+                       ((reinterpret_cast<uintptr_t>(cur_uv) & 3) == 0);
 
   for (;;) {
     if (tid == 0) {
@@ -74,28 +78,30 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
     __syncthreads();
     const int mby = s.row;
     if (mby >= g.mbh) return;
+    // Source words of macroblock mbx: thread t < 64 holds luma row t/4, word
+    // t%4; threads 64..95 chroma row (t-64)/4, word (t-64)%4 (NV12 pairs).
+    // Read one macroblock ahead, off the row's dependency chain.
+    auto src_word = [&](int mbx_) -> uint32_t {
+      const int Xs = mbx_ * 16, Ys = mby * 16;
+      if (tid < 64) {
+        const int row = tid >> 2, gx = Xs + 4 * (tid & 3);
+        const uint8_t* rp = cur_y + (size_t)clampi(Ys + row, 0, g.H - 1) * cur_pitch;
+        if (src_vec && gx + 4 <= g.W) return __ldg(reinterpret_cast<const uint32_t*>(rp + gx));
+        uint32_t w = 0;
+        for (int k = 0; k < 4; ++k) w |= (uint32_t)__ldg(rp + clampi(gx + k, 0, g.W - 1)) << (8 * k);
+        return w;
+      }
+      const int i = tid - 64, row = i >> 2, pair = (Xs >> 1) + 2 * (i & 3);
+      const uint8_t* rp = cur_uv + (size_t)clampi((Ys >> 1) + row, 0, g.H / 2 - 1) * cur_pitch;
+      if (src_vec && pair + 2 <= g.W / 2) return __ldg(reinterpret_cast<const uint32_t*>(rp + 2 * pair));
+      uint32_t w = 0;
+      for (int k = 0; k < 4; ++k) w |= (uint32_t)__ldg(rp + 2 * clampi(pair + (k >> 1), 0, g.W / 2 - 1) + (k & 1)) << (8 * k);
+      return w;
+    };
+    uint32_t pf = src_word(0);
     for (int mbx = 0; mbx < g.mbw; ++mbx) {
       const int mb = mby * g.mbw + mbx, X = mbx * 16, Y = mby * 16, Xc = X >> 1, Yc = Y >> 1;
-      // ---- wait for the top neighbour ----------------------------------
-      if (tid == 0 && mby > 0) {
-        const uint32_t* pf = sc.progress(mby - 1);
-        bool ok = false, other = false;
-        const uint64_t t0 = global_ns(), budget = (uint64_t)max_wait * 1000u;  // max_wait in microseconds
-        for (uint32_t it = 0;; ++it) {
-          if (load_acquire(pf) >= (uint32_t)(mbx + 1)) { ok = true; break; }
-          if (load_acquire(sc.err()) != 0u) { other = true; break; }
-          if ((it & 15) == 15 && global_ns() - t0 > budget) break;
-          if (it > 4) __nanosleep(32);
-        }
-        if (!ok) {
-          if (!other && atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u) atomicExch(sc.err_detail(), (uint32_t)mb);
-          s.abort_flag = 1;
-        }
-      }
-      __syncthreads();
-      if (s.abort_flag) return;
-
-      // ---- neighbours (reconstructed, read from L2) and source ----------
+      const uint32_t total = (uint32_t)(g.mbw * g.mbh);
       const uint32_t sl = slice_of((uint32_t)mb, total, (uint32_t)num_slices);
       const bool top_exists = mby > 0, left_exists = mbx > 0;
       const bool top_av = top_exists && slice_of((uint32_t)(mb - g.mbw), total, (uint32_t)num_slices) == sl;
@@ -106,27 +112,65 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
       const bool plane_av = top_av && left_av &&
                             (!(flags & B200ENC_INTRA_CORNER_CHECK) ||
                              slice_of((uint32_t)(mb - g.mbw - 1), total, (uint32_t)num_slices) == sl);
-      if (tid < 16) {
-        s.top[tid] = top_exists ? __ldcg(rec_y + (size_t)clampi(Y - 1, 0, rmy) * rec_pitch + clampi(X + tid, 0, rmx)) : 128;
-      } else if (tid < 32) {
-        const int i = tid - 16;
-        s.left[i] = left_exists ? __ldcg(rec_y + (size_t)clampi(Y + i, 0, rmy) * rec_pitch + clampi(X - 1, 0, rmx)) : 128;
-      } else if (tid < 48) {
-        const int i = tid - 32, pl = i >> 3, k = i & 7;
-        s.tuv[pl][k] = top_av ? __ldcg(rec_uv + (size_t)clampi(Yc - 1, 0, cmy) * rec_pitch + 2 * clampi(Xc + k, 0, cmx) + pl) : 128;
-      } else if (tid < 64) {
-        const int i = tid - 48, pl = i >> 3, k = i & 7;
-        s.luv[pl][k] = left_av ? __ldcg(rec_uv + (size_t)clampi(Yc + k, 0, cmy) * rec_pitch + 2 * clampi(Xc - 1, 0, cmx) + pl) : 128;
-      } else if (tid == 64) {
-        s.corner = (top_exists && left_exists) ? __ldcg(rec_y + (size_t)clampi(Y - 1, 0, rmy) * rec_pitch + clampi(X - 1, 0, rmx)) : 128;
+      // ---- this MB's source (prefetched), the next MB's source requested --
+      {
+        const uint32_t w = pf;
+        if (tid < 64) {
+          const int row = tid >> 2, c0 = 4 * (tid & 3);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) s.src[row][c0 + k] = (int16_t)((w >> (8 * k)) & 255u);
+        } else {
+          const int i = tid - 64, row = i >> 2, x0 = 2 * (i & 3);
+          s.srcc[0][row][x0] = (int16_t)(w & 255u);
+          s.srcc[1][row][x0] = (int16_t)((w >> 8) & 255u);
+          s.srcc[0][row][x0 + 1] = (int16_t)((w >> 16) & 255u);
+          s.srcc[1][row][x0 + 1] = (int16_t)(w >> 24);
+        }
+        if (mbx + 1 < g.mbw) pf = src_word(mbx + 1);
       }
-      for (int i = tid; i < 256; i += 96)
-        s.src[i >> 4][i & 15] = __ldg(cur_y + (size_t)clampi(Y + (i >> 4), 0, g.H - 1) * cur_pitch + clampi(X + (i & 15), 0, g.W - 1));
-      for (int i = tid; i < 128; i += 96) {
-        const int pl = i >> 6, y = (i >> 3) & 7, x = i & 7;
-        s.srcc[pl][y][x] = __ldg(cur_uv + (size_t)clampi(Yc + y, 0, g.H / 2 - 1) * cur_pitch + 2 * clampi(Xc + x, 0, g.W / 2 - 1) + pl);
+      // ---- left and corner neighbours: this CTA's own previous MB --------
+      // (still in s.ry / s.ruv; rows past the clamp limit read its last row,
+      // as the clamped reads of the reference do)
+      if (tid < 16) {
+        s.left[tid] = left_exists ? s.ry[min(tid, rmy - Y)][15] : 128;
+      } else if (tid < 32) {
+        const int i = tid - 16, pl = i >> 3, k = i & 7;
+        s.luv[pl][k] = left_av ? s.ruv[min(k, cmy - Yc)][14 + pl] : 128;
+      } else if (tid == 32) {
+        s.corner = (top_exists && left_exists) ? s.prev_top15 : 128;
+      }
+      // ---- wait for the top neighbour, then its bottom lines --------------
+      if (tid == 0 && mby > 0) {
+        const uint32_t* pf_row = sc.progress(mby - 1);
+        bool ok = false, other = false;
+        const uint64_t t0 = global_ns(), budget = (uint64_t)max_wait * 1000u;  // max_wait in microseconds
+        for (uint32_t it = 0;; ++it) {
+          if (load_acquire(pf_row) >= (uint32_t)(mbx + 1)) { ok = true; break; }
+          if (load_acquire(sc.err()) != 0u) { other = true; break; }
+          if ((it & 15) == 15 && global_ns() - t0 > budget) break;
+          if (it > 16) __nanosleep(32);
+        }
+        if (!ok) {
+          if (!other && atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u) atomicExch(sc.err_detail(), (uint32_t)mb);
+          s.abort_flag = 1;
+        } else {
+          // 16-byte lines: row Y-1 from X, chroma row Yc-1 from 2*Xc (inside
+          // the picture's coded width; clamping applies when they are read)
+          *reinterpret_cast<uint4*>(s.topv) = __ldcg(reinterpret_cast<const uint4*>(rec_y + (size_t)(Y - 1) * rec_pitch + X));
+          *reinterpret_cast<uint4*>(s.topc) =
+              __ldcg(reinterpret_cast<const uint4*>(rec_uv + (size_t)(Yc - 1) * rec_pitch + X));
+        }
       }
       __syncthreads();
+      if (s.abort_flag) return;
+      if (tid < 16) {
+        s.top[tid] = top_exists ? s.topv[min(tid, rmx - X)] : 128;
+      } else if (tid < 32) {
+        const int i = tid - 16, pl = i >> 3, k = i & 7;
+        s.tuv[pl][k] = top_av ? s.topc[2 * min(k, cmx - Xc) + pl] : 128;
+      }
+      __syncthreads();
+      if (tid == 0) s.prev_top15 = s.topv[15];  // read by the next MB's corner, after the barriers below
 
       // ---- I16x16 candidates (intra_wavefront.comp:454-476) -------------
       if (tid < 32) {
@@ -314,6 +358,11 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
       __syncthreads();
 
       // ---- stores + publish progress ------------------------------------
+      // The row below reads only this MB's bottom luma and chroma lines
+      // (and, through its corner, those of MB x-1): the threads storing them
+      // fence their own stores, then thread 0 publishes after the barrier.
+      // The other stores need no fence (the next kernel on the stream sees
+      // them).
       if (tid < 48) {
         reinterpret_cast<uint4*>(levels + (size_t)mb * 384)[tid] = reinterpret_cast<const uint4*>(&s.lev[0][0])[tid];
       } else if (tid < 64) {
@@ -324,6 +373,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
           else
             for (int c = 0; c < 16 && X + c < g.RW; ++c) dst[c] = s.ry[row][c];
         }
+        if (row == 15) __threadfence();
       } else if (tid < 72) {
         const int row = tid - 64, gy = Yc + row;
         if (gy <= cmy) {
@@ -335,8 +385,8 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
               dst[2 * c + 1] = s.ruv[row][2 * c + 1];
             }
         }
+        if (row == 7) __threadfence();
       }
-      __threadfence();
       __syncthreads();
       if (tid == 0) store_release(sc.progress(mby), (uint32_t)(mbx + 1));
     }
