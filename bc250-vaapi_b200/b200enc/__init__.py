@@ -28,6 +28,8 @@ EXPORTS = [
     "b200enc_hevc_choose_luma_mode", "b200enc_hevc_deblock", "b200enc_hevc_build_hpel_10",
     "b200enc_hevc_motion_search_10", "b200enc_hevc_choose_luma_mode_10",
     "b200enc_tune_set", "b200enc_tune_get", "b200enc_tune_name", "b200enc_tune_load",
+    "b200enc_batch_create", "b200enc_batch_destroy", "b200enc_batch_stream", "b200enc_batch_set_graph",
+    "b200enc_batch_encode", "b200enc_batch_sync", "b200enc_batch_outputs", "b200enc_batch_graph_stats",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
     "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",
@@ -123,6 +125,17 @@ def load_library(path=LIB_PATH):
     lib.b200enc_ctx_set_me.argtypes = [ctypes.POINTER(GpuContext), _i, ctypes.c_char_p, ctypes.c_float]
     lib.b200enc_host_register.argtypes = [ctypes.POINTER(GpuContext), _vp, ctypes.c_size_t]
     lib.b200enc_host_unregister.argtypes = [ctypes.POINTER(GpuContext), _vp]
+    lib.b200enc_batch_create.restype = _vp
+    lib.b200enc_batch_create.argtypes = [_i, _vp, _vp, _i, _i, ctypes.c_float, _i]
+    lib.b200enc_batch_destroy.argtypes = [_vp]
+    lib.b200enc_batch_destroy.restype = None
+    lib.b200enc_batch_stream.restype = _vp
+    lib.b200enc_batch_stream.argtypes = [_vp]
+    lib.b200enc_batch_set_graph.argtypes = [_vp, _i]
+    lib.b200enc_batch_encode.argtypes = [_vp, _vp]
+    lib.b200enc_batch_sync.argtypes = [_vp]
+    lib.b200enc_batch_outputs.argtypes = [_vp, _i] + [ctypes.POINTER(_vp)] * 7 + [ctypes.POINTER(_i)]
+    lib.b200enc_batch_graph_stats.argtypes = [_vp, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long)]
     lib.b200enc_tune_set.argtypes = [_i, _i]
     lib.b200enc_tune_get.argtypes = [_i]
     lib.b200enc_tune_name.argtypes = [_i]
@@ -524,6 +537,79 @@ class Context:
         _check(self.L.b200enc_ctx_me_stats(ctypes.byref(self.ctx), *[ctypes.byref(x) for x in v]),
                "b200enc_ctx_me_stats")
         return tuple(x.value for x in v)
+
+
+class BatchFrame(ctypes.Structure):
+    _fields_ = [("y", _vp), ("uv", _vp), ("pitch", _i), ("qp", _i), ("is_intra", _i), ("num_slices", _i)]
+
+
+class Batch:
+    """Many streams of their own frame sizes through one launch per stage
+    (b200enc_batch_*): sizes = [(W, H), ...]; me_mode 0 full search, 1
+    learned (BF16 network), 3 learned (FP8 network)."""
+
+    def __init__(self, sizes, search_range=32, me_mode=0, conf=0.9, deblock=1, graph=False):
+        self.L = lib()
+        self.sizes = list(sizes)
+        n = len(self.sizes)
+        ws = (ctypes.c_int * n)(*[w for w, _ in self.sizes])
+        hs = (ctypes.c_int * n)(*[h for _, h in self.sizes])
+        self.h = self.L.b200enc_batch_create(n, ws, hs, search_range, me_mode, ctypes.c_float(conf), deblock)
+        if not self.h:
+            raise RuntimeError("b200enc_batch_create failed")
+        self.frames = (BatchFrame * n)()
+        _check(self.L.b200enc_batch_set_graph(self.h, int(graph)), "b200enc_batch_set_graph")
+
+    def close(self):
+        if self.h:
+            self.L.b200enc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stream(self):
+        return self.L.b200enc_batch_stream(self.h)
+
+    def encode(self, frames, qps, intra, num_slices=1):
+        """frames: NV12 objects, one per stream; qps, intra: per stream."""
+        for s, f in enumerate(frames):
+            self.frames[s] = BatchFrame(f.y.data_ptr(), f.uv.data_ptr(), f.pitch, int(qps[s]), int(bool(intra[s])),
+                                        num_slices)
+        _check(self.L.b200enc_batch_encode(self.h, self.frames), "b200enc_batch_encode")
+
+    def sync(self):
+        return self.L.b200enc_batch_sync(self.h)
+
+    def graph_stats(self):
+        a, b = ctypes.c_long(), ctypes.c_long()
+        _check(self.L.b200enc_batch_graph_stats(self.h, ctypes.byref(a), ctypes.byref(b)), "b200enc_batch_graph_stats")
+        return a.value, b.value
+
+    def outputs_host(self, s):
+        """Host copies of stream s's latest outputs and reconstruction."""
+        import numpy as np
+        import torch
+        p = [_vp() for _ in range(7)]
+        pitch = _i()
+        _check(self.L.b200enc_batch_outputs(self.h, s, *[ctypes.byref(x) for x in p], ctypes.byref(pitch)),
+               "b200enc_batch_outputs")
+        W, H = self.sizes[s]
+        CW, CH = coded(W, H)
+        mbs = (CW // 16) * (CH // 16)
+        torch.cuda.synchronize()
+        rd = lambda ptr, n: device_view(ptr.value, n).cpu().numpy()
+        out = {"levels": rd(p[0], mbs * 768).view(np.int16).reshape(mbs, 24, 16),
+               "dc": rd(p[1], mbs * 96).view(np.int32).reshape(mbs, 24),
+               "nz": rd(p[2], mbs * 96).view(np.uint32).reshape(mbs, 24),
+               "pred_mode": rd(p[3], mbs * 4).view(np.uint32),
+               "mv": rd(p[4], mbs * 16).view(np.int32).reshape(mbs, 4)}
+        out["rec_y"] = rd(p[5], CH * pitch.value).reshape(CH, pitch.value)[:, :CW]
+        out["rec_uv"] = rd(p[6], CH // 2 * pitch.value).reshape(CH // 2, pitch.value)[:, :CW]
+        return out
 
 
 class _DeviceSpan:

@@ -9,3 +9,18 @@
 
 // Value of an autotuned launch parameter (B200ENC_TUNE_*), 0 = the default.
 int b200enc_tuned(int key);
+
+// ---- batched stage launchers (batch.cu drives them) ------------------------
+namespace b200enc {
+struct BatchTab;
+}
+#include <cuda_runtime.h>
+int b200enc_me_batch_launch(const b200enc::BatchTab& bt, int range, const int* list, const int* count, int ctas,
+                            cudaStream_t st);
+int b200enc_p_frame_batch_launch(const b200enc::BatchTab& bt, int n, cudaStream_t st);
+int b200enc_i_frame_batch_launch(const b200enc::BatchTab& bt, int ctas, uint32_t max_wait, cudaStream_t st);
+int b200enc_deblock_batch_rows(int max_mbw, int max_mbh);
+int b200enc_deblock_batch_launch(const b200enc::BatchTab& bt, int max_mbw, int ctas, uint32_t max_wait,
+                                 cudaStream_t st);
+int b200enc_proposal_me_batch(void* h, const b200enc::BatchTab& bt, int n, int range, int lambda, int mode,
+                              float param, cudaStream_t st);

@@ -220,4 +220,56 @@ struct Scratch {
 };
 inline size_t scratch_words(int mbh) { return 4 + 2 * (size_t)mbh; }
 
+// ---------------------------------------------------------------------------
+// Batched steps (batch.cu): one frame of each of many streams, of uneven
+// sizes, through one launch per stage. Each stage walks the items of one
+// set of streams laid end to end (the P streams' macroblocks, the I
+// streams' macroblock rows, every stream's deblocking row groups); an item
+// finds its stream by binary search over the set's prefix sums.
+// ---------------------------------------------------------------------------
+struct BatchStream {
+  Geo g;
+  int qp, is_intra, num_slices, intra_flags;
+  int lambda, zero_thresh, has_hist;
+  const uint8_t *cur_y, *cur_uv;
+  int cur_pitch;
+  const uint8_t *ref_y, *ref_uv;  // the previous reconstruction (P frames)
+  uint8_t *rec_y, *rec_uv;        // this frame's reconstruction
+  int rec_pitch;                  // of both reconstructions
+  int16_t* levels;
+  int32_t* dc;
+  uint32_t *nz, *pred_mode;
+  MV* mv;             // this frame's field
+  const MV* mv_prev;  // the previous P frame's field (the learned form's history)
+  uint32_t *scr_intra, *scr_db;  // wavefront scratch (scratch_words(mbh) words each)
+};
+
+struct BatchSet {
+  const BatchStream* st;  // every stream of the batch
+  const int* idx;         // [n] the set's streams
+  const int* prefix;      // [n + 1] item offsets
+  int n;
+  __device__ __forceinline__ int total() const { return n > 0 ? prefix[n] : 0; }
+  // position k in the set of the stream holding `item` (0 <= item < total())
+  __device__ __forceinline__ int find(int item) const {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (prefix[mid] <= item) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  }
+  __device__ __forceinline__ const BatchStream& stream(int k) const { return st[idx[k]]; }
+};
+
+struct BatchTab {
+  BatchSet p_mbs;   // macroblocks of the streams coding a P frame (the compact P index)
+  BatchSet i_rows;  // macroblock rows of the streams coding an I frame
+  BatchSet groups;  // deblocking row groups of every stream
+  MV* mvc;          // motion vectors by compact P index
+  uint32_t* ticket; // [0] intra rows, [1] deblocking groups
+  int db_rows;      // macroblock rows per deblocking group
+};
+
 }  // namespace b200enc

@@ -177,36 +177,63 @@ __device__ __forceinline__ bool wait_shared(const volatile uint32_t* flag, const
   return false;
 }
 
-__global__ void deblock_kernel(int mbw, int mbh, int R, int qp, int is_intra,
-                                                      const uint32_t* __restrict__ nzm, const MV* __restrict__ mvs,
-                                                      uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch,
-                                                      uint32_t* scratch, uint32_t max_wait) {  // max_wait in microseconds
+// BATCH: the group tickets (bt.ticket[1]) run over the row groups of every
+// stream of a batch (bt.groups, R = bt.db_rows rows each); a group waits
+// only on its own stream's rows and scratch. Dynamic shared memory is sized
+// for the widest stream.
+template <bool BATCH>
+__global__ void deblock_kernel(int mbw_, int mbh_, int R, int qp_, int is_intra_,
+                                                      const uint32_t* __restrict__ nzm_, const MV* __restrict__ mvs_,
+                                                      uint8_t* rec_y_, uint8_t* rec_uv_, int rec_pitch_,
+                                                      uint32_t* scratch_, uint32_t max_wait, BatchTab bt) {  // max_wait in microseconds
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ int s_group, s_abort;
-  const DbPlan P = db_plan(mbw, R);
-  uint8_t* ly = smem + P.luma_off;
-  uint8_t* cy = smem + P.chroma_off;
-  uint8_t* bsm = smem + P.bs_off;
-  volatile uint32_t* prog = reinterpret_cast<volatile uint32_t*>(smem + P.prog_off);
-  const Scratch sc{scratch};
-  uint32_t* gprog_luma = scratch + 4;
-  uint32_t* gprog_chroma = scratch + 4 + mbh;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nthr = blockDim.x;
-  const int qpc = chroma_qp(qp);
-  const int al = kAlpha[qp], be = kBeta[qp], alc = kAlpha[qpc], bec = kBeta[qpc];
-  const int tcl1 = kTc0[qp][0], tcl2 = kTc0[qp][1], tcl3 = kTc0[qp][2];
-  const int tcc1 = kTc0[qpc][0], tcc2 = kTc0[qpc][1], tcc3 = kTc0[qpc][2];
 
   auto scol = [](int mx) { return 16 * (mx & (kDbRing - 1)); };  // byte offset of MB column mx in a ring row
 
   for (;;) {
     if (tid == 0) {
-      s_group = (int)atomicAdd(sc.ticket(), 1u);
+      s_group = (int)atomicAdd(BATCH ? bt.ticket + 1 : Scratch{scratch_}.ticket(), 1u);
       s_abort = 0;
     }
     __syncthreads();
-    const int y0 = s_group * R;
+    int mbw = mbw_, mbh = mbh_, qp = qp_, is_intra = is_intra_, rec_pitch = rec_pitch_;
+    const uint32_t* nzm = nzm_;
+    const MV* mvs = mvs_;
+    uint8_t *rec_y = rec_y_, *rec_uv = rec_uv_;
+    uint32_t* scratch = scratch_;
+    int group = s_group;
+    if (BATCH) {
+      if (group >= bt.groups.total()) return;
+      const int k = bt.groups.find(group);
+      const BatchStream& st = bt.groups.stream(k);
+      group -= bt.groups.prefix[k];
+      mbw = st.g.mbw;
+      mbh = st.g.mbh;
+      qp = st.qp;
+      is_intra = st.is_intra;
+      nzm = st.nz;
+      mvs = st.mv;
+      rec_y = st.rec_y;
+      rec_uv = st.rec_uv;
+      rec_pitch = st.rec_pitch;
+      scratch = st.scr_db;
+    }
+    const int y0 = group * R;
     if (y0 >= mbh) return;
+    const DbPlan P = db_plan(mbw, R);
+    uint8_t* ly = smem + P.luma_off;
+    uint8_t* cy = smem + P.chroma_off;
+    uint8_t* bsm = smem + P.bs_off;
+    volatile uint32_t* prog = reinterpret_cast<volatile uint32_t*>(smem + P.prog_off);
+    const Scratch sc{scratch};
+    uint32_t* gprog_luma = scratch + 4;
+    uint32_t* gprog_chroma = scratch + 4 + mbh;
+    const int qpc = chroma_qp(qp);
+    const int al = kAlpha[qp], be = kBeta[qp], alc = kAlpha[qpc], bec = kBeta[qpc];
+    const int tcl1 = kTc0[qp][0], tcl2 = kTc0[qp][1], tcl3 = kTc0[qp][2];
+    const int tcc1 = kTc0[qpc][0], tcc2 = kTc0[qpc][1], tcc3 = kTc0[qpc][2];
     const int rows = min(R, mbh - y0);
     const bool has_next = y0 + rows < mbh;
 
@@ -602,10 +629,31 @@ extern "C" int b200enc_deblock_launch(int mbw, int mbh, int qp, int is_intra, co
   const DbPlan P = db_plan(mbw, R);
   const int groups = (mbh + R - 1) / R;
   if (ctas <= 0 || ctas > groups) ctas = groups;
-  if (cudaFuncSetAttribute(deblock_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.bytes) != cudaSuccess)
+  if (cudaFuncSetAttribute(deblock_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.bytes) !=
+      cudaSuccess)
     return -1;
-  deblock_kernel<<<ctas, 64 * R + 128, P.bytes, (cudaStream_t)stream>>>(mbw, mbh, R, qp, is_intra, nz, (const MV*)mv, rec_y,
-                                                                  rec_uv, rec_pitch, scratch, max_wait);
+  deblock_kernel<false><<<ctas, 64 * R + 128, P.bytes, (cudaStream_t)stream>>>(
+      mbw, mbh, R, qp, is_intra, nz, (const MV*)mv, rec_y, rec_uv, rec_pitch, scratch, max_wait, BatchTab{});
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// Rows per group a batch's deblocking uses for streams up to max_mbw
+// macroblocks wide (0 if none fits).
+int b200enc_deblock_batch_rows(int max_mbw, int max_mbh) { return db_rows_per_cta(max_mbw, max_mbh); }
+
+// The deblocking of every stream of a batch: `ctas` persistent CTAs over
+// bt.groups (bt.db_rows rows per group; each stream's scratch zeroed and
+// bt.ticket[1] = 0 by the caller).
+int b200enc_deblock_batch_launch(const BatchTab& bt, int max_mbw, int ctas, uint32_t max_wait, cudaStream_t st) {
+  if (ctas <= 0) return 0;
+  const int R = bt.db_rows;
+  if (R <= 0) return -1;
+  const DbPlan P = db_plan(max_mbw, R);
+  if (cudaFuncSetAttribute(deblock_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.bytes) !=
+      cudaSuccess)
+    return -1;
+  deblock_kernel<true><<<ctas, 64 * R + 128, P.bytes, st>>>(0, 0, R, 0, 0, nullptr, nullptr, nullptr, nullptr, 0,
+                                                            nullptr, max_wait, bt);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -52,32 +52,69 @@ __device__ __forceinline__ int hsign(int row, int idx) {
   return ((m >> idx) & 1) ? -1 : 1;
 }
 
-__global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__ cur_y,
-                                                     const uint8_t* __restrict__ cur_uv, int cur_pitch, Geo g,
-                                                     int qp, int num_slices, int16_t* __restrict__ levels,
-                                                     int32_t* __restrict__ dc, uint32_t* __restrict__ nzm,
-                                                     uint32_t* __restrict__ pred_mode, MV* __restrict__ mvs,
-                                                     uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch,
-                                                     uint32_t* scratch, uint32_t max_wait, int flags) {
+// BATCH: the row tickets (bt.ticket[0]) run over the rows of every stream
+// of a batch that codes an I frame; a row waits on its own stream's
+// progress words (that stream's scratch). Tickets are taken in order and a
+// row only waits on an earlier row of its stream, so every wait is on a row
+// some running CTA owns.
+template <bool BATCH>
+__global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__ cur_y_,
+                                                     const uint8_t* __restrict__ cur_uv_, int cur_pitch_, Geo g_,
+                                                     int qp_, int num_slices_, int16_t* __restrict__ levels_,
+                                                     int32_t* __restrict__ dc_, uint32_t* __restrict__ nzm_,
+                                                     uint32_t* __restrict__ pred_mode_, MV* __restrict__ mvs_,
+                                                     uint8_t* rec_y_, uint8_t* rec_uv_, int rec_pitch_,
+                                                     uint32_t* scratch_, uint32_t max_wait, int flags_, BatchTab bt) {
   __shared__ IShared s;
-  const Scratch sc{scratch};
   const int tid = threadIdx.x;
   const int b = tid >> 2, r = tid & 3;
   const bool luma = b < 16;
-  const QP ql = make_qp(qp, true), qc = make_qp(chroma_qp(qp), true);
-  const QP& q = luma ? ql : qc;
-  const int rmx = g.RW - 1, rmy = g.RH - 1, cmx = g.RW / 2 - 1, cmy = g.RH / 2 - 1;
-  const bool src_vec = ((cur_pitch & 3) == 0) && ((reinterpret_cast<uintptr_t>(cur_y) & 3) == 0) &&
-                       ((reinterpret_cast<uintptr_t>(cur_uv) & 3) == 0);
 
   for (;;) {
     if (tid == 0) {
-      s.row = (int)atomicAdd(sc.ticket(), 1u);
+      s.row = (int)atomicAdd(BATCH ? bt.ticket : Scratch{scratch_}.ticket(), 1u);
       s.abort_flag = 0;
     }
     __syncthreads();
-    const int mby = s.row;
-    if (mby >= g.mbh) return;
+    const uint8_t *cur_y = cur_y_, *cur_uv = cur_uv_;
+    int cur_pitch = cur_pitch_, qp = qp_, num_slices = num_slices_, rec_pitch = rec_pitch_, flags = flags_;
+    Geo g = g_;
+    int16_t* levels = levels_;
+    int32_t* dc = dc_;
+    uint32_t *nzm = nzm_, *pred_mode = pred_mode_, *scratch = scratch_;
+    MV* mvs = mvs_;
+    uint8_t *rec_y = rec_y_, *rec_uv = rec_uv_;
+    int mby = s.row;
+    if (BATCH) {
+      if (mby >= bt.i_rows.total()) return;
+      const int k = bt.i_rows.find(mby);
+      const BatchStream& st = bt.i_rows.stream(k);
+      mby -= bt.i_rows.prefix[k];
+      g = st.g;
+      cur_y = st.cur_y;
+      cur_uv = st.cur_uv;
+      cur_pitch = st.cur_pitch;
+      qp = st.qp;
+      num_slices = st.num_slices;
+      flags = st.intra_flags;
+      levels = st.levels;
+      dc = st.dc;
+      nzm = st.nz;
+      pred_mode = st.pred_mode;
+      mvs = st.mv;
+      rec_y = st.rec_y;
+      rec_uv = st.rec_uv;
+      rec_pitch = st.rec_pitch;
+      scratch = st.scr_intra;
+    } else if (mby >= g.mbh) {
+      return;
+    }
+    const Scratch sc{scratch};
+    const QP ql = make_qp(qp, true), qc = make_qp(chroma_qp(qp), true);
+    const QP& q = luma ? ql : qc;
+    const int rmx = g.RW - 1, rmy = g.RH - 1, cmx = g.RW / 2 - 1, cmy = g.RH / 2 - 1;
+    const bool src_vec = ((cur_pitch & 3) == 0) && ((reinterpret_cast<uintptr_t>(cur_y) & 3) == 0) &&
+                         ((reinterpret_cast<uintptr_t>(cur_uv) & 3) == 0);
     // Source words of macroblock mbx: thread t < 64 holds luma row t/4, word
     // t%4; threads 64..95 chroma row (t-64)/4, word (t-64)%4 (NV12 pairs).
     // Read one macroblock ahead, off the row's dependency chain.
@@ -421,9 +458,19 @@ extern "C" int b200enc_i_frame_launch(const uint8_t* cur_y, const uint8_t* cur_u
   if (ctas <= 0) ctas = b200enc_tuned(B200ENC_TUNE_INTRA_CTAS);
   if (ctas <= 0) ctas = g.mbh;
   if (ctas > g.mbh) ctas = g.mbh;
-  i_frame_kernel<<<ctas, 96, 0, (cudaStream_t)stream>>>(cur_y, cur_uv, cur_pitch, g, qp, num_slices, levels, dc, nz,
-                                                       pred_mode, (MV*)mv, rec_y, rec_uv, rec_pitch, scratch,
-                                                       max_wait, flags);
+  i_frame_kernel<false><<<ctas, 96, 0, (cudaStream_t)stream>>>(cur_y, cur_uv, cur_pitch, g, qp, num_slices, levels, dc,
+                                                              nz, pred_mode, (MV*)mv, rec_y, rec_uv, rec_pitch,
+                                                              scratch, max_wait, flags, BatchTab{});
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// The intra wavefront of every I-frame stream of a batch: `ctas` persistent
+// CTAs over bt.i_rows (each stream's scratch zeroed and bt.ticket[0] = 0 by
+// the caller).
+int b200enc_i_frame_batch_launch(const BatchTab& bt, int ctas, uint32_t max_wait, cudaStream_t st) {
+  if (ctas <= 0) return 0;
+  i_frame_kernel<true><<<ctas, 96, 0, st>>>(nullptr, nullptr, 0, Geo{}, 0, 1, nullptr, nullptr, nullptr, nullptr,
+                                            nullptr, nullptr, nullptr, 0, nullptr, max_wait, 0, bt);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

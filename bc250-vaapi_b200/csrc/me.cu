@@ -32,27 +32,57 @@ struct MeShared {
   RefineShared rf;
 };
 
-template <int R, bool LIST>
-__global__ void __launch_bounds__(2 * R) me_full_search_kernel(const uint8_t* __restrict__ cur, int cur_pitch,
-                                                               const uint8_t* __restrict__ ref, int ref_pitch,
-                                                               Geo g, int lambda, int zero_thresh,
-                                                               MV* __restrict__ out, const int* __restrict__ mb_list,
-                                                               const int* __restrict__ mb_count, int flags) {
+// Where a CTA's macroblocks come from (MODE): 0 one CTA per MB of one frame;
+// 1 a persistent grid over a list of that frame's MBs; 2 a persistent grid
+// over every P macroblock of a batch; 3 over a list of compact batch P
+// indices (the learned form's fallback in a batch). The search itself is
+// the same in all four.
+enum : int { kMeGrid = 0, kMeList = 1, kMeBatch = 2, kMeBatchList = 3 };
+
+template <int R, int MODE>
+__global__ void __launch_bounds__(2 * R) me_full_search_kernel(const uint8_t* __restrict__ cur_, int cur_pitch_,
+                                                               const uint8_t* __restrict__ ref_, int ref_pitch_,
+                                                               Geo g_, int lambda_, int zero_thresh_,
+                                                               MV* __restrict__ out_, const int* __restrict__ mb_list,
+                                                               const int* __restrict__ mb_count, int flags,
+                                                               BatchTab bt) {
   constexpr int NT = 2 * R;
   using S = MeShared<R>;
   constexpr int WP = S::WP, WW = S::WW, SIDE = 2 * R + 1;
   __shared__ S sh;
   const int tid = threadIdx.x;
-  // list mode: a persistent grid walks the listed MBs; otherwise one CTA per MB
-  const int n_items = LIST ? *mb_count : 1;
-  for (int item = LIST ? (int)blockIdx.x : 0; item < n_items; item += LIST ? (int)gridDim.x : 1) {
+  const int n_items = MODE == kMeGrid ? 1 : (MODE == kMeBatch ? bt.p_mbs.total() : *mb_count);
+  for (int item = MODE == kMeGrid ? 0 : (int)blockIdx.x; item < n_items; item += MODE == kMeGrid ? 1 : (int)gridDim.x) {
   int mbx = blockIdx.x, mby = blockIdx.y;
-  if (LIST) {
+  const uint8_t* cur = cur_;
+  const uint8_t* ref = ref_;
+  int cur_pitch = cur_pitch_, ref_pitch = ref_pitch_, lambda = lambda_, zero_thresh = zero_thresh_;
+  Geo g = g_;
+  MV* o;
+  if (MODE == kMeList) {
     const int mb = mb_list[item];
     mby = mb / g.mbw;
     mbx = mb - mby * g.mbw;
-    __syncthreads();  // the previous item's shared memory is no longer read
   }
+  if (MODE == kMeBatch || MODE == kMeBatchList) {
+    const int ci = MODE == kMeBatch ? item : mb_list[item];
+    const int k = bt.p_mbs.find(ci);
+    const BatchStream& st = bt.p_mbs.stream(k);
+    const int local = ci - bt.p_mbs.prefix[k];
+    g = st.g;
+    mby = local / g.mbw;
+    mbx = local - mby * g.mbw;
+    cur = st.cur_y;
+    cur_pitch = st.cur_pitch;
+    ref = st.ref_y;
+    ref_pitch = st.rec_pitch;
+    lambda = st.lambda;
+    zero_thresh = st.zero_thresh;
+    o = bt.mvc + ci;
+  } else {
+    o = out_ + (size_t)mby * g.mbw + mbx;
+  }
+  if (MODE != kMeGrid) __syncthreads();  // the previous item's shared memory is no longer read
   const int X = mbx * 16, Y = mby * 16;
   const int ox = X - R - 4, oy = Y - R - 4;  // window origin (multiple of 4)
 
@@ -94,7 +124,6 @@ __global__ void __launch_bounds__(2 * R) me_full_search_kernel(const uint8_t* __
     z = sad4_acc(sh.cur[i], sh.win[(R + 4 + r) * WW + (R + 4) / 4 + w], z);
   }
   const uint32_t sad0 = block_sum<NT>(z, sh.red);
-  MV* o = out + (size_t)mby * g.mbw + mbx;
   if (zero_thresh >= 0 && sad0 <= (uint32_t)zero_thresh) {
     if (tid == 0) *o = MV{0, 0, sad0, (flags & B200ENC_ME_LOG_INTEGER) ? me_log_word(0, 0, true) : 0u};
     continue;
@@ -196,22 +225,27 @@ extern "C" int b200enc_me_full_search_ex(const uint8_t* cur_y, int cur_pitch, co
   dim3 grid = mb_list ? dim3(std::min(list_capacity, per_sm * sms)) : dim3(g.mbw, g.mbh);
   cudaStream_t st = (cudaStream_t)stream;
   const bool list = mb_list != nullptr;
+  const BatchTab none{};
   switch (range) {
     case 16:
       if (list)
-        me_full_search_kernel<16, true><<<grid, 32, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda,
-                                                             zero_thresh, (MV*)mv_out, mb_list, mb_count, flags);
+        me_full_search_kernel<16, kMeList><<<grid, 32, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda,
+                                                                zero_thresh, (MV*)mv_out, mb_list, mb_count, flags,
+                                                                none);
       else
-        me_full_search_kernel<16, false><<<grid, 32, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda,
-                                                              zero_thresh, (MV*)mv_out, mb_list, mb_count, flags);
+        me_full_search_kernel<16, kMeGrid><<<grid, 32, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda,
+                                                                zero_thresh, (MV*)mv_out, mb_list, mb_count, flags,
+                                                                none);
       break;
     case 32:
       if (list)
-        me_full_search_kernel<32, true><<<grid, 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda,
-                                                             zero_thresh, (MV*)mv_out, mb_list, mb_count, flags);
+        me_full_search_kernel<32, kMeList><<<grid, 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda,
+                                                                zero_thresh, (MV*)mv_out, mb_list, mb_count, flags,
+                                                                none);
       else
-        me_full_search_kernel<32, false><<<grid, 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda,
-                                                              zero_thresh, (MV*)mv_out, mb_list, mb_count, flags);
+        me_full_search_kernel<32, kMeGrid><<<grid, 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, lambda,
+                                                                zero_thresh, (MV*)mv_out, mb_list, mb_count, flags,
+                                                                none);
       break;
     default:
       return -1;
@@ -224,4 +258,33 @@ extern "C" int b200enc_me_full_search(const uint8_t* cur_y, int cur_pitch, const
                                       void* mv_out, void* stream) {
   return b200enc_me_full_search_ex(cur_y, cur_pitch, ref_y, ref_pitch, W, H, RW, RH, range, lambda, zero_thresh,
                                    mv_out, nullptr, nullptr, 0, 0, stream);
+}
+
+// Batched full search: every P macroblock of a batch (list == nullptr: a
+// persistent grid of `ctas` CTAs over the compact P index), or the compact
+// indices of a list (the learned form's fallback). MVs go to bt.mvc.
+int b200enc_me_batch_launch(const BatchTab& bt, int range, const int* list, const int* count, int ctas,
+                            cudaStream_t st) {
+  if (ctas <= 0) return -1;
+  switch (range) {
+    case 16:
+      if (list)
+        me_full_search_kernel<16, kMeBatchList><<<ctas, 32, 0, st>>>(nullptr, 0, nullptr, 0, Geo{}, 0, 0, nullptr,
+                                                                     list, count, 0, bt);
+      else
+        me_full_search_kernel<16, kMeBatch><<<ctas, 32, 0, st>>>(nullptr, 0, nullptr, 0, Geo{}, 0, 0, nullptr, nullptr,
+                                                                 nullptr, 0, bt);
+      break;
+    case 32:
+      if (list)
+        me_full_search_kernel<32, kMeBatchList><<<ctas, 64, 0, st>>>(nullptr, 0, nullptr, 0, Geo{}, 0, 0, nullptr,
+                                                                     list, count, 0, bt);
+      else
+        me_full_search_kernel<32, kMeBatch><<<ctas, 64, 0, st>>>(nullptr, 0, nullptr, 0, Geo{}, 0, 0, nullptr, nullptr,
+                                                                 nullptr, 0, bt);
+      break;
+    default:
+      return -1;
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -102,24 +102,66 @@ __device__ __forceinline__ void stage16_clamped(uint8_t* dst, const uint8_t* row
 
 // One CTA holds blockDim.y macroblocks of a row (the autotuner's tile
 // shape: 1, 2 or 4), 96 threads (three warps) each; a macroblock's shared
-// state is its slice of the dynamic shared memory.
-__global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict__ cur_y, const uint8_t* __restrict__ cur_uv,
-                                                  int cur_pitch, const uint8_t* __restrict__ ref_y,
-                                                  const uint8_t* __restrict__ ref_uv, int ref_pitch, Geo g, int qp,
-                                                  const MV* __restrict__ mvs, int16_t* __restrict__ levels,
-                                                  int32_t* __restrict__ dc, uint32_t* __restrict__ nzm,
-                                                  uint32_t* __restrict__ pred_mode, uint8_t* __restrict__ rec_y,
-                                                  uint8_t* __restrict__ rec_uv, int rec_pitch) {
+// state is its slice of the dynamic shared memory. BATCH: one CTA per P
+// macroblock of a batch (compact index blockIdx.x), which finds its stream,
+// takes its vector from the batch's compact field and stores it into the
+// stream's own field.
+template <bool BATCH>
+__global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict__ cur_y_, const uint8_t* __restrict__ cur_uv_,
+                                                  int cur_pitch_, const uint8_t* __restrict__ ref_y_,
+                                                  const uint8_t* __restrict__ ref_uv_, int ref_pitch_, Geo g_, int qp_,
+                                                  const MV* __restrict__ mvs, int16_t* __restrict__ levels_,
+                                                  int32_t* __restrict__ dc_, uint32_t* __restrict__ nzm_,
+                                                  uint32_t* __restrict__ pred_mode_, uint8_t* __restrict__ rec_y_,
+                                                  uint8_t* __restrict__ rec_uv_, int rec_pitch_, BatchTab bt) {
   extern __shared__ __align__(16) uint8_t p_smem[];
   PShared& s = reinterpret_cast<PShared*>(p_smem)[threadIdx.y];
   const int tid = threadIdx.x;
-  // a tile reaching past the right edge computes a copy of the last
-  // macroblock and stores nothing
-  const int mbx_t = blockIdx.x * blockDim.y + threadIdx.y;
-  const bool active = mbx_t < g.mbw;
-  const int mbx = active ? mbx_t : g.mbw - 1, mby = blockIdx.y, mb = mby * g.mbw + mbx;
+  const uint8_t *cur_y = cur_y_, *cur_uv = cur_uv_, *ref_y = ref_y_, *ref_uv = ref_uv_;
+  int cur_pitch = cur_pitch_, ref_pitch = ref_pitch_, qp = qp_, rec_pitch = rec_pitch_;
+  Geo g = g_;
+  int16_t* levels = levels_;
+  int32_t* dc = dc_;
+  uint32_t *nzm = nzm_, *pred_mode = pred_mode_;
+  uint8_t *rec_y = rec_y_, *rec_uv = rec_uv_;
+  bool active;
+  int mbx, mby, mb;
+  MV mv;
+  if (BATCH) {
+    const int ci = blockIdx.x;
+    const int k = bt.p_mbs.find(ci);
+    const BatchStream& st = bt.p_mbs.stream(k);
+    mb = ci - bt.p_mbs.prefix[k];
+    g = st.g;
+    mby = mb / g.mbw;
+    mbx = mb - mby * g.mbw;
+    active = true;
+    cur_y = st.cur_y;
+    cur_uv = st.cur_uv;
+    cur_pitch = st.cur_pitch;
+    ref_y = st.ref_y;
+    ref_uv = st.ref_uv;
+    ref_pitch = rec_pitch = st.rec_pitch;
+    qp = st.qp;
+    levels = st.levels;
+    dc = st.dc;
+    nzm = st.nz;
+    pred_mode = st.pred_mode;
+    rec_y = st.rec_y;
+    rec_uv = st.rec_uv;
+    mv = bt.mvc[ci];
+    if (tid == 0) st.mv[mb] = mv;
+  } else {
+    // a tile reaching past the right edge computes a copy of the last
+    // macroblock and stores nothing
+    const int mbx_t = blockIdx.x * blockDim.y + threadIdx.y;
+    active = mbx_t < g.mbw;
+    mbx = active ? mbx_t : g.mbw - 1;
+    mby = blockIdx.y;
+    mb = mby * g.mbw + mbx;
+    mv = mvs[mb];
+  }
   const int X = mbx * 16, Y = mby * 16, Xc = X >> 1, Yc = Y >> 1;
-  const MV mv = mvs[mb];
   const int ix0 = X + (mv.mvx >> 2), iy0 = Y + (mv.mvy >> 2), fx = mv.mvx & 3, fy = mv.mvy & 3;
   const int ixc = Xc + (mv.mvx >> 3), iyc = Yc + (mv.mvy >> 3), fxc = mv.mvx & 7, fyc = mv.mvy & 7;
   const int cmx = g.RW / 2 - 1, cmy = g.RH / 2 - 1;
@@ -288,8 +330,17 @@ extern "C" int b200enc_p_frame(const uint8_t* cur_y, const uint8_t* cur_uv, int 
   if ((ref_pitch & 1) || (((uintptr_t)ref_uv) & 1)) return -1;
   Geo g{W, H, RW, RH, (W + 15) / 16, (H + 15) / 16};
   const int T = b200enc_tuned(B200ENC_TUNE_PCHAIN_MBS_PER_CTA) > 0 ? b200enc_tuned(B200ENC_TUNE_PCHAIN_MBS_PER_CTA) : 1;
-  p_mb_kernel<<<dim3((g.mbw + T - 1) / T, g.mbh), dim3(96, T), T * sizeof(PShared), (cudaStream_t)stream>>>(
+  p_mb_kernel<false><<<dim3((g.mbw + T - 1) / T, g.mbh), dim3(96, T), T * sizeof(PShared), (cudaStream_t)stream>>>(
       cur_y, cur_uv, cur_pitch, ref_y, ref_uv, ref_pitch, g, qp, (const MV*)mv, levels, dc, nz, pred_mode, rec_y,
-      rec_uv, rec_pitch);
+      rec_uv, rec_pitch, BatchTab{});
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// The P chain of every P macroblock of a batch (n = the compact P count).
+int b200enc_p_frame_batch_launch(const BatchTab& bt, int n, cudaStream_t st) {
+  if (n <= 0) return 0;
+  p_mb_kernel<true><<<n, dim3(96, 1), sizeof(PShared), st>>>(nullptr, nullptr, 0, nullptr, nullptr, 0, Geo{}, 0,
+                                                             nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                             nullptr, 0, bt);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

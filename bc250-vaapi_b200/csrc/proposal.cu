@@ -52,18 +52,40 @@ __device__ __forceinline__ uint32_t pick8(const uint32_t (&w)[8], int i) {
   return (i & 4) ? hi : lo;
 }
 
-__global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restrict__ cur, int cur_pitch,
-                                                        const uint8_t* __restrict__ ref, int ref_pitch, Geo g,
-                                                        const MV* __restrict__ prev, int R, int zero_thresh,
-                                                        LpBuf b) {
+// BATCH: one CTA per compact P macroblock of a batch (the buffers of b are
+// indexed by that compact index); geometry, planes, history and the early-out
+// threshold come from the macroblock's stream.
+template <bool BATCH>
+__global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restrict__ cur_, int cur_pitch_,
+                                                        const uint8_t* __restrict__ ref_, int ref_pitch_, Geo g_,
+                                                        const MV* __restrict__ prev_, int R, int zero_thresh_,
+                                                        LpBuf b, BatchTab bt) {
   __shared__ uint32_t scw[64];   // current MB, 16 rows x 4 words (clamped to W, H)
   __shared__ uint32_t rfw[64];   // reference block at candidate 0
   __shared__ int scx[kCand], scy[kCand];
   __shared__ uint32_t ssad[kCand], sprev[9];
   __shared__ uint32_t sgrad[2][2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int mb = blockIdx.x;
-  const int mby = mb / g.mbw, mbx = mb - mby * g.mbw;
+  const int mb = blockIdx.x;  // index of the buffers of b
+  const uint8_t* cur = cur_;
+  const uint8_t* ref = ref_;
+  int cur_pitch = cur_pitch_, ref_pitch = ref_pitch_, zero_thresh = zero_thresh_;
+  Geo g = g_;
+  const MV* prev = prev_;
+  int lmb = mb;  // the macroblock within its frame
+  if (BATCH) {
+    const int k = bt.p_mbs.find(mb);
+    const BatchStream& st = bt.p_mbs.stream(k);
+    lmb = mb - bt.p_mbs.prefix[k];
+    g = st.g;
+    cur = st.cur_y;
+    cur_pitch = st.cur_pitch;
+    ref = st.ref_y;
+    ref_pitch = st.rec_pitch;
+    zero_thresh = st.zero_thresh;
+    prev = st.has_hist ? st.mv_prev : nullptr;
+  }
+  const int mby = lmb / g.mbw, mbx = lmb - mby * g.mbw;
   const int X = mbx * 16, Y = mby * 16;
   {
     const int r = tid >> 2, w = tid & 3;
@@ -247,10 +269,14 @@ struct RescoreWarp {
   RefineSimd rf;
 };
 
-__global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restrict__ cur, int cur_pitch,
-                                                         const uint8_t* __restrict__ ref, int ref_pitch, Geo g,
-                                                         int R, int lambda, int mbs, LpBuf b,
-                                                         MV* __restrict__ mv_out) {
+// BATCH: the listed macroblocks are compact P indices of a batch; each
+// takes its stream's geometry, planes and lambda, and its vector goes to
+// mv_out at the compact index.
+template <bool BATCH>
+__global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restrict__ cur_, int cur_pitch_,
+                                                         const uint8_t* __restrict__ ref_, int ref_pitch_, Geo g_,
+                                                         int R, int lambda_, int mbs, LpBuf b,
+                                                         MV* __restrict__ mv_out, BatchTab bt) {
   __shared__ RescoreWarp shw[4];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   RescoreWarp& sh = shw[wid];
@@ -258,7 +284,23 @@ __global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restri
   const int SIDE = 2 * R + 1;
   for (int li = blockIdx.x * 4 + wid; li < n; li += gridDim.x * 4) {
     const int mb = b.lists[li];
-    const int mby = mb / g.mbw, mbx = mb - mby * g.mbw;
+    const uint8_t* cur = cur_;
+    const uint8_t* ref = ref_;
+    int cur_pitch = cur_pitch_, ref_pitch = ref_pitch_, lambda = lambda_;
+    Geo g = g_;
+    int lmb = mb;
+    if (BATCH) {
+      const int k = bt.p_mbs.find(mb);
+      const BatchStream& st = bt.p_mbs.stream(k);
+      lmb = mb - bt.p_mbs.prefix[k];
+      g = st.g;
+      cur = st.cur_y;
+      cur_pitch = st.cur_pitch;
+      ref = st.ref_y;
+      ref_pitch = st.rec_pitch;
+      lambda = st.lambda;
+    }
+    const int mby = lmb / g.mbw, mbx = lmb - mby * g.mbw;
     const int X = mbx * 16, Y = mby * 16;
     const uint32_t sel = b.sel[mb];
     int valid = 0;
@@ -728,8 +770,8 @@ int b200enc_proposal_prepare(void* h, const uint8_t* cur_y, int cur_pitch, const
   if (mbs > P->max_mbs) return -1;
   cudaStream_t st = (cudaStream_t)stream;
   if (cudaMemsetAsync(P->b.counters, 0, 32, st) != cudaSuccess) return -1;
-  lp_prepare_kernel<<<mbs, 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, (const MV*)prev_mv, range,
-                                        zero_thresh, P->b);
+  lp_prepare_kernel<false><<<mbs, 64, 0, st>>>(cur_y, cur_pitch, ref_y, ref_pitch, g, (const MV*)prev_mv, range,
+                                               zero_thresh, P->b, BatchTab{});
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -804,8 +846,8 @@ int b200enc_proposal_me(void* h, const uint8_t* cur_y, int cur_pitch, const uint
   int sms = 148, dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int per_sm = b200enc_tuned(B200ENC_TUNE_RESCORE_CTAS_PER_SM) > 0 ? b200enc_tuned(B200ENC_TUNE_RESCORE_CTAS_PER_SM) : 8;
-  lp_rescore_kernel<<<std::max(1, std::min((mbs + 3) / 4, per_sm * sms)), 128, 0, st>>>(
-      cur_y, cur_pitch, ref_y, ref_pitch, g, range, lambda, mbs, P->b, (MV*)mv_out);
+  lp_rescore_kernel<false><<<std::max(1, std::min((mbs + 3) / 4, per_sm * sms)), 128, 0, st>>>(
+      cur_y, cur_pitch, ref_y, ref_pitch, g, range, lambda, mbs, P->b, (MV*)mv_out, BatchTab{});
   // join
   if (cudaEventRecord(P->ev_fb, P->side) != cudaSuccess || cudaStreamWaitEvent(st, P->ev_fb, 0) != cudaSuccess)
     return -1;
@@ -849,3 +891,34 @@ int b200enc_proposal_tensor(void* h, int which, void** ptr, size_t* bytes) {
 }
 
 }  // extern "C"
+
+// The learned form over every P macroblock of a batch (n = the compact P
+// count; modes 1 and 3): preparation, the network with its selection, the
+// fallback full search (list mode, side stream) and the re-scoring, as
+// b200enc_proposal_me does for one frame; every vector lands in bt.mvc.
+int b200enc_proposal_me_batch(void* h, const BatchTab& bt, int n, int range, int lambda, int mode, float param,
+                              cudaStream_t st) {
+  Proposal* P = static_cast<Proposal*>(h);
+  if (!P || n <= 0 || n > P->max_mbs || (mode != 1 && mode != 3) || (range != 16 && range != 32)) return -1;
+  if (cudaMemsetAsync(P->b.counters, 0, 32, st) != cudaSuccess) return -1;
+  lp_prepare_kernel<true><<<n, 64, 0, st>>>(nullptr, 0, nullptr, 0, Geo{}, nullptr, range, 0, P->b, bt);
+  if (mode == 1) {
+    if (lp_net_launch(n, P->b, P->wb, P->params, param, lambda, bt.mvc, P->err, st) != 0) return -1;
+  } else {
+    if (lp_net8_launch(n, P->b, P->params, P->w8, &P->w8_stale, param, lambda, bt.mvc, P->err, st) != 0) return -1;
+  }
+  int sms = 148, dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaEventRecord(P->ev_sel, st) != cudaSuccess || cudaStreamWaitEvent(P->side, P->ev_sel, 0) != cudaSuccess)
+    return -1;
+  const int fb_sm = b200enc_tuned(B200ENC_TUNE_FALLBACK_CTAS_PER_SM) > 0 ? b200enc_tuned(B200ENC_TUNE_FALLBACK_CTAS_PER_SM) : 8;
+  const int rc = b200enc_me_batch_launch(bt, range, P->b.lists + n, P->b.counters + 1, std::min(n, fb_sm * sms),
+                                         P->side);
+  const int rs_sm = b200enc_tuned(B200ENC_TUNE_RESCORE_CTAS_PER_SM) > 0 ? b200enc_tuned(B200ENC_TUNE_RESCORE_CTAS_PER_SM) : 8;
+  lp_rescore_kernel<true><<<std::max(1, std::min((n + 3) / 4, rs_sm * sms)), 128, 0, st>>>(
+      nullptr, 0, nullptr, 0, Geo{}, range, 0, n, P->b, bt.mvc, bt);
+  if (cudaEventRecord(P->ev_fb, P->side) != cudaSuccess || cudaStreamWaitEvent(st, P->ev_fb, 0) != cudaSuccess)
+    return -1;
+  return (rc == 0 && cudaGetLastError() == cudaSuccess) ? 0 : -1;
+}
+

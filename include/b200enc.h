@@ -158,6 +158,47 @@ int b200enc_deblock_noalloc(int mbw, int mbh, int qp, int is_intra,
                             const uint32_t *nz, const void *mv,
                             uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch, void *stream);
 
+/* ---- Multi-stream batches (no reference counterpart: the reference runs one
+ * Vulkan queue per VA context, approach1-compute-encoder/src/gpu_compute.h
+ * :246-250) ----------------------------------------------------------------
+ * A batch holds n streams of their own frame sizes (even widths and
+ * heights). b200enc_batch_encode codes one frame of every stream with one
+ * launch per stage over all of them: ME over every P macroblock of every P
+ * stream (me_mode 0 full search, 1 learned form with BF16 inference, 3 with
+ * FP8), the P chain over the same macroblocks, the intra wavefront over
+ * every I stream's macroblock rows, and the deblocking wavefront (deblock !=
+ * 0) over every stream's row groups. Each stream's outputs and
+ * reconstruction equal a single-stream context's (b200enc_ctx_*, same
+ * search range, lambda 5, zero-MV threshold 512, clamping at the coded size,
+ * the intra corner check) given the same frames, QPs and frame kinds.
+ * Sources are device NV12 planes (pitch a multiple of 4, at least the
+ * width); a stream's first frame must be intra. Work is enqueued on the
+ * batch's stream (b200enc_batch_stream); b200enc_batch_sync waits and
+ * returns -1 if a wavefront gave up. With b200enc_batch_set_graph(b, 1)
+ * each step is captured as a CUDA graph and launched, the executable graph
+ * updated in place while the step's shape stays the same. Outputs
+ * (b200enc_batch_outputs: levels, dc, nz, pred_mode, mv and the
+ * reconstruction of the latest step, in the single-frame layouts) stay
+ * valid until the next encode. */
+typedef struct {
+    const uint8_t *y, *uv; /* device NV12 */
+    int pitch;             /* bytes */
+    int qp;                /* 0..51 */
+    int is_intra;
+    int num_slices;        /* >= 1 */
+} b200enc_batch_frame_t;
+void *b200enc_batch_create(int n_streams, const int *widths, const int *heights, int search_range, int me_mode,
+                           float conf, int deblock);
+void b200enc_batch_destroy(void *b);
+void *b200enc_batch_stream(void *b);
+int b200enc_batch_set_graph(void *b, int enable);
+int b200enc_batch_encode(void *b, const b200enc_batch_frame_t *frames);
+int b200enc_batch_sync(void *b);
+int b200enc_batch_outputs(void *b, int s, void **levels, void **dc, void **nz, void **pred_mode, void **mv,
+                          void **rec_y, void **rec_uv, int *rec_pitch);
+/* Graph instantiations and in-place updates so far. */
+int b200enc_batch_graph_stats(void *b, long *instantiations, long *updates);
+
 /* Launch parameters picked by the autotuner (no reference counterpart: the
  * reference's dispatch sizes are fixed in gpu_compute.c). Each changes how
  * a kernel's work is laid out, never its results. 0 = the built-in default.
