@@ -35,6 +35,7 @@ using namespace b200enc;
 constexpr uint32_t kBatchMaxWaitUs = 2000000u;
 
 size_t up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+int pad16(int mbs) { return (mbs + 15) & ~15; }
 
 struct StreamState {
   int W, H, mbw, mbh, pitch;
@@ -192,7 +193,7 @@ void* b200enc_batch_create(int n_streams, const int* widths, const int* heights,
     bytes += 2 * up(t.rec_bytes, 256) + up(mbs * 768, 256) + 2 * up(mbs * 96, 256) + up(mbs * 4, 256) +
              2 * up(mbs * 16, 256);
     scr_words += 2 * scratch_words(t.mbh);
-    b->total_mbs += (int)mbs;
+    b->total_mbs += pad16((int)mbs);  // the compact P index, tile-aligned per stream
     b->max_mbw = std::max(b->max_mbw, t.mbw);
     b->max_mbh = std::max(b->max_mbh, t.mbh);
   }
@@ -326,10 +327,13 @@ int b200enc_batch_encode(void* h, const b200enc_batch_frame_t* frames) {
       ++ni;
       n_irows += t.mbh;
     } else {
+      // each P stream's range starts on a network tile (16 macroblocks), so
+      // the FP8 network's per-tile activation scales see the same macroblocks
+      // as in a single-stream run; the padding macroblocks are skipped
       ip[np] = s;
-      pp[np + 1] = pp[np] + mbs;
+      pp[np + 1] = pp[np] + pad16(mbs);
       ++np;
-      n_p += mbs;
+      n_p += pad16(mbs);
     }
     const int groups = (t.mbh + b->db_rows - 1) / b->db_rows;
     ig[ng] = s;

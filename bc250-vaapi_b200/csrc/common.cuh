@@ -264,7 +264,9 @@ struct BatchSet {
 };
 
 struct BatchTab {
-  BatchSet p_mbs;   // macroblocks of the streams coding a P frame (the compact P index)
+  BatchSet p_mbs;   // macroblocks of the streams coding a P frame (the compact P index); each
+                    // stream's range is padded to a multiple of 16 items, the padding items
+                    // (local index >= the stream's macroblock count) do no work
   BatchSet i_rows;  // macroblock rows of the streams coding an I frame
   BatchSet groups;  // deblocking row groups of every stream
   MV* mvc;          // motion vectors by compact P index

@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(2 * R) me_full_search_kernel(const uint8_t* __
     o = out_ + (size_t)mby * g.mbw + mbx;
   }
   if (MODE != kMeGrid) __syncthreads();  // the previous item's shared memory is no longer read
+  if ((MODE == kMeBatch || MODE == kMeBatchList) && mby >= g.mbh) continue;  // padding of the compact index
   const int X = mbx * 16, Y = mby * 16;
   const int ox = X - R - 4, oy = Y - R - 4;  // window origin (multiple of 4)
 

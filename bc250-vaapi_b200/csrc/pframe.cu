@@ -133,6 +133,7 @@ __global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict_
     const BatchStream& st = bt.p_mbs.stream(k);
     mb = ci - bt.p_mbs.prefix[k];
     g = st.g;
+    if (mb >= g.mbw * g.mbh) return;  // padding of the compact index (uniform over the CTA)
     mby = mb / g.mbw;
     mbx = mb - mby * g.mbw;
     active = true;

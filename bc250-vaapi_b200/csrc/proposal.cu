@@ -78,6 +78,18 @@ __global__ void __launch_bounds__(64) lp_prepare_kernel(const uint8_t* __restric
     const BatchStream& st = bt.p_mbs.stream(k);
     lmb = mb - bt.p_mbs.prefix[k];
     g = st.g;
+    if (lmb >= g.mbw * g.mbh) {
+      // padding of the compact index: the zero inputs a tile's rows past the
+      // end of a frame have, and an early-out state so nothing selects it
+      *reinterpret_cast<uint4*>(b.x0 + ((size_t)mb * 64 + tid) * 8) = make_uint4(0u, 0u, 0u, 0u);
+      b.f[(size_t)mb * kFIn + 32 + tid] = __float2bfloat16_rn(0.f);
+      if (tid < kCand) {
+        b.cand[mb * kCand + tid] = 0;
+        b.cand_sad[mb * kCand + tid] = 0u;
+      }
+      if (tid == 0) b.state[mb] = kStEarly;
+      return;
+    }
     cur = st.cur_y;
     cur_pitch = st.cur_pitch;
     ref = st.ref_y;

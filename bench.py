@@ -653,6 +653,138 @@ def run_gpu(args):
     group.close()
 
 
+MS_MIX = [(640, 480, 24), (1280, 720, 24), (1920, 1080, 12), (2560, 1440, 4)]
+MS_RESIDENT = 8
+
+
+def _ms_frames(w, h, seed, n):
+    from b200enc import synth
+    seq = synth.Sequence(w, h, seed=seed, pan=True, noise_patch=w >= 1280)
+    return [seq.frame(t) for t in range(n)]
+
+
+def run_multistream(args):
+    """The batched multi-stream workload: 64 concurrent streams (24 x
+    640x480, 24 x 1280x720, 12 x 1920x1080, 4 x 2560x1440), per-stream QP
+    uniform in 20..40 (seeded), IPPP with an IDR every 60 frames and the
+    streams' IDRs spread over the GOP, search range 32. A step is one frame
+    of every stream through b200enc_batch_encode (one launch per stage for
+    all 64 streams, each step a captured CUDA graph), in the plain and the
+    learned (FP8 network) forms, device-timed with CUDA events on the
+    batch's stream; the same streams through 64 independent single-stream
+    contexts (one CUDA stream each, ~12 launches per frame) are timed beside
+    them. Each stream cycles 8 resident synthetic frames (>= 800 MB in all,
+    larger than L2). Prints one JSON line."""
+    import multiprocessing as mp
+    import numpy as np
+    import torch
+    import b200enc
+    sizes = [(w, h) for (w, h, n) in MS_MIX for _ in range(n)]
+    S = len(sizes)
+    rs = np.random.Generator(np.random.PCG64(4))
+    qps = [int(q) for q in rs.integers(20, 41, S)]
+    phase = [(s * GOP) // S for s in range(S)]
+    with mp.get_context("spawn").Pool(max(1, (os.cpu_count() or 2) - 1)) as pool:
+        host = pool.starmap(_ms_frames, [(w, h, 500 + s, MS_RESIDENT) for s, (w, h) in enumerate(sizes)])
+    dev = [[b200enc.NV12.from_host(y, uv) for (y, uv) in fr] for fr in host]
+    mbs_per_step = sum(((w + 15) // 16) * ((h + 15) // 16) for (w, h) in sizes)
+
+    def kinds(t):
+        return [t == 0 or (t + phase[s]) % GOP == 0 for s in range(S)]
+
+    def time_batch(me_mode, graph):
+        b = b200enc.Batch(sizes, search_range=RANGE, me_mode=me_mode, deblock=1, graph=graph)
+        st = torch.cuda.ExternalStream(b.stream())
+        t = 0
+        for _ in range(args.warmup):
+            b.encode([dev[s][t % MS_RESIDENT] for s in range(S)], qps, kinds(t))
+            t += 1
+        assert b.sync() == 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        h0 = time.perf_counter()
+        for _ in range(args.steps):
+            b.encode([dev[s][t % MS_RESIDENT] for s in range(S)], qps, kinds(t))
+            t += 1
+        host_s = time.perf_counter() - h0
+        e1.record(st)
+        assert b.sync() == 0
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        gs = b.graph_stats()
+        b.close()
+        return ms, host_s, gs
+
+    def time_contexts(me_mode):
+        ctxs = []
+        for s in range(S):
+            c = b200enc.Context()
+            c.configure(search_range=RANGE, lam=LAMBDA, zero_thresh=512, coded_clamp=True, deblock=1)
+            c.set_me(me_mode)
+            ctxs.append(c)
+        streams = [torch.cuda.ExternalStream(c.stream()) for c in ctxs]
+        control = torch.cuda.Stream()
+        t = 0
+
+        def step(t):
+            k = kinds(t)
+            for s, c in enumerate(ctxs):
+                w, h = sizes[s]
+                c.encode_device(dev[s][t % MS_RESIDENT], w, h, qps[s], k[s], 1, False)
+
+        for _ in range(args.warmup):
+            step(t)
+            t += 1
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(control)
+        for x in streams:
+            x.wait_event(e0)
+        for _ in range(args.steps):
+            step(t)
+            t += 1
+        for x in streams:
+            ev = torch.cuda.Event()
+            ev.record(x)
+            control.wait_event(ev)
+        e1.record(control)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        for c in ctxs:
+            c.close()
+        return ms
+
+    res = {}
+    for name, mode in (("learned", LEARNED), ("plain", 0)):
+        ms, host_s, gs = time_batch(mode, True)
+        res[name] = {"value": round(S * args.steps / (ms / 1000.0), 2), "unit": "frames/s",
+                     "mb_per_s": round(mbs_per_step * args.steps / (ms / 1000.0), 1),
+                     "ms_per_step": round(ms / args.steps, 4),
+                     "host_issue_ms_per_step": round(1000.0 * host_s / args.steps, 4),
+                     "graph_instantiations_updates": list(gs)}
+        ms_c = time_contexts(mode)
+        res[name + "_contexts"] = {"value": round(S * args.steps / (ms_c / 1000.0), 2), "unit": "frames/s",
+                                   "ms_per_step": round(ms_c / args.steps, 4),
+                                   "note": "the same streams through 64 single-stream contexts"}
+    ms_d, _, _ = time_batch(LEARNED, False)
+    res["learned_no_graph"] = {"value": round(S * args.steps / (ms_d / 1000.0), 2), "unit": "frames/s",
+                               "ms_per_step": round(ms_d / args.steps, 4)}
+    line = {"metric": "batched multi-stream H.264 encode fps (64 streams, mixed resolutions)",
+            "value": res["learned"]["value"], "unit": "frames/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["learned"]["ms_per_step"], "higher_is_better": True,
+            "dtype": "u8/int32 (integer path), fp8 e4m3 (proposal network inference)",
+            "data": "synthetic (seeded generator per stream)",
+            "config": {"workload": "h264_multistream_64_mixed_batched", "streams": S,
+                       "mix": [f"{n}x{w}x{h}" for (w, h, n) in MS_MIX], "qp": "uniform 20..40 per stream (seeded)",
+                       "search_range": RANGE, "gop": GOP, "gop_phase": "stream s: s*gop/streams",
+                       "deblock": True, "resident_frames_per_stream": MS_RESIDENT,
+                       "l2": f"{sum(f.buf.numel() for fr in dev for f in fr) >> 20} MiB resident > L2"},
+            "macroblocks_per_step": mbs_per_step, **res,
+            "speedup_vs_plain": round(res["learned"]["value"] / res["plain"]["value"], 3),
+            "batch_vs_contexts": round(res["learned"]["value"] / res["learned_contexts"]["value"], 3)}
+    print(json.dumps(line), flush=True)
+
+
 def run_hevc_deblock(args):
     """HEVC deblocking (b200enc_hevc_deblock) on seeded synthetic pictures:
     1080p 8-bit and 2160p 10-bit, enough resident copies to exceed L2, timed
@@ -721,6 +853,8 @@ def main():
                     help="run only this S-stream arm (warm-up + steps) and print nothing: a profiler's launch list")
     ap.add_argument("--streams", type=int, default=8)
     ap.add_argument("--conf", type=float, default=0.9)
+    ap.add_argument("--workload", choices=["h264_1080p", "multistream"], default="h264_1080p",
+                    help="multistream: the 64-stream mixed-resolution batch (own JSON line)")
     ap.add_argument("--hevc-deblock", action="store_true",
                     help="time b200enc_hevc_deblock instead of the H.264 encode (own JSON lines)")
     args = ap.parse_args()
@@ -728,6 +862,8 @@ def main():
         args.warmup = 3
     if args.hevc_deblock:
         run_hevc_deblock(args)
+    elif args.workload == "multistream" and args.impl != "reference":
+        run_multistream(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
