@@ -211,22 +211,15 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
 
       // ---- I16x16 candidates (intra_wavefront.comp:454-476) -------------
       if (tid < 32) {
-        // lane-parallel sums; lane 0 finishes
-        int st = tid < 16 ? s.top[tid] : 0, sl2 = tid < 16 ? s.left[tid] : 0;
-        int hterm = 0, vterm = 0;
-        if (tid < 8) {
-          const int l = (6 - tid >= 0) ? s.top[6 - tid] : s.corner;
-          hterm = (tid + 1) * (s.top[8 + tid] - l);
-          const int a = (6 - tid >= 0) ? s.left[6 - tid] : s.corner;
-          vterm = (tid + 1) * (s.left[8 + tid] - a);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          st += __shfl_xor_sync(0xffffffffu, st, o);
-          sl2 += __shfl_xor_sync(0xffffffffu, sl2, o);
-          hterm += __shfl_xor_sync(0xffffffffu, hterm, o);
-          vterm += __shfl_xor_sync(0xffffffffu, vterm, o);
-        }
+        // lane sums without divergence (every lane loads, lanes outside a
+        // term contribute 0), reduced in one instruction each; lane 0 finishes
+        const int t = tid & 15, k = tid & 7;
+        const int tv = s.top[t], lv = s.left[t];
+        const int lt = k <= 6 ? s.top[6 - k] : s.corner, la = k <= 6 ? s.left[6 - k] : s.corner;
+        const int st = __reduce_add_sync(0xffffffffu, tid < 16 ? tv : 0);
+        const int sl2 = __reduce_add_sync(0xffffffffu, tid < 16 ? lv : 0);
+        const int hterm = __reduce_add_sync(0xffffffffu, tid < 8 ? (k + 1) * (s.top[8 + k] - lt) : 0);
+        const int vterm = __reduce_add_sync(0xffffffffu, tid < 8 ? (k + 1) * (s.left[8 + k] - la) : 0);
         if (tid == 0) {
           int dcv;
           if (top_av && left_av) dcv = (st + sl2 + 16) >> 5;
@@ -345,15 +338,27 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
       __syncthreads();
 
       // ---- DC paths ----------------------------------------------------
+      // The luma DC transform (A1/src/encoder_h264.c:711-730) is a 2-D
+      // Hadamard: out[i][k] = sum_ab h_k(a) h_i(b) in[a][b] (+1 >> 1 forward).
+      // Lanes t = 4a + b of warp 0 hold in[a][b]; two butterfly stages along
+      // b (xor 1, 2) and two along a (xor 4, 8) leave lane 4q + p with the
+      // sum for the Walsh rows (p, q) in sequency order; h's rows are those
+      // rows permuted (row 0 <- 0, 1 <- 2, 2 <- 3, 3 <- 1), so lane 4q + p
+      // holds out[i][k] with i = kRow[p], k = kRow[q]. Integer sums: exact in
+      // any order.
+      auto dc_hadamard = [&](int v) -> int {
+#pragma unroll
+        for (int m = 1; m <= 8; m <<= 1) {
+          const int o = __shfl_xor_sync(0x0000ffffu, v, m);
+          v = (tid & m) ? o - v : v + o;
+        }
+        return v;
+      };
       if (tid < 16) {
-        // luma: out[i][k] = (sum_ab h_k(a) h_i(b) in[a][b] + 1) >> 1, quantize
-        const int i = tid >> 2, k = tid & 3;
-        int sum = 0;
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-          for (int bb = 0; bb < 4; ++bb) sum += hsign(k, a) * hsign(i, bb) * s.ldc[4 * a + bb];
-        s.ldl[tid] = quantize_dc((sum + 1) >> 1, ql);
+        const int row_of[4] = {0, 3, 1, 2};  // sequency index -> row of h
+        const int i = row_of[tid & 3], k = row_of[tid >> 2];
+        const int sum = dc_hadamard(s.ldc[tid]);
+        s.ldl[4 * i + k] = quantize_dc((sum + 1) >> 1, ql);
       } else if (tid == 64 || tid == 80) {
         const int pl = (tid - 64) >> 4;
         const int c0 = s.cdc[4 * pl], c1 = s.cdc[4 * pl + 1], c2 = s.cdc[4 * pl + 2], c3 = s.cdc[4 * pl + 3];
@@ -366,13 +371,10 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
       }
       __syncwarp();
       if (tid < 16) {
-        const int i = tid >> 2, k = tid & 3;
-        int f = 0;
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-          for (int bb = 0; bb < 4; ++bb) f += hsign(k, a) * hsign(i, bb) * s.ldl[4 * a + bb];
-        s.ldcval[tid] = dequant_dc_luma(f, ql);
+        const int row_of[4] = {0, 3, 1, 2};
+        const int i = row_of[tid & 3], k = row_of[tid >> 2];
+        const int f = dc_hadamard(s.ldl[tid]);
+        s.ldcval[4 * i + k] = dequant_dc_luma(f, ql);
       }
       __syncthreads();
 

@@ -273,7 +273,7 @@ __global__ void lp_select_kernel(int mbs, LpBuf b, int mode, float param, int la
 // (20 mod 32): the 25 offsets of two candidates that a warp scores at once
 // then read 32 different banks, where 8-word rows put offsets 0 and 4 rows
 // apart, and the next candidate, on the same banks.
-constexpr int kPatchRows = 27, kPatchWords = 8, kPatchStride = 9;
+constexpr int kPatchRows = 27, kPatchStride = 9;  // 8 words used per row
 struct RescoreWarp {
   uint32_t patch[4][kPatchRows * kPatchStride + 1];
   uint32_t cur[64];
@@ -328,6 +328,7 @@ __global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restri
     // selected candidates occupy the low slots (the selection fills them in order)
     const int nk = __popc(__ballot_sync(0xffffffffu, valid) & 0xfu);
     __syncwarp();
+    const bool ref_vec = ((ref_pitch & 15) == 0) && ((reinterpret_cast<uintptr_t>(ref) & 15) == 0);
     // stage the current MB (clamped to W, H) and the candidate patches
     for (int i = lane; i < 64; i += 32) {
       const int r = i >> 2, w = i & 3;
@@ -342,12 +343,41 @@ __global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restri
       }
       sh.cur[i] = v;
     }
-    for (int i = lane; i < nk * kPatchRows * kPatchWords; i += 32) {
-      const int k = i / (kPatchRows * kPatchWords), rem = i - k * (kPatchRows * kPatchWords);
-      const int r = rem / kPatchWords, w = rem - r * kPatchWords;
-      const int xa = (X + sh.ccx[k] - 5) & ~3;
+    // one patch row (8 words from xa = (X+cx-5) & ~3) per lane and pass:
+    // three 16-byte loads from xa & ~15 where the 48 bytes lie inside the
+    // row of a 16-byte aligned plane, else the clamped word loads
+    for (int t = lane; t < nk * kPatchRows; t += 32) {
+      const int k = t / kPatchRows, r = t - k * kPatchRows;
+      const int xa = (X + sh.ccx[k] - 5) & ~3, xa16 = xa & ~15, off = (xa - xa16) >> 2;
       const uint8_t* rp = ref + (size_t)clampi(Y + sh.ccy[k] - 5 + r, 0, g.RH - 1) * ref_pitch;
-      sh.patch[k][r * kPatchStride + w] = load_word_clamped(rp, xa + 4 * w, g.RW);
+      uint32_t* dst = sh.patch[k] + r * kPatchStride;
+      if (ref_vec && xa16 >= 0 && xa16 + 48 <= g.RW) {
+        const uint4 a = __ldg(reinterpret_cast<const uint4*>(rp + xa16));
+        const uint4 b2 = __ldg(reinterpret_cast<const uint4*>(rp + xa16 + 16));
+        const uint4 c = __ldg(reinterpret_cast<const uint4*>(rp + xa16 + 32));
+        const uint32_t u[12] = {a.x, a.y, a.z, a.w, b2.x, b2.y, b2.z, b2.w, c.x, c.y, c.z, c.w};
+        switch (off) {  // word w of the patch row is u[off + w]
+          case 0:
+#pragma unroll
+            for (int w = 0; w < 8; ++w) dst[w] = u[w];
+            break;
+          case 1:
+#pragma unroll
+            for (int w = 0; w < 8; ++w) dst[w] = u[w + 1];
+            break;
+          case 2:
+#pragma unroll
+            for (int w = 0; w < 8; ++w) dst[w] = u[w + 2];
+            break;
+          default:
+#pragma unroll
+            for (int w = 0; w < 8; ++w) dst[w] = u[w + 3];
+            break;
+        }
+      } else {
+#pragma unroll
+        for (int w = 0; w < 8; ++w) dst[w] = load_word_clamped(rp, xa + 4 * w, g.RW);
+      }
     }
     __syncwarp();
 
