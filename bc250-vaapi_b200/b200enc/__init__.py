@@ -26,7 +26,7 @@ EXPORTS = [
     "b200enc_hevc_transform_quant_4x4", "b200enc_hevc_dequant_itransform_4x4", "b200enc_hevc_transform_quant_8x8",
     "b200enc_hevc_dequant_itransform_8x8", "b200enc_hevc_build_hpel", "b200enc_hevc_motion_search",
     "b200enc_hevc_choose_luma_mode", "b200enc_hevc_deblock", "b200enc_hevc_build_hpel_10",
-    "b200enc_hevc_motion_search_10", "b200enc_hevc_choose_luma_mode_10",
+    "b200enc_hevc_motion_search_10", "b200enc_hevc_choose_luma_mode_10", "b200enc_hevc_build_hpel_host",
     "b200enc_tune_set", "b200enc_tune_get", "b200enc_tune_name", "b200enc_tune_load",
     "b200enc_batch_create", "b200enc_batch_destroy", "b200enc_batch_stream", "b200enc_batch_set_graph",
     "b200enc_batch_encode", "b200enc_batch_sync", "b200enc_batch_outputs", "b200enc_batch_graph_stats",

@@ -721,4 +721,59 @@ int b200enc_hevc_choose_luma_mode_10(const uint16_t* src_y, int src_pitch, const
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
+// The same planes from and to host memory, for a host encoder that keeps its
+// reconstruction and search planes in host buffers (the reference's
+// hevc_encoder_t: prev_recon_y, hpel[4], hpel_stride). Each calling thread
+// keeps its own device workspace and stream, grown to the largest picture
+// it has seen; the call returns when the four planes are in `planes`.
+namespace {
+struct HpelWork {
+  cudaStream_t st = nullptr;
+  void* buf = nullptr;
+  size_t bytes = 0;
+  ~HpelWork() {
+    if (buf) cudaFree(buf);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+thread_local HpelWork t_hpel;
+}  // namespace
+
+int b200enc_hevc_build_hpel_host(const void* recon, int w, int h, int bit_depth, int margin, void* const planes[4],
+                                 int plane_stride) {
+  if (!recon || !planes || w <= 0 || h <= 0 || (bit_depth != 8 && bit_depth != 10)) return -1;
+  if (margin < 0 || margin > 256 || plane_stride < w + 2 * margin) return -1;
+  for (int i = 0; i < 4; ++i)
+    if (!planes[i]) return -1;
+  const size_t bps = bit_depth == 8 ? 1 : 2;
+  const int rows = h + 2 * margin;
+  const size_t rec_bytes = (size_t)w * h * bps, plane_bytes = (size_t)plane_stride * rows * bps;
+  const size_t need = ((rec_bytes + 255) & ~(size_t)255) + 4 * ((plane_bytes + 255) & ~(size_t)255);
+  HpelWork& wk = t_hpel;
+  if (!wk.st && cudaStreamCreateWithFlags(&wk.st, cudaStreamNonBlocking) != cudaSuccess) return -1;
+  if (wk.bytes < need) {
+    if (wk.buf) cudaFree(wk.buf);
+    wk.buf = nullptr;
+    wk.bytes = 0;
+    if (cudaMalloc(&wk.buf, need) != cudaSuccess) return -1;
+    wk.bytes = need;
+  }
+  uint8_t* d = static_cast<uint8_t*>(wk.buf);
+  uint8_t* drec = d;
+  uint8_t* dp[4];
+  for (int i = 0; i < 4; ++i) dp[i] = d + ((rec_bytes + 255) & ~(size_t)255) + i * ((plane_bytes + 255) & ~(size_t)255);
+  if (cudaMemcpyAsync(drec, recon, rec_bytes, cudaMemcpyHostToDevice, wk.st) != cudaSuccess) return -1;
+  const int rc = bit_depth == 8
+                     ? b200enc_hevc_build_hpel(drec, w, w, h, margin, dp[0], dp[1], dp[2], dp[3], plane_stride, wk.st)
+                     : b200enc_hevc_build_hpel_10(reinterpret_cast<const uint16_t*>(drec), w, w, h, margin,
+                                                  reinterpret_cast<uint16_t*>(dp[0]),
+                                                  reinterpret_cast<uint16_t*>(dp[1]),
+                                                  reinterpret_cast<uint16_t*>(dp[2]),
+                                                  reinterpret_cast<uint16_t*>(dp[3]), plane_stride, wk.st);
+  if (rc != 0) return -1;
+  for (int i = 0; i < 4; ++i)
+    if (cudaMemcpyAsync(planes[i], dp[i], plane_bytes, cudaMemcpyDeviceToHost, wk.st) != cudaSuccess) return -1;
+  return cudaStreamSynchronize(wk.st) == cudaSuccess ? 0 : -1;
+}
+
 }  // extern "C"

@@ -329,6 +329,17 @@ int b200enc_hevc_build_hpel_10(const uint16_t *recon, int pitch, int w, int h, i
                                uint16_t *plane_h, uint16_t *plane_v, uint16_t *plane_hv, int plane_pitch,
                                void *stream);
 
+/* b200enc_hevc_build_hpel(_10) from and to host memory, for a host encoder
+ * that keeps its reconstruction and planes in host buffers: recon is w x h
+ * samples (pitch w; bytes at 8 bits, 16-bit words at 10), planes[4] (I, H,
+ * V, HV) each (h + 2*margin) rows of plane_stride samples; replaces the
+ * reference's build_hpel_8 / build_hpel_10 on its hevc_encoder_t
+ * (approach1-compute-encoder/src/hevc_enc_template.c:390-397). Uses a
+ * per-thread device workspace and stream; returns when the planes are in
+ * host memory. 0 / -1. */
+int b200enc_hevc_build_hpel_host(const void *recon, int w, int h, int bit_depth, int margin, void *const planes[4],
+                                 int plane_stride);
+
 /* Motion search of 8x8 CUs against the planes of b200enc_hevc_build_hpel
  * (8-bit), one job per CU: the reference's motion_search
  * (approach1-compute-encoder/src/hevc_enc_template.c:958-1043, with

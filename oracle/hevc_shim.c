@@ -2,23 +2,13 @@
  * hevc_shim.c - TEST INFRASTRUCTURE ONLY. Compiles the reference's HEVC
  * host encoder where it lies (approach1-compute-encoder/src/encoder_h265.c,
  * included, with its hevc_enc_template.c) so the tests can call the static
- * primitive the B200 kernels replace, and stubs the entry points the
- * encoder imports but these tests never reach (the x265 fallback and two
- * gpu_compute_* calls). The public transform/quant functions come from the
+ * primitive the B200 kernels replace, and stubs the two gpu_compute_* entry
+ * points the encoder imports but these tests never reach (hevc_link_stubs.c
+ * has the rest). The public transform/quant functions come from the
  * reference's hevc_intra.c, linked in as is.
  */
 #include "encoder_h265.c"
 
-hevc_x265_t *hevc_x265_create(void) { return NULL; }
-int hevc_x265_encode(hevc_x265_t *x, const hevc_x265_config_t *cfg, const uint8_t *y, int y_stride,
-                     const uint8_t *uv, int uv_stride, bool force_idr, int frame_qp, uint8_t *out,
-                     size_t out_cap)
-{
-    (void)x; (void)cfg; (void)y; (void)y_stride; (void)uv; (void)uv_stride; (void)force_idr;
-    (void)frame_qp; (void)out; (void)out_cap;
-    return -1;
-}
-void hevc_x265_destroy(hevc_x265_t *x) { (void)x; }
 int gpu_compute_download_nv12(gpu_context_t *ctx, gpu_image_t *image, gpu_memory_t memory, uint8_t *y_plane,
                               int y_pitch, uint8_t *uv_plane, int uv_pitch, int width, int height)
 {
@@ -27,9 +17,6 @@ int gpu_compute_download_nv12(gpu_context_t *ctx, gpu_image_t *image, gpu_memory
     return -1;
 }
 FILE *bc250_debug_dump_open(const char *name, const char *what) { (void)name; (void)what; return NULL; }
-/* The decoder's row wait (hevc_wpp.c), referenced by decoder-side motion
- * compensation in hevc_mc.c; the encoder never calls it. */
-void hevcd_await_rows(const void *g, int rows) { (void)g; (void)rows; }
 
 /* build_hpel (hevc_enc_template.c:390) of the 8-bit encoder on a w x h
  * reconstruction (pitch w): the whole-sample plane and the three half-sample
