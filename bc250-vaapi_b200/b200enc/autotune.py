@@ -1,11 +1,12 @@
 """Autotuner of the encoder's launch shapes.
 
-The library reads five launch parameters from a process-wide table
+The library reads six launch parameters from a process-wide table
 (include/b200enc.h, B200ENC_TUNE_*): macroblock rows per deblocking CTA (the
 wavefront's rows per CTA), macroblocks per P-chain CTA (the CTA tile shape),
 the persistent grids of the learned form's re-scoring and fallback search,
-and the intra wavefront's CTA count. None changes a result; each changes how
-the work maps onto the 148 SMs. This module times the candidates of each on
+the intra wavefront's CTA count, and whether the full search stages its
+reference windows by TMA or by word loads. None changes a result; each
+changes how the work maps onto the 148 SMs. This module times the candidates of each on
 the device for one frame size, by coordinate descent over the knobs with the
 library's own per-stage CUDA-event timing (b200enc_ctx_perf), keeps the
 fastest, and caches the choice per device and frame size in a JSON file; a
@@ -18,11 +19,11 @@ import os
 import time
 
 KEYS = {"deblock_rows": 0, "pchain_mbs_per_cta": 1, "rescore_ctas_per_sm": 2, "fallback_ctas_per_sm": 3,
-        "intra_ctas": 4}
+        "intra_ctas": 4, "me_stage": 5}
 # the stage whose time each knob changes (b200enc_ctx_perf_read keys), and on which frames
 STAGE = {"deblock_rows": ("deblock", False), "pchain_mbs_per_cta": ("chain", False),
          "rescore_ctas_per_sm": ("me", False), "fallback_ctas_per_sm": ("me", False),
-         "intra_ctas": ("chain", True)}
+         "intra_ctas": ("chain", True), "me_stage": ("me", False)}
 
 
 def candidates(name, mbh):
@@ -34,6 +35,8 @@ def candidates(name, mbh):
         return [2, 4, 8, 12, 16]
     if name == "intra_ctas":
         return sorted({max(1, mbh // 2), mbh})
+    if name == "me_stage":
+        return [2, 1]
     raise KeyError(name)
 
 

@@ -91,7 +91,7 @@ NET_CONF = (0.5, 0.7, 0.8, 0.9, 0.95, 0.98)
 CAND_COST = (-1.0, 24.0, 16.0, 12.0, 8.0, 6.0, 4.0, 3.0)  # fallback cost per pel of the no-network baseline
 
 
-def evaluate(P, samples, W, H, R=32, lam=5, net_conf=NET_CONF, cand_cost=CAND_COST):
+def evaluate(P, samples, W, H, R=32, lam=5, net_conf=NET_CONF, cand_cost=CAND_COST, net_mode=None):
     """Validation figures over held-out samples, for the network at each
     confidence threshold and for the same candidate search without the
     network at each fallback cost threshold. A 'miss' is an MB that did not
@@ -100,13 +100,14 @@ def evaluate(P, samples, W, H, R=32, lam=5, net_conf=NET_CONF, cand_cost=CAND_CO
     search's; rates are over MBs that are neither zero-MV early-outs nor
     without history. 'gain' compares, at the network's fallback rate, the
     baseline's miss rate (interpolated along its threshold sweep) with the
-    network's."""
+    network's. net_mode: the ME mode of the network (BF16 by default)."""
     import torch
     import b200enc as gpu
     from b200enc import proposal as pp
     CW, CH = gpu.coded(W, H)
     mbs = (CW // 16) * (CH // 16)
-    configs = [("net", pp.Proposal.NETWORK, c) for c in net_conf] + \
+    net_mode = pp.Proposal.NETWORK if net_mode is None else net_mode
+    configs = [("net", net_mode, c) for c in net_conf] + \
               [("cand", pp.Proposal.CANDIDATES, c) for c in cand_cost]
     stats = {(k, c): dict(valid=0, fallback=0, miss=0) for k, _, c in configs}
     top1 = 0

@@ -15,6 +15,10 @@ namespace b200enc {
 struct BatchTab;
 }
 #include <cuda_runtime.h>
+int b200enc_me_full_search_err(const uint8_t* cur_y, int cur_pitch, const uint8_t* ref_y, int ref_pitch, int W,
+                               int H, int RW, int RH, int range, int lambda, int zero_thresh, void* mv_out,
+                               const int* mb_list, const int* mb_count, int list_capacity, int flags, uint32_t* err,
+                               cudaStream_t st);
 int b200enc_me_batch_launch(const b200enc::BatchTab& bt, int range, const int* list, const int* count, int ctas,
                             cudaStream_t st);
 int b200enc_p_frame_batch_launch(const b200enc::BatchTab& bt, int n, cudaStream_t st);

@@ -308,8 +308,10 @@ int encode_frame(gpu_context_t* ctx, Impl* m, const uint8_t* y, const uint8_t* u
                                   m->range, lambda, m->zero_thresh, m->me_mode, m->conf, m->d_mv, m->stream);
         m->last_learned = true;
       } else {
-        rc |= b200enc_me_full_search(y, src_pitch, ref_y, ref_pitch, W, H, ref_RW, ref_RH, m->range, lambda,
-                                     m->zero_thresh, m->d_mv, m->stream);
+        // a window copy that never completes lands in the frame's status
+        // (the intra scratch's error word, unused by P frames)
+        rc |= b200enc_me_full_search_err(y, src_pitch, ref_y, ref_pitch, W, H, ref_RW, ref_RH, m->range, lambda,
+                                         m->zero_thresh, m->d_mv, nullptr, nullptr, 0, 0, scr0 + 1, m->stream);
       }
     }
     m->mv_hist = have_ref;

@@ -776,4 +776,22 @@ int b200enc_hevc_build_hpel_host(const void* recon, int w, int h, int bit_depth,
   return cudaStreamSynchronize(wk.st) == cudaSuccess ? 0 : -1;
 }
 
+int b200enc_pin_host(void* ptr, size_t bytes) {
+  if (!ptr || bytes == 0) return -1;
+  if (cudaHostRegister(ptr, bytes, cudaHostRegisterDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return 0;
+}
+
+int b200enc_unpin_host(void* ptr) {
+  if (!ptr) return -1;
+  if (cudaHostUnregister(ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return 0;
+}
+
 }  // extern "C"

@@ -3,7 +3,8 @@
 // The kernels' shapes that do not change their results (macroblock rows per
 // deblocking CTA, macroblocks per P-chain CTA, the persistent grids of the
 // learned form's re-scoring and fallback search, the intra wavefront's CTA
-// count) are read at launch from one process-wide table. Zero means the
+// count, whether the full search stages its windows by TMA or by loads) are
+// read at launch from one process-wide table. Zero means the
 // built-in default. The table is set through b200enc_tune_set, or loaded
 // from a file of "name value" lines (b200enc_tune_load; the environment
 // variable B200ENC_TUNE_FILE names one to load before the first launch).
@@ -32,6 +33,7 @@ constexpr Knob kKnobs[B200ENC_TUNE_COUNT] = {
     {"rescore_ctas_per_sm", 1, 16},   // persistent re-scoring grid, CTAs per SM
     {"fallback_ctas_per_sm", 1, 16},  // persistent fallback full-search grid, CTAs per SM
     {"intra_ctas", 1, 1 << 16},       // CTAs of the intra wavefront (rows in flight)
+    {"me_stage", 1, 2},               // full-search window staging: 1 word loads, 2 TMA
 };
 
 std::atomic<int> g_tune[B200ENC_TUNE_COUNT];

@@ -1,7 +1,7 @@
 // umma.cuh - tcgen05 (5th-generation tensor core) building blocks for sm_100a:
 // shared-memory matrix descriptors in the canonical K-major no-swizzle layout,
 // the kind::f16 (BF16) and kind::f8f6f4 (E4M3) instruction descriptors, MMA
-// issue/commit, bounded mbarrier waits and TMEM loads.
+// issue/commit, bounded mbarrier waits, plain 2-D TMA loads and TMEM loads.
 //
 // Canonical K-major no-swizzle layout of an operand tile of `rows` rows
 // (rows a multiple of 8): core matrices of 8 rows x 16 bytes (8 BF16), rows
@@ -98,6 +98,25 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Arrive on an mbarrier and add `bytes` to the transaction count its
+// current phase waits for (the issuing thread of a TMA copy).
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// 2-D tiled TMA load of the tensor map's box at element coordinates (x, y)
+// into shared memory, completing `bar`'s transaction count. The map lives in
+// kernel parameter space (__grid_constant__). Plain load: no cluster
+// multicast. x times the element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
 }
 
 // Bounded wait on an mbarrier phase; false after ~max_ns without completion.

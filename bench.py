@@ -785,6 +785,60 @@ def run_multistream(args):
     print(json.dumps(line), flush=True)
 
 
+def run_hevc(args):
+    """HEVC encode through the reference's host encoder (hevc_encoder_encode_raw;
+    wavefront rows on all host threads, QP 27 pinned, 1920x1080, 8-bit and
+    Main10) as shipped (oracle/_ref/libhevcref.so) and with its half-sample
+    planes built on the GPU (oracle/_ref/libhevcenc_b200.so, the binding in
+    bc250-vaapi_b200/binding/hevc_hpel_binding.c): frames/s by wall clock
+    over `steps` frames after `warmup` frames. The two streams are byte for
+    byte the same (tests/test_gpu_hevc_encode.py). Prints one JSON line."""
+    import ctypes
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import test_gpu_hevc_encode as he
+    n = args.warmup + args.steps
+    res = {}
+    for bd in (8, 10):
+        frames = he.frames_8bit(W, H, min(n, 30), 7) if bd == 8 else he.frames_p010(W, H, min(n, 30), 7)
+        for name, so in (("reference", he.REF_SO), ("gpu_hpel", he.GPU_SO)):
+            os.environ["BC250_HEVC_QP"] = "27"
+            L = ctypes.CDLL(so)
+            L.hevc_encoder_create_depth.restype = ctypes.c_void_p
+            L.hevc_encoder_create_depth.argtypes = [ctypes.c_void_p] + [ctypes.c_uint32] * 4 + [ctypes.c_int]
+            L.hevc_encoder_set_gop_size.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+            L.hevc_encoder_encode_raw.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                                  ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]
+            L.hevc_encoder_destroy.argtypes = [ctypes.c_void_p]
+            e = L.hevc_encoder_create_depth(None, W, H, 30, 8_000_000, bd)
+            os.environ.pop("BC250_HEVC_QP", None)
+            L.hevc_encoder_set_gop_size(e, GOP)
+            out = np.zeros(W * H * 6, np.uint8)
+            t0 = None
+            nbytes = 0
+            for k in range(n):
+                if k == args.warmup:
+                    t0 = time.perf_counter()
+                y, uv = frames[k % len(frames)]
+                r = L.hevc_encoder_encode_raw(e, y.ctypes.data, y.strides[0], uv.ctypes.data, uv.strides[0],
+                                              out.ctypes.data, out.nbytes)
+                assert r > 0
+                if k >= args.warmup:
+                    nbytes += r
+            dt = time.perf_counter() - t0
+            L.hevc_encoder_destroy(e)
+            res[f"{name}_{bd}bit"] = {"value": round(args.steps / dt, 2), "unit": "frames/s",
+                                      "mbit_per_frame": round(8 * nbytes / args.steps / 1e6, 4)}
+    line = {"metric": "HEVC 1080p encode fps (reference host encoder, half-sample planes on the GPU)",
+            "value": res["gpu_hpel_8bit"]["value"], "unit": "frames/s", "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "host_cores": os.cpu_count(),
+            "config": {"workload": "hevc_1080p_wpp_qp27", "width": W, "height": H, "qp": 27, "gop": GOP,
+                       "threads": os.cpu_count()}, **res,
+            "note": "wall clock per frame through hevc_encoder_encode_raw; the RD loop, CABAC and the other "
+                    "primitives stay on the host cores"}
+    print(json.dumps(line), flush=True)
+
+
 def run_hevc_deblock(args):
     """HEVC deblocking (b200enc_hevc_deblock) on seeded synthetic pictures:
     1080p 8-bit and 2160p 10-bit, enough resident copies to exceed L2, timed
@@ -853,7 +907,7 @@ def main():
                     help="run only this S-stream arm (warm-up + steps) and print nothing: a profiler's launch list")
     ap.add_argument("--streams", type=int, default=8)
     ap.add_argument("--conf", type=float, default=0.9)
-    ap.add_argument("--workload", choices=["h264_1080p", "multistream"], default="h264_1080p",
+    ap.add_argument("--workload", choices=["h264_1080p", "multistream", "hevc"], default="h264_1080p",
                     help="multistream: the 64-stream mixed-resolution batch (own JSON line)")
     ap.add_argument("--hevc-deblock", action="store_true",
                     help="time b200enc_hevc_deblock instead of the H.264 encode (own JSON lines)")
@@ -864,6 +918,8 @@ def main():
         run_hevc_deblock(args)
     elif args.workload == "multistream" and args.impl != "reference":
         run_multistream(args)
+    elif args.workload == "hevc" and args.impl != "reference":
+        run_hevc(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

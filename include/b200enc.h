@@ -65,6 +65,15 @@ int b200enc_me_full_search_ex(const uint8_t *cur_y, int cur_pitch,
                               void *mv_out, const int *mb_list, const int *mb_count,
                               int list_capacity, int flags, void *stream);
 
+/* The full search stages each reference window with one TMA copy when the
+ * window lies inside the plane (base and pitch 16-byte aligned); the wait
+ * for it is bounded (2 s). A copy that never completes leaves the MB's
+ * mv_out entry {0, 0, sad 0xffffffff} and sets a sticky device word: this
+ * returns it (0 none, 1 wait timeout, -1 on a CUDA error), clearing it when
+ * `clear` is non-zero. Contexts (gpu_compute.h) report it through the
+ * frame's status instead. */
+int b200enc_me_wait_errors(int clear);
+
 /* Fused P-frame chain given MVs: MC prediction, residual, forward 4x4, AC
  * quant (inter rounding), nz masks, chroma DC, dequant, inverse, recon.
  * Replaces residual_predict.comp (P path) + dct_transform.comp +
@@ -210,7 +219,8 @@ int b200enc_batch_graph_stats(void *b, long *instantiations, long *updates);
 #define B200ENC_TUNE_RESCORE_CTAS_PER_SM 2  /* learned re-scoring grid, CTAs per SM, 1..16 (default 8) */
 #define B200ENC_TUNE_FALLBACK_CTAS_PER_SM 3 /* fallback full-search grid, CTAs per SM, 1..16 (default 8) */
 #define B200ENC_TUNE_INTRA_CTAS 4           /* intra wavefront CTAs (rows in flight), >= 1 (default: one per row) */
-#define B200ENC_TUNE_COUNT 5
+#define B200ENC_TUNE_ME_STAGE 5             /* full-search window staging: 1 word loads, 2 TMA (default TMA) */
+#define B200ENC_TUNE_COUNT 6
 /* Sets a knob (0 restores the default); -1 for an unknown key or a value
  * out of range. */
 int b200enc_tune_set(int key, int value);
@@ -339,6 +349,14 @@ int b200enc_hevc_build_hpel_10(const uint16_t *recon, int pitch, int w, int h, i
  * host memory. 0 / -1. */
 int b200enc_hevc_build_hpel_host(const void *recon, int w, int h, int bit_depth, int margin, void *const planes[4],
                                  int plane_stride);
+
+/* Page-locks a long-lived host buffer (cudaHostRegister) so that the copies
+ * of b200enc_hevc_build_hpel_host to and from it run as DMA without a
+ * bounce copy; b200enc_unpin_host undoes it and must run before the buffer
+ * is freed. 0 / -1 (already pinned, or the driver refused: copies then stay
+ * pageable and correct). */
+int b200enc_pin_host(void *ptr, size_t bytes);
+int b200enc_unpin_host(void *ptr);
 
 /* Motion search of 8x8 CUs against the planes of b200enc_hevc_build_hpel
  * (8-bit), one job per CU: the reference's motion_search

@@ -1,6 +1,7 @@
 """The autotuner's launch shapes change no result: every candidate value of
 every knob (deblocking rows per CTA, P-chain macroblocks per CTA, the
-re-scoring and fallback grids, the intra wavefront's CTA count) gives the
+re-scoring and fallback grids, the intra wavefront's CTA count, the full
+search's window staging by TMA or by loads) gives the
 default's staged outputs and reconstruction bit for bit, on the learned form
 at 1920x1080 (I frame, a full-search P frame, learned P frames); and the
 tuner's choice is one of the candidates and is applied to the table."""

@@ -22,7 +22,7 @@ PRE = ("import sys; sys.path.insert(0, 'bc250-vaapi_b200'); import b200enc; from
 
 
 def test_names_match_the_python_keys():
-    out = _run(PRE + "print(','.join(L.b200enc_tune_name(k).decode() for k in range(5)), L.b200enc_tune_name(5))")
+    out = _run(PRE + "print(','.join(L.b200enc_tune_name(k).decode() for k in range(6)), L.b200enc_tune_name(6))")
     names, last = out.split()
     assert last == "None"
     sys.path.insert(0, os.path.join(ROOT, "bc250-vaapi_b200"))
@@ -34,24 +34,25 @@ def test_set_get_ranges():
     out = _run(PRE + "print(L.b200enc_tune_get(0), L.b200enc_tune_set(0, 3), L.b200enc_tune_get(0), "
                "L.b200enc_tune_set(0, 7), L.b200enc_tune_set(1, 3), L.b200enc_tune_set(1, 4), "
                "L.b200enc_tune_set(2, 17), L.b200enc_tune_set(4, 68), L.b200enc_tune_set(9, 1), "
-               "L.b200enc_tune_get(9), L.b200enc_tune_set(0, 0), L.b200enc_tune_get(0))")
-    assert out.split() == ["0", "0", "3", "-1", "-1", "0", "-1", "0", "-1", "-1", "0", "0"]
+               "L.b200enc_tune_get(9), L.b200enc_tune_set(0, 0), L.b200enc_tune_get(0), "
+               "L.b200enc_tune_set(5, 3), L.b200enc_tune_set(5, 1))")
+    assert out.split() == ["0", "0", "3", "-1", "-1", "0", "-1", "0", "-1", "-1", "0", "0", "-1", "0"]
 
 
 def test_tune_file_round_trip(tmp_path):
     p = tmp_path / "tune.txt"
     _run(PRE + f"autotune.write_tune_file({str(p)!r}, {{'deblock_rows': 5, 'pchain_mbs_per_cta': 2, "
-               "'rescore_ctas_per_sm': 12, 'fallback_ctas_per_sm': 4, 'intra_ctas': 34})")
+               "'rescore_ctas_per_sm': 12, 'fallback_ctas_per_sm': 4, 'intra_ctas': 34, 'me_stage': 1})")
     text = p.read_text()
     assert "deblock_rows 5" in text and text.startswith("#")
     # loaded explicitly
-    out = _run(PRE + f"print(L.b200enc_tune_load({str(p)!r}.encode()), [L.b200enc_tune_get(k) for k in range(5)])")
-    assert out == "5 [5, 2, 12, 4, 34]"
+    out = _run(PRE + f"print(L.b200enc_tune_load({str(p)!r}.encode()), [L.b200enc_tune_get(k) for k in range(6)])")
+    assert out == "6 [5, 2, 12, 4, 34, 1]"
     # loaded from the environment before the first use
-    out = _run(PRE + "print([L.b200enc_tune_get(k) for k in range(5)])", env={"B200ENC_TUNE_FILE": str(p)})
-    assert out == "[5, 2, 12, 4, 34]"
+    out = _run(PRE + "print([L.b200enc_tune_get(k) for k in range(6)])", env={"B200ENC_TUNE_FILE": str(p)})
+    assert out == "[5, 2, 12, 4, 34, 1]"
     # out-of-range lines are skipped, the rest kept
     p.write_text("deblock_rows 9\npchain_mbs_per_cta 4\nbogus 3\n")
-    out = _run(PRE + f"print(L.b200enc_tune_load({str(p)!r}.encode()), [L.b200enc_tune_get(k) for k in range(5)])")
-    assert out == "1 [0, 4, 0, 0, 0]"
+    out = _run(PRE + f"print(L.b200enc_tune_load({str(p)!r}.encode()), [L.b200enc_tune_get(k) for k in range(6)])")
+    assert out == "1 [0, 4, 0, 0, 0, 0]"
     assert _run(PRE + "print(L.b200enc_tune_load(b'/nonexistent/tune.txt'))") == "-1"
