@@ -40,6 +40,45 @@ def candidates(name, mbh):
     raise KeyError(name)
 
 
+def throughput_candidates(name, mbh):
+    """Candidates of a knob when the objective is a many-stream workload's
+    throughput: wider deblocking groups than the single-stream latency
+    optimum can pay there (fewer CTAs and group boundaries per frame)."""
+    if name == "deblock_rows":
+        return [3, 4, 5, 6]
+    if name in ("rescore_ctas_per_sm", "fallback_ctas_per_sm"):
+        return [4, 8, 12, 16]
+    return candidates(name, mbh)
+
+
+def tune_throughput(run, mbh, names=None, reps=3, log=None):
+    """Coordinate descent over the knobs (`names`, default all) for the
+    throughput of the caller's workload: `run()` encodes a fixed number of
+    steps of it and returns their device milliseconds. Each candidate is
+    scored by the median of `reps` runs; the fastest value of a knob is kept
+    before the next knob is tried. Returns ({name: value}, {name: {value:
+    ms}}) and leaves the table set to the choice. The number of run() calls
+    depends only on the candidate lists, so ranks of a multi-GPU job that
+    tune side by side make the same calls (run() may hold a barrier)."""
+    names = list(names or KEYS)
+    best = {name: 0 for name in KEYS}
+    apply(best)
+    scores_all = {}
+    for name in names:
+        scores = {}
+        for v in throughput_candidates(name, mbh):
+            apply({name: v})
+            t = sorted(run() for _ in range(reps))
+            scores[v] = t[len(t) // 2]
+        pick = min(scores, key=lambda v: (scores[v], v))
+        best[name] = pick
+        apply({name: pick})
+        scores_all[name] = scores
+        if log:
+            log(f"autotune {name}: " + ", ".join(f"{v}={ms:.3f}ms" for v, ms in scores.items()) + f" -> {pick}")
+    return best, scores_all
+
+
 def default_cache():
     base = os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache")
     return os.path.join(base, "b200enc", "tune.json")

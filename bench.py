@@ -512,14 +512,36 @@ def run_gpu(args):
             c.close()
         group.close()
         return
-    ms_l, launches, _, clk = arm(LEARNED, S, K, Wm, clocks=True)
-    ms_p, _, _, _ = arm(0, S, K, Wm)
-    ms_b, _, _, _ = arm(1, S, K, Wm)  # the learned form with the network's inference in BF16
+    from b200enc import autotune
+    tuned = {}
+
+    def tune_arm(mode):
+        """Launch parameters of one form, picked by the autotuner for this
+        workload's throughput (8 streams, 24 steps per score, median of 3);
+        both forms get their own."""
+        if args.no_tune:
+            autotune.apply({k2: 0 for k2 in autotune.KEYS})
+            return {k2: 0 for k2 in autotune.KEYS}
+        names = [n for n in autotune.KEYS
+                 if mode != 0 or n not in ("rescore_ctas_per_sm", "fallback_ctas_per_sm")]
+        t0 = time.perf_counter()
+        vals, scores = autotune.tune_throughput(lambda: arm(mode, S, 24, 3)[0], MBH, names, reps=3)
+        tuned["learned" if mode else "plain"] = {
+            "values": {n: vals[n] for n in names}, "seconds": round(time.perf_counter() - t0, 2),
+            "ms_per_24_steps": {n: {str(v): round(t, 3) for v, t in sc.items()} for n, sc in scores.items()}}
+        return vals
+
     k1 = max(K, 2 * GOP)
+    vals_l = tune_arm(LEARNED)
+    ms_l, launches, _, clk = arm(LEARNED, S, K, Wm, clocks=True)
+    ms_b, _, _, _ = arm(1, S, K, Wm)  # the learned form with the network's inference in BF16
     ms_l1, _, perf_l1, _ = arm(LEARNED, 1, k1, Wm, perf=True)
     me_counts = ctxs[0].me_stats()  # the learned form's last P frame
+    tune_arm(0)
+    ms_p, _, _, _ = arm(0, S, K, Wm)
     ms_p1, _, perf_p1, _ = arm(0, 1, k1, Wm, perf=True)
     mvf = ctxs[0].mv_field()  # the plain form's last P frame: early-outs are MV 0 with SAD <= 512
+    autotune.apply(vals_l)  # e2e and the full encode run the learned form
     searched = int(MBS - np.count_nonzero((mvf[:, 0] == 0) & (mvf[:, 1] == 0) & (mvf[:, 2].view(np.uint32) <= 512)))
     fps = replicas.aggregate_rate(ws, S * K, ms_l)
     fps_plain = replicas.aggregate_rate(ws, S * K, ms_p)
@@ -643,6 +665,7 @@ def run_gpu(args):
                              "frac": round(pipe_bytes * fps / ws / 1e9 / peak, 5),
                              "note": "algorithmic bytes of ME + P chain + deblock per P frame x learned-form fps"},
             "clocks": clk,
+            "tune": tuned or None,
         }
         if ws == 1 and not args.no_cpu_baseline:
             spf, info = cpu_reference_frame_time(host_frames[0][:2], budget_s=15.0)
@@ -903,6 +926,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-full-encode", action="store_true", help="skip the full-encode figure (host entropy coding)")
+    ap.add_argument("--no-tune", action="store_true", help="built-in launch parameters instead of autotuned ones")
     ap.add_argument("--profile-arm", choices=["learned", "plain", "learned_bf16"], default=None,
                     help="run only this S-stream arm (warm-up + steps) and print nothing: a profiler's launch list")
     ap.add_argument("--streams", type=int, default=8)
