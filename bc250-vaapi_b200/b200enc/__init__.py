@@ -28,7 +28,7 @@ EXPORTS = [
     "b200enc_hevc_choose_luma_mode", "b200enc_hevc_deblock", "b200enc_hevc_build_hpel_10",
     "b200enc_hevc_motion_search_10", "b200enc_hevc_choose_luma_mode_10", "b200enc_hevc_build_hpel_host",
     "b200enc_tune_set", "b200enc_tune_get", "b200enc_tune_name", "b200enc_tune_load", "b200enc_me_wait_errors",
-    "b200enc_pin_host", "b200enc_unpin_host",
+    "b200enc_pin_host", "b200enc_unpin_host", "b200enc_deblock_noalloc_status",
     "b200enc_batch_create", "b200enc_batch_destroy", "b200enc_batch_stream", "b200enc_batch_set_graph",
     "b200enc_batch_encode", "b200enc_batch_sync", "b200enc_batch_outputs", "b200enc_batch_graph_stats",
     # include/gpu_compute.h
@@ -145,6 +145,7 @@ def load_library(path=LIB_PATH):
     lib.b200enc_me_wait_errors.argtypes = [_i]
     lib.b200enc_pin_host.argtypes = [_vp, ctypes.c_size_t]
     lib.b200enc_unpin_host.argtypes = [_vp]
+    lib.b200enc_deblock_noalloc_status.argtypes = [_vp, _vp]
     return lib
 
 

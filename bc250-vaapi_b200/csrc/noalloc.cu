@@ -118,3 +118,14 @@ extern "C" int b200enc_deblock_noalloc(int mbw, int mbh, int qp, int is_intra, c
   return b200enc_deblock_launch(mbw, mbh, qp, is_intra, nz, mv, rec_y, rec_uv, rec_pitch, scratch, 0, 2000000u,
                                 stream);
 }
+
+extern "C" int b200enc_deblock_noalloc_status(uint32_t* status_host, void* stream) {
+  if (!status_host) return -1;
+  uint32_t* scratch = scratch_in_current_context();
+  if (!scratch) return -1;
+  // word 1 of the scratch layout is the error code
+  return cudaMemcpyAsync(status_host, scratch + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                         (cudaStream_t)stream) == cudaSuccess
+             ? 0
+             : -1;
+}

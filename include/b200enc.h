@@ -160,12 +160,16 @@ int b200enc_deblock_launch(int mbw, int mbh, int qp, int is_intra, const uint32_
  *   - Every call on a device shares the one array and zeroes the part it
  *     uses on `stream` before launching: calls whose work overlaps on the GPU
  *     (two streams at once) race on it and must be serialised by the caller.
- * Status: there is no scratch pointer to hand to b200enc_wavefront_status,
- * so a bounded wait that gave up (only if the GPU stopped running the
- * kernel's CTAs for 2 s) is not reported through this entry point. */
+ * Status: b200enc_deblock_noalloc_status enqueues, on `stream` after the
+ * call, a copy of the built-in array's error word into *status_host (0, or
+ * 1 when a bounded wait gave up: only if the GPU stopped running the
+ * kernel's CTAs for 2 s; the picture is then partly filtered); the word is
+ * valid once the stream has reached it. It allocates nothing: a page-locked
+ * *status_host keeps the copy asynchronous. 0 / -1. */
 int b200enc_deblock_noalloc(int mbw, int mbh, int qp, int is_intra,
                             const uint32_t *nz, const void *mv,
                             uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch, void *stream);
+int b200enc_deblock_noalloc_status(uint32_t *status_host, void *stream);
 
 /* ---- Multi-stream batches (no reference counterpart: the reference runs one
  * Vulkan queue per VA context, approach1-compute-encoder/src/gpu_compute.h

@@ -55,7 +55,11 @@ def test_noalloc_deblock_matches_caller_scratch_twice(gpu):
                                        ctypes.c_void_p(got.uv.data_ptr()), got.pitch,
                                        ctypes.c_void_p(stream.cuda_stream))
         assert rc == 0, f"call {call}: rc={rc}"
+        status = torch.full((1,), 7, dtype=torch.int32).pin_memory()
+        assert L.b200enc_deblock_noalloc_status(ctypes.c_void_p(status.data_ptr()),
+                                                ctypes.c_void_p(stream.cuda_stream)) == 0
         torch.cuda.synchronize()
+        assert int(status[0]) == 0, f"call {call}: status {int(status[0])}"
         assert torch.equal(got.buf, want.buf), f"call {call}: no-alloc deblocking differs"
         assert not torch.equal(got.buf, gpu.NV12.from_host(y, uv).buf), "the filter should change the picture"
 
@@ -101,3 +105,4 @@ def test_noalloc_deblock_rejects_bad_arguments(gpu):
     assert L.b200enc_deblock_noalloc(0, 4, 30, 0, p, p, p, p, 128, None) == -1
     assert L.b200enc_deblock_noalloc(8, 4, 30, 0, None, p, p, p, 128, None) == -1
     assert L.b200enc_deblock_noalloc(8, 4, 30, 0, p, p, p, p, 64, None) == -1  # pitch below 8 MBs
+    assert L.b200enc_deblock_noalloc_status(None, None) == -1
