@@ -715,7 +715,10 @@ def run_multistream(args):
     def kinds(t):
         return [t == 0 or (t + phase[s]) % GOP == 0 for s in range(S)]
 
-    def time_batch(me_mode, graph):
+    from b200enc import autotune
+    tuned = {}
+
+    def time_batch(me_mode, graph, tune=False):
         b = b200enc.Batch(sizes, search_range=RANGE, me_mode=me_mode, deblock=1, graph=graph)
         st = torch.cuda.ExternalStream(b.stream())
         t = 0
@@ -723,6 +726,29 @@ def run_multistream(args):
             b.encode([dev[s][t % MS_RESIDENT] for s in range(S)], qps, kinds(t))
             t += 1
         assert b.sync() == 0
+        if tune and not args.no_tune:
+            # launch shapes for this form's batched throughput: 4 steps per
+            # score, median of 3, on the same batch (steps continue the GOPs)
+            tt = [t]
+
+            def run4():
+                a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a0.record(st)
+                for _ in range(4):
+                    b.encode([dev[s][tt[0] % MS_RESIDENT] for s in range(S)], qps, kinds(tt[0]))
+                    tt[0] += 1
+                a1.record(st)
+                assert b.sync() == 0
+                return a0.elapsed_time(a1)
+            # the knobs a batch reads at every step (its deblocking rows are
+            # fixed when it is created, its P chain and full search have one
+            # shape): the learned form's persistent grids
+            names = ["rescore_ctas_per_sm", "fallback_ctas_per_sm"]
+            h0 = time.perf_counter()
+            vals, _ = autotune.tune_throughput(run4, max(h for _, h in sizes) // 16, names, reps=3)
+            tuned["learned" if me_mode else "plain"] = {"values": {n: vals[n] for n in names},
+                                                        "seconds": round(time.perf_counter() - h0, 2)}
+            t = tt[0]
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
         h0 = time.perf_counter()
@@ -779,7 +805,7 @@ def run_multistream(args):
 
     res = {}
     for name, mode in (("learned", LEARNED), ("plain", 0)):
-        ms, host_s, gs = time_batch(mode, True)
+        ms, host_s, gs = time_batch(mode, True, tune=mode != 0)
         res[name] = {"value": round(S * args.steps / (ms / 1000.0), 2), "unit": "frames/s",
                      "mb_per_s": round(mbs_per_step * args.steps / (ms / 1000.0), 1),
                      "ms_per_step": round(ms / args.steps, 4),
@@ -789,6 +815,9 @@ def run_multistream(args):
         res[name + "_contexts"] = {"value": round(S * args.steps / (ms_c / 1000.0), 2), "unit": "frames/s",
                                    "ms_per_step": round(ms_c / args.steps, 4),
                                    "note": "the same streams through 64 single-stream contexts"}
+    autotune.apply({k: 0 for k in autotune.KEYS})
+    if "learned" in tuned:
+        autotune.apply(tuned["learned"]["values"])
     ms_d, _, _ = time_batch(LEARNED, False)
     res["learned_no_graph"] = {"value": round(S * args.steps / (ms_d / 1000.0), 2), "unit": "frames/s",
                                "ms_per_step": round(ms_d / args.steps, 4)}
@@ -804,7 +833,8 @@ def run_multistream(args):
                        "l2": f"{sum(f.buf.numel() for fr in dev for f in fr) >> 20} MiB resident > L2"},
             "macroblocks_per_step": mbs_per_step, **res,
             "speedup_vs_plain": round(res["learned"]["value"] / res["plain"]["value"], 3),
-            "batch_vs_contexts": round(res["learned"]["value"] / res["learned_contexts"]["value"], 3)}
+            "batch_vs_contexts": round(res["learned"]["value"] / res["learned_contexts"]["value"], 3),
+            "tune": tuned or None}
     print(json.dumps(line), flush=True)
 
 
