@@ -13,9 +13,16 @@
 // recorded error.
 //
 // Within a macroblock the work is the reference's, laid out for warps:
-// 96 threads, each 4x4 block owned by a lane quad (luma blocks in warps
-// 0-1, chroma in warp 2), the 4x4 luma DC Hadamard done by 16 lanes as
-// signed 16-term sums.
+// three compute warps, each 4x4 block owned by a lane quad (luma blocks in
+// warps 0-1, chroma in warp 2), the 4x4 luma DC Hadamard as butterfly
+// stages over 16 lanes. Two more warps keep the row-to-row handoff off the
+// compute warps' path: a loader warp waits for the row above's progress
+// and fetches the next macroblocks' top lines into a two-slot buffer ahead
+// of use, and a publisher warp stores each macroblock's bottom luma and
+// chroma lines (from a two-slot copy), fences them and publishes the row's
+// progress, while the compute warps go on with the next macroblock. The
+// compute warps synchronise among themselves with a named barrier (96
+// threads); the five warps meet only at the start and end of a row.
 #include "b200enc_internal.h"
 #include "common.cuh"
 
@@ -23,9 +30,15 @@ namespace b200enc {
 
 struct IShared {
   int top[16], left[16], corner;
-  alignas(16) uint8_t topv[16];    // row Y-1 from X (luma), raw
-  alignas(16) uint8_t topc[16];    // row Yc-1 from 2*Xc (NV12 pairs), raw
-  int prev_top15;                  // byte 15 of the previous MB's topv: the corner of this MB
+  alignas(16) uint8_t topv[2][16];  // row Y-1 from X (luma), raw; slot mbx & 1 (loader warp)
+  alignas(16) uint8_t topc[2][16];  // row Yc-1 from 2*Xc (NV12 pairs), raw
+  alignas(16) uint8_t boty[2][16];  // this MB's bottom luma line, slot mbx & 1 (publisher warp)
+  alignas(16) uint8_t botc[2][16];  // this MB's bottom chroma line (NV12 pairs)
+  int prev_top15;                   // byte 15 of the previous MB's topv: the corner of this MB
+  int top_ready;                    // top lines loaded for MBs < top_ready (loader)
+  int top_used;                     // top-line slots of MBs < top_used consumed (compute)
+  int stored;                       // bottom lines of MBs < stored in boty/botc (compute)
+  int published;                    // progress published for MBs < published (publisher)
   int tuv[2][8], luv[2][8];
   int sad[4][3];
   int mode, dcv, pa, pb, pc, top_av, left_av;
@@ -58,7 +71,7 @@ __device__ __forceinline__ int hsign(int row, int idx) {
 // row only waits on an earlier row of its stream, so every wait is on a row
 // some running CTA owns.
 template <bool BATCH>
-__global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__ cur_y_,
+__global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict__ cur_y_,
                                                      const uint8_t* __restrict__ cur_uv_, int cur_pitch_, Geo g_,
                                                      int qp_, int num_slices_, int16_t* __restrict__ levels_,
                                                      int32_t* __restrict__ dc_, uint32_t* __restrict__ nzm_,
@@ -70,10 +83,19 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
   const int b = tid >> 2, r = tid & 3;
   const bool luma = b < 16;
 
+  // the compute warps' barrier (named barrier 1, warps 0-2)
+  auto csync = []() { asm volatile("bar.sync 1, 96;" ::: "memory"); };
+  auto vload = [](const int& w) { return *reinterpret_cast<const volatile int*>(&w); };
+  auto vstore = [](int& w, int v) {
+    __threadfence_block();
+    *reinterpret_cast<volatile int*>(&w) = v;
+  };
+
   for (;;) {
     if (tid == 0) {
       s.row = (int)atomicAdd(BATCH ? bt.ticket : Scratch{scratch_}.ticket(), 1u);
       s.abort_flag = 0;
+      s.top_ready = s.top_used = s.stored = s.published = 0;
     }
     __syncthreads();
     const uint8_t *cur_y = cur_y_, *cur_uv = cur_uv_;
@@ -135,6 +157,101 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
       for (int k = 0; k < 4; ++k) w |= (uint32_t)__ldg(rp + 2 * clampi(pair + (k >> 1), 0, g.W / 2 - 1) + (k & 1)) << (8 * k);
       return w;
     };
+    const uint64_t budget = (uint64_t)max_wait * 1000u;  // max_wait in microseconds
+    // Bounded wait of one lane on a shared word (written by another warp of
+    // this CTA after a block-scope fence): false on timeout (error recorded)
+    // or when a wait elsewhere in the CTA gave up. The fence after a
+    // successful wait orders the writer's earlier shared-memory writes before
+    // this thread's later reads.
+    auto wait_local = [&](const int& w, int need, uint32_t where) -> bool {
+      const uint64_t t0 = global_ns();
+      for (uint32_t it = 0;; ++it) {
+        if (vload(w) >= need) {
+          __threadfence_block();
+          return true;
+        }
+        if (vload(s.abort_flag)) return false;
+        if ((it & 15) == 15 && global_ns() - t0 > budget) {
+          if (atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u) atomicExch(sc.err_detail(), where);
+          vstore(s.abort_flag, 1);
+          return false;
+        }
+        if (it > 16) __nanosleep(32);
+      }
+    };
+    if (tid >= 96) {
+      const int lane = tid & 31;
+      if (tid < 128) {
+        // ---- loader warp: the row above's bottom lines, ahead of use -------
+        if (lane == 0) {
+          if (mby == 0) {
+            vstore(s.top_ready, g.mbw);  // no top neighbour: nothing to load
+          } else {
+            const uint32_t* pf_row = sc.progress(mby - 1);
+            for (int m = 0; m < g.mbw; ++m) {
+              const int X = m * 16, Y = mby * 16, Yc = Y >> 1;
+              const uint64_t t0 = global_ns();
+              bool ok = false;
+              for (uint32_t it = 0;; ++it) {
+                if (load_acquire(pf_row) >= (uint32_t)(m + 1)) { ok = true; break; }
+                if (load_acquire(sc.err()) != 0u || vload(s.abort_flag)) break;
+                if ((it & 15) == 15 && global_ns() - t0 > budget) {
+                  if (atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u)
+                    atomicExch(sc.err_detail(), (uint32_t)(mby * g.mbw + m));
+                  break;
+                }
+                if (it > 16) __nanosleep(32);
+              }
+              // the slot's previous macroblock (m - 2) has been read
+              if (!ok || !wait_local(s.top_used, m - 1, (uint32_t)(mby * g.mbw + m))) {
+                vstore(s.abort_flag, 1);
+                break;
+              }
+              // 16-byte lines: row Y-1 from X, chroma row Yc-1 from 2*Xc
+              // (inside the picture's coded width; clamping applies when they
+              // are read)
+              *reinterpret_cast<uint4*>(s.topv[m & 1]) =
+                  __ldcg(reinterpret_cast<const uint4*>(rec_y + (size_t)(Y - 1) * rec_pitch + X));
+              *reinterpret_cast<uint4*>(s.topc[m & 1]) =
+                  __ldcg(reinterpret_cast<const uint4*>(rec_uv + (size_t)(Yc - 1) * rec_pitch + X));
+              vstore(s.top_ready, m + 1);
+            }
+          }
+        }
+      } else if (lane == 0) {
+        // ---- publisher warp: bottom lines to the plane, fence, progress ----
+        // The row below reads only each macroblock's bottom luma and chroma
+        // lines (and, through its corner, those of the macroblock before);
+        // this thread stores them itself, so its own fence orders them before
+        // the progress word.
+        for (int m = 0; m < g.mbw; ++m) {
+          if (!wait_local(s.stored, m + 1, (uint32_t)(mby * g.mbw + m))) break;
+          const int X = m * 16, Y = mby * 16, Yc = Y >> 1;
+          if (Y + 15 <= rmy) {
+            uint8_t* dst = rec_y + (size_t)(Y + 15) * rec_pitch + X;
+            if (X + 16 <= g.RW) __stcg(reinterpret_cast<uint4*>(dst), *reinterpret_cast<const uint4*>(s.boty[m & 1]));
+            else
+              for (int c = 0; c < 16 && X + c < g.RW; ++c) dst[c] = s.boty[m & 1][c];
+          }
+          if (Yc + 7 <= cmy) {
+            uint8_t* dst = rec_uv + (size_t)(Yc + 7) * rec_pitch + X;
+            if ((X >> 1) + 8 <= cmx + 1) __stcg(reinterpret_cast<uint4*>(dst), *reinterpret_cast<const uint4*>(s.botc[m & 1]));
+            else
+              for (int c = 0; c < 8 && (X >> 1) + c <= cmx; ++c) {
+                dst[2 * c] = s.botc[m & 1][2 * c];
+                dst[2 * c + 1] = s.botc[m & 1][2 * c + 1];
+              }
+          }
+          __threadfence();
+          store_release(sc.progress(mby), (uint32_t)(m + 1));
+          vstore(s.published, m + 1);
+        }
+      }
+      __syncthreads();  // the row's end: all five warps
+      if (s.abort_flag) return;
+      continue;
+    }
+
     uint32_t pf = src_word(0);
     for (int mbx = 0; mbx < g.mbw; ++mbx) {
       const int mb = mby * g.mbw + mbx, X = mbx * 16, Y = mby * 16, Xc = X >> 1, Yc = Y >> 1;
@@ -176,38 +293,25 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
       } else if (tid == 32) {
         s.corner = (top_exists && left_exists) ? s.prev_top15 : 128;
       }
-      // ---- wait for the top neighbour, then its bottom lines --------------
-      if (tid == 0 && mby > 0) {
-        const uint32_t* pf_row = sc.progress(mby - 1);
-        bool ok = false, other = false;
-        const uint64_t t0 = global_ns(), budget = (uint64_t)max_wait * 1000u;  // max_wait in microseconds
-        for (uint32_t it = 0;; ++it) {
-          if (load_acquire(pf_row) >= (uint32_t)(mbx + 1)) { ok = true; break; }
-          if (load_acquire(sc.err()) != 0u) { other = true; break; }
-          if ((it & 15) == 15 && global_ns() - t0 > budget) break;
-          if (it > 16) __nanosleep(32);
-        }
-        if (!ok) {
-          if (!other && atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u) atomicExch(sc.err_detail(), (uint32_t)mb);
-          s.abort_flag = 1;
-        } else {
-          // 16-byte lines: row Y-1 from X, chroma row Yc-1 from 2*Xc (inside
-          // the picture's coded width; clamping applies when they are read)
-          *reinterpret_cast<uint4*>(s.topv) = __ldcg(reinterpret_cast<const uint4*>(rec_y + (size_t)(Y - 1) * rec_pitch + X));
-          *reinterpret_cast<uint4*>(s.topc) =
-              __ldcg(reinterpret_cast<const uint4*>(rec_uv + (size_t)(Yc - 1) * rec_pitch + X));
-        }
+      // ---- the top neighbour's bottom lines, loaded ahead by the loader ---
+      if (tid == 0) {
+        if (mby > 0) wait_local(s.top_ready, mbx + 1, (uint32_t)mb);
+        wait_local(s.published, mbx - 1, (uint32_t)mb);  // bottom-line slot of MB mbx - 2 copied out
       }
-      __syncthreads();
-      if (s.abort_flag) return;
+      csync();
+      if (vload(s.abort_flag)) break;
+      const int slot = mbx & 1;
       if (tid < 16) {
-        s.top[tid] = top_exists ? s.topv[min(tid, rmx - X)] : 128;
+        s.top[tid] = top_exists ? s.topv[slot][min(tid, rmx - X)] : 128;
       } else if (tid < 32) {
         const int i = tid - 16, pl = i >> 3, k = i & 7;
-        s.tuv[pl][k] = top_av ? s.topc[2 * min(k, cmx - Xc) + pl] : 128;
+        s.tuv[pl][k] = top_av ? s.topc[slot][2 * min(k, cmx - Xc) + pl] : 128;
       }
-      __syncthreads();
-      if (tid == 0) s.prev_top15 = s.topv[15];  // read by the next MB's corner, after the barriers below
+      csync();
+      if (tid == 0) {
+        s.prev_top15 = s.topv[slot][15];  // read by the next MB's corner, after the barriers below
+        vstore(s.top_used, mbx + 1);      // the slot is free for MB mbx + 2
+      }
 
       // ---- I16x16 candidates (intra_wavefront.comp:454-476) -------------
       if (tid < 32) {
@@ -236,7 +340,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
           }
         }
       }
-      __syncthreads();
+      csync();
       {
         uint32_t sdc = 0, sv = 0, shh = 0, spl = 0;
         for (int i = tid; i < 256; i += 96) {
@@ -260,7 +364,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
           s.sad[3][tid >> 5] = (int)spl;
         }
       }
-      __syncthreads();
+      csync();
       if (tid == 0) {
         const uint32_t sdc = s.sad[0][0] + s.sad[0][1] + s.sad[0][2], sv = s.sad[1][0] + s.sad[1][1] + s.sad[1][2];
         const uint32_t shh = s.sad[2][0] + s.sad[2][1] + s.sad[2][2], spl = s.sad[3][0] + s.sad[3][1] + s.sad[3][2];
@@ -273,7 +377,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
         pred_mode[mb] = (uint32_t)mode;  // chroma mode bits 2-3 = 0 (DC)
         mvs[mb] = MV{0, 0, 0u, 0u};
       }
-      __syncthreads();
+      csync();
 
       // ---- predictions -------------------------------------------------
       const int mode = s.mode;
@@ -300,7 +404,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
         else v = (top_av && left_av) ? (t1 + l1 + 4) >> 3 : top_av ? (t1 + 2) >> 2 : left_av ? (l1 + 2) >> 2 : 128;
         s.cdcval[tid] = v;  // temporarily: the predictor value of block 16+tid
       }
-      __syncthreads();
+      csync();
       if (!luma) {
         const int pv = s.cdcval[b - 16];
 #pragma unroll
@@ -335,7 +439,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
         if (luma) s.ldc[b] = x[0];
         else s.cdc[b - 16] = x[0];
       }
-      __syncthreads();
+      csync();
 
       // ---- DC paths ----------------------------------------------------
       // The luma DC transform (A1/src/encoder_h264.c:711-730) is a 2-D
@@ -376,7 +480,7 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
         const int f = dc_hadamard(s.ldl[tid]);
         s.ldcval[4 * i + k] = dequant_dc_luma(f, ql);
       }
-      __syncthreads();
+      csync();
 
       // ---- dequant + inverse + recon -----------------------------------
       int d[4];
@@ -394,28 +498,26 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
         for (int i = 0; i < 4; ++i)
           s.ruv[4 * (sub >> 1) + i][2 * (4 * (sub & 1) + r) + pl] = (uint8_t)clip1(s.pred[b][4 * i + r] + d[i]);
       }
-      __syncthreads();
+      csync();
 
-      // ---- stores + publish progress ------------------------------------
-      // The row below reads only this MB's bottom luma and chroma lines
-      // (and, through its corner, those of MB x-1): the threads storing them
-      // fence their own stores, then thread 0 publishes after the barrier.
+      // ---- stores; the bottom lines go to the publisher warp --------------
       // The other stores need no fence (the next kernel on the stream sees
-      // them).
+      // them). The bottom lines' slot was freed before this MB started
+      // (MB mbx - 2 published).
       if (tid < 48) {
         reinterpret_cast<uint4*>(levels + (size_t)mb * 384)[tid] = reinterpret_cast<const uint4*>(&s.lev[0][0])[tid];
       } else if (tid < 64) {
         const int row = tid - 48, gy = Y + row;
-        if (gy < g.RH) {
+        if (row < 15 && gy < g.RH) {
           uint8_t* dst = rec_y + (size_t)gy * rec_pitch + X;
           if (X + 16 <= g.RW) __stcg(reinterpret_cast<uint4*>(dst), *reinterpret_cast<const uint4*>(s.ry[row]));
           else
             for (int c = 0; c < 16 && X + c < g.RW; ++c) dst[c] = s.ry[row][c];
         }
-        if (row == 15) __threadfence();
+        if (row == 15) *reinterpret_cast<uint4*>(s.boty[slot]) = *reinterpret_cast<const uint4*>(s.ry[row]);
       } else if (tid < 72) {
         const int row = tid - 64, gy = Yc + row;
-        if (gy <= cmy) {
+        if (row < 7 && gy <= cmy) {
           uint8_t* dst = rec_uv + (size_t)gy * rec_pitch + X;
           if (Xc + 8 <= cmx + 1) __stcg(reinterpret_cast<uint4*>(dst), *reinterpret_cast<const uint4*>(s.ruv[row]));
           else
@@ -424,11 +526,13 @@ __global__ void __launch_bounds__(96) i_frame_kernel(const uint8_t* __restrict__
               dst[2 * c + 1] = s.ruv[row][2 * c + 1];
             }
         }
-        if (row == 7) __threadfence();
+        if (row == 7) *reinterpret_cast<uint4*>(s.botc[slot]) = *reinterpret_cast<const uint4*>(s.ruv[row]);
       }
-      __syncthreads();
-      if (tid == 0) store_release(sc.progress(mby), (uint32_t)(mbx + 1));
+      csync();
+      if (tid == 0) vstore(s.stored, mbx + 1);
     }
+    __syncthreads();  // the row's end: all five warps
+    if (s.abort_flag) return;
   }
 }
 
@@ -460,7 +564,7 @@ extern "C" int b200enc_i_frame_launch(const uint8_t* cur_y, const uint8_t* cur_u
   if (ctas <= 0) ctas = b200enc_tuned(B200ENC_TUNE_INTRA_CTAS);
   if (ctas <= 0) ctas = g.mbh;
   if (ctas > g.mbh) ctas = g.mbh;
-  i_frame_kernel<false><<<ctas, 96, 0, (cudaStream_t)stream>>>(cur_y, cur_uv, cur_pitch, g, qp, num_slices, levels, dc,
+  i_frame_kernel<false><<<ctas, 160, 0, (cudaStream_t)stream>>>(cur_y, cur_uv, cur_pitch, g, qp, num_slices, levels, dc,
                                                               nz, pred_mode, (MV*)mv, rec_y, rec_uv, rec_pitch,
                                                               scratch, max_wait, flags, BatchTab{});
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
@@ -471,7 +575,7 @@ extern "C" int b200enc_i_frame_launch(const uint8_t* cur_y, const uint8_t* cur_u
 // the caller).
 int b200enc_i_frame_batch_launch(const BatchTab& bt, int ctas, uint32_t max_wait, cudaStream_t st) {
   if (ctas <= 0) return 0;
-  i_frame_kernel<true><<<ctas, 96, 0, st>>>(nullptr, nullptr, 0, Geo{}, 0, 1, nullptr, nullptr, nullptr, nullptr,
+  i_frame_kernel<true><<<ctas, 160, 0, st>>>(nullptr, nullptr, 0, Geo{}, 0, 1, nullptr, nullptr, nullptr, nullptr,
                                             nullptr, nullptr, nullptr, 0, nullptr, max_wait, 0, bt);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
