@@ -41,12 +41,12 @@ struct IShared {
   int published;                    // progress published for MBs < published (publisher)
   int tuv[2][8], luv[2][8];
   int sad[4][3];
-  int mode, dcv, pa, pb, pc, top_av, left_av;
+  int dcv, pa, pb, pc;
   int row;
   int abort_flag;
   int16_t src[16][16];
   int16_t srcc[2][8][8];
-  int16_t pred[24][16];
+  int cpred[8];                     // chroma DC predictor of blocks 16..23
   alignas(16) int16_t lev[24][16];
   int32_t ldc[16];     // pre-quant luma DC coefficients (block raster)
   int32_t ldl[16];     // quantized luma DC (natural order)
@@ -86,10 +86,24 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
   // the compute warps' barrier (named barrier 1, warps 0-2)
   auto csync = []() { asm volatile("bar.sync 1, 96;" ::: "memory"); };
   auto vload = [](const int& w) { return *reinterpret_cast<const volatile int*>(&w); };
+  // acquire load of a shared word: orders this thread's later accesses
+  // after it without waiting for its earlier ones (a fence would wait for
+  // the source prefetch in flight)
+  auto aload = [](const int& w) {
+    int v;
+    asm volatile("ld.acquire.cta.shared::cta.b32 %0, [%1];" : "=r"(v)
+                 : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(&w)))
+                 : "memory");
+    return v;
+  };
+  // release of a shared word: a block-scope fence, then the store. The
+  // compute warps' writer is kSyncTid, a thread that never stores to global
+  // memory, so its fence has nothing in flight to wait for.
   auto vstore = [](int& w, int v) {
     __threadfence_block();
     *reinterpret_cast<volatile int*>(&w) = v;
   };
+  constexpr int kSyncTid = 73;  // warp 2, quad row 1: no global stores, only the source prefetch
 
   for (;;) {
     if (tid == 0) {
@@ -160,16 +174,12 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
     const uint64_t budget = (uint64_t)max_wait * 1000u;  // max_wait in microseconds
     // Bounded wait of one lane on a shared word (written by another warp of
     // this CTA after a block-scope fence): false on timeout (error recorded)
-    // or when a wait elsewhere in the CTA gave up. The fence after a
-    // successful wait orders the writer's earlier shared-memory writes before
-    // this thread's later reads.
+    // or when a wait elsewhere in the CTA gave up. The acquire load orders
+    // this thread's later reads after the writer's earlier writes.
     auto wait_local = [&](const int& w, int need, uint32_t where) -> bool {
       const uint64_t t0 = global_ns();
       for (uint32_t it = 0;; ++it) {
-        if (vload(w) >= need) {
-          __threadfence_block();
-          return true;
-        }
+        if (aload(w) >= need) return true;
         if (vload(s.abort_flag)) return false;
         if ((it & 15) == 15 && global_ns() - t0 > budget) {
           if (atomicCAS(sc.err(), 0u, kErrWaitTimeout) == 0u) atomicExch(sc.err_detail(), where);
@@ -294,36 +304,33 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
         s.corner = (top_exists && left_exists) ? s.prev_top15 : 128;
       }
       // ---- the top neighbour's bottom lines, loaded ahead by the loader ---
-      if (tid == 0) {
+      if (tid == kSyncTid) {
         if (mby > 0) wait_local(s.top_ready, mbx + 1, (uint32_t)mb);
         wait_local(s.published, mbx - 1, (uint32_t)mb);  // bottom-line slot of MB mbx - 2 copied out
       }
       csync();
       if (vload(s.abort_flag)) break;
       const int slot = mbx & 1;
-      if (tid < 16) {
-        s.top[tid] = top_exists ? s.topv[slot][min(tid, rmx - X)] : 128;
-      } else if (tid < 32) {
-        const int i = tid - 16, pl = i >> 3, k = i & 7;
-        s.tuv[pl][k] = top_av ? s.topc[slot][2 * min(k, cmx - Xc) + pl] : 128;
-      }
-      csync();
-      if (tid == 0) {
-        s.prev_top15 = s.topv[slot][15];  // read by the next MB's corner, after the barriers below
-        vstore(s.top_used, mbx + 1);      // the slot is free for MB mbx + 2
-      }
 
-      // ---- I16x16 candidates (intra_wavefront.comp:454-476) -------------
+      // ---- top lines, I16x16 candidates (intra_wavefront.comp:454-476),
+      //      chroma DC predictors --------------------------------------------
+      // Warp 0 spreads the luma top line and forms the candidate sums from
+      // registers and shuffles (lane sums without divergence: every lane
+      // loads, lanes outside a term contribute 0); warp 2 spreads the chroma
+      // top line and forms the chroma DC predictors (intra_wavefront.comp:
+      // 612-641).
       if (tid < 32) {
-        // lane sums without divergence (every lane loads, lanes outside a
-        // term contribute 0), reduced in one instruction each; lane 0 finishes
         const int t = tid & 15, k = tid & 7;
-        const int tv = s.top[t], lv = s.left[t];
-        const int lt = k <= 6 ? s.top[6 - k] : s.corner, la = k <= 6 ? s.left[6 - k] : s.corner;
+        const int tv = top_exists ? s.topv[slot][min(t, rmx - X)] : 128;
+        const int lv = s.left[t];
+        if (tid < 16) s.top[tid] = tv;
+        const int t6 = __shfl_sync(0xffffffffu, tv, (6 - k) & 15), t8 = __shfl_sync(0xffffffffu, tv, 8 + k);
+        const int lt = k <= 6 ? t6 : s.corner, la = k <= 6 ? s.left[6 - k] : s.corner;
         const int st = __reduce_add_sync(0xffffffffu, tid < 16 ? tv : 0);
         const int sl2 = __reduce_add_sync(0xffffffffu, tid < 16 ? lv : 0);
-        const int hterm = __reduce_add_sync(0xffffffffu, tid < 8 ? (k + 1) * (s.top[8 + k] - lt) : 0);
+        const int hterm = __reduce_add_sync(0xffffffffu, tid < 8 ? (k + 1) * (t8 - lt) : 0);
         const int vterm = __reduce_add_sync(0xffffffffu, tid < 8 ? (k + 1) * (s.left[8 + k] - la) : 0);
+        const int t15 = __shfl_sync(0xffffffffu, tv, 15);
         if (tid == 0) {
           int dcv;
           if (top_av && left_av) dcv = (st + sl2 + 16) >> 5;
@@ -332,15 +339,37 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
           else dcv = 128;
           s.dcv = dcv;
           if (plane_av) {
-            s.pa = 16 * (s.left[15] + s.top[15]);
+            s.pa = 16 * (s.left[15] + t15);
             s.pb = (5 * hterm + 32) >> 6;
             s.pc = (5 * vterm + 32) >> 6;
           } else {
             s.pa = s.pb = s.pc = 0;
           }
+          s.prev_top15 = s.topv[slot][15];  // read by the next MB's corner, after the barriers below
+        }
+      } else if (tid >= 64 && tid < 80) {
+        const int i = tid - 64, pl = i >> 3, k = i & 7;
+        s.tuv[pl][k] = top_av ? s.topc[slot][2 * min(k, cmx - Xc) + pl] : 128;
+        __syncwarp(0x0000ffffu);
+        if (i < 8) {
+          const int pl2 = i >> 2, sub = i & 3;
+          const int t0 = s.tuv[pl2][0] + s.tuv[pl2][1] + s.tuv[pl2][2] + s.tuv[pl2][3];
+          const int t1 = s.tuv[pl2][4] + s.tuv[pl2][5] + s.tuv[pl2][6] + s.tuv[pl2][7];
+          const int l0 = s.luv[pl2][0] + s.luv[pl2][1] + s.luv[pl2][2] + s.luv[pl2][3];
+          const int l1 = s.luv[pl2][4] + s.luv[pl2][5] + s.luv[pl2][6] + s.luv[pl2][7];
+          int v;
+          if (sub == 0) v = (top_av && left_av) ? (t0 + l0 + 4) >> 3 : top_av ? (t0 + 2) >> 2 : left_av ? (l0 + 2) >> 2 : 128;
+          else if (sub == 1) v = top_av ? (t1 + 2) >> 2 : left_av ? (l0 + 2) >> 2 : 128;
+          else if (sub == 2) v = left_av ? (l1 + 2) >> 2 : top_av ? (t0 + 2) >> 2 : 128;
+          else v = (top_av && left_av) ? (t1 + l1 + 4) >> 3 : top_av ? (t1 + 2) >> 2 : left_av ? (l1 + 2) >> 2 : 128;
+          s.cpred[i] = v;  // the predictor of chroma block 16 + i
         }
       }
       csync();
+      // the top-line slot has been read by both warps: free it for MB mbx + 2
+      if (tid == kSyncTid) vstore(s.top_used, mbx + 1);
+
+      // ---- the four I16x16 SADs -----------------------------------------
       {
         uint32_t sdc = 0, sv = 0, shh = 0, spl = 0;
         for (int i = tid; i < 256; i += 96) {
@@ -350,13 +379,10 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
           if (left_av) shh += (uint32_t)abs(v - s.left[y]);
           if (plane_av) spl += (uint32_t)abs(v - clip1((s.pa + s.pb * (x - 7) + s.pc * (y - 7) + 16) >> 5));
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          sdc += __shfl_xor_sync(0xffffffffu, sdc, o);
-          sv += __shfl_xor_sync(0xffffffffu, sv, o);
-          shh += __shfl_xor_sync(0xffffffffu, shh, o);
-          spl += __shfl_xor_sync(0xffffffffu, spl, o);
-        }
+        sdc = __reduce_add_sync(0xffffffffu, sdc);
+        sv = __reduce_add_sync(0xffffffffu, sv);
+        shh = __reduce_add_sync(0xffffffffu, shh);
+        spl = __reduce_add_sync(0xffffffffu, spl);
         if ((tid & 31) == 0) {
           s.sad[0][tid >> 5] = (int)sdc;
           s.sad[1][tid >> 5] = (int)sv;
@@ -365,50 +391,40 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
         }
       }
       csync();
-      if (tid == 0) {
+      // ---- mode decision, taken by every thread from the same sums --------
+      int mode;
+      {
         const uint32_t sdc = s.sad[0][0] + s.sad[0][1] + s.sad[0][2], sv = s.sad[1][0] + s.sad[1][1] + s.sad[1][2];
         const uint32_t shh = s.sad[2][0] + s.sad[2][1] + s.sad[2][2], spl = s.sad[3][0] + s.sad[3][1] + s.sad[3][2];
         uint32_t best = sdc;
-        int mode = 2;
+        mode = 2;
         if (top_av && sv < best) { best = sv; mode = 0; }
         if (left_av && shh < best) { best = shh; mode = 1; }
         if (plane_av && spl < best) { best = spl; mode = 3; }
-        s.mode = mode;
+      }
+      if (tid == 0) {
         pred_mode[mb] = (uint32_t)mode;  // chroma mode bits 2-3 = 0 (DC)
         mvs[mb] = MV{0, 0, 0u, 0u};
       }
-      csync();
-
-      // ---- predictions -------------------------------------------------
-      const int mode = s.mode;
-      for (int i = tid; i < 256; i += 96) {
-        const int x = i & 15, y = i >> 4;
-        int pv;
-        if (mode == 0) pv = s.top[x];
-        else if (mode == 1) pv = s.left[y];
-        else if (mode == 3) pv = clip1((s.pa + s.pb * (x - 7) + s.pc * (y - 7) + 16) >> 5);
-        else pv = s.dcv;
-        s.pred[(y >> 2) * 4 + (x >> 2)][(y & 3) * 4 + (x & 3)] = (int16_t)pv;
-      }
-      if (tid < 8) {
-        // chroma DC predictor per plane and sub-block (intra_wavefront.comp:612-641)
-        const int pl = tid >> 2, sub = tid & 3;
-        const int t0 = s.tuv[pl][0] + s.tuv[pl][1] + s.tuv[pl][2] + s.tuv[pl][3];
-        const int t1 = s.tuv[pl][4] + s.tuv[pl][5] + s.tuv[pl][6] + s.tuv[pl][7];
-        const int l0 = s.luv[pl][0] + s.luv[pl][1] + s.luv[pl][2] + s.luv[pl][3];
-        const int l1 = s.luv[pl][4] + s.luv[pl][5] + s.luv[pl][6] + s.luv[pl][7];
-        int v;
-        if (sub == 0) v = (top_av && left_av) ? (t0 + l0 + 4) >> 3 : top_av ? (t0 + 2) >> 2 : left_av ? (l0 + 2) >> 2 : 128;
-        else if (sub == 1) v = top_av ? (t1 + 2) >> 2 : left_av ? (l0 + 2) >> 2 : 128;
-        else if (sub == 2) v = left_av ? (l1 + 2) >> 2 : top_av ? (t0 + 2) >> 2 : 128;
-        else v = (top_av && left_av) ? (t1 + l1 + 4) >> 3 : top_av ? (t1 + 2) >> 2 : left_av ? (l1 + 2) >> 2 : 128;
-        s.cdcval[tid] = v;  // temporarily: the predictor value of block 16+tid
-      }
-      csync();
-      if (!luma) {
-        const int pv = s.cdcval[b - 16];
+      // The prediction of this thread's block row, formed where it is used
+      // (residual and reconstruction) instead of being stored: luma sample
+      // (x, y) of the chosen mode, or the chroma block's DC predictor.
+      const int dcv = s.dcv, pa = s.pa, pb = s.pb, pc = s.pc;
+      auto luma_pred = [&](int x, int y) -> int {
+        if (mode == 0) return s.top[x];
+        if (mode == 1) return s.left[y];
+        if (mode == 3) return clip1((pa + pb * (x - 7) + pc * (y - 7) + 16) >> 5);
+        return dcv;
+      };
+      int pred_row[4];
+      if (luma) {
+        const int bx = b & 3, by = b >> 2;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) s.pred[b][4 * r + i] = (int16_t)pv;
+        for (int i = 0; i < 4; ++i) pred_row[i] = luma_pred(4 * bx + i, 4 * by + r);
+      } else {
+        const int pv = s.cpred[b - 16];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) pred_row[i] = pv;
       }
 
       // ---- forward + AC quant (position 0 is carried by the DC paths) ----
@@ -416,11 +432,11 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
       if (luma) {
         const int bx = b & 3, by = b >> 2;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) x[i] = s.src[4 * by + r][4 * bx + i] - s.pred[b][4 * r + i];
+        for (int i = 0; i < 4; ++i) x[i] = s.src[4 * by + r][4 * bx + i] - pred_row[i];
       } else {
         const int pl = (b - 16) >> 2, sub = (b - 16) & 3;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) x[i] = s.srcc[pl][4 * (sub >> 1) + r][4 * (sub & 1) + i] - s.pred[b][4 * r + i];
+        for (int i = 0; i < 4; ++i) x[i] = s.srcc[pl][4 * (sub >> 1) + r][4 * (sub & 1) + i] - pred_row[i];
       }
       quad_forward(x, r);  // x[i] = coef[i][r]
       uint32_t nz = 0;
@@ -487,16 +503,17 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
 #pragma unroll
       for (int i = 0; i < 4; ++i) d[i] = dequant_ac(s.lev[b][4 * r + i], 4 * r + i, q);
       if (r == 0) d[0] = (luma ? s.ldcval[b] : s.cdcval[b - 16]) + 32;
-      quad_inverse(d, r);
+      quad_inverse(d, r);  // d[i] = res[i][r]: column r of the block
       if (luma) {
         const int bx = b & 3, by = b >> 2;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) s.ry[4 * by + i][4 * bx + r] = (uint8_t)clip1(s.pred[b][4 * i + r] + d[i]);
+        for (int i = 0; i < 4; ++i) s.ry[4 * by + i][4 * bx + r] = (uint8_t)clip1(luma_pred(4 * bx + r, 4 * by + i) + d[i]);
       } else {
         const int pl = (b - 16) >> 2, sub = (b - 16) & 3;
+        const int pv = pred_row[0];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-          s.ruv[4 * (sub >> 1) + i][2 * (4 * (sub & 1) + r) + pl] = (uint8_t)clip1(s.pred[b][4 * i + r] + d[i]);
+          s.ruv[4 * (sub >> 1) + i][2 * (4 * (sub & 1) + r) + pl] = (uint8_t)clip1(pv + d[i]);
       }
       csync();
 
@@ -529,7 +546,7 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
         if (row == 7) *reinterpret_cast<uint4*>(s.botc[slot]) = *reinterpret_cast<const uint4*>(s.ruv[row]);
       }
       csync();
-      if (tid == 0) vstore(s.stored, mbx + 1);
+      if (tid == kSyncTid) vstore(s.stored, mbx + 1);
     }
     __syncthreads();  // the row's end: all five warps
     if (s.abort_flag) return;
