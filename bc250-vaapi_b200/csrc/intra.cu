@@ -18,9 +18,10 @@
 // stages over 16 lanes. Two more warps keep the row-to-row handoff off the
 // compute warps' path: a loader warp waits for the row above's progress
 // and fetches the next macroblocks' top lines into a two-slot buffer ahead
-// of use, and a publisher warp stores each macroblock's bottom luma and
-// chroma lines (from a two-slot copy), fences them and publishes the row's
-// progress, while the compute warps go on with the next macroblock. The
+// of use, and a publisher warp stores each macroblock's levels and
+// reconstruction (kept in two-slot shared buffers), fences them and
+// publishes the row's progress, while the compute warps go on with the
+// next macroblock. The
 // compute warps synchronise among themselves with a named barrier (96
 // threads); the five warps meet only at the start and end of a row.
 #include "b200enc_internal.h"
@@ -32,12 +33,10 @@ struct IShared {
   int top[16], left[16], corner;
   alignas(16) uint8_t topv[2][16];  // row Y-1 from X (luma), raw; slot mbx & 1 (loader warp)
   alignas(16) uint8_t topc[2][16];  // row Yc-1 from 2*Xc (NV12 pairs), raw
-  alignas(16) uint8_t boty[2][16];  // this MB's bottom luma line, slot mbx & 1 (publisher warp)
-  alignas(16) uint8_t botc[2][16];  // this MB's bottom chroma line (NV12 pairs)
   int prev_top15;                   // byte 15 of the previous MB's topv: the corner of this MB
   int top_ready;                    // top lines loaded for MBs < top_ready (loader)
   int top_used;                     // top-line slots of MBs < top_used consumed (compute)
-  int stored;                       // bottom lines of MBs < stored in boty/botc (compute)
+  int stored;                       // levels and reconstruction of MBs < stored complete (compute)
   int published;                    // progress published for MBs < published (publisher)
   int tuv[2][8], luv[2][8];
   int sad[4][3];
@@ -47,14 +46,14 @@ struct IShared {
   int16_t src[16][16];
   int16_t srcc[2][8][8];
   int cpred[8];                     // chroma DC predictor of blocks 16..23
-  alignas(16) int16_t lev[24][16];
+  alignas(16) int16_t lev[2][24][16];  // slot mbx & 1: written by the compute warps, stored by the publisher
   int32_t ldc[16];     // pre-quant luma DC coefficients (block raster)
   int32_t ldl[16];     // quantized luma DC (natural order)
   int32_t ldcval[16];  // dequantized luma DC per block
   int32_t cdc[8];
   int32_t cdcval[8];
-  alignas(16) uint8_t ry[16][16];
-  alignas(16) uint8_t ruv[8][16];
+  alignas(16) uint8_t ry[2][16][16];  // slot mbx & 1 (the next MB's left neighbour, the publisher's source)
+  alignas(16) uint8_t ruv[2][8][16];
 };
 
 __device__ __forceinline__ int hsign(int row, int idx) {
@@ -228,33 +227,48 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
             }
           }
         }
-      } else if (lane == 0) {
-        // ---- publisher warp: bottom lines to the plane, fence, progress ----
+      } else {
+        // ---- publisher warp: the macroblock's levels and reconstruction to
+        //      memory, fence, progress ----------------------------------------
         // The row below reads only each macroblock's bottom luma and chroma
         // lines (and, through its corner, those of the macroblock before);
-        // this thread stores them itself, so its own fence orders them before
-        // the progress word.
+        // every lane fences its own stores and lane 0 publishes after the
+        // warp has met, so the progress word follows them.
         for (int m = 0; m < g.mbw; ++m) {
-          if (!wait_local(s.stored, m + 1, (uint32_t)(mby * g.mbw + m))) break;
-          const int X = m * 16, Y = mby * 16, Yc = Y >> 1;
-          if (Y + 15 <= rmy) {
-            uint8_t* dst = rec_y + (size_t)(Y + 15) * rec_pitch + X;
-            if (X + 16 <= g.RW) __stcg(reinterpret_cast<uint4*>(dst), *reinterpret_cast<const uint4*>(s.boty[m & 1]));
-            else
-              for (int c = 0; c < 16 && X + c < g.RW; ++c) dst[c] = s.boty[m & 1][c];
-          }
-          if (Yc + 7 <= cmy) {
-            uint8_t* dst = rec_uv + (size_t)(Yc + 7) * rec_pitch + X;
-            if ((X >> 1) + 8 <= cmx + 1) __stcg(reinterpret_cast<uint4*>(dst), *reinterpret_cast<const uint4*>(s.botc[m & 1]));
-            else
-              for (int c = 0; c < 8 && (X >> 1) + c <= cmx; ++c) {
-                dst[2 * c] = s.botc[m & 1][2 * c];
-                dst[2 * c + 1] = s.botc[m & 1][2 * c + 1];
-              }
+          int go = 0;
+          if (lane == 0) go = wait_local(s.stored, m + 1, (uint32_t)(mby * g.mbw + m)) ? 1 : 0;
+          if (!__shfl_sync(0xffffffffu, go, 0)) break;
+          __syncwarp();           // orders lane 0's acquire before the other lanes' reads
+          (void)aload(s.stored);  // and each lane acquires the word lane 0 saw
+          const int sl = m & 1, X = m * 16, Y = mby * 16, Yc = Y >> 1, mbi = mby * g.mbw + m;
+          for (int i = lane; i < 48; i += 32)
+            reinterpret_cast<uint4*>(levels + (size_t)mbi * 384)[i] = reinterpret_cast<const uint4*>(&s.lev[sl][0][0])[i];
+          if (lane < 16) {
+            const int gy = Y + lane;
+            if (gy <= rmy) {
+              uint8_t* dst = rec_y + (size_t)gy * rec_pitch + X;
+              if (X + 16 <= g.RW) __stcg(reinterpret_cast<uint4*>(dst), *reinterpret_cast<const uint4*>(s.ry[sl][lane]));
+              else
+                for (int c = 0; c < 16 && X + c < g.RW; ++c) dst[c] = s.ry[sl][lane][c];
+            }
+          } else if (lane < 24) {
+            const int row = lane - 16, gy = Yc + row;
+            if (gy <= cmy) {
+              uint8_t* dst = rec_uv + (size_t)gy * rec_pitch + X;
+              if ((X >> 1) + 8 <= cmx + 1) __stcg(reinterpret_cast<uint4*>(dst), *reinterpret_cast<const uint4*>(s.ruv[sl][row]));
+              else
+                for (int c = 0; c < 8 && (X >> 1) + c <= cmx; ++c) {
+                  dst[2 * c] = s.ruv[sl][row][2 * c];
+                  dst[2 * c + 1] = s.ruv[sl][row][2 * c + 1];
+                }
+            }
           }
           __threadfence();
-          store_release(sc.progress(mby), (uint32_t)(m + 1));
-          vstore(s.published, m + 1);
+          __syncwarp();
+          if (lane == 0) {
+            store_release(sc.progress(mby), (uint32_t)(m + 1));
+            vstore(s.published, m + 1);
+          }
         }
       }
       __syncthreads();  // the row's end: all five warps
@@ -292,25 +306,25 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
         }
         if (mbx + 1 < g.mbw) pf = src_word(mbx + 1);
       }
+      const int slot = mbx & 1;  // this MB's top-line, level and reconstruction slots
       // ---- left and corner neighbours: this CTA's own previous MB --------
       // (still in s.ry / s.ruv; rows past the clamp limit read its last row,
       // as the clamped reads of the reference do)
       if (tid < 16) {
-        s.left[tid] = left_exists ? s.ry[min(tid, rmy - Y)][15] : 128;
+        s.left[tid] = left_exists ? s.ry[slot ^ 1][min(tid, rmy - Y)][15] : 128;
       } else if (tid < 32) {
         const int i = tid - 16, pl = i >> 3, k = i & 7;
-        s.luv[pl][k] = left_av ? s.ruv[min(k, cmy - Yc)][14 + pl] : 128;
+        s.luv[pl][k] = left_av ? s.ruv[slot ^ 1][min(k, cmy - Yc)][14 + pl] : 128;
       } else if (tid == 32) {
         s.corner = (top_exists && left_exists) ? s.prev_top15 : 128;
       }
       // ---- the top neighbour's bottom lines, loaded ahead by the loader ---
       if (tid == kSyncTid) {
         if (mby > 0) wait_local(s.top_ready, mbx + 1, (uint32_t)mb);
-        wait_local(s.published, mbx - 1, (uint32_t)mb);  // bottom-line slot of MB mbx - 2 copied out
+        wait_local(s.published, mbx - 1, (uint32_t)mb);  // the slots of MB mbx - 2 are stored
       }
       csync();
       if (vload(s.abort_flag)) break;
-      const int slot = mbx & 1;
 
       // ---- top lines, I16x16 candidates (intra_wavefront.comp:454-476),
       //      chroma DC predictors --------------------------------------------
@@ -444,7 +458,7 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
       for (int i = 0; i < 4; ++i) {
         const int pos = 4 * i + r;
         const int l = pos == 0 ? 0 : quant_ac(x[i], pos, q);
-        s.lev[b][pos] = (int16_t)clampi(l, -32768, 32767);
+        s.lev[slot][b][pos] = (int16_t)clampi(l, -32768, 32767);
         nz |= (l != 0 ? 1u : 0u) << pos;
       }
       nz |= __shfl_xor_sync(0xffffffffu, nz, 1);
@@ -479,15 +493,16 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
         const int i = row_of[tid & 3], k = row_of[tid >> 2];
         const int sum = dc_hadamard(s.ldc[tid]);
         s.ldl[4 * i + k] = quantize_dc((sum + 1) >> 1, ql);
-      } else if (tid == 64 || tid == 80) {
-        const int pl = (tid - 64) >> 4;
+      } else if (tid >= 64 && tid < 72) {
+        // chroma DC of one plane per 4 lanes: lane o quantises Hadamard output
+        // o, then forms inverse output o from the group's four levels
+        const int j = tid - 64, pl = j >> 2, o = j & 3;
         const int c0 = s.cdc[4 * pl], c1 = s.cdc[4 * pl + 1], c2 = s.cdc[4 * pl + 2], c3 = s.cdc[4 * pl + 3];
-        const int l0 = quantize_dc(c0 + c1 + c2 + c3, qc), l1 = quantize_dc(c0 - c1 + c2 - c3, qc);
-        const int l2 = quantize_dc(c0 + c1 - c2 - c3, qc), l3 = quantize_dc(c0 - c1 - c2 + c3, qc);
-        s.cdcval[4 * pl + 0] = dequant_dc_chroma(l0 + l1 + l2 + l3, qc);
-        s.cdcval[4 * pl + 1] = dequant_dc_chroma(l0 - l1 + l2 - l3, qc);
-        s.cdcval[4 * pl + 2] = dequant_dc_chroma(l0 + l1 - l2 - l3, qc);
-        s.cdcval[4 * pl + 3] = dequant_dc_chroma(l0 - l1 - l2 + l3, qc);
+        const int sb = (o & 1) ? -1 : 1, sc2 = (o & 2) ? -1 : 1;  // signs of c1/c3 and c2/c3
+        const int lo = quantize_dc(c0 + sb * c1 + sc2 * c2 + sb * sc2 * c3, qc);
+        const int g0 = __shfl_sync(0x000000ffu, lo, 4 * pl), g1 = __shfl_sync(0x000000ffu, lo, 4 * pl + 1);
+        const int g2 = __shfl_sync(0x000000ffu, lo, 4 * pl + 2), g3 = __shfl_sync(0x000000ffu, lo, 4 * pl + 3);
+        s.cdcval[4 * pl + o] = dequant_dc_chroma(g0 + sb * g1 + sc2 * g2 + sb * sc2 * g3, qc);
       }
       __syncwarp();
       if (tid < 16) {
@@ -501,49 +516,20 @@ __global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict_
       // ---- dequant + inverse + recon -----------------------------------
       int d[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) d[i] = dequant_ac(s.lev[b][4 * r + i], 4 * r + i, q);
+      for (int i = 0; i < 4; ++i) d[i] = dequant_ac(s.lev[slot][b][4 * r + i], 4 * r + i, q);
       if (r == 0) d[0] = (luma ? s.ldcval[b] : s.cdcval[b - 16]) + 32;
       quad_inverse(d, r);  // d[i] = res[i][r]: column r of the block
       if (luma) {
         const int bx = b & 3, by = b >> 2;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) s.ry[4 * by + i][4 * bx + r] = (uint8_t)clip1(luma_pred(4 * bx + r, 4 * by + i) + d[i]);
+        for (int i = 0; i < 4; ++i)
+          s.ry[slot][4 * by + i][4 * bx + r] = (uint8_t)clip1(luma_pred(4 * bx + r, 4 * by + i) + d[i]);
       } else {
         const int pl = (b - 16) >> 2, sub = (b - 16) & 3;
         const int pv = pred_row[0];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-          s.ruv[4 * (sub >> 1) + i][2 * (4 * (sub & 1) + r) + pl] = (uint8_t)clip1(pv + d[i]);
-      }
-      csync();
-
-      // ---- stores; the bottom lines go to the publisher warp --------------
-      // The other stores need no fence (the next kernel on the stream sees
-      // them). The bottom lines' slot was freed before this MB started
-      // (MB mbx - 2 published).
-      if (tid < 48) {
-        reinterpret_cast<uint4*>(levels + (size_t)mb * 384)[tid] = reinterpret_cast<const uint4*>(&s.lev[0][0])[tid];
-      } else if (tid < 64) {
-        const int row = tid - 48, gy = Y + row;
-        if (row < 15 && gy < g.RH) {
-          uint8_t* dst = rec_y + (size_t)gy * rec_pitch + X;
-          if (X + 16 <= g.RW) __stcg(reinterpret_cast<uint4*>(dst), *reinterpret_cast<const uint4*>(s.ry[row]));
-          else
-            for (int c = 0; c < 16 && X + c < g.RW; ++c) dst[c] = s.ry[row][c];
-        }
-        if (row == 15) *reinterpret_cast<uint4*>(s.boty[slot]) = *reinterpret_cast<const uint4*>(s.ry[row]);
-      } else if (tid < 72) {
-        const int row = tid - 64, gy = Yc + row;
-        if (row < 7 && gy <= cmy) {
-          uint8_t* dst = rec_uv + (size_t)gy * rec_pitch + X;
-          if (Xc + 8 <= cmx + 1) __stcg(reinterpret_cast<uint4*>(dst), *reinterpret_cast<const uint4*>(s.ruv[row]));
-          else
-            for (int c = 0; c < 8 && Xc + c <= cmx; ++c) {
-              dst[2 * c] = s.ruv[row][2 * c];
-              dst[2 * c + 1] = s.ruv[row][2 * c + 1];
-            }
-        }
-        if (row == 7) *reinterpret_cast<uint4*>(s.botc[slot]) = *reinterpret_cast<const uint4*>(s.ruv[row]);
+          s.ruv[slot][4 * (sub >> 1) + i][2 * (4 * (sub & 1) + r) + pl] = (uint8_t)clip1(pv + d[i]);
       }
       csync();
       if (tid == kSyncTid) vstore(s.stored, mbx + 1);
