@@ -64,9 +64,13 @@ __device__ __forceinline__ int mf_of(int rem, int pt) { return kMF[rem][pt]; }
 __device__ __forceinline__ int v_of(int rem, int pt) { return kV[rem][pt]; }
 __device__ __forceinline__ int dc_ls(int rem) { return kDcLs[rem]; }
 
-// Quantizer constants for one QP, computed once per thread.
+// Quantizer constants for one QP, computed once per thread: the MF and V
+// entries of the QP's row are held in registers, so a coefficient's
+// constant is a selection on its position class rather than a
+// constant-memory load whose address differs from lane to lane.
 struct QP {
   int per, rem, f_shift, f;  // f = rounding offset of the AC quantizer
+  int mf0, mf1, mf2, v0, v1, v2;
 };
 __device__ __forceinline__ QP make_qp(int qp, bool intra) {
   QP q;
@@ -74,16 +78,24 @@ __device__ __forceinline__ QP make_qp(int qp, bool intra) {
   q.rem = qp - 6 * q.per;
   q.f_shift = 15 + q.per;
   q.f = (1 << q.f_shift) / (intra ? 3 : 6);
+  q.mf0 = mf_of(q.rem, 0);
+  q.mf1 = mf_of(q.rem, 1);
+  q.mf2 = mf_of(q.rem, 2);
+  q.v0 = v_of(q.rem, 0);
+  q.v1 = v_of(q.rem, 1);
+  q.v2 = v_of(q.rem, 2);
   return q;
 }
+__device__ __forceinline__ int qp_mf(const QP& q, int pt) { return pt == 0 ? q.mf0 : (pt == 1 ? q.mf1 : q.mf2); }
+__device__ __forceinline__ int qp_v(const QP& q, int pt) { return pt == 0 ? q.v0 : (pt == 1 ? q.v1 : q.v2); }
 
 __device__ __forceinline__ int quant_ac(int c, int pos, const QP& q) {
   const int a = c < 0 ? -c : c;
-  const int l = (a * mf_of(q.rem, pos_type(pos)) + q.f) >> q.f_shift;
+  const int l = (a * qp_mf(q, pos_type(pos)) + q.f) >> q.f_shift;
   return c < 0 ? -l : l;
 }
 __device__ __forceinline__ int dequant_ac(int level, int pos, const QP& q) {
-  const int scale = 16 * v_of(q.rem, pos_type(pos));
+  const int scale = 16 * qp_v(q, pos_type(pos));
   if (q.per >= 4) return (level * scale) << (q.per - 4);
   return (level * scale + (1 << (3 - q.per))) >> (4 - q.per);
 }

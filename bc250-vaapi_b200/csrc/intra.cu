@@ -70,7 +70,7 @@ __device__ __forceinline__ int hsign(int row, int idx) {
 // row only waits on an earlier row of its stream, so every wait is on a row
 // some running CTA owns.
 template <bool BATCH>
-__global__ void __launch_bounds__(160) i_frame_kernel(const uint8_t* __restrict__ cur_y_,
+__global__ void __launch_bounds__(160, 1) i_frame_kernel(const uint8_t* __restrict__ cur_y_,
                                                      const uint8_t* __restrict__ cur_uv_, int cur_pitch_, Geo g_,
                                                      int qp_, int num_slices_, int16_t* __restrict__ levels_,
                                                      int32_t* __restrict__ dc_, uint32_t* __restrict__ nzm_,
