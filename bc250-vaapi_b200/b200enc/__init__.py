@@ -16,7 +16,7 @@ LIB_PATH = os.path.normpath(os.path.join(HERE, "..", "lib", "libb200enc.so"))
 EXPORTS = [
     # include/b200enc.h
     "b200enc_me_full_search", "b200enc_p_frame", "b200enc_wavefront_scratch_bytes", "b200enc_i_frame",
-    "b200enc_deblock", "b200enc_wavefront_status", "b200enc_i_frame_launch", "b200enc_deblock_launch",
+    "b200enc_deblock", "b200enc_deblock_tiles", "b200enc_wavefront_status", "b200enc_i_frame_launch", "b200enc_deblock_launch",
     "b200enc_deblock_noalloc", "b200enc_gemm_bf16", "b200enc_me_full_search_ex",
     "b200enc_proposal_num_params", "b200enc_proposal_create", "b200enc_proposal_destroy",
     "b200enc_proposal_set_params", "b200enc_proposal_get_params", "b200enc_proposal_prepare",
@@ -83,6 +83,7 @@ def load_library(path=LIB_PATH):
     lib.b200enc_i_frame.argtypes = [_vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i,
                                     _vp, ctypes.c_size_t, _i, _i, _vp]
     lib.b200enc_deblock.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, ctypes.c_size_t, _i, _vp]
+    lib.b200enc_deblock_tiles.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp]
     lib.b200enc_me_full_search.argtypes = [_vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp]
     lib.b200enc_me_full_search_ex.argtypes = [_vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _i, _i,
                                               _vp]
@@ -279,6 +280,13 @@ def i_frame(cur, W, H, RW, RH, qp, num_slices, out, rec, scr, ctas=0, stream=Non
 def deblock(mbw, mbh, qp, is_intra, nz, mv, rec, scr, ctas=0, stream=None):
     _check(lib().b200enc_deblock(mbw, mbh, qp, int(is_intra), _p(nz), _p(mv), rec.yp(), rec.uvp(), rec.pitch,
                                  _p(scr), scr.numel() * 4, ctas, _stream(stream)), "b200enc_deblock")
+
+
+def deblock_tiles(mbw, mbh, qp, is_intra, nz, mv, src, dst, status, stream=None):
+    """Tile deblocking from the unfiltered planes `src` into `dst` (same
+    pitch, no overlap); `status` is a device int32 tensor of >= 4 words."""
+    _check(lib().b200enc_deblock_tiles(mbw, mbh, qp, int(is_intra), _p(nz), _p(mv), src.yp(), src.uvp(), dst.yp(),
+                                       dst.uvp(), src.pitch, _p(status), _stream(stream)), "b200enc_deblock_tiles")
 
 
 GEMM_ACCUMULATE, GEMM_RELU, GEMM_OUT_BF16 = 1, 2, 4

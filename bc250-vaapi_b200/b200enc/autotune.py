@@ -1,11 +1,13 @@
 """Autotuner of the encoder's launch shapes.
 
-The library reads six launch parameters from a process-wide table
-(include/b200enc.h, B200ENC_TUNE_*): macroblock rows per deblocking CTA (the
-wavefront's rows per CTA), macroblocks per P-chain CTA (the CTA tile shape),
-the persistent grids of the learned form's re-scoring and fallback search,
-the intra wavefront's CTA count, and whether the full search stages its
-reference windows by TMA or by word loads. None changes a result; each
+The library reads eight launch parameters from a process-wide table
+(include/b200enc.h, B200ENC_TUNE_*): macroblock rows per CTA of the
+deblocking wavefront (the stage-level b200enc_deblock), macroblocks per
+P-chain CTA (the CTA tile shape), the persistent grids of the learned form's
+re-scoring and fallback search, the intra wavefront's CTA count, whether the
+full search stages its reference windows by TMA or by word loads, and the
+tile shape of the tile deblocking that encoding contexts and batches run.
+None changes a result; each
 changes how the work maps onto the 148 SMs. This module times the candidates of each on
 the device for one frame size, by coordinate descent over the knobs with the
 library's own per-stage CUDA-event timing (b200enc_ctx_perf), keeps the
@@ -19,11 +21,15 @@ import os
 import time
 
 KEYS = {"deblock_rows": 0, "pchain_mbs_per_cta": 1, "rescore_ctas_per_sm": 2, "fallback_ctas_per_sm": 3,
-        "intra_ctas": 4, "me_stage": 5}
+        "intra_ctas": 4, "me_stage": 5, "deblock_tile_w": 6, "deblock_tile_h": 7}
+# the knobs an encoding context (and a batch) reads; deblock_rows shapes only
+# the stage-level wavefront deblocking (b200enc_deblock)
+TUNED = [n for n in KEYS if n != "deblock_rows"]
 # the stage whose time each knob changes (b200enc_ctx_perf_read keys), and on which frames
 STAGE = {"deblock_rows": ("deblock", False), "pchain_mbs_per_cta": ("chain", False),
          "rescore_ctas_per_sm": ("me", False), "fallback_ctas_per_sm": ("me", False),
-         "intra_ctas": ("chain", True), "me_stage": ("me", False)}
+         "intra_ctas": ("chain", True), "me_stage": ("me", False),
+         "deblock_tile_w": ("deblock", False), "deblock_tile_h": ("deblock", False)}
 
 
 def candidates(name, mbh):
@@ -37,6 +43,10 @@ def candidates(name, mbh):
         return sorted({max(1, mbh // 2), mbh})
     if name == "me_stage":
         return [2, 1]
+    if name == "deblock_tile_w":
+        return [4, 6, 8]
+    if name == "deblock_tile_h":
+        return [2, 4, 6, 8]
     raise KeyError(name)
 
 
@@ -60,7 +70,7 @@ def tune_throughput(run, mbh, names=None, reps=3, log=None):
     ms}}) and leaves the table set to the choice. The number of run() calls
     depends only on the candidate lists, so ranks of a multi-GPU job that
     tune side by side make the same calls (run() may hold a barrier)."""
-    names = list(names or KEYS)
+    names = list(names or TUNED)
     best = {name: 0 for name in KEYS}
     apply(best)
     scores_all = {}
@@ -140,7 +150,7 @@ def tune(frames, W, H, qp=27, search_range=32, lam=5, learned_mode=3, conf=0.9, 
     best = {name: 0 for name in KEYS}
     apply(best)
     try:
-        for name in KEYS:
+        for name in TUNED:
             stage, intra = STAGE[name]
             mode = learned_mode if name in ("rescore_ctas_per_sm", "fallback_ctas_per_sm") else 0
             ctx.set_me(mode, conf=conf)

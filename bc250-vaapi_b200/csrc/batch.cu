@@ -12,7 +12,8 @@
 //   learned form: preparation, network, fallback search, re-scoring),
 //   the P chain over the same macroblocks,
 //   the intra wavefront over every I stream's macroblock rows,
-//   the deblocking wavefront over every stream's row groups,
+//   the tile deblocking over every stream's tiles (out of place, into the
+//   buffer of the previous reconstruction),
 //   status words D2H.
 // Every stage kernel is the single-frame kernel's body behind a stream
 // lookup (binary search of the item in the set's prefix sums), so each
@@ -77,7 +78,8 @@ struct Batch {
   size_t scratch_words = 0;
   uint32_t* status_host = nullptr;
   MV* mvc = nullptr;
-  int total_mbs = 0, max_mbw = 0, max_mbh = 0, db_rows = 4;
+  int total_mbs = 0, max_mbw = 0, max_mbh = 0;
+  int db_tw = 8, db_th = 8;  // tile deblocking's tile shape, read from the tune table at each step
   TableLayout lay{1};
   uint8_t* dtab = nullptr;
   uint8_t* htab[2] = {nullptr, nullptr};
@@ -138,7 +140,8 @@ int enqueue_step(Batch* b, const uint8_t* htab, int np, int ni, int ng, int n_p,
   bt.groups = set(b->lay.idx_g, b->lay.pre_g, kg);
   bt.mvc = b->mvc;
   bt.ticket = b->scratch + (b->scratch_words - 2);
-  bt.db_rows = b->db_rows;
+  bt.db_rows = b->db_th;
+  bt.db_cols = b->db_tw;
   if (n_p > 0) {
     if (b->me_mode == 0)
       rc |= b200enc_me_batch_launch(bt, b->range, nullptr, nullptr, n_p, st) != 0;
@@ -148,7 +151,7 @@ int enqueue_step(Batch* b, const uint8_t* htab, int np, int ni, int ng, int n_p,
   }
   if (n_irows > 0) rc |= b200enc_i_frame_batch_launch(bt, n_irows, kBatchMaxWaitUs, st) != 0;
   if (b->deblock && n_groups > 0)
-    rc |= b200enc_deblock_batch_launch(bt, b->max_mbw, n_groups, kBatchMaxWaitUs, st) != 0;
+    rc |= b200enc_deblock_tiles_batch_launch(bt, n_groups, kBatchMaxWaitUs, st) != 0;
   // status: error words of every stream's two scratch regions
   rc |= cudaMemcpyAsync(b->status_host, b->scratch, b->scratch_words * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess;
   return rc ? -1 : 0;
@@ -199,9 +202,8 @@ void* b200enc_batch_create(int n_streams, const int* widths, const int* heights,
   }
   b->scratch_words = scr_words + 2;  // + the two tickets
   bytes += up(b->scratch_words * 4, 256) + up((size_t)b->total_mbs * 16, 256);
-  b->db_rows = b200enc_deblock_batch_rows(b->max_mbw, b->max_mbh);
   b->lay = TableLayout(n_streams);
-  if (b->db_rows <= 0 || cudaMalloc(&b->arena, bytes) != cudaSuccess ||
+  if (cudaMalloc(&b->arena, bytes) != cudaSuccess ||
       cudaMalloc(&b->dtab, b->lay.bytes) != cudaSuccess ||
       cudaMallocHost(&b->htab[0], b->lay.bytes) != cudaSuccess ||
       cudaMallocHost(&b->htab[1], b->lay.bytes) != cudaSuccess ||
@@ -290,6 +292,7 @@ int b200enc_batch_encode(void* h, const b200enc_batch_frame_t* frames) {
   int* pg = reinterpret_cast<int*>(ht + b->lay.pre_g);
   int np = 0, ni = 0, ng = 0, n_p = 0, n_irows = 0, n_groups = 0;
   pp[0] = pi[0] = pg[0] = 0;
+  b200enc_deblock_tile_count(1, 1, &b->db_tw, &b->db_th);
   for (int s = 0; s < b->n; ++s) {
     const b200enc_batch_frame_t& f = frames[s];
     StreamState& t = b->ss[s];
@@ -320,6 +323,10 @@ int b200enc_batch_encode(void* h, const b200enc_batch_frame_t* frames) {
     d.mv_prev = t.mv[t.mv_cur];
     d.scr_intra = t.scr_intra;
     d.scr_db = t.scr_db;
+    // deblocked out of place into the previous reconstruction, which the
+    // step's ME and P chain have read before the deblocking launch
+    d.db_y = t.rec[t.cur];
+    d.db_uv = t.rec[t.cur] + luma;
     const int mbs = t.mbw * t.mbh;
     if (f.is_intra) {
       ii[ni] = s;
@@ -335,7 +342,7 @@ int b200enc_batch_encode(void* h, const b200enc_batch_frame_t* frames) {
       ++np;
       n_p += pad16(mbs);
     }
-    const int groups = (t.mbh + b->db_rows - 1) / b->db_rows;
+    const int groups = b200enc_deblock_tile_count(t.mbw, t.mbh, nullptr, nullptr);
     ig[ng] = s;
     pg[ng + 1] = pg[ng] + groups;
     ++ng;
@@ -381,7 +388,7 @@ int b200enc_batch_encode(void* h, const b200enc_batch_frame_t* frames) {
   b->pending = true;
   for (int s = 0; s < b->n; ++s) {
     StreamState& t = b->ss[s];
-    t.cur ^= 1;
+    if (!b->deblock) t.cur ^= 1;  // deblocked: the reconstruction is back in rec[cur]
     t.mv_cur ^= 1;
     t.has_recon = true;
     t.has_hist = !frames[s].is_intra;

@@ -236,7 +236,7 @@ inline size_t scratch_words(int mbh) { return 4 + 2 * (size_t)mbh; }
 // Batched steps (batch.cu): one frame of each of many streams, of uneven
 // sizes, through one launch per stage. Each stage walks the items of one
 // set of streams laid end to end (the P streams' macroblocks, the I
-// streams' macroblock rows, every stream's deblocking row groups); an item
+// streams' macroblock rows, every stream's deblocking tiles); an item
 // finds its stream by binary search over the set's prefix sums.
 // ---------------------------------------------------------------------------
 struct BatchStream {
@@ -254,6 +254,7 @@ struct BatchStream {
   MV* mv;             // this frame's field
   const MV* mv_prev;  // the previous P frame's field (the learned form's history)
   uint32_t *scr_intra, *scr_db;  // wavefront scratch (scratch_words(mbh) words each)
+  uint8_t *db_y, *db_uv;          // the deblocked reconstruction (tile deblocking; not rec_y/rec_uv)
 };
 
 struct BatchSet {
@@ -280,10 +281,11 @@ struct BatchTab {
                     // stream's range is padded to a multiple of 16 items, the padding items
                     // (local index >= the stream's macroblock count) do no work
   BatchSet i_rows;  // macroblock rows of the streams coding an I frame
-  BatchSet groups;  // deblocking row groups of every stream
+  BatchSet groups;  // deblocking tiles of every stream
   MV* mvc;          // motion vectors by compact P index
   uint32_t* ticket; // [0] intra rows, [1] deblocking groups
-  int db_rows;      // macroblock rows per deblocking group
+  int db_rows;      // macroblock rows per deblocking group (tile deblocking: tile height)
+  int db_cols;      // tile deblocking: tile width in macroblocks
 };
 
 }  // namespace b200enc

@@ -36,6 +36,8 @@
 //   * boundary strengths of the whole group are computed up front.
 // Waits are bounded; on timeout a CTA records the error and leaves, and
 // every waiter gives up as soon as it sees a recorded error.
+#include <algorithm>
+
 #include "b200enc_internal.h"
 #include "common.cuh"
 
@@ -125,6 +127,156 @@ __device__ __forceinline__ void chroma_strong(int p1, int& p0, int& q0, int q1, 
 }
 
 __device__ __forceinline__ int tc0_for(int bs, int t1, int t2, int t3) { return bs == 1 ? t1 : (bs == 2 ? t2 : t3); }
+
+// Filter thresholds of one picture (uniform QP): luma and chroma alpha/beta
+// and tC0 for bS 1..3.
+struct DbQ {
+  int al, be, alc, bec, tcl1, tcl2, tcl3, tcc1, tcc2, tcc3, is_intra;
+};
+
+__device__ __forceinline__ DbQ db_q(int qp, int is_intra) {
+  const int qpc = chroma_qp(qp);
+  return DbQ{kAlpha[qp], kBeta[qp], kAlpha[qpc], kBeta[qpc], kTc0[qp][0], kTc0[qp][1], kTc0[qp][2],
+             kTc0[qpc][0], kTc0[qpc][1], kTc0[qpc][2], is_intra};
+}
+
+// One macroblock's filtering steps on samples in shared memory, one warp per
+// step, lanes 0..15 (the callers skip them when alpha or beta is 0). `bs` is
+// the macroblock's 32 boundary strengths ([dir][edge][segment]).
+//
+// Vertical edges of a luma macroblock: lane = sample row. `row` is the
+// macroblock row's first sample row, `xo` the macroblock's byte offset in it,
+// `xl` the left macroblock's (used iff has_left); 20 samples from p3 of the
+// left edge to q3 of the last internal edge, in registers.
+__device__ __forceinline__ void luma_v_step(uint8_t* row, int sp, int xo, int xl, bool has_left, const uint8_t* bs,
+                                            int lane, const DbQ& q) {
+  uint8_t* rowb = row + (size_t)lane * sp;
+  uint32_t* rw = reinterpret_cast<uint32_t*>(rowb + xo);
+  uint32_t* lw = reinterpret_cast<uint32_t*>(rowb + xl + 12);
+  int v[20];
+  const uint32_t w0 = has_left ? *lw : 0u;
+  const uint32_t w1 = rw[0], w2 = rw[1], w3 = rw[2], w4 = rw[3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = (w0 >> (8 * k)) & 255;
+    v[4 + k] = (w1 >> (8 * k)) & 255;
+    v[8 + k] = (w2 >> (8 * k)) & 255;
+    v[12 + k] = (w3 >> (8 * k)) & 255;
+    v[16 + k] = (w4 >> (8 * k)) & 255;
+  }
+  const int seg = lane >> 2;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int b = bs[e * 4 + seg];
+    const int i = 4 + 4 * e;
+    if (q.is_intra && e == 0)
+      luma_strong(v[i - 4], v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], v[i + 3], b, q.al, q.be);
+    else
+      luma_normal(v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], b, q.al, q.be,
+                  tc0_for(b, q.tcl1, q.tcl2, q.tcl3));
+  }
+  uint32_t o[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k)
+    o[k] = (uint32_t)v[4 * k] | ((uint32_t)v[4 * k + 1] << 8) | ((uint32_t)v[4 * k + 2] << 16) |
+           ((uint32_t)v[4 * k + 3] << 24);
+  if (has_left) *lw = o[0];
+  rw[0] = o[1];
+  rw[1] = o[2];
+  rw[2] = o[3];
+  rw[3] = o[4];
+}
+
+// Vertical edges of one chroma plane's sample row (lane = plane * 8 + row):
+// chroma samples 8mx-2 .. 8mx+7 (every other byte of the NV12 row).
+__device__ __forceinline__ void chroma_v_step(uint8_t* row, int sp, int xo, int xl, bool has_left, const uint8_t* bs,
+                                              int lane, const DbQ& q) {
+  const int pl = lane >> 3, i = lane & 7;
+  uint8_t* rowb = row + (size_t)i * sp;
+  uint8_t* cur = rowb + xo + pl;
+  uint8_t* left = rowb + xl + pl;
+  int v[10];
+  v[0] = has_left ? left[12] : 0;
+  v[1] = has_left ? left[14] : 0;
+#pragma unroll
+  for (int k = 2; k < 10; ++k) v[k] = cur[2 * (k - 2)];
+  const int seg = i >> 1;
+#pragma unroll
+  for (int e = 0; e < 4; e += 2) {
+    const int b = bs[e * 4 + seg];
+    const int j = 2 + 2 * e;
+    if (q.is_intra && e == 0)
+      chroma_strong(v[j - 2], v[j - 1], v[j], v[j + 1], b, q.alc, q.bec);
+    else
+      chroma_normal(v[j - 2], v[j - 1], v[j], v[j + 1], b, q.alc, q.bec, tc0_for(b, q.tcc1, q.tcc2, q.tcc3));
+  }
+  if (has_left) left[14] = (uint8_t)v[1];
+#pragma unroll
+  for (int k = 2; k < 10; ++k) cur[2 * (k - 2)] = (uint8_t)v[k];
+}
+
+// Horizontal edges of a luma macroblock: lane = sample column, rows -4..15;
+// `top` is the sample row four rows above the macroblock.
+__device__ __forceinline__ void luma_h_step(uint8_t* top, int sp, int xo, const uint8_t* bs, int lane, const DbQ& q) {
+  uint8_t* col = top + xo + lane;
+  int v[20];
+#pragma unroll
+  for (int r = 0; r < 20; ++r) v[r] = col[(size_t)r * sp];
+  const int seg = lane >> 2;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int b = bs[16 + e * 4 + seg];
+    const int i = 4 + 4 * e;
+    if (q.is_intra && e == 0)
+      luma_strong(v[i - 4], v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], v[i + 3], b, q.al, q.be);
+    else
+      luma_normal(v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], b, q.al, q.be,
+                  tc0_for(b, q.tcl1, q.tcl2, q.tcl3));
+  }
+#pragma unroll
+  for (int r = 1; r < 19; ++r) col[(size_t)r * sp] = (uint8_t)v[r];
+}
+
+// Horizontal edges of a chroma macroblock: lane = plane + 2 * column, rows
+// -2..7; `top` is the chroma sample row two rows above the macroblock.
+__device__ __forceinline__ void chroma_h_step(uint8_t* top, int sp, int xo, const uint8_t* bs, int lane,
+                                              const DbQ& q) {
+  const int pl = lane >> 3, i = lane & 7;
+  uint8_t* col = top + xo + 2 * i + pl;
+  int v[10];
+#pragma unroll
+  for (int r = 0; r < 10; ++r) v[r] = col[(size_t)r * sp];
+  const int seg = i >> 1;
+#pragma unroll
+  for (int e = 0; e < 4; e += 2) {
+    const int b = bs[16 + e * 4 + seg];
+    const int j = 2 + 2 * e;
+    if (q.is_intra && e == 0)
+      chroma_strong(v[j - 2], v[j - 1], v[j], v[j + 1], b, q.alc, q.bec);
+    else
+      chroma_normal(v[j - 2], v[j - 1], v[j], v[j + 1], b, q.alc, q.bec, tc0_for(b, q.tcc1, q.tcc2, q.tcc3));
+  }
+#pragma unroll
+  for (int r = 1; r < 9; ++r) col[(size_t)r * sp] = (uint8_t)v[r];
+}
+
+// Boundary strength (clause 8.7.2.1 for this encoder's macroblock kinds) of
+// segment k of edge e in direction dir of macroblock mb; has_edge0 = the
+// macroblock edge is filtered (a left / upper neighbour inside the picture
+// being deblocked).
+__device__ __forceinline__ int db_bs(int k, int e, int dir, int mb, int mbw, bool has_edge0, int is_intra,
+                                     const uint32_t* __restrict__ nzm, const MV* __restrict__ mvs) {
+  if (e == 0 && !has_edge0) return 0;
+  if (is_intra) return e == 0 ? 4 : 3;
+  const int mbp = e ? mb : (dir == 0 ? mb - 1 : mb - mbw);
+  const int bq = dir == 0 ? k * 4 + e : e * 4 + k;
+  const int bp = e ? (dir == 0 ? bq - 1 : bq - 4) : (dir == 0 ? k * 4 + 3 : 12 + k);
+  if ((__ldg(nzm + (size_t)mbp * 24 + bp) | __ldg(nzm + (size_t)mb * 24 + bq)) & 0xffffu) return 2;
+  if (e != 0) return 0;
+  const int2 a = __ldg(reinterpret_cast<const int2*>(mvs + mbp));
+  const int2 c = __ldg(reinterpret_cast<const int2*>(mvs + mb));
+  return (abs(a.x - c.x) >= 4 || abs(a.y - c.y) >= 4) ? 1 : 0;
+}
 
 // Shared-memory plan of one CTA (dynamic shared memory). The group's rows
 // are held as a ring of kDbRing macroblock columns (column mx in slot
@@ -230,37 +382,16 @@ __global__ void deblock_kernel(int mbw_, int mbh_, int R, int qp_, int is_intra_
     const Scratch sc{scratch};
     uint32_t* gprog_luma = scratch + 4;
     uint32_t* gprog_chroma = scratch + 4 + mbh;
-    const int qpc = chroma_qp(qp);
-    const int al = kAlpha[qp], be = kBeta[qp], alc = kAlpha[qpc], bec = kBeta[qpc];
-    const int tcl1 = kTc0[qp][0], tcl2 = kTc0[qp][1], tcl3 = kTc0[qp][2];
-    const int tcc1 = kTc0[qpc][0], tcc2 = kTc0[qpc][1], tcc3 = kTc0[qpc][2];
+    const DbQ q = db_q(qp, is_intra);
     const int rows = min(R, mbh - y0);
     const bool has_next = y0 + rows < mbh;
 
     // ---- prologue: progress words and the group's boundary strengths -----
     for (int i = tid; i < 2 * R + 4; i += nthr) prog[i] = 0u;
     for (int i = tid; i < rows * mbw * 32; i += nthr) {
-      // clause 8.7.2.1 for this encoder's macroblock kinds
       const int k = i & 3, e = (i >> 2) & 3, dir = (i >> 4) & 1, m = i >> 5;
-      const int my = y0 + m / mbw, mx = m % mbw, mb = my * mbw + mx;
-      int bs = 0;
-      if (e > 0 || (dir == 0 ? mx > 0 : my > 0)) {
-        if (is_intra) {
-          bs = e == 0 ? 4 : 3;
-        } else {
-          const int mbp = e ? mb : (dir == 0 ? mb - 1 : mb - mbw);
-          const int bq = dir == 0 ? k * 4 + e : e * 4 + k;
-          const int bp = e ? (dir == 0 ? bq - 1 : bq - 4) : (dir == 0 ? k * 4 + 3 : 12 + k);
-          if ((__ldg(nzm + (size_t)mbp * 24 + bp) | __ldg(nzm + (size_t)mb * 24 + bq)) & 0xffffu) {
-            bs = 2;
-          } else if (e == 0) {
-            const int2 a = __ldg(reinterpret_cast<const int2*>(mvs + mbp));
-            const int2 c = __ldg(reinterpret_cast<const int2*>(mvs + mb));
-            bs = (abs(a.x - c.x) >= 4 || abs(a.y - c.y) >= 4) ? 1 : 0;
-          }
-        }
-      }
-      bsm[i] = (uint8_t)bs;
+      const int my = y0 + m / mbw, mx = m % mbw;
+      bsm[i] = (uint8_t)db_bs(k, e, dir, my * mbw + mx, mbw, dir == 0 ? mx > 0 : my > 0, is_intra, nzm, mvs);
     }
     __syncthreads();
 
@@ -455,71 +586,11 @@ __global__ void deblock_kernel(int mbw_, int mbh_, int R, int qp_, int is_intra_
         __syncwarp();
         const uint8_t* bs = bsrow + mx * 32;
         if (is_luma) {
-          if (al && be && lane < 16) {
-            // vertical edges: this lane's sample row, 20 samples from p3 of
-            // the left edge to q3 of the last internal edge, in registers
-            uint8_t* rowb = ly + (size_t)(4 + 16 * wr + lane) * P.sp;
-            uint32_t* rw = reinterpret_cast<uint32_t*>(rowb + scol(mx));
-            uint32_t* lw = reinterpret_cast<uint32_t*>(rowb + scol(mx - 1) + 12);
-            int v[20];
-            const uint32_t w0 = mx > 0 ? *lw : 0u;
-            const uint32_t w1 = rw[0], w2 = rw[1], w3 = rw[2], w4 = rw[3];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-              v[k] = (w0 >> (8 * k)) & 255;
-              v[4 + k] = (w1 >> (8 * k)) & 255;
-              v[8 + k] = (w2 >> (8 * k)) & 255;
-              v[12 + k] = (w3 >> (8 * k)) & 255;
-              v[16 + k] = (w4 >> (8 * k)) & 255;
-            }
-            const int seg = lane >> 2;
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const int b = bs[e * 4 + seg];
-              const int i = 4 + 4 * e;
-              if (is_intra && e == 0)
-                luma_strong(v[i - 4], v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], v[i + 3], b, al, be);
-              else
-                luma_normal(v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], b, al, be, tc0_for(b, tcl1, tcl2, tcl3));
-            }
-            uint32_t o[5];
-#pragma unroll
-            for (int k = 0; k < 5; ++k)
-              o[k] = (uint32_t)v[4 * k] | ((uint32_t)v[4 * k + 1] << 8) | ((uint32_t)v[4 * k + 2] << 16) |
-                     ((uint32_t)v[4 * k + 3] << 24);
-            if (mx > 0) *lw = o[0];
-            rw[0] = o[1];
-            rw[1] = o[2];
-            rw[2] = o[3];
-            rw[3] = o[4];
-          }
+          if (q.al && q.be && lane < 16)
+            luma_v_step(ly + (size_t)(4 + 16 * wr) * P.sp, P.sp, scol(mx), scol(mx - 1), mx > 0, bs, lane, q);
         } else {
-          if (alc && bec && lane < 16) {
-            // vertical edges of one chroma plane's sample row: chroma
-            // samples 8mx-2 .. 8mx+7 (every other byte of the NV12 row)
-            const int pl = lane >> 3, i = lane & 7;
-            uint8_t* rowb = cy + (size_t)(2 + 8 * wr + i) * P.sp;
-            uint8_t* row = rowb + scol(mx) + pl;
-            uint8_t* left = rowb + scol(mx - 1) + pl;
-            int v[10];
-            v[0] = mx > 0 ? left[12] : 0;
-            v[1] = mx > 0 ? left[14] : 0;
-#pragma unroll
-            for (int k = 2; k < 10; ++k) v[k] = row[2 * (k - 2)];
-            const int seg = i >> 1;
-#pragma unroll
-            for (int e = 0; e < 4; e += 2) {
-              const int b = bs[e * 4 + seg];
-              const int j = 2 + 2 * e;
-              if (is_intra && e == 0)
-                chroma_strong(v[j - 2], v[j - 1], v[j], v[j + 1], b, alc, bec);
-              else
-                chroma_normal(v[j - 2], v[j - 1], v[j], v[j + 1], b, alc, bec, tc0_for(b, tcc1, tcc2, tcc3));
-            }
-            if (mx > 0) left[14] = (uint8_t)v[1];
-#pragma unroll
-            for (int k = 2; k < 10; ++k) row[2 * (k - 2)] = (uint8_t)v[k];
-          }
+          if (q.alc && q.bec && lane < 16)
+            chroma_v_step(cy + (size_t)(2 + 8 * wr) * P.sp, P.sp, scol(mx), scol(mx - 1), mx > 0, bs, lane, q);
         }
         __syncwarp();
         // Macroblock mx-1's samples are final for this row now (the left
@@ -546,45 +617,9 @@ __global__ void deblock_kernel(int mbw_, int mbh_, int R, int qp_, int is_intra_
         }
         __syncwarp();
         if (is_luma) {
-          if (al && be && lane < 16) {
-            // horizontal edges: this lane's sample column, rows -4..15
-            uint8_t* col = ly + (size_t)(16 * wr) * P.sp + scol(mx) + lane;
-            int v[20];
-#pragma unroll
-            for (int r = 0; r < 20; ++r) v[r] = col[(size_t)r * P.sp];
-            const int seg = lane >> 2;
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const int b = bs[16 + e * 4 + seg];
-              const int i = 4 + 4 * e;
-              if (is_intra && e == 0)
-                luma_strong(v[i - 4], v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], v[i + 3], b, al, be);
-              else
-                luma_normal(v[i - 3], v[i - 2], v[i - 1], v[i], v[i + 1], v[i + 2], b, al, be, tc0_for(b, tcl1, tcl2, tcl3));
-            }
-#pragma unroll
-            for (int r = 1; r < 19; ++r) col[(size_t)r * P.sp] = (uint8_t)v[r];
-          }
+          if (q.al && q.be && lane < 16) luma_h_step(ly + (size_t)(16 * wr) * P.sp, P.sp, scol(mx), bs, lane, q);
         } else {
-          if (alc && bec && lane < 16) {
-            const int pl = lane >> 3, i = lane & 7;
-            uint8_t* col = cy + (size_t)(8 * wr) * P.sp + scol(mx) + 2 * i + pl;
-            int v[10];
-#pragma unroll
-            for (int r = 0; r < 10; ++r) v[r] = col[(size_t)r * P.sp];
-            const int seg = i >> 1;
-#pragma unroll
-            for (int e = 0; e < 4; e += 2) {
-              const int b = bs[16 + e * 4 + seg];
-              const int j = 2 + 2 * e;
-              if (is_intra && e == 0)
-                chroma_strong(v[j - 2], v[j - 1], v[j], v[j + 1], b, alc, bec);
-              else
-                chroma_normal(v[j - 2], v[j - 1], v[j], v[j + 1], b, alc, bec, tc0_for(b, tcc1, tcc2, tcc3));
-            }
-#pragma unroll
-            for (int r = 1; r < 9; ++r) col[(size_t)r * P.sp] = (uint8_t)v[r];
-          }
+          if (q.alc && q.bec && lane < 16) chroma_h_step(cy + (size_t)(8 * wr) * P.sp, P.sp, scol(mx), bs, lane, q);
         }
         if (mx == mbw - 1) {  // all of the row's macroblocks are final
           __syncwarp();
@@ -596,6 +631,204 @@ __global__ void deblock_kernel(int mbw_, int mbh_, int R, int qp_, int is_intra_
     }
     __syncthreads();
     if (s_abort) return;
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Tile deblocking. Raster-order deblocking reaches only a short distance: a
+// filter changes at most three samples either side of an edge and reads at
+// most four, edges are four samples apart, and the value one edge hands to
+// the next (its q1, read back as the next edge's p2) depends on that edge's
+// own inputs only, so a change does not travel along a row or a column. As a
+// result the deblocked samples of a tile of macroblocks are those of the
+// raster-order deblocking of the tile with one macroblock of margin on every
+// side (clipped at the picture), treated as a picture of its own (no
+// filtering on the margin's outer edges). The oracle checks this against
+// whole-picture deblocking on random and adversarial content, intra and
+// inter, for several tile shapes (tests/test_deblock_tiles.py).
+//
+// So each CTA takes one tile: it loads the tile and its margin from the
+// unfiltered reconstruction (`src`) into shared memory, deblocks it there in
+// raster order (the row wavefront of the kernel above, one luma and one
+// chroma warp per macroblock row, rows a macroblock step apart), and stores
+// the tile alone to `dst`. CTAs never wait on one another; a picture is
+// mbw/TW x mbh/TH independent tiles of (TW + TH + 3) dependent steps each,
+// instead of one wavefront of mbw + mbh - 1 steps. `dst` must not overlap
+// `src` (neighbouring tiles read each other's samples as their margin).
+// ---------------------------------------------------------------------------
+constexpr int kDbTileMax = 8;  // TW, TH <= 8
+
+struct DbTilePlan {
+  int sp;  // shared-memory row stride: 16 * (TW + 2) + 4 bytes, an odd word count
+  size_t luma_off, chroma_off, bs_off, prog_off, bytes;
+};
+
+__host__ __device__ inline DbTilePlan db_tile_plan(int TW, int TH) {
+  DbTilePlan p;
+  p.sp = 16 * (TW + 2) + 4;
+  p.luma_off = 0;                                                    // 4 margin rows + 16 (TH + 2) rows
+  p.chroma_off = (size_t)(16 * (TH + 2) + 4) * p.sp;                 // 2 margin rows + 8 (TH + 2) rows
+  p.bs_off = p.chroma_off + (size_t)(8 * (TH + 2) + 2) * p.sp;       // [MB][dir][edge][segment]
+  p.prog_off = (p.bs_off + (size_t)(TH + 2) * (TW + 2) * 32 + 15) & ~(size_t)15;
+  p.bytes = p.prog_off + 2 * (TH + 2) * sizeof(uint32_t);            // progress: luma rows, chroma rows
+  return p;
+}
+
+// BATCH: one CTA per tile of every stream of a batch (bt.groups counts each
+// stream's tiles; bt.db_rows = TH, bt.db_cols = TW); the stream's unfiltered
+// reconstruction is rec_y/rec_uv, the deblocked one goes to db_y/db_uv.
+template <bool BATCH>
+__global__ void __launch_bounds__(64 * (kDbTileMax + 2)) deblock_tile_kernel(
+    int mbw_, int mbh_, int TW, int TH, int qp_, int is_intra_, const uint32_t* __restrict__ nzm_,
+    const MV* __restrict__ mvs_, const uint8_t* __restrict__ src_y_, const uint8_t* __restrict__ src_uv_,
+    uint8_t* __restrict__ dst_y_, uint8_t* __restrict__ dst_uv_, int pitch_, uint32_t* status_, uint32_t max_wait,
+    BatchTab bt) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nthr = blockDim.x;
+  int mbw = mbw_, mbh = mbh_, qp = qp_, is_intra = is_intra_, pitch = pitch_;
+  const uint32_t* nzm = nzm_;
+  const MV* mvs = mvs_;
+  const uint8_t *src_y = src_y_, *src_uv = src_uv_;
+  uint8_t *dst_y = dst_y_, *dst_uv = dst_uv_;
+  uint32_t* status = status_;
+  int tile = blockIdx.x;
+  if (BATCH) {
+    if (tile >= bt.groups.total()) return;
+    TW = bt.db_cols;
+    TH = bt.db_rows;
+    const int k = bt.groups.find(tile);
+    const BatchStream& st = bt.groups.stream(k);
+    tile -= bt.groups.prefix[k];
+    mbw = st.g.mbw;
+    mbh = st.g.mbh;
+    qp = st.qp;
+    is_intra = st.is_intra;
+    nzm = st.nz;
+    mvs = st.mv;
+    src_y = st.rec_y;
+    src_uv = st.rec_uv;
+    dst_y = st.db_y;
+    dst_uv = st.db_uv;
+    pitch = st.rec_pitch;
+    status = st.scr_db;
+  }
+  const int ntx = (mbw + TW - 1) / TW;
+  const int tx = tile % ntx, ty = tile / ntx;
+  const int x0 = tx * TW, y0 = ty * TH;
+  if (y0 >= mbh) return;
+  const int x1 = min(mbw, x0 + TW), y1 = min(mbh, y0 + TH);
+  // the deblocked region: the tile and its margin, clipped at the picture
+  const int rx0 = max(0, x0 - 1), ry0 = max(0, y0 - 1), rx1 = min(mbw, x1 + 1), ry1 = min(mbh, y1 + 1);
+  const int RWr = rx1 - rx0, RHr = ry1 - ry0;
+  const DbTilePlan P = db_tile_plan(TW, TH);
+  uint8_t* ly = smem + P.luma_off;    // row 4 = picture row 16 * ry0, byte 0 = column 16 * rx0
+  uint8_t* cy = smem + P.chroma_off;  // row 2 = picture row 8 * ry0
+  uint8_t* bsm = smem + P.bs_off;
+  volatile uint32_t* prog = reinterpret_cast<volatile uint32_t*>(smem + P.prog_off);
+  const Scratch sc{status};
+  const DbQ q = db_q(qp, is_intra);
+
+  // ---- load the region, boundary strengths, progress words -----------------
+  {
+    const int lrows = 16 * RHr, crows = 8 * RHr, n = (lrows + crows) * RWr;
+    for (int i = tid; i < n; i += nthr) {
+      const int r = i / RWr, c = i - r * RWr;
+      const bool lu = r < lrows;
+      const int rr = lu ? r : r - lrows;
+      const uint8_t* g = lu ? src_y + (size_t)(16 * ry0 + rr) * pitch + 16 * (rx0 + c)
+                            : src_uv + (size_t)(8 * ry0 + rr) * pitch + 16 * (rx0 + c);
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(g));
+      uint32_t* d = reinterpret_cast<uint32_t*>((lu ? ly + (size_t)(4 + rr) * P.sp : cy + (size_t)(2 + rr) * P.sp) +
+                                                16 * c);
+      d[0] = v.x;
+      d[1] = v.y;
+      d[2] = v.z;
+      d[3] = v.w;
+    }
+    // the margin rows above the region are read (never changed: the top
+    // edges of the region's first row have bS 0) by its first row's
+    // horizontal steps; give them defined contents
+    for (int i = tid; i < 6 * (P.sp / 4); i += nthr) {
+      const int r = i / (P.sp / 4), w = i - r * (P.sp / 4);
+      reinterpret_cast<uint32_t*>(r < 4 ? ly + (size_t)r * P.sp : cy + (size_t)(r - 4) * P.sp)[w] = 0u;
+    }
+    for (int i = tid; i < RHr * RWr * 32; i += nthr) {
+      const int k = i & 3, e = (i >> 2) & 3, dir = (i >> 4) & 1, m = i >> 5;
+      const int lyr = m / RWr, lxr = m - lyr * RWr;
+      bsm[i] = (uint8_t)db_bs(k, e, dir, (ry0 + lyr) * mbw + rx0 + lxr, mbw, dir == 0 ? lxr > 0 : lyr > 0, is_intra,
+                              nzm, mvs);
+    }
+    for (int i = tid; i < 2 * (TH + 2); i += nthr) prog[i] = 0u;
+  }
+  __syncthreads();
+
+  // ---- the region's rows, one luma and one chroma warp each ----------------
+  {
+    const bool is_luma = warp < TH + 2;
+    const int wr = is_luma ? warp : warp - (TH + 2);
+    if (wr < RHr) {
+      const uint8_t* bsrow = bsm + (size_t)wr * RWr * 32;
+      volatile uint32_t* my_prog = prog + (is_luma ? 0 : TH + 2) + wr;
+      const volatile uint32_t* up_prog = my_prog - 1;
+      const bool on = is_luma ? (q.al && q.be) : (q.alc && q.bec);
+      uint8_t* vrow = is_luma ? ly + (size_t)(4 + 16 * wr) * P.sp : cy + (size_t)(2 + 8 * wr) * P.sp;
+      uint8_t* htop = is_luma ? ly + (size_t)(16 * wr) * P.sp : cy + (size_t)(8 * wr) * P.sp;
+      for (int mx = 0; mx < RWr; ++mx) {
+        const uint8_t* bs = bsrow + mx * 32;
+        // vertical edges: this row's own samples only
+        if (on && lane < 16) {
+          if (is_luma)
+            luma_v_step(vrow, P.sp, 16 * mx, 16 * (mx - 1), mx > 0, bs, lane, q);
+          else
+            chroma_v_step(vrow, P.sp, 16 * mx, 16 * (mx - 1), mx > 0, bs, lane, q);
+        }
+        __syncwarp();
+        if (mx > 0) {  // macroblock mx-1 of this row is final
+          __threadfence_block();
+          __syncwarp();
+          if (lane == 0) *my_prog = (uint32_t)mx;
+        }
+        // horizontal edges of mx: the row above has filtered the vertical
+        // edges of mx+1 (all of its row at the last macroblock)
+        if (wr > 0) {
+          if (!wait_shared(up_prog, sc, (uint32_t)(mx + 1), max_wait,
+                           (uint32_t)((ry0 + wr) * mbw + rx0 + mx)))
+            break;
+          __threadfence_block();
+        }
+        __syncwarp();
+        if (on && lane < 16) {
+          if (is_luma)
+            luma_h_step(htop, P.sp, 16 * mx, bs, lane, q);
+          else
+            chroma_h_step(htop, P.sp, 16 * mx, bs, lane, q);
+        }
+        if (mx == RWr - 1) {
+          __syncwarp();
+          __threadfence_block();
+          __syncwarp();
+          if (lane == 0) *my_prog = (uint32_t)RWr;
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- store the tile (whatever a failed wait left: the status says so) -----
+  {
+    const int tw = x1 - x0, lrows = 16 * (y1 - y0), crows = 8 * (y1 - y0), n = (lrows + crows) * tw;
+    const int ox = x0 - rx0, oy = y0 - ry0;  // the tile's macroblock offset in the region
+    for (int i = tid; i < n; i += nthr) {
+      const int r = i / tw, c = i - r * tw;
+      const bool lu = r < lrows;
+      const int rr = lu ? r : r - lrows;
+      const uint32_t* s4 = reinterpret_cast<const uint32_t*>(
+          (lu ? ly + (size_t)(4 + 16 * oy + rr) * P.sp : cy + (size_t)(2 + 8 * oy + rr) * P.sp) + 16 * (ox + c));
+      uint8_t* g = lu ? dst_y + (size_t)(16 * y0 + rr) * pitch + 16 * (x0 + c)
+                      : dst_uv + (size_t)(8 * y0 + rr) * pitch + 16 * (x0 + c);
+      *reinterpret_cast<uint4*>(g) = make_uint4(s4[0], s4[1], s4[2], s4[3]);
+    }
   }
 }
 
@@ -667,4 +900,74 @@ extern "C" int b200enc_deblock(int mbw, int mbh, int qp, int is_intra, const uin
   if (cudaMemsetAsync(scratch, 0, b200enc_wavefront_scratch_bytes(mbh), (cudaStream_t)stream) != cudaSuccess) return -1;
   return b200enc_deblock_launch(mbw, mbh, qp, is_intra, nz, mv, rec_y, rec_uv, rec_pitch, (uint32_t*)scratch, ctas,
                                 kMaxWaitUsDb, stream);
+}
+
+// Tile shape of the tile deblocking (TW x TH macroblocks): 8 x 8 unless the
+// autotuner chose otherwise.
+static void db_tile_shape(int* tw, int* th) {
+  const int w = b200enc_tuned(B200ENC_TUNE_DEBLOCK_TILE_W), h = b200enc_tuned(B200ENC_TUNE_DEBLOCK_TILE_H);
+  *tw = w > 0 ? std::min(w, kDbTileMax) : 8;
+  *th = h > 0 ? std::min(h, kDbTileMax) : 8;
+}
+
+int b200enc_deblock_tiles_launch(int mbw, int mbh, int qp, int is_intra, const uint32_t* nz, const void* mv,
+                                 const uint8_t* src_y, const uint8_t* src_uv, uint8_t* dst_y, uint8_t* dst_uv,
+                                 int pitch, uint32_t* status, uint32_t max_wait, cudaStream_t stream) {
+  int TW, TH;
+  db_tile_shape(&TW, &TH);
+  const DbTilePlan P = db_tile_plan(TW, TH);
+  if (cudaFuncSetAttribute(deblock_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.bytes) !=
+      cudaSuccess)
+    return -1;
+  const int tiles = ((mbw + TW - 1) / TW) * ((mbh + TH - 1) / TH);
+  deblock_tile_kernel<false><<<tiles, 64 * (TH + 2), P.bytes, stream>>>(
+      mbw, mbh, TW, TH, qp, is_intra, nz, (const MV*)mv, src_y, src_uv, dst_y, dst_uv, pitch, status, max_wait,
+      BatchTab{});
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// Tiles of a stream of mbw x mbh macroblocks under the current tile shape,
+// and the shape itself (for a batch's table).
+int b200enc_deblock_tile_count(int mbw, int mbh, int* tw, int* th) {
+  int TW, TH;
+  db_tile_shape(&TW, &TH);
+  if (tw) *tw = TW;
+  if (th) *th = TH;
+  return ((mbw + TW - 1) / TW) * ((mbh + TH - 1) / TH);
+}
+
+// The tile deblocking of every stream of a batch: one CTA per tile
+// (bt.groups over the streams' tiles, bt.db_cols x bt.db_rows each).
+int b200enc_deblock_tiles_batch_launch(const BatchTab& bt, int tiles, uint32_t max_wait, cudaStream_t st) {
+  if (tiles <= 0) return 0;
+  const int TW = bt.db_cols, TH = bt.db_rows;
+  if (TW < 1 || TH < 1 || TW > kDbTileMax || TH > kDbTileMax) return -1;
+  const DbTilePlan P = db_tile_plan(TW, TH);
+  if (cudaFuncSetAttribute(deblock_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.bytes) !=
+      cudaSuccess)
+    return -1;
+  deblock_tile_kernel<true><<<tiles, 64 * (TH + 2), P.bytes, st>>>(0, 0, 0, 0, 0, 0, nullptr, nullptr, nullptr,
+                                                                   nullptr, nullptr, nullptr, 0, nullptr, max_wait,
+                                                                   bt);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int b200enc_deblock_tiles(int mbw, int mbh, int qp, int is_intra, const uint32_t* nz, const void* mv,
+                                     const uint8_t* src_y, const uint8_t* src_uv, uint8_t* dst_y, uint8_t* dst_uv,
+                                     int pitch, uint32_t* status, void* stream) {
+  if (!nz || !mv || !src_y || !src_uv || !dst_y || !dst_uv || !status || mbw <= 0 || mbh <= 0 || qp < 0 || qp > 51)
+    return -1;
+  const uintptr_t a = (uintptr_t)src_y | (uintptr_t)src_uv | (uintptr_t)dst_y | (uintptr_t)dst_uv;
+  if ((pitch & 15) || (a & 15) || pitch < mbw * 16) return -1;
+  // the destination planes must not overlap the source planes
+  const uint8_t *s0 = src_y, *s1 = src_y + (size_t)pitch * mbh * 16, *c0 = src_uv, *c1 = src_uv + (size_t)pitch * mbh * 8;
+  const uint8_t *d0 = dst_y, *d1 = dst_y + (size_t)pitch * mbh * 16, *e0 = dst_uv, *e1 = dst_uv + (size_t)pitch * mbh * 8;
+  auto overlap = [](const uint8_t* a0, const uint8_t* a1, const uint8_t* b0, const uint8_t* b1) {
+    return a0 < b1 && b0 < a1;
+  };
+  if (overlap(d0, d1, s0, s1) || overlap(d0, d1, c0, c1) || overlap(e0, e1, s0, s1) || overlap(e0, e1, c0, c1))
+    return -1;
+  if (cudaMemsetAsync(status, 0, 16, (cudaStream_t)stream) != cudaSuccess) return -1;
+  return b200enc_deblock_tiles_launch(mbw, mbh, qp, is_intra, nz, mv, src_y, src_uv, dst_y, dst_uv, pitch, status,
+                                      kMaxWaitUsDb, (cudaStream_t)stream);
 }

@@ -322,9 +322,13 @@ int encode_frame(gpu_context_t* ctx, Impl* m, const uint8_t* y, const uint8_t* u
   perf_mark(m, 2);
   const bool db = m->deblock >= 0 ? m->deblock != 0 : !fast_mode();
   if (db) {
+    // Deblocked as independent tiles from the unfiltered reconstruction
+    // into the other buffer: the previous reconstruction, which nothing
+    // reads once the P chain (or the intra wavefront) has run.
     rc |= cudaMemsetAsync(scr1, 0, m->scratch_words * 4, m->stream) == cudaSuccess ? 0 : -1;
-    rc |= b200enc_deblock_launch(m->mbw, m->mbh, qp, is_intra, m->d_nz, m->d_mv, out_y, out_uv, m->pitch, scr1, 0,
-                                 kWavefrontMaxWaitUs, m->stream);
+    uint8_t* db_y = m->rec[m->cur];
+    rc |= b200enc_deblock_tiles_launch(m->mbw, m->mbh, qp, is_intra, m->d_nz, m->d_mv, out_y, out_uv, db_y,
+                                       db_y + luma, m->pitch, scr1, kWavefrontMaxWaitUs, m->stream);
   }
   perf_mark(m, 3);
   if (stage) {
@@ -343,7 +347,7 @@ int encode_frame(gpu_context_t* ctx, Impl* m, const uint8_t* y, const uint8_t* u
     m->ev_count++;
   }
   if (rc != 0) return -1;
-  m->cur ^= 1;
+  if (!db) m->cur ^= 1;  // deblocked: the latest reconstruction is back in rec[cur]
   ctx->has_recon_frame = true;
   publish_recon(ctx, m);
   return 0;

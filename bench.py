@@ -522,7 +522,7 @@ def run_gpu(args):
         if args.no_tune:
             autotune.apply({k2: 0 for k2 in autotune.KEYS})
             return {k2: 0 for k2 in autotune.KEYS}
-        names = [n for n in autotune.KEYS
+        names = [n for n in autotune.TUNED
                  if mode != 0 or n not in ("rescore_ctas_per_sm", "fallback_ctas_per_sm")]
         t0 = time.perf_counter()
         vals, scores = autotune.tune_throughput(lambda: arm(mode, S, 24, 3)[0], MBH, names, reps=3)
@@ -740,10 +740,11 @@ def run_multistream(args):
                 a1.record(st)
                 assert b.sync() == 0
                 return a0.elapsed_time(a1)
-            # the knobs a batch reads at every step (its deblocking rows are
-            # fixed when it is created, its P chain and full search have one
-            # shape): the learned form's persistent grids
-            names = ["rescore_ctas_per_sm", "fallback_ctas_per_sm"]
+            # the knobs a batch reads at every step (its P chain and full
+            # search have one shape): the deblocking tile and the learned
+            # form's persistent grids
+            names = ["deblock_tile_w", "deblock_tile_h"] + (
+                ["rescore_ctas_per_sm", "fallback_ctas_per_sm"] if me_mode else [])
             h0 = time.perf_counter()
             vals, _ = autotune.tune_throughput(run4, max(h for _, h in sizes) // 16, names, reps=3)
             tuned["learned" if me_mode else "plain"] = {"values": {n: vals[n] for n in names},

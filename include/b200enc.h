@@ -126,6 +126,22 @@ int b200enc_deblock(int mbw, int mbh, int qp, int is_intra,
                     uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch,
                     void *scratch, size_t scratch_bytes, int ctas, void *stream);
 
+/* The same deblocking (identical output), from an unfiltered reconstruction
+ * src_y/src_uv to a separate destination dst_y/dst_uv (same pitch; the
+ * destination planes must not overlap the source planes), as independent
+ * tiles: each tile of TW x TH macroblocks (8 x 8 unless tuned,
+ * B200ENC_TUNE_DEBLOCK_TILE_W/_H) is deblocked in raster order together with
+ * one macroblock of margin on every side and stored alone, which reproduces
+ * the whole picture's raster order on the tile. Replaces the same shader
+ * dispatch as b200enc_deblock (src/gpu_compute.c:3261-3290). `status` is 16
+ * bytes of device memory, zeroed here; word 1 is nonzero if a wait inside a
+ * tile gave up. Pitch and bases must be multiples of 16. */
+int b200enc_deblock_tiles(int mbw, int mbh, int qp, int is_intra,
+                          const uint32_t *nz, const void *mv,
+                          const uint8_t *src_y, const uint8_t *src_uv,
+                          uint8_t *dst_y, uint8_t *dst_uv, int pitch,
+                          uint32_t *status, void *stream);
+
 /* The two wavefront kernels with a caller-prepared scratch (NOT cleared
  * here) and an explicit time bound, in microseconds, on each progress wait.
  * For callers that manage the scratch themselves, and for tests of the
@@ -224,7 +240,9 @@ int b200enc_batch_graph_stats(void *b, long *instantiations, long *updates);
 #define B200ENC_TUNE_FALLBACK_CTAS_PER_SM 3 /* fallback full-search grid, CTAs per SM, 1..16 (default 8) */
 #define B200ENC_TUNE_INTRA_CTAS 4           /* intra wavefront CTAs (rows in flight), >= 1 (default: one per row) */
 #define B200ENC_TUNE_ME_STAGE 5             /* full-search window staging: 1 word loads, 2 TMA (default TMA) */
-#define B200ENC_TUNE_COUNT 6
+#define B200ENC_TUNE_DEBLOCK_TILE_W 6       /* tile deblocking: tile width in macroblocks, 1..8 (default 8) */
+#define B200ENC_TUNE_DEBLOCK_TILE_H 7       /* tile deblocking: tile height in macroblocks, 1..8 (default 8) */
+#define B200ENC_TUNE_COUNT 8
 /* Sets a knob (0 restores the default); -1 for an unknown key or a value
  * out of range. */
 int b200enc_tune_set(int key, int value);

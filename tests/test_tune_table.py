@@ -22,7 +22,7 @@ PRE = ("import sys; sys.path.insert(0, 'bc250-vaapi_b200'); import b200enc; from
 
 
 def test_names_match_the_python_keys():
-    out = _run(PRE + "print(','.join(L.b200enc_tune_name(k).decode() for k in range(6)), L.b200enc_tune_name(6))")
+    out = _run(PRE + "print(','.join(L.b200enc_tune_name(k).decode() for k in range(8)), L.b200enc_tune_name(8))")
     names, last = out.split()
     assert last == "None"
     sys.path.insert(0, os.path.join(ROOT, "bc250-vaapi_b200"))
