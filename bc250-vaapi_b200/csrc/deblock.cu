@@ -679,7 +679,7 @@ __host__ __device__ inline DbTilePlan db_tile_plan(int TW, int TH) {
 // stream's tiles; bt.db_rows = TH, bt.db_cols = TW); the stream's unfiltered
 // reconstruction is rec_y/rec_uv, the deblocked one goes to db_y/db_uv.
 template <bool BATCH>
-__global__ void __launch_bounds__(64 * (kDbTileMax + 2)) deblock_tile_kernel(
+__global__ void __launch_bounds__(64 * (kDbTileMax + 2), 2) deblock_tile_kernel(
     int mbw_, int mbh_, int TW, int TH, int qp_, int is_intra_, const uint32_t* __restrict__ nzm_,
     const MV* __restrict__ mvs_, const uint8_t* __restrict__ src_y_, const uint8_t* __restrict__ src_uv_,
     uint8_t* __restrict__ dst_y_, uint8_t* __restrict__ dst_uv_, int pitch_, uint32_t* status_, uint32_t max_wait,
