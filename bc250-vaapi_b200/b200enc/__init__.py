@@ -31,6 +31,7 @@ EXPORTS = [
     "b200enc_pin_host", "b200enc_unpin_host", "b200enc_deblock_noalloc_status",
     "b200enc_batch_create", "b200enc_batch_destroy", "b200enc_batch_stream", "b200enc_batch_set_graph",
     "b200enc_batch_encode", "b200enc_batch_sync", "b200enc_batch_outputs", "b200enc_batch_graph_stats",
+    "b200enc_cavlc_scratch_bytes", "b200enc_cavlc_slices",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
     "gpu_compute_create_image", "gpu_compute_destroy_image", "gpu_compute_get_nv12_layout",
@@ -83,6 +84,9 @@ def load_library(path=LIB_PATH):
     lib.b200enc_i_frame.argtypes = [_vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i,
                                     _vp, ctypes.c_size_t, _i, _i, _vp]
     lib.b200enc_deblock.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, ctypes.c_size_t, _i, _vp]
+    lib.b200enc_cavlc_scratch_bytes.argtypes = [_i, _i]
+    lib.b200enc_cavlc_scratch_bytes.restype = ctypes.c_size_t
+    lib.b200enc_cavlc_slices.argtypes = [_vp, _vp]
     lib.b200enc_deblock_tiles.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp]
     lib.b200enc_me_full_search.argtypes = [_vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp]
     lib.b200enc_me_full_search_ex.argtypes = [_vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _i, _i,
@@ -379,6 +383,54 @@ def hevc_choose_luma_mode(src, recon, width, height, jobs, modes, preds, stream=
 HEVC_MVF = _np.dtype([("mv", "<i2", (2, 2)), ("ref_poc", "<i4", (2,)), ("pred_flag", "u1"), ("pad", "u1", (3,))])
 HEVC_SLICE_FILTER = _np.dtype([("beta_offset", "<i2"), ("tc_offset", "<i2"), ("disabled", "u1"),
                                ("across_slices", "u1"), ("pad", "u1", (2,))])
+
+
+class CavlcParams(ctypes.Structure):
+    """b200enc_cavlc_t (include/b200enc.h)."""
+    _fields_ = [("mbw", _i), ("mbh", _i), ("qp", _i), ("is_intra", _i), ("num_slices", _i), ("quality_level", _i),
+                ("levels", _vp), ("dc", _vp), ("nz", _vp), ("pred_mode", _vp), ("mv", _vp),
+                ("header", _vp), ("header_bits", _vp), ("out", _vp), ("slice_cap", ctypes.c_size_t),
+                ("out_bytes", _vp), ("scratch", _vp), ("scratch_bytes", ctypes.c_size_t)]
+
+
+def cavlc_slices(mbw, mbh, qp, is_intra, num_slices, levels, dc, nz, pred_mode, mv, headers=None,
+                 quality_level=4, slice_cap=None, stream=None):
+    """CAVLC slice data of one picture on the GPU from device pointers (ints)
+    to its staged outputs; headers: None or a list of (bits, nbits) per
+    slice, bits an int holding nbits (<= 128) header bits. Returns a list of
+    each slice's RBSP bytes."""
+    import numpy as np
+    import torch
+    L = lib()
+    mbs = mbw * mbh
+    cap = slice_cap or ((mbs * 2560 // num_slices + 4096 + 3) // 4 * 4)
+    out = torch.zeros(num_slices * cap, dtype=torch.uint8, device="cuda")
+    nbytes = torch.zeros(num_slices, dtype=torch.int32, device="cuda")
+    sb = L.b200enc_cavlc_scratch_bytes(mbw, mbh)
+    scratch = torch.empty(sb + 256, dtype=torch.uint8, device="cuda")
+    sp = (scratch.data_ptr() + 255) // 256 * 256
+    hdr = hb = None
+    if headers is not None:
+        hdr = np.zeros((num_slices, 16), np.uint8)
+        hb = np.zeros(num_slices, np.int32)
+        for k, (bits, n) in enumerate(headers):
+            hb[k] = n
+            hdr[k] = np.frombuffer(((bits << (128 - n)) if n else 0).to_bytes(16, "big"), np.uint8)
+    prm = CavlcParams(mbw, mbh, qp, int(is_intra), num_slices, quality_level, _vp(levels), _vp(dc), _vp(nz),
+                      _vp(pred_mode) if pred_mode else None, _vp(mv),
+                      _vp(hdr.ctypes.data) if hdr is not None else None,
+                      _vp(hb.ctypes.data) if hb is not None else None, _vp(out.data_ptr()), cap,
+                      _vp(nbytes.data_ptr()), _vp(sp), sb)
+    _check(L.b200enc_cavlc_slices(ctypes.byref(prm), _stream(stream)), "b200enc_cavlc_slices")
+    torch.cuda.synchronize()
+    n = nbytes.cpu().numpy().view(np.uint32)
+    o = out.cpu().numpy()
+    res = []
+    for k in range(num_slices):
+        if n[k] == 0xffffffff:
+            raise RuntimeError(f"slice {k} outgrew its region")
+        res.append(o[k * cap:k * cap + int(n[k])].tobytes())
+    return res
 
 
 class HevcDeblockParams(ctypes.Structure):

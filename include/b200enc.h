@@ -492,6 +492,39 @@ int b200enc_hevc_deblock(const b200enc_hevc_deblock_t *p, void *stream);
  * incomplete and must not be used), -1 = the read failed. */
 int b200enc_wavefront_status(const void *scratch, void *stream);
 
+/* CAVLC slice data on the GPU: every slice of one picture coded exactly as
+ * the reference's host encoder codes it (its CAVLC macroblock loop,
+ * src/encoder_h264.c:3128-3290: I16x16 macroblocks in I slices, P_Skip runs
+ * and P_L0_16x16 macroblocks in P slices, residual blocks by src/cavlc.c),
+ * from the picture's staged outputs already in device memory (levels, DC,
+ * nz masks, prediction modes, vectors: the layouts of include/gpu_compute.h).
+ * Each slice's output is its RBSP: the caller's slice header bits (up to 128,
+ * MSB first, 16 bytes per slice in `header`; none when header_bits is NULL),
+ * the slice data, then rbsp_trailing_bits - ready for emulation prevention
+ * and a NAL header. quality_level is the host encoder's (its P_Skip rule
+ * changes at >= 5). out_bytes[s] is 0xffffffff when slice s outgrew
+ * slice_cap (or a macroblock outgrew 2560 bytes). Asynchronous on `stream`;
+ * returns -1 for bad arguments. No reference counterpart as a GPU routine:
+ * it takes the host's entropy loop (DEVLOG: 57 % of a 1440p frame) off the
+ * host. */
+typedef struct {
+    int mbw, mbh, qp, is_intra, num_slices, quality_level;
+    const int16_t *levels;       /* device [mbs][24][16] */
+    const int32_t *dc;           /* device [mbs][24] raw DC terms */
+    const uint32_t *nz;          /* device [mbs][24] */
+    const uint32_t *pred_mode;   /* device [mbs] (I slices) */
+    const void *mv;              /* device [mbs] gpu_mv_t */
+    const uint8_t *header;       /* host [num_slices][16] or NULL */
+    const int *header_bits;      /* host [num_slices] (0..128) or NULL */
+    uint8_t *out;                /* device: slice s at out + s * slice_cap */
+    size_t slice_cap;            /* bytes per slice, a multiple of 4 */
+    uint32_t *out_bytes;         /* device [num_slices] */
+    void *scratch;               /* device, 256-byte aligned */
+    size_t scratch_bytes;        /* >= b200enc_cavlc_scratch_bytes(mbw, mbh) */
+} b200enc_cavlc_t;
+size_t b200enc_cavlc_scratch_bytes(int mbw, int mbh);
+int b200enc_cavlc_slices(const b200enc_cavlc_t *p, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,34 @@ def ref_available():
     return os.path.exists(REF_SO)
 
 
+CAVLC_SO = os.path.join(HERE, "_ref", "libcavlcref.so")
+_cavlc = None
+
+
+def cavlc_ref_available():
+    return os.path.exists(CAVLC_SO)
+
+
+def ref_cavlc_slice_data(mbw, mbh, qp, is_idr, start_mb, end_mb, levels, dc, nz, pred_modes, mvs,
+                         quality_level=4, cap=None):
+    """The reference's CAVLC slice data (encoder_h264.c's macroblock loop and
+    encoders, cavlc.c) for macroblocks [start_mb, end_mb), from bit 0, with
+    rbsp_trailing_bits: bytes."""
+    global _cavlc
+    if _cavlc is None:
+        _cavlc = ctypes.CDLL(CAVLC_SO)
+    cap = cap or (end_mb - start_mb) * 2560 + 4096
+    out = np.zeros(cap, np.uint8)
+    a = [np.ascontiguousarray(levels, np.int16), np.ascontiguousarray(dc, np.int32),
+         np.ascontiguousarray(nz, np.uint32), np.ascontiguousarray(pred_modes, np.uint32),
+         np.ascontiguousarray(mvs, np.int32)]
+    n = _cavlc.refshim_cavlc_slice_data(mbw, mbh, qp, int(is_idr), quality_level, start_mb, end_mb,
+                                        *[_p(x) for x in a], _p(out), cap)
+    if n < 0:
+        raise ValueError("slice data overflow")
+    return out[:n].tobytes()
+
+
 def ref():
     global _ref
     if _ref is None:
