@@ -71,6 +71,7 @@ struct CavlcArgs {
   uint8_t* out;
   uint32_t slice_cap;  // bytes per slice region (multiple of 4)
   uint32_t* out_bytes; // [ns]
+  uint8_t* out_copy;   // where the stream bytes go (out itself, or e.g. mapped page-locked host memory)
 };
 
 __device__ __forceinline__ uint32_t slice_start(uint32_t s, uint32_t total, uint32_t ns) {
@@ -482,14 +483,16 @@ __global__ void __launch_bounds__(128) cavlc_pack_kernel(CavlcArgs a) {
   }
 }
 
-// MSB-first words -> stream bytes, in place.
+// MSB-first words -> stream bytes (in place, or into out_copy: only the
+// slice's bytes cross to a host mapping).
 __global__ void cavlc_bytes_kernel(CavlcArgs a) {
   const int s = blockIdx.y;
-  const uint32_t nb = a.out_bytes[s];
+  const uint32_t nb = a.sl[4 * s + 2] ? 0xffffffffu : (a.sl[4 * s + 0] + 7u) >> 3;
   if (nb == 0xffffffffu) return;
-  uint32_t* dst = reinterpret_cast<uint32_t*>(a.out + (size_t)s * a.slice_cap);
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(a.out + (size_t)s * a.slice_cap);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(a.out_copy + (size_t)s * a.slice_cap);
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < (nb + 3u) >> 2; k += gridDim.x * blockDim.x)
-    dst[k] = __byte_perm(dst[k], 0u, 0x0123);
+    dst[k] = __byte_perm(src[k], 0u, 0x0123);
 }
 
 }  // namespace b200enc
@@ -533,7 +536,8 @@ extern "C" int b200enc_cavlc_slices(const b200enc_cavlc_t* p, void* stream) {
   if (!p->levels || !p->dc || !p->nz || !p->mv || (p->is_intra && !p->pred_mode) || !p->out || !p->out_bytes ||
       !p->scratch)
     return -1;
-  if ((p->slice_cap & 3) || p->slice_cap < 4 || (((uintptr_t)p->out) & 3) || (((uintptr_t)p->scratch) & 255))
+  if ((p->slice_cap & 3) || p->slice_cap < 4 || (((uintptr_t)p->out) & 3) || (((uintptr_t)p->out_copy) & 3) ||
+      (((uintptr_t)p->scratch) & 255))
     return -1;
   const CavlcLayout L = cavlc_layout(p->mbw, p->mbh);
   if (p->scratch_bytes < L.bytes) return -1;
@@ -572,6 +576,7 @@ extern "C" int b200enc_cavlc_slices(const b200enc_cavlc_t* p, void* stream) {
   a.out = p->out;
   a.slice_cap = (uint32_t)std::min<size_t>(p->slice_cap, 0xfffffffcu);
   a.out_bytes = p->out_bytes;
+  a.out_copy = p->out_copy ? p->out_copy : p->out;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int mbs = p->mbw * p->mbh;
   if (cudaMemsetAsync(a.err, 0, 4, st) != cudaSuccess) return -1;

@@ -13,6 +13,7 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
@@ -39,6 +40,11 @@ struct Slot {
   uint32_t* status = nullptr;  // wavefront error words (intra, deblock)
   cudaEvent_t start = nullptr, done = nullptr;
   bool pending = false;
+  // GPU entropy coding: the slice RBSPs (no header) the GPU wrote into this
+  // page-locked, device-mapped memory, and their byte counts
+  uint8_t* slices = nullptr;
+  uint32_t* slice_bytes = nullptr;
+  int num_slices = 0;
 };
 
 struct Shadow {
@@ -88,6 +94,14 @@ struct Impl {
   int ev_head = 0, ev_count = 0;
   double stage_ms[2][4] = {};  // [intra][me, chain, deblock, staging]
   long stage_frames[2] = {0, 0};
+  // GPU entropy coding (b200enc_ctx_set_entropy): 0 off, 1 CAVLC slice data
+  // beside the staged outputs, 2 CAVLC slice data instead of the staged
+  // levels, DC, nz masks and modes
+  int entropy = 0, quality = 4;
+  void* d_cavlc = nullptr;     // b200enc_cavlc_scratch_bytes
+  size_t cavlc_bytes = 0;
+  uint8_t* d_slices = nullptr;  // the slices' bit words
+  size_t slices_bytes = 0;
 };
 
 Impl* impl_of(const gpu_context_t* ctx) { return ctx ? static_cast<Impl*>(ctx->impl) : nullptr; }
@@ -111,6 +125,11 @@ void free_frame_buffers(Impl* m) {
   cudaFree(m->d_mv);
   cudaFree(m->d_mv_prev);
   cudaFree(m->d_scratch);
+  cudaFree(m->d_cavlc);
+  cudaFree(m->d_slices);
+  m->d_cavlc = nullptr;
+  m->d_slices = nullptr;
+  m->cavlc_bytes = m->slices_bytes = 0;
   if (m->prop) b200enc_proposal_destroy(m->prop);
   m->prop = nullptr;
   m->prop_mbs = 0;
@@ -129,6 +148,10 @@ void free_frame_buffers(Impl* m) {
     cudaFreeHost(s.mv);
     cudaFreeHost(s.nz);
     cudaFreeHost(s.status);
+    cudaFreeHost(s.slices);
+    cudaFreeHost(s.slice_bytes);
+    s.slices = nullptr;
+    s.slice_bytes = nullptr;
     s.levels = nullptr;
     s.dc = nullptr;
     s.pred_mode = s.nz = s.status = nullptr;
@@ -254,6 +277,39 @@ int ensure_proposal(Impl* m) {
   return 0;
 }
 
+// Slice capacity of one slice region for a frame of `mbs` macroblocks in
+// `ns` slices: the reference's CAVLC allowance (2560 bytes per macroblock,
+// encoder_h264.c:3083-3086) for the largest slice, plus its header slack.
+size_t slice_cap_of(size_t mbs, int ns) { return align_up(((mbs + ns - 1) / ns) * 2560 + 4096, 256); }
+
+// Buffers of the GPU entropy coder, allocated on first use (every slot's
+// region holds 16 slices of the largest size).
+int ensure_entropy(Impl* m) {
+  if (m->d_cavlc) return 0;
+  const size_t mbs = (size_t)m->mbw * m->mbh;
+  m->cavlc_bytes = b200enc_cavlc_scratch_bytes(m->mbw, m->mbh);
+  m->slices_bytes = 16 * slice_cap_of(mbs, 16) + mbs * 2560;
+  bool ok = cudaMalloc(&m->d_cavlc, m->cavlc_bytes) == cudaSuccess &&
+            cudaMalloc(&m->d_slices, m->slices_bytes) == cudaSuccess;
+  for (Slot& s : m->slot)
+    ok = ok && cudaHostAlloc(&s.slices, m->slices_bytes, cudaHostAllocMapped) == cudaSuccess &&
+         cudaHostAlloc(&s.slice_bytes, 16 * sizeof(uint32_t), cudaHostAllocMapped) == cudaSuccess;
+  if (!ok) {
+    cudaFree(m->d_cavlc);
+    cudaFree(m->d_slices);
+    m->d_cavlc = nullptr;
+    m->d_slices = nullptr;
+    for (Slot& s : m->slot) {
+      cudaFreeHost(s.slices);
+      cudaFreeHost(s.slice_bytes);
+      s.slices = nullptr;
+      s.slice_bytes = nullptr;
+    }
+    return -1;
+  }
+  return 0;
+}
+
 // The whole hot path of one frame, enqueued on the context stream.
 int encode_frame(gpu_context_t* ctx, Impl* m, const uint8_t* y, const uint8_t* uv, int src_pitch, int W, int H, int qp,
                  int is_intra, int num_slices, int me_mode, const gpu_mv_t* cpu_mvs, bool stage) {
@@ -331,13 +387,45 @@ int encode_frame(gpu_context_t* ctx, Impl* m, const uint8_t* y, const uint8_t* u
                                        db_y + luma, m->pitch, scr1, kWavefrontMaxWaitUs, m->stream);
   }
   perf_mark(m, 3);
+  sl.num_slices = 0;
+  if (m->entropy) {
+    // the slice data of every slice, written by the GPU straight into the
+    // slot's mapped host memory (only the bytes of the slices cross the bus)
+    if (ensure_entropy(m) != 0) return -1;
+    b200enc_cavlc_t cp{};
+    cp.mbw = m->mbw;
+    cp.mbh = m->mbh;
+    cp.qp = qp;
+    cp.is_intra = is_intra ? 1 : 0;
+    cp.num_slices = std::min(num_slices, 16);
+    cp.quality_level = m->quality;
+    cp.levels = m->d_levels;
+    cp.dc = m->d_dc;
+    cp.nz = m->d_nz;
+    cp.pred_mode = m->d_pred_mode;
+    cp.mv = m->d_mv;
+    cp.out = m->d_slices;
+    cp.slice_cap = slice_cap_of(mbs, cp.num_slices);
+    uint8_t* dev_slices = nullptr;
+    uint32_t* dev_bytes = nullptr;
+    rc |= cudaHostGetDevicePointer((void**)&dev_slices, sl.slices, 0) == cudaSuccess ? 0 : -1;
+    rc |= cudaHostGetDevicePointer((void**)&dev_bytes, sl.slice_bytes, 0) == cudaSuccess ? 0 : -1;
+    cp.out_copy = dev_slices;
+    cp.out_bytes = dev_bytes;
+    cp.scratch = m->d_cavlc;
+    cp.scratch_bytes = m->cavlc_bytes;
+    if (rc == 0) rc |= b200enc_cavlc_slices(&cp, m->stream);
+    sl.num_slices = cp.num_slices;
+  }
   if (stage) {
     cudaStream_t st = m->stream;
-    rc |= cudaMemcpyAsync(sl.levels, m->d_levels, mbs * 768, cudaMemcpyDeviceToHost, st) == cudaSuccess ? 0 : -1;
-    rc |= cudaMemcpyAsync(sl.dc, m->d_dc, mbs * 96, cudaMemcpyDeviceToHost, st) == cudaSuccess ? 0 : -1;
-    rc |= cudaMemcpyAsync(sl.pred_mode, m->d_pred_mode, mbs * 4, cudaMemcpyDeviceToHost, st) == cudaSuccess ? 0 : -1;
+    if (m->entropy != 2) {
+      rc |= cudaMemcpyAsync(sl.levels, m->d_levels, mbs * 768, cudaMemcpyDeviceToHost, st) == cudaSuccess ? 0 : -1;
+      rc |= cudaMemcpyAsync(sl.dc, m->d_dc, mbs * 96, cudaMemcpyDeviceToHost, st) == cudaSuccess ? 0 : -1;
+      rc |= cudaMemcpyAsync(sl.pred_mode, m->d_pred_mode, mbs * 4, cudaMemcpyDeviceToHost, st) == cudaSuccess ? 0 : -1;
+      rc |= cudaMemcpyAsync(sl.nz, m->d_nz, mbs * 96, cudaMemcpyDeviceToHost, st) == cudaSuccess ? 0 : -1;
+    }
     rc |= cudaMemcpyAsync(sl.mv, m->d_mv, mbs * 16, cudaMemcpyDeviceToHost, st) == cudaSuccess ? 0 : -1;
-    rc |= cudaMemcpyAsync(sl.nz, m->d_nz, mbs * 96, cudaMemcpyDeviceToHost, st) == cudaSuccess ? 0 : -1;
     rc |= cudaMemcpyAsync(sl.status, scr0 + 1, 4, cudaMemcpyDeviceToHost, st) == cudaSuccess ? 0 : -1;
     rc |= cudaMemcpyAsync(sl.status + 1, scr1 + 1, 4, cudaMemcpyDeviceToHost, st) == cudaSuccess ? 0 : -1;
   }
@@ -727,6 +815,92 @@ int b200enc_ctx_set_me(gpu_context_t* ctx, int mode, const char* weights, float 
     return rc;
   }
   return 0;
+}
+
+int b200enc_ctx_set_entropy(gpu_context_t* ctx, int mode, int quality_level) {
+  Impl* m = impl_of(ctx);
+  if (!m || mode < 0 || mode > 2 || quality_level < 1 || quality_level > 7) return -1;
+  m->entropy = mode;
+  m->quality = quality_level;
+  return 0;
+}
+
+namespace {
+
+// Appends bits MSB first to a byte stream, inserting emulation_prevention_
+// three_byte (7.4.1: after two zero bytes, a byte <= 3 is preceded by 0x03;
+// the reference's bs_rbsp_to_ebsp, bitstream.c:233-250, does the same).
+struct NalOut {
+  uint8_t* p;
+  size_t cap, n = 0;
+  int zeros = 0;
+  uint64_t acc = 0;
+  int nacc = 0;
+  bool over = false;
+  void byte(uint8_t b) {
+    if (zeros == 2 && b <= 3) {
+      raw(3);
+      zeros = 0;
+    }
+    raw(b);
+    zeros = b == 0 ? zeros + 1 : 0;
+  }
+  void raw(uint8_t b) {
+    if (n < cap) p[n] = b;
+    else over = true;
+    ++n;
+  }
+  void put(int bits, uint32_t v) {  // bits <= 32
+    if (bits <= 0) return;
+    if (bits < 32) v &= (1u << bits) - 1u;
+    acc = (acc << bits) | v;
+    nacc += bits;
+    while (nacc >= 8) {
+      nacc -= 8;
+      byte((uint8_t)(acc >> nacc));
+    }
+    acc &= nacc ? ((1ull << nacc) - 1ull) : 0ull;
+  }
+};
+
+}  // namespace
+
+int b200enc_ctx_slice_nals(gpu_context_t* ctx, int slot, const uint8_t* headers, const int* header_bits,
+                           int nal_ref_idc, int nal_unit_type, uint8_t* out, size_t cap, size_t* written) {
+  Impl* m = impl_of(ctx);
+  if (!m || slot < 0 || slot > 1 || !out || !written || nal_ref_idc < 0 || nal_ref_idc > 3 || nal_unit_type < 1 ||
+      nal_unit_type > 31)
+    return -1;
+  Slot& sl = m->slot[slot];
+  if (!sl.slices || sl.num_slices <= 0) return -1;
+  if (gpu_compute_sync_slot(ctx, slot) != 0) return -1;
+  NalOut o{out, cap};
+  for (int s = 0; s < sl.num_slices; ++s) {
+    const uint32_t nb = sl.slice_bytes[s];
+    if (nb == 0xffffffffu || nb == 0) return -1;
+    const int hb = header_bits ? header_bits[s] : 0;
+    if (hb < 0 || hb > 128 || (hb > 0 && !headers)) return -1;
+    // start code and NAL header (never escaped), then the RBSP: the caller's
+    // header bits, the slice data (the GPU's RBSP up to its stop bit), the
+    // stop bit and the alignment zeros
+    o.raw(0);
+    o.raw(0);
+    o.raw(0);
+    o.raw(1);
+    o.raw((uint8_t)((nal_ref_idc << 5) | nal_unit_type));
+    o.zeros = 0;
+    const uint8_t* h = headers ? headers + 16 * s : nullptr;
+    for (int k = 0; k < hb; k += 8) o.put(std::min(8, hb - k), (uint32_t)(h[k >> 3] >> (8 - std::min(8, hb - k))));
+    const uint8_t* d = sl.slices + (size_t)s * slice_cap_of((size_t)m->mbw * m->mbh, sl.num_slices);
+    const uint8_t last = d[nb - 1];
+    const int data_bits_last = 7 - __builtin_ctz(last);  // bits before the stop bit in the last byte
+    for (uint32_t k = 0; k + 1 < nb; ++k) o.put(8, d[k]);
+    o.put(data_bits_last, (uint32_t)(last >> (8 - data_bits_last)));
+    o.put(1, 1u);
+    if (o.nacc) o.put(8 - o.nacc, 0u);
+  }
+  *written = o.n;
+  return o.over ? -1 : 0;
 }
 
 int b200enc_ctx_me_stats(gpu_context_t* ctx, int* learned, int* fallback, int* early) {

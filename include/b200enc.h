@@ -519,6 +519,9 @@ typedef struct {
     uint8_t *out;                /* device: slice s at out + s * slice_cap */
     size_t slice_cap;            /* bytes per slice, a multiple of 4 */
     uint32_t *out_bytes;         /* device [num_slices] */
+    uint8_t *out_copy;           /* NULL: the bytes end in `out`; else the bytes go here (same layout; `out` is
+                                    then work space), e.g. page-locked host memory mapped for the device, so
+                                    only each slice's bytes cross the bus */
     void *scratch;               /* device, 256-byte aligned */
     size_t scratch_bytes;        /* >= b200enc_cavlc_scratch_bytes(mbw, mbh) */
 } b200enc_cavlc_t;

@@ -205,6 +205,27 @@ int b200enc_ctx_set_me(gpu_context_t *ctx, int mode, const char *weights, float 
  * candidates, MBs that fell back to the full search, zero-MV early-outs
  * (synchronises the context stream). */
 int b200enc_ctx_me_stats(gpu_context_t *ctx, int *learned, int *fallback, int *early);
+/* Entropy coding on the GPU (no reference counterpart: the reference codes
+ * slices on the host, encoder_h264.c:3128-3290, 57 % of a 1440p frame by its
+ * DEVLOG). mode 1: every dispatched frame also gets its CAVLC slice data
+ * coded on the GPU (b200enc_cavlc_slices) into the slot's page-locked
+ * memory, beside the usual staging; mode 2: the same, and the slot's levels,
+ * DC, nz and mode staging copies are skipped (a caller that does not run the
+ * host entropy coder: ~8 MB less over the bus per 1080p frame); 0 (default):
+ * off. quality_level is the host encoder's (1..7, default 4; its P_Skip rule
+ * changes at >= 5). */
+int b200enc_ctx_set_entropy(gpu_context_t *ctx, int mode, int quality_level);
+/* The Annex B NAL units of a slot's slices (after gpu_compute_end_picture;
+ * waits for the slot like gpu_compute_sync_slot): for each slice a 4-byte
+ * start code, the NAL header (nal_ref_idc, nal_unit_type), then the RBSP -
+ * the caller's slice header (header_bits[s] bits, MSB first, from
+ * headers + 16 * s) followed by the GPU's slice data and rbsp_trailing_bits -
+ * with emulation prevention (7.4.1), as the reference's encoder assembles
+ * its slices (encoder_h264.c:3429-3470). The bytes go to out (cap bytes);
+ * *written gets their count. Returns 0, or -1 (entropy mode off, bad
+ * arguments, a slice that outgrew its region, cap too small). */
+int b200enc_ctx_slice_nals(gpu_context_t *ctx, int slot, const uint8_t *headers, const int *header_bits,
+                           int nal_ref_idc, int nal_unit_type, uint8_t *out, size_t cap, size_t *written);
 
 /* Per-stage GPU timing with CUDA events, the equivalent of the reference's
  * BC250_PERF_STATS timestamps (gpu_compute.c:50-67). enable resets the
