@@ -530,6 +530,23 @@ class Context:
     def sync(self, slot):
         return self.L.gpu_compute_sync_slot(ctypes.byref(self.ctx), slot)
 
+    def set_entropy(self, mode, quality_level=4):
+        """GPU entropy coding (b200enc_ctx_set_entropy): 0 off, 1 beside the
+        staging, 2 instead of the level staging."""
+        _check(self.L.b200enc_ctx_set_entropy(ctypes.byref(self.ctx), mode, quality_level),
+               "b200enc_ctx_set_entropy")
+
+    def slice_nals(self, slot, headers, header_bits, nal_ref_idc, nal_unit_type, out):
+        """Annex B slice NAL units of a slot into the uint8 numpy array `out`
+        (headers: uint8 [slices][16], header_bits: int32 [slices]); returns
+        the byte count."""
+        n = ctypes.c_size_t()
+        _check(self.L.b200enc_ctx_slice_nals(ctypes.byref(self.ctx), slot, _vp(headers.ctypes.data),
+                                             _vp(header_bits.ctypes.data), nal_ref_idc, nal_unit_type,
+                                             _vp(out.ctypes.data), out.nbytes, ctypes.byref(n)),
+               "b200enc_ctx_slice_nals")
+        return n.value
+
     def staging(self, slot):
         """numpy views of the slot's staging buffers (valid until resubmitted)."""
         import numpy as np
