@@ -15,7 +15,8 @@
 //   1. cavlc_info_kernel: per macroblock, the skip decision, coded block
 //      pattern and every coded block's TotalCoeff;
 //   2. cavlc_mb_kernel: per macroblock, its header and residual bits (one
-//      thread per macroblock, into a private region of the scratch);
+//      warp per macroblock, a lane per block, into a private region of the
+//      scratch);
 //   3. cavlc_slice_kernel: per slice (one CTA), the skip runs and every
 //      coded macroblock's bit offset (two block-wide scans), the slice's
 //      length; it zeroes the slice's output words;
@@ -260,13 +261,24 @@ __device__ void luma_dc_levels(const int32_t* d, const QP& q, int16_t out[16]) {
 }
 
 // ---- 2. per macroblock: header and residual bits --------------------------------
-__global__ void __launch_bounds__(64) cavlc_mb_kernel(CavlcArgs a) {
-  const int mb = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per macroblock; each lane writes one syntax element group into its
+// own bit buffer, in the order the reference writes them: lane 0 the header,
+// 1 the I16x16 luma DC block, 2..17 the luma blocks (spec order), 18 and 19 the
+// chroma DC blocks, 20..27 the chroma AC blocks (Cb then Cr). A warp scan of
+// the lanes' lengths places them; the lanes OR their words into the warp's
+// shared copy of the macroblock's region, which is then stored.
+constexpr int kCavlcLaneWords = 24;  // one block: at most 16 escaped levels (~36 bits each) + tokens
+constexpr int kCavlcMbWarps = 4;
+
+__global__ void __launch_bounds__(32 * kCavlcMbWarps) cavlc_mb_kernel(CavlcArgs a) {
+  __shared__ uint32_t shw[kCavlcMbWarps][kCavlcMbWords];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int mb = blockIdx.x * kCavlcMbWarps + wi;
   const int mbs = a.mbw * a.mbh;
   if (mb >= mbs) return;
   const uint32_t info = a.info[mb];
   if (info & 1u) {  // skipped: its run is counted by the slice pass
-    a.nbits[mb] = 0;
+    if (lane == 0) a.nbits[mb] = 0;
     return;
   }
   const int mbx = mb % a.mbw, mby = mb / a.mbw;
@@ -274,45 +286,80 @@ __global__ void __launch_bounds__(64) cavlc_mb_kernel(CavlcArgs a) {
   const int16_t* lv = a.levels + (size_t)mb * 384;
   const int32_t* dcm = a.dc + (size_t)mb * 24;
   const int cbp_c = (int)((info >> 8) & 3u);
+  const bool intra = a.is_intra != 0;
+  uint32_t lw[kCavlcLaneWords];
   BitW b;
-  bw_init(b, a.words + (size_t)mb * kCavlcMbWords, kCavlcMbWords);
-  const QP qc = make_qp(chroma_qp(a.qp), a.is_intra != 0);
-  int cdc[2][4];
-  chroma_dc(dcm + 16, cdc[0]);
-  chroma_dc(dcm + 20, cdc[1]);
-  for (int p = 0; p < 2; ++p)
-    for (int i = 0; i < 4; ++i) cdc[p][i] = quantize_dc(cdc[p][i], qc);
-  if (a.is_intra) {
-    int n;
-    const bool left = nb_ok(mbx, mby, -1, 0, a.mbw, start, &n), top = nb_ok(mbx, mby, 0, -1, a.mbw, start, &n);
-    const uint32_t pm = a.pred_mode[mb];
-    const int lac = (int)((info >> 1) & 1u);
-    put_i16_header(b, sanitize_i16((int)(pm & 3u), top, left), sanitize_chroma((int)((pm >> 2) & 3u), top, left), cbp_c,
-                   lac);
-    int16_t ldc[16];
-    luma_dc_levels(dcm, make_qp(a.qp, true), ldc);
-    put_4x4(b, ldc, false, luma_nc(a.tcs, mb, mbx, mby, a.mbw, start, 0));
-    if (lac)
-      for (int k = 0; k < 16; ++k)
-        put_4x4(b, lv + (kBlkY4[k] * 4 + kBlkX4[k]) * 16, true, luma_nc(a.tcs, mb, mbx, mby, a.mbw, start, k));
-  } else {
-    int px, py;
-    mv_pred(a.mv, mbx, mby, a.mbw, start, &px, &py);
-    const int cbp_l = (int)((info >> 1) & 15u);
-    put_p16_header(b, a.mv[mb].mvx - px, a.mv[mb].mvy - py, cbp_l | (cbp_c << 4));
-    for (int k = 0; k < 16; ++k)
-      if (cbp_l & (1 << (k >> 2)))
-        put_4x4(b, lv + (kBlkY4[k] * 4 + kBlkX4[k]) * 16, false, luma_nc(a.tcs, mb, mbx, mby, a.mbw, start, k));
+  bw_init(b, lw, kCavlcLaneWords);
+  if (lane == 0) {
+    if (intra) {
+      int n;
+      const bool left = nb_ok(mbx, mby, -1, 0, a.mbw, start, &n), top = nb_ok(mbx, mby, 0, -1, a.mbw, start, &n);
+      const uint32_t pm = a.pred_mode[mb];
+      put_i16_header(b, sanitize_i16((int)(pm & 3u), top, left), sanitize_chroma((int)((pm >> 2) & 3u), top, left),
+                     cbp_c, (int)((info >> 1) & 1u));
+    } else {
+      int px, py;
+      mv_pred(a.mv, mbx, mby, a.mbw, start, &px, &py);
+      put_p16_header(b, a.mv[mb].mvx - px, a.mv[mb].mvy - py, (int)((info >> 1) & 15u) | (cbp_c << 4));
+    }
+  } else if (lane == 1) {
+    if (intra) {
+      int16_t ldc[16];
+      luma_dc_levels(dcm, make_qp(a.qp, true), ldc);
+      put_4x4(b, ldc, false, luma_nc(a.tcs, mb, mbx, mby, a.mbw, start, 0));
+    }
+  } else if (lane < 18) {
+    const int k = lane - 2;
+    const bool coded = intra ? ((info >> 1) & 1u) : ((info >> (1 + (k >> 2))) & 1u);
+    if (coded)
+      put_4x4(b, lv + (kBlkY4[k] * 4 + kBlkX4[k]) * 16, intra, luma_nc(a.tcs, mb, mbx, mby, a.mbw, start, k));
+  } else if (lane < 20) {
+    if (cbp_c >= 1) {
+      const QP qc = make_qp(chroma_qp(a.qp), intra);
+      int c[4];
+      chroma_dc(dcm + 16 + 4 * (lane - 18), c);
+      for (int i = 0; i < 4; ++i) c[i] = quantize_dc(c[i], qc);
+      put_block(b, c, 4, 4);
+    }
+  } else if (lane < 28) {
+    if (cbp_c == 2) {
+      const int p = (lane - 20) >> 2, k = (lane - 20) & 3;
+      put_4x4(b, lv + (16 + 4 * p + k) * 16, true, chroma_nc(a.tcs, mb, mbx, mby, a.mbw, start, 16 + 4 * p, k));
+    }
   }
-  if (cbp_c >= 1)
-    for (int p = 0; p < 2; ++p) put_block(b, cdc[p], 4, 4);
-  if (cbp_c == 2)
-    for (int p = 0; p < 2; ++p)
-      for (int k = 0; k < 4; ++k)
-        put_4x4(b, lv + (16 + 4 * p + k) * 16, true, chroma_nc(a.tcs, mb, mbx, mby, a.mbw, start, 16 + 4 * p, k));
   bw_flush(b);
-  a.nbits[mb] = b.pos;
-  if (b.over) atomicExch(a.err, 1u);
+  // place the lanes' bits one after another
+  const uint32_t len = b.pos;
+  uint32_t off = len;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, off, o);
+    if (lane >= o) off += y;
+  }
+  const uint32_t total = __shfl_sync(0xffffffffu, off, 31);
+  off -= len;
+  const bool over = __any_sync(0xffffffffu, b.over) || total > 32u * kCavlcMbWords;
+  if (over) {
+    if (lane == 0) {
+      atomicExch(a.err, 1u);
+      a.nbits[mb] = 0;
+    }
+    return;
+  }
+  uint32_t* sw = shw[wi];
+  const uint32_t nw = (total + 31u) >> 5;
+  for (uint32_t k = lane; k < nw; k += 32) sw[k] = 0u;
+  __syncwarp();
+  for (uint32_t k = 0; 32u * k < len; ++k) {
+    const int m = (int)min(32u, len - 32u * k);
+    const uint32_t v = lw[k] >> (32 - m), left = m < 32 ? v << (32 - m) : v;
+    const uint32_t pos = off + 32u * k, wd = pos >> 5, sh = pos & 31u;
+    atomicOr(sw + wd, left >> sh);
+    if (sh + (uint32_t)m > 32u) atomicOr(sw + wd + 1, left << (32u - sh));
+  }
+  __syncwarp();
+  uint32_t* dst = a.words + (size_t)mb * kCavlcMbWords;
+  for (uint32_t k = lane; k < nw; k += 32) dst[k] = sw[k];
+  if (lane == 0) a.nbits[mb] = total;
 }
 
 // ---- 3. per slice: skip runs, offsets, length --------------------------------------
@@ -581,7 +628,7 @@ extern "C" int b200enc_cavlc_slices(const b200enc_cavlc_t* p, void* stream) {
   const int mbs = p->mbw * p->mbh;
   if (cudaMemsetAsync(a.err, 0, 4, st) != cudaSuccess) return -1;
   cavlc_info_kernel<<<(mbs + 127) / 128, 128, 0, st>>>(a);
-  cavlc_mb_kernel<<<(mbs + 63) / 64, 64, 0, st>>>(a);
+  cavlc_mb_kernel<<<(mbs + kCavlcMbWarps - 1) / kCavlcMbWarps, 32 * kCavlcMbWarps, 0, st>>>(a);
   cavlc_slice_kernel<<<p->num_slices, kCavlcScanThreads, 0, st>>>(a, h);
   cavlc_pack_kernel<<<(mbs + 127) / 128, 128, 0, st>>>(a);
   cavlc_bytes_kernel<<<dim3(16, p->num_slices), 256, 0, st>>>(a);
