@@ -23,11 +23,17 @@ inference is timed beside them (learned_bf16).
          every context stream waits on, end event after every context stream
          has drained), max over ranks (weak scaling: independent streams per
          GPU, no collective on the data path).
-  e2e    the learned form through the reference boundary (per stream
-         gpu_compute_upload_nv12 from pinned host memory,
-         begin/dispatch/end_picture; then sync_slot and a host read of the
-         staged outputs), S streams, double-buffered over the boundary's two
-         staging slots (step k+1 is submitted before step k is read back).
+  e2e    the learned form through the reference boundary with the
+         bitstream as the result: per stream gpu_compute_upload_nv12 from
+         pinned host memory, begin/dispatch/end_picture with GPU entropy
+         coding (b200enc_ctx_set_entropy mode 2: CAVLC slice data written by
+         the GPU into mapped host memory), then b200enc_ctx_slice_nals
+         assembling the frame's Annex B slice NAL units on the host (one
+         thread per stream); S streams, double-buffered over the boundary's
+         two slots (step k+1 is submitted before step k is collected).
+  e2e_staging  the same boundary with the staged outputs as the result
+         (sync_slot and a host read of the levels, DC, nz, modes, vectors the
+         reference's host entropy coder consumes).
   full_encode  the rate an application sees: S streams, one host thread
          each, through the reference's unchanged host encoder
          (h264_encoder_encode_frame_ext in oracle/_ref/libh264enc_b200.so:
@@ -760,15 +766,18 @@ def run_gpu(args):
                                "MB (zero-MV early-outs of the last P frame excluded) / ME stage time"},
             "bd_rate": rd_record(),
             "gpu_launches": launches,
-            "e2e": {"value": round(e2e_fps, 2), "unit": "frames/s", "h2d_bytes_per_step": S * H2D_PER_STEP,
-                    "d2h_bytes_per_step": S * D2H_PER_STEP},
+            "e2e": {"value": round(ent_fps, 2), "unit": "frames/s", "h2d_bytes_per_step": S * H2D_PER_STEP,
+                    "d2h_bytes_per_step": int(S * (MBS * 16 + 8) + round(ent_mbit * 1e6 / 8) * S),
+                    "output": "the Annex B slice NAL units of every frame (GPU CAVLC, 4 slices)",
+                    "mbit_per_frame": round(ent_mbit, 4),
+                    "path": "learned form through the boundary with host buffers: pinned upload, GPU stages, GPU "
+                            "CAVLC slice data into mapped host memory, slice NAL units assembled on the host (one "
+                            "thread per stream)"},
+            "e2e_staging": {"value": round(e2e_fps, 2), "unit": "frames/s", "h2d_bytes_per_step": S * H2D_PER_STEP,
+                            "d2h_bytes_per_step": S * D2H_PER_STEP,
+                            "path": "the reference boundary's staged levels, DC, nz masks, modes and vectors read "
+                                    "back every step (what the reference's host entropy coder consumes)"},
             "full_encode": fe or None,
-            "e2e_gpu_entropy": {"value": round(ent_fps, 2), "unit": "frames/s", "mbit_per_frame": round(ent_mbit, 4),
-                                "slices_per_frame": 4, "entropy": "CAVLC on the GPU",
-                                "note": "learned form through the boundary with host buffers: pinned upload, GPU "
-                                        "stages, GPU CAVLC slice data into mapped host memory, Annex B slice NAL "
-                                        "units assembled on the host (one thread per stream); the bitstream is "
-                                        "the output, no level staging"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(ach / peak, 5), "peak_kind": peak_kind,
                          "traffic": (round(tr * MBS) if tr is not None else None),
