@@ -26,7 +26,8 @@ int b200enc_i_frame_batch_launch(const b200enc::BatchTab& bt, int ctas, uint32_t
 int b200enc_deblock_batch_rows(int max_mbw, int max_mbh);
 int b200enc_deblock_tiles_launch(int mbw, int mbh, int qp, int is_intra, const uint32_t* nz, const void* mv,
                                  const uint8_t* src_y, const uint8_t* src_uv, uint8_t* dst_y, uint8_t* dst_uv,
-                                 int pitch, uint32_t* status, uint32_t max_wait, cudaStream_t stream);
+                                 int pitch, uint32_t* status, uint32_t max_wait, cudaStream_t stream,
+                                 const uint8_t* t8 = nullptr);
 int b200enc_deblock_tile_count(int mbw, int mbh, int* tw, int* th);
 int b200enc_deblock_tiles_batch_launch(const b200enc::BatchTab& bt, int tiles, uint32_t max_wait, cudaStream_t st);
 int b200enc_deblock_batch_launch(const b200enc::BatchTab& bt, int max_mbw, int ctas, uint32_t max_wait,

@@ -264,14 +264,27 @@ __device__ __forceinline__ void chroma_h_step(uint8_t* top, int sp, int xo, cons
 // segment k of edge e in direction dir of macroblock mb; has_edge0 = the
 // macroblock edge is filtered (a left / upper neighbour inside the picture
 // being deblocked).
+// Nonzero levels in the transform block holding 4x4 block b (raster) of
+// macroblock mb: the 4x4 block, or with the 8x8 transform (t8[mb]) its 8x8
+// block (h264_deblock.c:119-137).
+__device__ __forceinline__ uint32_t db_coef(const uint32_t* __restrict__ nzm, const uint8_t* __restrict__ t8, int mb,
+                                            int b) {
+  const uint32_t* n = nzm + (size_t)mb * 24;
+  if (!t8 || !t8[mb]) return __ldg(n + b) & 0xffffu;
+  const int c = b & 10;
+  return (__ldg(n + c) | __ldg(n + c + 1) | __ldg(n + c + 4) | __ldg(n + c + 5)) & 0xffffu;
+}
+
 __device__ __forceinline__ int db_bs(int k, int e, int dir, int mb, int mbw, bool has_edge0, int is_intra,
-                                     const uint32_t* __restrict__ nzm, const MV* __restrict__ mvs) {
+                                     const uint32_t* __restrict__ nzm, const MV* __restrict__ mvs,
+                                     const uint8_t* __restrict__ t8 = nullptr) {
   if (e == 0 && !has_edge0) return 0;
+  if ((e & 1) && t8 && t8[mb]) return 0;  // no luma edge inside an 8x8 transform block (h264_deblock.c:294,324)
   if (is_intra) return e == 0 ? 4 : 3;
   const int mbp = e ? mb : (dir == 0 ? mb - 1 : mb - mbw);
   const int bq = dir == 0 ? k * 4 + e : e * 4 + k;
   const int bp = e ? (dir == 0 ? bq - 1 : bq - 4) : (dir == 0 ? k * 4 + 3 : 12 + k);
-  if ((__ldg(nzm + (size_t)mbp * 24 + bp) | __ldg(nzm + (size_t)mb * 24 + bq)) & 0xffffu) return 2;
+  if (db_coef(nzm, t8, mbp, bp) | db_coef(nzm, t8, mb, bq)) return 2;
   if (e != 0) return 0;
   const int2 a = __ldg(reinterpret_cast<const int2*>(mvs + mbp));
   const int2 c = __ldg(reinterpret_cast<const int2*>(mvs + mb));
@@ -681,7 +694,8 @@ __host__ __device__ inline DbTilePlan db_tile_plan(int TW, int TH) {
 template <bool BATCH>
 __global__ void __launch_bounds__(64 * (kDbTileMax + 2), 2) deblock_tile_kernel(
     int mbw_, int mbh_, int TW, int TH, int qp_, int is_intra_, const uint32_t* __restrict__ nzm_,
-    const MV* __restrict__ mvs_, const uint8_t* __restrict__ src_y_, const uint8_t* __restrict__ src_uv_,
+    const MV* __restrict__ mvs_, const uint8_t* __restrict__ t8_, const uint8_t* __restrict__ src_y_,
+    const uint8_t* __restrict__ src_uv_,
     uint8_t* __restrict__ dst_y_, uint8_t* __restrict__ dst_uv_, int pitch_, uint32_t* status_, uint32_t max_wait,
     BatchTab bt) {
   extern __shared__ __align__(16) uint8_t smem[];
@@ -757,7 +771,7 @@ __global__ void __launch_bounds__(64 * (kDbTileMax + 2), 2) deblock_tile_kernel(
       const int k = i & 3, e = (i >> 2) & 3, dir = (i >> 4) & 1, m = i >> 5;
       const int lyr = m / RWr, lxr = m - lyr * RWr;
       bsm[i] = (uint8_t)db_bs(k, e, dir, (ry0 + lyr) * mbw + rx0 + lxr, mbw, dir == 0 ? lxr > 0 : lyr > 0, is_intra,
-                              nzm, mvs);
+                              nzm, mvs, BATCH ? nullptr : t8_);
     }
     for (int i = tid; i < 2 * (TH + 2); i += nthr) prog[i] = 0u;
   }
@@ -912,7 +926,8 @@ static void db_tile_shape(int* tw, int* th) {
 
 int b200enc_deblock_tiles_launch(int mbw, int mbh, int qp, int is_intra, const uint32_t* nz, const void* mv,
                                  const uint8_t* src_y, const uint8_t* src_uv, uint8_t* dst_y, uint8_t* dst_uv,
-                                 int pitch, uint32_t* status, uint32_t max_wait, cudaStream_t stream) {
+                                 int pitch, uint32_t* status, uint32_t max_wait, cudaStream_t stream,
+                                 const uint8_t* t8) {
   int TW, TH;
   db_tile_shape(&TW, &TH);
   const DbTilePlan P = db_tile_plan(TW, TH);
@@ -921,8 +936,8 @@ int b200enc_deblock_tiles_launch(int mbw, int mbh, int qp, int is_intra, const u
     return -1;
   const int tiles = ((mbw + TW - 1) / TW) * ((mbh + TH - 1) / TH);
   deblock_tile_kernel<false><<<tiles, 64 * (TH + 2), P.bytes, stream>>>(
-      mbw, mbh, TW, TH, qp, is_intra, nz, (const MV*)mv, src_y, src_uv, dst_y, dst_uv, pitch, status, max_wait,
-      BatchTab{});
+      mbw, mbh, TW, TH, qp, is_intra, nz, (const MV*)mv, t8, src_y, src_uv, dst_y, dst_uv, pitch, status,
+      max_wait, BatchTab{});
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -947,14 +962,27 @@ int b200enc_deblock_tiles_batch_launch(const BatchTab& bt, int tiles, uint32_t m
       cudaSuccess)
     return -1;
   deblock_tile_kernel<true><<<tiles, 64 * (TH + 2), P.bytes, st>>>(0, 0, 0, 0, 0, 0, nullptr, nullptr, nullptr,
-                                                                   nullptr, nullptr, nullptr, 0, nullptr, max_wait,
-                                                                   bt);
+                                                                   nullptr, nullptr, nullptr, nullptr, 0, nullptr,
+                                                                   max_wait, bt);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
+
+extern "C" int b200enc_deblock_tiles_t8(int mbw, int mbh, int qp, int is_intra, const uint32_t* nz,
+                                        const uint8_t* t8, const void* mv, const uint8_t* src_y,
+                                        const uint8_t* src_uv, uint8_t* dst_y, uint8_t* dst_uv, int pitch,
+                                        uint32_t* status, void* stream);
 
 extern "C" int b200enc_deblock_tiles(int mbw, int mbh, int qp, int is_intra, const uint32_t* nz, const void* mv,
                                      const uint8_t* src_y, const uint8_t* src_uv, uint8_t* dst_y, uint8_t* dst_uv,
                                      int pitch, uint32_t* status, void* stream) {
+  return b200enc_deblock_tiles_t8(mbw, mbh, qp, is_intra, nz, nullptr, mv, src_y, src_uv, dst_y, dst_uv, pitch,
+                                  status, stream);
+}
+
+extern "C" int b200enc_deblock_tiles_t8(int mbw, int mbh, int qp, int is_intra, const uint32_t* nz,
+                                        const uint8_t* t8, const void* mv, const uint8_t* src_y,
+                                        const uint8_t* src_uv, uint8_t* dst_y, uint8_t* dst_uv, int pitch,
+                                        uint32_t* status, void* stream) {
   if (!nz || !mv || !src_y || !src_uv || !dst_y || !dst_uv || !status || mbw <= 0 || mbh <= 0 || qp < 0 || qp > 51)
     return -1;
   const uintptr_t a = (uintptr_t)src_y | (uintptr_t)src_uv | (uintptr_t)dst_y | (uintptr_t)dst_uv;
@@ -969,5 +997,5 @@ extern "C" int b200enc_deblock_tiles(int mbw, int mbh, int qp, int is_intra, con
     return -1;
   if (cudaMemsetAsync(status, 0, 16, (cudaStream_t)stream) != cudaSuccess) return -1;
   return b200enc_deblock_tiles_launch(mbw, mbh, qp, is_intra, nz, mv, src_y, src_uv, dst_y, dst_uv, pitch, status,
-                                      kMaxWaitUsDb, (cudaStream_t)stream);
+                                      kMaxWaitUsDb, (cudaStream_t)stream, t8);
 }

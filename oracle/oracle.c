@@ -807,12 +807,24 @@ static void filt_chroma(uint8_t *q, int d, int bs, int alpha, int beta, int tc0)
     q[0] = (uint8_t)clip1(q0 - delta);
 }
 
-static int bs_of(int is_intra, int mb_edge, const uint32_t *nz, const orc_mv_t *mv, int mbp, int bp, int mbq, int bq)
+/* Whether the transform block holding 4x4 block b (raster) of macroblock mb
+ * has a coefficient: the 4x4 block, or with the 8x8 transform the 8x8 block
+ * whose four 4x4 blocks are ORed (A1/src/h264_deblock.c:119-137). */
+static int has_coef(const uint32_t *nz, const uint8_t *t8, int mb, int b)
+{
+    if (!t8 || !t8[mb]) return (nz[(size_t)mb * 24 + b] & 0xffff) != 0;
+    const int c = b & 10;
+    return ((nz[(size_t)mb * 24 + c] | nz[(size_t)mb * 24 + c + 1] | nz[(size_t)mb * 24 + c + 4] |
+             nz[(size_t)mb * 24 + c + 5]) & 0xffff) != 0;
+}
+
+static int bs_of(int is_intra, int mb_edge, const uint32_t *nz, const uint8_t *t8, const orc_mv_t *mv, int mbp,
+                 int bp, int mbq, int bq)
 {
     /* Clause 8.7.2.1 for this encoder's macroblock kinds
      * (A1/src/h264_deblock.c:139-210). */
     if (is_intra) return mb_edge ? 4 : 3;
-    if ((nz[(size_t)mbp * 24 + bp] & 0xffff) || (nz[(size_t)mbq * 24 + bq] & 0xffff)) return 2;
+    if (has_coef(nz, t8, mbp, bp) || has_coef(nz, t8, mbq, bq)) return 2;
     if (iabs(mv[mbp].mvx - mv[mbq].mvx) >= 4 || iabs(mv[mbp].mvy - mv[mbq].mvy) >= 4) return 1;
     return 0;
 }
@@ -820,8 +832,8 @@ static int bs_of(int is_intra, int mb_edge, const uint32_t *nz, const orc_mv_t *
 /* One filtering step of macroblock mb: its vertical edges (dir 0, left to
  * right) or its horizontal edges (dir 1, top to bottom), luma and chroma
  * (A1/src/h264_deblock.c:263-347). Uniform QP so qPav = QP. */
-static void deblock_step(int mbw, int qp, int is_intra, const uint32_t *nz, const orc_mv_t *mv, uint8_t *ry,
-                         uint8_t *ruv, int rp, int mb, int dir)
+static void deblock_step(int mbw, int qp, int is_intra, const uint32_t *nz, const uint8_t *t8, const orc_mv_t *mv,
+                         uint8_t *ry, uint8_t *ruv, int rp, int mb, int dir)
 {
     const int qpc = orc_chroma_qp(qp);
     const int a = ALPHA[qp], b = BETA[qp], ac = ALPHA[qpc], bc = BETA[qpc];
@@ -830,11 +842,13 @@ static void deblock_step(int mbw, int qp, int is_intra, const uint32_t *nz, cons
     uint8_t *pc = ruv + (size_t)my * 8 * rp + mx * 16;
     for (int e = 0; e < 4; e++) {
         if (e == 0 && (dir == 0 ? mx == 0 : my == 0)) continue;
+        /* 8x8 transform: no luma edge inside the 8x8 blocks (h264_deblock.c:294,324) */
+        if ((e & 1) && t8 && t8[mb]) continue;
         int mbp = e ? mb : (dir == 0 ? mb - 1 : mb - mbw);
         for (int k = 0; k < 4; k++) {
             int bq = dir == 0 ? k * 4 + e : e * 4 + k;
             int bp = e ? (dir == 0 ? bq - 1 : bq - 4) : (dir == 0 ? k * 4 + 3 : 12 + k);
-            int bs = bs_of(is_intra, e == 0, nz, mv, mbp, bp, mb, bq);
+            int bs = bs_of(is_intra, e == 0, nz, t8, mv, mbp, bp, mb, bq);
             if (!bs) continue;
             if (a && b) {
                 int tc0 = bs < 4 ? TC0[qp][bs - 1] : 0;
@@ -857,6 +871,15 @@ static void deblock_step(int mbw, int qp, int is_intra, const uint32_t *nz, cons
     }
 }
 
+void orc_deblock_frame_t8(int mbw, int mbh, int qp, int is_intra, const uint32_t *nz, const uint8_t *t8,
+                          const orc_mv_t *mv, uint8_t *ry, uint8_t *ruv, int rp)
+{
+    for (int mb = 0; mb < mbw * mbh; mb++) {
+        deblock_step(mbw, qp, is_intra, nz, t8, mv, ry, ruv, rp, mb, 0);
+        deblock_step(mbw, qp, is_intra, nz, t8, mv, ry, ruv, rp, mb, 1);
+    }
+}
+
 void orc_deblock_frame(int mbw, int mbh, int qp, int is_intra, const uint32_t *nz, const orc_mv_t *mv,
                        uint8_t *ry, uint8_t *ruv, int rp)
 {
@@ -864,8 +887,8 @@ void orc_deblock_frame(int mbw, int mbh, int qp, int is_intra, const uint32_t *n
      * to right, then the horizontal edges top to bottom (clause 8.7,
      * A1/src/h264_deblock.c:263-347). */
     for (int mb = 0; mb < mbw * mbh; mb++) {
-        deblock_step(mbw, qp, is_intra, nz, mv, ry, ruv, rp, mb, 0);
-        deblock_step(mbw, qp, is_intra, nz, mv, ry, ruv, rp, mb, 1);
+        deblock_step(mbw, qp, is_intra, nz, NULL, mv, ry, ruv, rp, mb, 0);
+        deblock_step(mbw, qp, is_intra, nz, NULL, mv, ry, ruv, rp, mb, 1);
     }
 }
 
@@ -876,7 +899,7 @@ int orc_deblock_steps(int mbw, int mbh, int qp, int is_intra, const uint32_t *nz
     for (int i = 0; i < nsteps; i++) {
         const int mb = steps[i] >> 1, dir = steps[i] & 1;
         if (steps[i] < 0 || mb >= mbw * mbh) return -1;
-        deblock_step(mbw, qp, is_intra, nz, mv, ry, ruv, rp, mb, dir);
+        deblock_step(mbw, qp, is_intra, nz, NULL, mv, ry, ruv, rp, mb, dir);
     }
     return 0;
 }
@@ -903,4 +926,106 @@ void orc_encode_frame(const orc_frame_t *f, const orc_me_params_t *p, int is_int
 void orc_set_threads(int n)
 {
     if (n > 0) omp_set_num_threads(n);
+}
+
+/* ------------------------------------------------ 8x8 transform (High) */
+
+/* Forward 8x8 integer transform, one dimension: the published core transform
+ * whose inverse is clause 8.5.13.2 (the encoder side of
+ * transform_size_8x8_flag; the reference's encoder has none, its decoder
+ * the inverse, A1/src/h264_recon.c:158-189). */
+static void fwd8_1d(int32_t *d, int st)
+{
+    const int32_t s0 = d[0], s1 = d[st], s2 = d[2 * st], s3 = d[3 * st];
+    const int32_t s4 = d[4 * st], s5 = d[5 * st], s6 = d[6 * st], s7 = d[7 * st];
+    const int32_t a0 = s0 + s7, a1 = s1 + s6, a2 = s2 + s5, a3 = s3 + s4;
+    const int32_t b0 = a0 + a3, b1 = a1 + a2, b2 = a0 - a3, b3 = a1 - a2;
+    const int32_t a4 = s0 - s7, a5 = s1 - s6, a6 = s2 - s5, a7 = s3 - s4;
+    const int32_t b4 = a5 + a6 + ((a4 >> 1) + a4);
+    const int32_t b5 = a4 - a7 - ((a6 >> 1) + a6);
+    const int32_t b6 = a4 + a7 - ((a5 >> 1) + a5);
+    const int32_t b7 = a5 - a6 + ((a7 >> 1) + a7);
+    d[0] = b0 + b1;
+    d[4 * st] = b0 - b1;
+    d[2 * st] = b2 + (b3 >> 1);
+    d[6 * st] = (b2 >> 1) - b3;
+    d[st] = b4 + (b7 >> 2);
+    d[7 * st] = (b4 >> 2) - b7;
+    d[3 * st] = b5 + (b6 >> 2);
+    d[5 * st] = b6 - (b5 >> 2);
+}
+
+/* Position class of raster position p of an 8x8 block (the six classes of
+ * normAdjust8x8, clause 8.5.9 (8-318)). */
+static int cls8(int p)
+{
+    const int i = p >> 3, j = p & 7;
+    if ((i & 3) == 0 && (j & 3) == 0) return 0;
+    if ((i & 1) && (j & 1)) return 1;
+    if ((i & 3) == 2 && (j & 3) == 2) return 2;
+    if (((i & 3) == 0 && (j & 1)) || ((i & 1) && (j & 3) == 0)) return 3;
+    if (((i & 3) == 0 && (j & 3) == 2) || ((i & 3) == 2 && (j & 3) == 0)) return 4;
+    return 5;
+}
+
+/* normAdjust8x8 v[qp % 6][class] (8-318), the decoder's dequantisation
+ * factor / 16 under flat scaling lists, and the encoder's quantisation
+ * multipliers MF8 = round(2^22 / (v * norm)) of the same classes. */
+static const int V8[6][6] = {{20, 18, 32, 19, 25, 24}, {22, 19, 35, 21, 28, 26}, {26, 23, 42, 24, 33, 31},
+                             {28, 25, 45, 26, 35, 33}, {32, 28, 51, 30, 40, 38}, {36, 32, 58, 34, 46, 43}};
+static const int MF8[6][6] = {{13107, 11428, 20972, 12222, 16777, 15481}, {11916, 10826, 19174, 11058, 14980, 14290},
+                              {10082, 8943, 15978, 9675, 12710, 11985},   {9362, 8228, 14913, 8931, 11984, 11259},
+                              {8192, 7346, 13159, 7740, 10486, 9777},     {7282, 6428, 11570, 6830, 9118, 8640}};
+
+void orc_fwd_quant8(const int16_t res[64], int16_t lev[64], int qp, int intra)
+{
+    int32_t t[64];
+    for (int n = 0; n < 64; n++) t[n] = res[n];
+    for (int r = 0; r < 8; r++) fwd8_1d(t + 8 * r, 1);
+    for (int c = 0; c < 8; c++) fwd8_1d(t + c, 8);
+    const int per = qp / 6, rem = qp % 6, sh = 16 + per;
+    const int64_t f = ((int64_t)1 << sh) / (intra ? 3 : 6);
+    for (int n = 0; n < 64; n++) {
+        const int64_t a = t[n] < 0 ? -(int64_t)t[n] : t[n];
+        const int64_t l = (a * MF8[rem][cls8(n)] + f) >> sh;
+        lev[n] = (int16_t)(t[n] < 0 ? -l : l);
+    }
+}
+
+/* Scaling (8.5.13.1, flat lists), the inverse transform (8.5.13.2) and the
+ * add with clipping, onto the 8x8 prediction at dst. */
+void orc_dequant_idct8_add(const int16_t lev[64], uint8_t *dst, int stride, int qp)
+{
+    int32_t t[64];
+    const int per = qp / 6, rem = qp % 6;
+    for (int n = 0; n < 64; n++) {
+        const int32_t ls = 16 * V8[rem][cls8(n)];
+        t[n] = per >= 6 ? (lev[n] * ls) << (per - 6) : (lev[n] * ls + (1 << (5 - per))) >> (6 - per);
+    }
+    for (int pass = 0; pass < 2; pass++)
+        for (int k = 0; k < 8; k++) {
+            int32_t *d = pass == 0 ? t + 8 * k : t + k;
+            const int st = pass == 0 ? 1 : 8;
+            const int32_t a0 = d[0] + d[4 * st], a2 = d[0] - d[4 * st];
+            const int32_t a4 = (d[2 * st] >> 1) - d[6 * st], a6 = (d[6 * st] >> 1) + d[2 * st];
+            const int32_t b0 = a0 + a6, b2 = a2 + a4, b4 = a2 - a4, b6 = a0 - a6;
+            const int32_t a1 = -d[3 * st] + d[5 * st] - d[7 * st] - (d[7 * st] >> 1);
+            const int32_t a3 = d[st] + d[7 * st] - d[3 * st] - (d[3 * st] >> 1);
+            const int32_t a5 = -d[st] + d[7 * st] + d[5 * st] + (d[5 * st] >> 1);
+            const int32_t a7 = d[3 * st] + d[5 * st] + d[st] + (d[st] >> 1);
+            const int32_t b1 = (a7 >> 2) + a1, b3 = a3 + (a5 >> 2), b5 = (a3 >> 2) - a5, b7 = a7 - (a1 >> 2);
+            d[0] = b0 + b7;
+            d[7 * st] = b0 - b7;
+            d[st] = b2 + b5;
+            d[6 * st] = b2 - b5;
+            d[2 * st] = b4 + b3;
+            d[5 * st] = b4 - b3;
+            d[3 * st] = b6 + b1;
+            d[4 * st] = b6 - b1;
+        }
+    for (int y = 0; y < 8; y++)
+        for (int x = 0; x < 8; x++) {
+            const int v = dst[y * stride + x] + ((t[y * 8 + x] + 32) >> 6);
+            dst[y * stride + x] = (uint8_t)(v < 0 ? 0 : (v > 255 ? 255 : v));
+        }
 }

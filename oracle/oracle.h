@@ -136,6 +136,11 @@ void orc_deblock_frame(int mbw, int mbh, int qp, int is_intra,
  * edges); orc_deblock_frame is the raster order 0, 1, 2, 3, ... Returns -1
  * for a step outside the picture. For checking that a parallel schedule
  * keeps the raster order's result. */
+/* orc_deblock_frame with the 8x8 transform in the macroblocks whose t8 byte
+ * is nonzero (t8 NULL: none): their odd luma edges are not filtered and the
+ * coefficient test of a boundary strength looks at the 8x8 block. */
+void orc_deblock_frame_t8(int mbw, int mbh, int qp, int is_intra, const uint32_t *nz, const uint8_t *t8,
+                          const orc_mv_t *mv, uint8_t *ry, uint8_t *ruv, int rp);
 int orc_deblock_steps(int mbw, int mbh, int qp, int is_intra,
                       const uint32_t *nz, const orc_mv_t *mv,
                       uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch,
@@ -153,5 +158,13 @@ void orc_set_threads(int n);
 #ifdef __cplusplus
 }
 #endif
+
+/* H.264 High profile 8x8 transform: forward integer transform and
+ * quantisation with flat scaling lists (the encoder side), and scaling,
+ * inverse transform and the add onto a prediction (clause 8.5.13, the
+ * decoder side, pinned to the reference decoder's h264d_idct8_add).
+ * Coefficients and levels in raster order. */
+void orc_fwd_quant8(const int16_t res[64], int16_t lev[64], int qp, int intra);
+void orc_dequant_idct8_add(const int16_t lev[64], uint8_t *dst, int stride, int qp);
 
 #endif

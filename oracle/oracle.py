@@ -178,6 +178,13 @@ def deblock(mbw, mbh, qp, is_intra, nz, mv, rec_y, rec_uv):
                             _p(np.ascontiguousarray(mv, np.int32)), _p(rec_y), _p(rec_uv), rec_y.shape[1])
 
 
+def deblock_t8(mbw, mbh, qp, is_intra, nz, t8, mv, rec_y, rec_uv):
+    """Deblocking with the 8x8 transform in the macroblocks whose t8 byte is set."""
+    lib().orc_deblock_frame_t8(mbw, mbh, qp, int(is_intra), _p(np.ascontiguousarray(nz, np.uint32)),
+                               _p(np.ascontiguousarray(t8, np.uint8)), _p(np.ascontiguousarray(mv, np.int32)),
+                               _p(rec_y), _p(rec_uv), rec_y.shape[1])
+
+
 def deblock_steps(mbw, mbh, qp, is_intra, nz, mv, rec_y, rec_uv, steps):
     """The deblocking steps (2 * mb + dir) in the given order (oracle.h)."""
     st = np.ascontiguousarray(steps, np.int32)
@@ -210,6 +217,42 @@ def interp_luma(ref_y, RW, RH, qx, qy):
 
 
 # ---------------------------------------------------------------- reference
+
+def fwd_quant8(res, qp, intra):
+    """Forward 8x8 transform + quantisation of int16 [n][64] residual blocks."""
+    res = np.ascontiguousarray(res, np.int16).reshape(-1, 64)
+    lev = np.zeros_like(res)
+    for i in range(res.shape[0]):
+        lib().orc_fwd_quant8(_p(res[i]), _p(lev[i]), qp, int(intra))
+    return lev
+
+
+def dequant_idct8_add(lev, pred, qp):
+    """Scaling + inverse 8x8 + add onto uint8 [8][8] predictions ([n][8][8])."""
+    lev = np.ascontiguousarray(lev, np.int16).reshape(-1, 64)
+    out = np.ascontiguousarray(pred, np.uint8).reshape(-1, 8, 8).copy()
+    for i in range(lev.shape[0]):
+        lib().orc_dequant_idct8_add(_p(lev[i]), _p(out[i]), 8, qp)
+    return out
+
+
+def ref_idct8_add(lev, pred, qp):
+    """The reference decoder's h264d_idct8_add on the same blocks."""
+    lev = np.ascontiguousarray(lev, np.int16).reshape(-1, 64).copy()
+    out = np.ascontiguousarray(pred, np.uint8).reshape(-1, 8, 8).copy()
+    for i in range(lev.shape[0]):
+        ref().refshim_idct8_add(_p(out[i]), 8, _p(lev[i]), qp)
+    return out
+
+
+def ref_deblock_t8(mbw, mbh, qp, is_intra, nz, t8, mv, rec_y, rec_uv):
+    """The reference decoder's deblocking with 8x8-transform macroblocks (t8)."""
+    r = ref().refshim_deblock_nv12_t8(mbw, mbh, qp, int(is_intra), _p(np.ascontiguousarray(nz, np.uint32)),
+                                      _p(np.ascontiguousarray(t8, np.uint8)), _p(np.ascontiguousarray(mv, np.int32)),
+                                      _p(rec_y), _p(rec_uv), rec_y.shape[1])
+    if r != 0:
+        raise RuntimeError("refshim_deblock_nv12_t8 failed")
+
 
 def ref_deblock(mbw, mbh, qp, is_intra, nz, mv, rec_y, rec_uv):
     r = ref().refshim_deblock_nv12(mbw, mbh, qp, int(is_intra), _p(np.ascontiguousarray(nz, np.uint32)),

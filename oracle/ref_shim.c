@@ -7,10 +7,11 @@
  * the CPU baseline. Nothing here is part of the product library.
  *
  * Wrapped reference entry points:
- *   h264d_deblock_picture  A1/src/h264_deblock.c:349
+ *   h264d_deblock_picture  A1/src/h264_deblock.c:349 (also with 8x8-transform macroblocks)
  *   h264d_mc_fetch_luma / h264d_mc_luma    A1/src/h264_mc.c:278
  *   h264d_mc_fetch_chroma / h264d_mc_chroma A1/src/h264_mc.c:344
  *   h264d_dequant_build / h264d_idct4_add   A1/src/h264_recon.c:113
+ *   h264d_idct8_add         A1/src/h264_recon.c:191
  *   cpu_simd_sad_16x16     A1/src/cpu_simd_me.c:136
  *   cpu_simd_me_search_frame A1/src/cpu_simd_me.c:275
  *   h264_intra16_luma_dc_transform A1/src/encoder_h264.c:775
@@ -37,9 +38,11 @@ typedef struct {
 /* Deblock an NV12 picture through the reference decoder's filter, with the
  * macroblock description this encoder emits (all I16x16 or all P16x16 with
  * one reference picture, uniform QP, idc 0, zero offsets). */
-int refshim_deblock_nv12(int mbw, int mbh, int qp, int is_intra,
-                         const uint32_t *nz, const shim_mv_t *mv,
-                         uint8_t *y, uint8_t *uv, int pitch)
+/* The same with the 8x8 transform in the macroblocks whose t8 byte is set
+ * (NULL: none), as the decoder's transform_size_8x8_flag. */
+int refshim_deblock_nv12_t8(int mbw, int mbh, int qp, int is_intra,
+                            const uint32_t *nz, const uint8_t *t8, const shim_mv_t *mv,
+                            uint8_t *y, uint8_t *uv, int pitch)
 {
     const int n = mbw * mbh, cw = mbw * 8, ch = mbh * 8;
     h264d_mb_t *mbs = calloc((size_t)n, sizeof(*mbs));
@@ -51,6 +54,7 @@ int refshim_deblock_nv12(int mbw, int mbh, int qp, int is_intra,
         m->type = is_intra ? H264D_MB_I_16x16 : H264D_MB_P_16x16;
         m->intra = (uint8_t)(is_intra ? 1 : 0);
         m->qpy = (int8_t)qp;
+        m->transform8x8 = (uint8_t)(t8 && t8[i] ? 1 : 0);
         for (int p = 0; p < 4; p++) {
             m->ref[0][p] = is_intra ? -1 : 0;
             m->ref[1][p] = -1;
@@ -77,6 +81,13 @@ int refshim_deblock_nv12(int mbw, int mbh, int qp, int is_intra,
         }
     free(mbs); free(sl); free(cb); free(cr);
     return 0;
+}
+
+int refshim_deblock_nv12(int mbw, int mbh, int qp, int is_intra,
+                         const uint32_t *nz, const shim_mv_t *mv,
+                         uint8_t *y, uint8_t *uv, int pitch)
+{
+    return refshim_deblock_nv12_t8(mbw, mbh, qp, is_intra, nz, NULL, mv, y, uv, pitch);
 }
 
 /* A w x h luma prediction at quarter-pel position (qx, qy) of the top-left
@@ -116,6 +127,19 @@ void refshim_idct4_add(uint8_t *dst, int stride, int16_t block[16], int qp, int 
     memset(&dq, 0, sizeof(dq));
     h264d_dequant_build(&dq, qp, flat4, flat8);
     h264d_idct4_add(dst, stride, block, dq.d4[0], qp, dc_ready != 0);
+}
+
+/* 8x8: the reference decoder's scaling (flat lists) and inverse transform,
+ * added to dst (h264d_idct8_add, A1/src/h264_recon.c:191). */
+void refshim_idct8_add(uint8_t *dst, int stride, int16_t block[64], int qp)
+{
+    static uint8_t flat4[6][16], flat8[6][64];
+    static int init;
+    if (!init) { memset(flat4, 16, sizeof(flat4)); memset(flat8, 16, sizeof(flat8)); init = 1; }
+    h264d_dequant_t dq;
+    memset(&dq, 0, sizeof(dq));
+    h264d_dequant_build(&dq, qp, flat4, flat8);
+    h264d_idct8_add(dst, stride, block, dq.d8[0], qp);
 }
 
 uint32_t refshim_sad16(const uint8_t *a, int pa, const uint8_t *b, int pb)
