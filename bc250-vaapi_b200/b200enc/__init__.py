@@ -31,6 +31,7 @@ EXPORTS = [
     "b200enc_pin_host", "b200enc_unpin_host", "b200enc_deblock_noalloc_status",
     "b200enc_batch_create", "b200enc_batch_destroy", "b200enc_batch_stream", "b200enc_batch_set_graph",
     "b200enc_batch_encode", "b200enc_batch_sync", "b200enc_batch_outputs", "b200enc_batch_graph_stats",
+    "b200enc_h264_t8_forward", "b200enc_h264_t8_recon", "b200enc_deblock_tiles_t8",
     "b200enc_cavlc_scratch_bytes", "b200enc_cavlc_slices", "b200enc_ctx_set_entropy", "b200enc_ctx_slice_nals",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
@@ -84,6 +85,9 @@ def load_library(path=LIB_PATH):
     lib.b200enc_i_frame.argtypes = [_vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i,
                                     _vp, ctypes.c_size_t, _i, _i, _vp]
     lib.b200enc_deblock.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, ctypes.c_size_t, _i, _vp]
+    lib.b200enc_h264_t8_forward.argtypes = [_vp, _vp, _vp, _i, _i, _i, _vp]
+    lib.b200enc_h264_t8_recon.argtypes = [_vp, _vp, _vp, _i, _i, _i, _vp]
+    lib.b200enc_deblock_tiles_t8.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp]
     lib.b200enc_cavlc_scratch_bytes.argtypes = [_i, _i]
     lib.b200enc_cavlc_scratch_bytes.restype = ctypes.c_size_t
     lib.b200enc_cavlc_slices.argtypes = [_vp, _vp]

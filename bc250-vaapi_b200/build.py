@@ -12,7 +12,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "lib", "libb200enc.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["me.cu", "pframe.cu", "intra.cu", "deblock.cu", "gpu_compute_abi.cu", "noalloc.cu", "tc_gemm.cu", "proposal.cu", "proposal_infer.cu", "proposal_infer8.cu", "hevc.cu", "hevc_deblock.cu", "tune.cu", "batch.cu", "cavlc.cu"]
+SOURCES = ["me.cu", "pframe.cu", "intra.cu", "deblock.cu", "gpu_compute_abi.cu", "noalloc.cu", "tc_gemm.cu", "proposal.cu", "proposal_infer.cu", "proposal_infer8.cu", "hevc.cu", "hevc_deblock.cu", "tune.cu", "batch.cu", "cavlc.cu", "t8x8.cu"]
 
 
 def sources():

@@ -492,6 +492,31 @@ int b200enc_hevc_deblock(const b200enc_hevc_deblock_t *p, void *stream);
  * incomplete and must not be used), -1 = the read failed. */
 int b200enc_wavefront_status(const void *scratch, void *stream);
 
+/* H.264 High-profile 8x8 luma transform (transform_size_8x8_flag). No
+ * counterpart in the reference's encoder, which codes 4x4 transforms only;
+ * the decoder half is its decoder's h264d_idct8_add (src/h264_recon.c:191).
+ * b200enc_h264_t8_forward: forward integer transform and quantisation (flat
+ * scaling lists; intra rounding 1/3 or inter 1/6) of n residual blocks,
+ * int16 [n][64] raster, into levels int16 [n][64]; nz[n] (may be NULL) gets
+ * each block's nonzero mask (bit p = level p != 0). Both arrays 16-byte
+ * aligned. b200enc_h264_t8_recon: scaling (clause 8.5.13.1, flat lists),
+ * inverse transform (8.5.13.2) and the add with clipping onto the 8x8
+ * prediction at plane + xy[i][1] * pitch + xy[i][0], replaced by the
+ * reconstruction (blocks must not overlap). Device pointers; asynchronous on
+ * `stream`; -1 for bad arguments. */
+int b200enc_h264_t8_forward(const int16_t *residual, int16_t *levels, unsigned long long *nz, int n, int qp,
+                            int intra, void *stream);
+int b200enc_h264_t8_recon(const int16_t *levels, const int32_t *xy, uint8_t *plane, int pitch, int n, int qp,
+                          void *stream);
+/* b200enc_deblock_tiles with 8x8-transform macroblocks: t8[mb] nonzero marks
+ * a macroblock coded with transform_size_8x8_flag (its odd internal luma
+ * edges are not filtered, the coefficient test of a boundary strength looks
+ * at its 8x8 blocks: src/h264_deblock.c:119-137, 294, 324); t8 device memory
+ * [mbw * mbh] or NULL. */
+int b200enc_deblock_tiles_t8(int mbw, int mbh, int qp, int is_intra, const uint32_t *nz, const uint8_t *t8,
+                             const void *mv, const uint8_t *src_y, const uint8_t *src_uv, uint8_t *dst_y,
+                             uint8_t *dst_uv, int pitch, uint32_t *status, void *stream);
+
 /* CAVLC slice data on the GPU: every slice of one picture coded exactly as
  * the reference's host encoder codes it (its CAVLC macroblock loop,
  * src/encoder_h264.c:3128-3290: I16x16 macroblocks in I slices, P_Skip runs
