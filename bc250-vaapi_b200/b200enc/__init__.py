@@ -31,7 +31,7 @@ EXPORTS = [
     "b200enc_pin_host", "b200enc_unpin_host", "b200enc_deblock_noalloc_status",
     "b200enc_batch_create", "b200enc_batch_destroy", "b200enc_batch_stream", "b200enc_batch_set_graph",
     "b200enc_batch_encode", "b200enc_batch_sync", "b200enc_batch_outputs", "b200enc_batch_graph_stats",
-    "b200enc_h264_t8_forward", "b200enc_h264_t8_recon", "b200enc_deblock_tiles_t8",
+    "b200enc_h264_t8_forward", "b200enc_h264_t8_recon", "b200enc_deblock_tiles_t8", "b200enc_p_frame_t8",
     "b200enc_cavlc_scratch_bytes", "b200enc_cavlc_slices", "b200enc_ctx_set_entropy", "b200enc_ctx_slice_nals",
     # include/gpu_compute.h
     "bc250_gpu_init", "bc250_gpu_destroy", "gpu_compute_init", "gpu_compute_terminate",
@@ -85,6 +85,8 @@ def load_library(path=LIB_PATH):
     lib.b200enc_i_frame.argtypes = [_vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i,
                                     _vp, ctypes.c_size_t, _i, _i, _vp]
     lib.b200enc_deblock.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, ctypes.c_size_t, _i, _vp]
+    lib.b200enc_p_frame_t8.argtypes = [_vp, _vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp,
+                                       _vp, _i, _i, _vp]
     lib.b200enc_h264_t8_forward.argtypes = [_vp, _vp, _vp, _i, _i, _i, _vp]
     lib.b200enc_h264_t8_recon.argtypes = [_vp, _vp, _vp, _i, _i, _i, _vp]
     lib.b200enc_deblock_tiles_t8.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp]
@@ -396,11 +398,12 @@ class CavlcParams(ctypes.Structure):
     _fields_ = [("mbw", _i), ("mbh", _i), ("qp", _i), ("is_intra", _i), ("num_slices", _i), ("quality_level", _i),
                 ("levels", _vp), ("dc", _vp), ("nz", _vp), ("pred_mode", _vp), ("mv", _vp),
                 ("header", _vp), ("header_bits", _vp), ("out", _vp), ("slice_cap", ctypes.c_size_t),
-                ("out_bytes", _vp), ("out_copy", _vp), ("scratch", _vp), ("scratch_bytes", ctypes.c_size_t)]
+                ("out_bytes", _vp), ("out_copy", _vp), ("scratch", _vp), ("scratch_bytes", ctypes.c_size_t),
+                ("transform8x8", _i)]
 
 
 def cavlc_slices(mbw, mbh, qp, is_intra, num_slices, levels, dc, nz, pred_mode, mv, headers=None,
-                 quality_level=4, slice_cap=None, stream=None):
+                 quality_level=4, slice_cap=None, stream=None, transform8x8=0):
     """CAVLC slice data of one picture on the GPU from device pointers (ints)
     to its staged outputs; headers: None or a list of (bits, nbits) per
     slice, bits an int holding nbits (<= 128) header bits. Returns a list of
@@ -426,7 +429,7 @@ def cavlc_slices(mbw, mbh, qp, is_intra, num_slices, levels, dc, nz, pred_mode, 
                       _vp(pred_mode) if pred_mode else None, _vp(mv),
                       _vp(hdr.ctypes.data) if hdr is not None else None,
                       _vp(hb.ctypes.data) if hb is not None else None, _vp(out.data_ptr()), cap,
-                      _vp(nbytes.data_ptr()), None, _vp(sp), sb)
+                      _vp(nbytes.data_ptr()), None, _vp(sp), sb, int(transform8x8))
     _check(L.b200enc_cavlc_slices(ctypes.byref(prm), _stream(stream)), "b200enc_cavlc_slices")
     torch.cuda.synchronize()
     n = nbytes.cpu().numpy().view(np.uint32)

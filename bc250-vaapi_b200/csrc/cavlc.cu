@@ -32,6 +32,7 @@
 #include "b200enc_internal.h"
 #include "cavlc_core.h"
 #include "common.cuh"
+#include "t8x8.cuh"
 
 namespace b200enc {
 
@@ -54,6 +55,7 @@ struct CavlcHdr {
 
 struct CavlcArgs {
   int mbw, mbh, qp, is_intra, ns, quality;
+  int t8;  // P macroblocks code their luma with the 8x8 transform (levels in 8x8 raster order)
   const int16_t* levels;
   const int32_t* dc;
   const uint32_t* nz;
@@ -300,7 +302,8 @@ __global__ void __launch_bounds__(32 * kCavlcMbWarps) cavlc_mb_kernel(CavlcArgs 
     } else {
       int px, py;
       mv_pred(a.mv, mbx, mby, a.mbw, start, &px, &py);
-      put_p16_header(b, a.mv[mb].mvx - px, a.mv[mb].mvy - py, (int)((info >> 1) & 15u) | (cbp_c << 4));
+      put_p16_header(b, a.mv[mb].mvx - px, a.mv[mb].mvy - py, (int)((info >> 1) & 15u) | (cbp_c << 4),
+                     a.t8);
     }
   } else if (lane == 1) {
     if (intra) {
@@ -311,8 +314,15 @@ __global__ void __launch_bounds__(32 * kCavlcMbWarps) cavlc_mb_kernel(CavlcArgs 
   } else if (lane < 18) {
     const int k = lane - 2;
     const bool coded = intra ? ((info >> 1) & 1u) : ((info >> (1 + (k >> 2))) & 1u);
-    if (coded)
+    if (coded && a.t8 && !intra) {
+      // 8x8 block k >> 2 as its 4x4 block k & 3: scan positions (k & 3) + 4j (7.3.5.3.2)
+      int sc[16];
+      const int16_t* l8 = lv + 64 * (k >> 2);
+      for (int j = 0; j < 16; ++j) sc[j] = l8[kZigzag8[4 * j + (k & 3)]];
+      put_block(b, sc, 16, nc_class(luma_nc(a.tcs, mb, mbx, mby, a.mbw, start, k)));
+    } else if (coded) {
       put_4x4(b, lv + (kBlkY4[k] * 4 + kBlkX4[k]) * 16, intra, luma_nc(a.tcs, mb, mbx, mby, a.mbw, start, k));
+    }
   } else if (lane < 20) {
     if (cbp_c >= 1) {
       const QP qc = make_qp(chroma_qp(a.qp), intra);
@@ -607,6 +617,7 @@ extern "C" int b200enc_cavlc_slices(const b200enc_cavlc_t* p, void* stream) {
   a.is_intra = p->is_intra ? 1 : 0;
   a.ns = p->num_slices;
   a.quality = p->quality_level;
+  a.t8 = p->transform8x8 ? 1 : 0;
   a.levels = p->levels;
   a.dc = p->dc;
   a.nz = p->nz;

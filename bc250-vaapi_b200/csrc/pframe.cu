@@ -13,6 +13,7 @@
 // warps, so the chroma DC exchange stays inside warp 2.
 #include "b200enc_internal.h"
 #include "common.cuh"
+#include "t8x8.cuh"
 
 namespace b200enc {
 
@@ -33,6 +34,7 @@ struct PShared {
   int32_t dcval[8];        // dequantized chroma DC per chroma block
   alignas(16) uint8_t ry[16][16];  // reconstructed luma
   alignas(16) uint8_t ruv[8][16];  // reconstructed chroma (NV12)
+  int32_t t8[4][65];               // 8x8 luma transform: the four blocks between their row and column passes
 };
 
 // Horizontal / vertical 6-tap raw sums on a staged patch `p` (row pitch ps)
@@ -113,7 +115,8 @@ __global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict_
                                                   const MV* __restrict__ mvs, int16_t* __restrict__ levels_,
                                                   int32_t* __restrict__ dc_, uint32_t* __restrict__ nzm_,
                                                   uint32_t* __restrict__ pred_mode_, uint8_t* __restrict__ rec_y_,
-                                                  uint8_t* __restrict__ rec_uv_, int rec_pitch_, BatchTab bt) {
+                                                  uint8_t* __restrict__ rec_uv_, int rec_pitch_, BatchTab bt,
+                                                  int t8 = 0) {
   extern __shared__ __align__(16) uint8_t p_smem[];
   PShared& s = reinterpret_cast<PShared*>(p_smem)[threadIdx.y];
   const int tid = threadIdx.x;
@@ -223,29 +226,80 @@ __global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict_
   __syncthreads();
 
   // ---- forward + quant: quad (b, r) owns row r of block b ---------------
+  // (with the 8x8 luma transform, warp 0 codes the four 8x8 luma blocks
+  // instead and warp 1 has no luma block; chroma is the same)
   const int b = tid >> 2, r = tid & 3;
   const bool luma = b < 16;
+  const bool quad = !(t8 && luma);
   const QP q = make_qp(luma ? qp : chroma_qp(qp), false);
   int x[4];
+  if (quad) {
 #pragma unroll
-  for (int i = 0; i < 4; ++i) x[i] = s.res[b][4 * r + i];
-  quad_forward(x, r);  // x[i] = coef[i][r]
-  uint32_t nz = 0;
+    for (int i = 0; i < 4; ++i) x[i] = s.res[b][4 * r + i];
+    quad_forward(x, r);  // x[i] = coef[i][r]
+    uint32_t nz = 0;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int pos = 4 * i + r;
-    const int l = quant_ac(x[i], pos, q);
-    s.lev[b][pos] = (int16_t)clampi(l, -32768, 32767);
-    nz |= (l != 0 ? 1u : 0u) << pos;
-  }
-  nz |= __shfl_xor_sync(0xffffffffu, nz, 1);
-  nz |= __shfl_xor_sync(0xffffffffu, nz, 2);
-  if (r == 0) {
-    if (active) {
-      nzm[(size_t)mb * 24 + b] = nz;
-      dc[(size_t)mb * 24 + b] = x[0];
+    for (int i = 0; i < 4; ++i) {
+      const int pos = 4 * i + r;
+      const int l = quant_ac(x[i], pos, q);
+      s.lev[b][pos] = (int16_t)clampi(l, -32768, 32767);
+      nz |= (l != 0 ? 1u : 0u) << pos;
     }
-    if (!luma) s.cdc[b - 16] = x[0];
+    nz |= __shfl_xor_sync(0xffffffffu, nz, 1);
+    nz |= __shfl_xor_sync(0xffffffffu, nz, 2);
+    if (r == 0) {
+      if (active) {
+        nzm[(size_t)mb * 24 + b] = nz;
+        dc[(size_t)mb * 24 + b] = x[0];
+      }
+      if (!luma) s.cdc[b - 16] = x[0];
+    }
+  }
+  // 8x8 luma (warp 0): block q8 = tid >> 3 (raster of the four), thread k8
+  // owns its row k8, then its column k8. Levels in raster order at
+  // lev[0..255] (block q8 at 64 * q8); the nz word of 4x4 block 4 * q8 + i
+  // (spec order) holds the nonzero mask of the 16 levels CAVLC codes as that
+  // block: 8x8 scan positions i, i + 4, ... (7.3.5.3.2).
+  const int q8 = tid >> 3, k8 = tid & 7, qx = 8 * (q8 & 1), qy = 8 * (q8 >> 1);
+  const int per8 = qp / 6, rem8 = qp - 6 * per8;
+  if (t8 && tid < 32) {
+    auto res_at = [&](int xx, int yy) { return (int)s.res[(yy >> 2) * 4 + (xx >> 2)][(yy & 3) * 4 + (xx & 3)]; };
+    int v[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) v[c] = res_at(qx + c, qy + k8);
+    fwd8(v);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) s.t8[q8][8 * k8 + c] = v[c];
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = s.t8[q8][8 * i + k8];
+    fwd8(v);
+    const int sh = 16 + per8;
+    const long long f = (1ll << sh) / 6;  // inter rounding
+    uint32_t m[4] = {0u, 0u, 0u, 0u};
+    int16_t* lev8 = &s.lev[0][0] + 64 * q8;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int l = quant8(v[i], i, k8, rem8, sh, f);
+      lev8[8 * i + k8] = (int16_t)clampi(l, -32768, 32767);
+      const int z = kZigzag8Inv[8 * i + k8];
+      m[z & 3] |= (l != 0 ? 1u : 0u) << (z >> 2);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      m[j] |= __shfl_xor_sync(0xffffffffu, m[j], 1);
+      m[j] |= __shfl_xor_sync(0xffffffffu, m[j], 2);
+      m[j] |= __shfl_xor_sync(0xffffffffu, m[j], 4);
+    }
+    if (k8 == 0 && active) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        // spec block 4 * q8 + i -> raster: quadrant origin (qx / 4, qy / 4) + (i & 1, i >> 1)
+        const int rb = (qy / 4 + (i >> 1)) * 4 + qx / 4 + (i & 1);
+        nzm[(size_t)mb * 24 + rb] = m[i];
+        dc[(size_t)mb * 24 + rb] = 0;
+      }
+    }
   }
   __syncwarp();
   // chroma DC Hadamard + quant + inverse + dequant (reconstruct.comp:393-414),
@@ -263,19 +317,39 @@ __global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict_
   __syncwarp();
 
   // ---- dequant + inverse + recon ----------------------------------------
-  int d[4];
+  if (t8 && tid < 32) {  // 8x8 luma: scaling + inverse (8.5.13) onto the prediction
+    const int16_t* lev8 = &s.lev[0][0] + 64 * q8;
+    int v[8];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) d[i] = dequant_ac(s.lev[b][4 * r + i], 4 * r + i, q);
-  if (r == 0) {
-    if (!luma) d[0] = s.dcval[b - 16];
-    d[0] += 32;
+    for (int c = 0; c < 8; ++c) v[c] = scale8(lev8[8 * k8 + c], k8, c, per8, rem8);
+    inv8(v);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) s.t8[q8][8 * k8 + c] = v[c];
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = s.t8[q8][8 * i + k8];
+    inv8(v);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int yy = qy + i, xx = qx + k8;
+      s.ry[yy][xx] = (uint8_t)clip1(s.pred[(yy >> 2) * 4 + (xx >> 2)][(yy & 3) * 4 + (xx & 3)] + ((v[i] + 32) >> 6));
+    }
   }
-  quad_inverse(d, r);  // d[i] = res[i][r]
-  if (luma) {
+  int d[4];
+  if (quad) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) d[i] = dequant_ac(s.lev[b][4 * r + i], 4 * r + i, q);
+    if (r == 0) {
+      if (!luma) d[0] = s.dcval[b - 16];
+      d[0] += 32;
+    }
+    quad_inverse(d, r);  // d[i] = res[i][r]
+  }
+  if (quad && luma) {
     const int bx = b & 3, by = b >> 2;
 #pragma unroll
     for (int i = 0; i < 4; ++i) s.ry[4 * by + i][4 * bx + r] = (uint8_t)clip1(s.pred[b][4 * i + r] + d[i]);
-  } else {
+  } else if (quad) {
     const int pl = (b - 16) >> 2, sub = (b - 16) & 3;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -319,10 +393,23 @@ __global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict_
 
 using namespace b200enc;
 
+extern "C" int b200enc_p_frame_t8(const uint8_t* cur_y, const uint8_t* cur_uv, int cur_pitch, const uint8_t* ref_y,
+                                  const uint8_t* ref_uv, int ref_pitch, int W, int H, int RW, int RH, int qp,
+                                  const void* mv, int16_t* levels, int32_t* dc, uint32_t* nz, uint32_t* pred_mode,
+                                  uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch, int t8, void* stream);
+
 extern "C" int b200enc_p_frame(const uint8_t* cur_y, const uint8_t* cur_uv, int cur_pitch, const uint8_t* ref_y,
                                const uint8_t* ref_uv, int ref_pitch, int W, int H, int RW, int RH, int qp,
                                const void* mv, int16_t* levels, int32_t* dc, uint32_t* nz, uint32_t* pred_mode,
                                uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch, void* stream) {
+  return b200enc_p_frame_t8(cur_y, cur_uv, cur_pitch, ref_y, ref_uv, ref_pitch, W, H, RW, RH, qp, mv, levels, dc,
+                            nz, pred_mode, rec_y, rec_uv, rec_pitch, 0, stream);
+}
+
+extern "C" int b200enc_p_frame_t8(const uint8_t* cur_y, const uint8_t* cur_uv, int cur_pitch, const uint8_t* ref_y,
+                                  const uint8_t* ref_uv, int ref_pitch, int W, int H, int RW, int RH, int qp,
+                                  const void* mv, int16_t* levels, int32_t* dc, uint32_t* nz, uint32_t* pred_mode,
+                                  uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch, int t8, void* stream) {
   if (!cur_y || !cur_uv || !ref_y || !ref_uv || !mv || !levels || !dc || !nz || !pred_mode || !rec_y || !rec_uv)
     return -1;
   if (qp < 0 || qp > 51 || W <= 0 || H <= 0 || RW <= 1 || RH <= 1) return -1;
@@ -333,7 +420,7 @@ extern "C" int b200enc_p_frame(const uint8_t* cur_y, const uint8_t* cur_uv, int 
   const int T = b200enc_tuned(B200ENC_TUNE_PCHAIN_MBS_PER_CTA) > 0 ? b200enc_tuned(B200ENC_TUNE_PCHAIN_MBS_PER_CTA) : 1;
   p_mb_kernel<false><<<dim3((g.mbw + T - 1) / T, g.mbh), dim3(96, T), T * sizeof(PShared), (cudaStream_t)stream>>>(
       cur_y, cur_uv, cur_pitch, ref_y, ref_uv, ref_pitch, g, qp, (const MV*)mv, levels, dc, nz, pred_mode, rec_y,
-      rec_uv, rec_pitch, BatchTab{});
+      rec_uv, rec_pitch, BatchTab{}, t8 ? 1 : 0);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -492,6 +492,21 @@ int b200enc_hevc_deblock(const b200enc_hevc_deblock_t *p, void *stream);
  * incomplete and must not be used), -1 = the read failed. */
 int b200enc_wavefront_status(const void *scratch, void *stream);
 
+/* b200enc_p_frame with t8 != 0: the luma of every macroblock through the 8x8
+ * transform (High profile, transform_size_8x8_flag) instead of sixteen 4x4
+ * ones; chroma unchanged. Levels: the four 8x8 luma blocks in raster order
+ * at levels[mb][0..255] (block q at 64 q, raster within), chroma at
+ * [256..383] as before; the nz word of 4x4 block 4q + i (spec order) holds
+ * the nonzero mask of the 16 levels CAVLC codes as that block (8x8 scan
+ * positions i, i + 4, ..., 7.3.5.3.2). No reference counterpart (the
+ * reference's encoder codes 4x4 only); its decoder reconstructs the same
+ * pictures from such levels. */
+int b200enc_p_frame_t8(const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
+                       const uint8_t *ref_y, const uint8_t *ref_uv, int ref_pitch,
+                       int W, int H, int RW, int RH, int qp, const void *mv,
+                       int16_t *levels, int32_t *dc, uint32_t *nz, uint32_t *pred_mode,
+                       uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch, int t8, void *stream);
+
 /* H.264 High-profile 8x8 luma transform (transform_size_8x8_flag). No
  * counterpart in the reference's encoder, which codes 4x4 transforms only;
  * the decoder half is its decoder's h264d_idct8_add (src/h264_recon.c:191).
@@ -549,6 +564,8 @@ typedef struct {
                                     only each slice's bytes cross the bus */
     void *scratch;               /* device, 256-byte aligned */
     size_t scratch_bytes;        /* >= b200enc_cavlc_scratch_bytes(mbw, mbh) */
+    int transform8x8;            /* P slices: the luma of coded macroblocks uses the 8x8 transform (levels and nz
+                                    words as b200enc_p_frame_t8 leaves them; transform_size_8x8_flag is written) */
 } b200enc_cavlc_t;
 size_t b200enc_cavlc_scratch_bytes(int mbw, int mbh);
 int b200enc_cavlc_slices(const b200enc_cavlc_t *p, void *stream);
