@@ -86,7 +86,7 @@ def load_library(path=LIB_PATH):
                                     _vp, ctypes.c_size_t, _i, _i, _vp]
     lib.b200enc_deblock.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, ctypes.c_size_t, _i, _vp]
     lib.b200enc_p_frame_t8.argtypes = [_vp, _vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp,
-                                       _vp, _i, _i, _vp]
+                                       _vp, _i, _i, _vp, _vp]
     lib.b200enc_h264_t8_forward.argtypes = [_vp, _vp, _vp, _i, _i, _i, _vp]
     lib.b200enc_h264_t8_recon.argtypes = [_vp, _vp, _vp, _i, _i, _i, _vp]
     lib.b200enc_deblock_tiles_t8.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp]
@@ -273,6 +273,15 @@ def p_frame(cur, ref, W, H, RW, RH, qp, mv, out, rec, stream=None):
                                  rec.uvp(), rec.pitch, _stream(stream)), "b200enc_p_frame")
 
 
+def p_frame_t8(cur, ref, W, H, RW, RH, qp, mv, out, rec, t8, t8_flags=None, stream=None):
+    """The P chain with the 8x8 luma transform: t8 1 for every macroblock, 2
+    chosen per macroblock (t8_flags: a device uint8 tensor [mbs] or None)."""
+    _check(lib().b200enc_p_frame_t8(cur.yp(), cur.uvp(), cur.pitch, ref.yp(), ref.uvp(), ref.pitch, W, H, RW, RH, qp,
+                                    _p(mv), _p(out.levels), _p(out.dc), _p(out.nz), _p(out.pred_mode), rec.yp(),
+                                    rec.uvp(), rec.pitch, int(t8), _p(t8_flags) if t8_flags is not None else None,
+                                    _stream(stream)), "b200enc_p_frame_t8")
+
+
 def scratch(mbh, device="cuda"):
     import torch
     n = lib().b200enc_wavefront_scratch_bytes(mbh)
@@ -399,11 +408,11 @@ class CavlcParams(ctypes.Structure):
                 ("levels", _vp), ("dc", _vp), ("nz", _vp), ("pred_mode", _vp), ("mv", _vp),
                 ("header", _vp), ("header_bits", _vp), ("out", _vp), ("slice_cap", ctypes.c_size_t),
                 ("out_bytes", _vp), ("out_copy", _vp), ("scratch", _vp), ("scratch_bytes", ctypes.c_size_t),
-                ("transform8x8", _i)]
+                ("transform8x8", _i), ("t8_flags", _vp)]
 
 
 def cavlc_slices(mbw, mbh, qp, is_intra, num_slices, levels, dc, nz, pred_mode, mv, headers=None,
-                 quality_level=4, slice_cap=None, stream=None, transform8x8=0):
+                 quality_level=4, slice_cap=None, stream=None, transform8x8=0, t8_flags=None):
     """CAVLC slice data of one picture on the GPU from device pointers (ints)
     to its staged outputs; headers: None or a list of (bits, nbits) per
     slice, bits an int holding nbits (<= 128) header bits. Returns a list of
@@ -429,7 +438,8 @@ def cavlc_slices(mbw, mbh, qp, is_intra, num_slices, levels, dc, nz, pred_mode, 
                       _vp(pred_mode) if pred_mode else None, _vp(mv),
                       _vp(hdr.ctypes.data) if hdr is not None else None,
                       _vp(hb.ctypes.data) if hb is not None else None, _vp(out.data_ptr()), cap,
-                      _vp(nbytes.data_ptr()), None, _vp(sp), sb, int(transform8x8))
+                      _vp(nbytes.data_ptr()), None, _vp(sp), sb, int(transform8x8),
+                      _vp(t8_flags) if t8_flags else None)
     _check(L.b200enc_cavlc_slices(ctypes.byref(prm), _stream(stream)), "b200enc_cavlc_slices")
     torch.cuda.synchronize()
     n = nbytes.cpu().numpy().view(np.uint32)

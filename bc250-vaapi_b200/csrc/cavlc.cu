@@ -56,6 +56,7 @@ struct CavlcHdr {
 struct CavlcArgs {
   int mbw, mbh, qp, is_intra, ns, quality;
   int t8;  // P macroblocks code their luma with the 8x8 transform (levels in 8x8 raster order)
+  const uint8_t* t8f;  // NULL, or per macroblock: 0 = this one codes 4x4 blocks after all
   const int16_t* levels;
   const int32_t* dc;
   const uint32_t* nz;
@@ -303,7 +304,7 @@ __global__ void __launch_bounds__(32 * kCavlcMbWarps) cavlc_mb_kernel(CavlcArgs 
       int px, py;
       mv_pred(a.mv, mbx, mby, a.mbw, start, &px, &py);
       put_p16_header(b, a.mv[mb].mvx - px, a.mv[mb].mvy - py, (int)((info >> 1) & 15u) | (cbp_c << 4),
-                     a.t8);
+                     a.t8, !a.t8f || a.t8f[mb]);
     }
   } else if (lane == 1) {
     if (intra) {
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(32 * kCavlcMbWarps) cavlc_mb_kernel(CavlcArgs 
   } else if (lane < 18) {
     const int k = lane - 2;
     const bool coded = intra ? ((info >> 1) & 1u) : ((info >> (1 + (k >> 2))) & 1u);
-    if (coded && a.t8 && !intra) {
+    if (coded && a.t8 && !intra && (!a.t8f || a.t8f[mb])) {
       // 8x8 block k >> 2 as its 4x4 block k & 3: scan positions (k & 3) + 4j (7.3.5.3.2)
       int sc[16];
       const int16_t* l8 = lv + 64 * (k >> 2);
@@ -618,6 +619,7 @@ extern "C" int b200enc_cavlc_slices(const b200enc_cavlc_t* p, void* stream) {
   a.ns = p->num_slices;
   a.quality = p->quality_level;
   a.t8 = p->transform8x8 ? 1 : 0;
+  a.t8f = p->t8_flags;
   a.levels = p->levels;
   a.dc = p->dc;
   a.nz = p->nz;

@@ -332,12 +332,15 @@ CAVLC_HD void put_i16_header(BitW& b, int mode, int chroma_mode, int cbp_chroma,
 }
 // t8: the macroblock's luma uses the 8x8 transform (transform_size_8x8_flag,
 // present when the luma pattern is nonzero, 7.3.5).
-CAVLC_HD void put_p16_header(BitW& b, int mvd_x, int mvd_y, int cbp, int t8 = 0) {
+// t8_mode: the picture parameter set has transform_8x8_mode_flag, so every
+// macroblock with a coded luma block carries transform_size_8x8_flag (t8,
+// 7.3.5: 0 for a macroblock coded with 4x4 transforms).
+CAVLC_HD void put_p16_header(BitW& b, int mvd_x, int mvd_y, int cbp, int t8_mode = 0, int t8 = 0) {
   put_ue(b, 0u);
   put_se(b, mvd_x);
   put_se(b, mvd_y);
   put_ue(b, B200_CAVLC_TAB(cbp_code)[cbp]);
-  if (t8 && (cbp & 15)) put(b, 1, 1u);
+  if (t8_mode && (cbp & 15)) put(b, 1, t8 ? 1u : 0u);
   if (cbp > 0) put_se(b, 0);
 }
 

@@ -35,6 +35,7 @@ struct PShared {
   alignas(16) uint8_t ry[16][16];  // reconstructed luma
   alignas(16) uint8_t ruv[8][16];  // reconstructed chroma (NV12)
   int32_t t8[4][65];               // 8x8 luma transform: the four blocks between their row and column passes
+  int32_t cost[3];                 // 4x4 (two warps' halves) and 8x8 Hadamard costs of the luma residual
 };
 
 // Horizontal / vertical 6-tap raw sums on a staged patch `p` (row pitch ps)
@@ -116,7 +117,7 @@ __global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict_
                                                   int32_t* __restrict__ dc_, uint32_t* __restrict__ nzm_,
                                                   uint32_t* __restrict__ pred_mode_, uint8_t* __restrict__ rec_y_,
                                                   uint8_t* __restrict__ rec_uv_, int rec_pitch_, BatchTab bt,
-                                                  int t8 = 0) {
+                                                  int t8 = 0, uint8_t* __restrict__ t8_flags = nullptr) {
   extern __shared__ __align__(16) uint8_t p_smem[];
   PShared& s = reinterpret_cast<PShared*>(p_smem)[threadIdx.y];
   const int tid = threadIdx.x;
@@ -225,12 +226,74 @@ __global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict_
   }
   __syncthreads();
 
+  // ---- 4x4 or 8x8 luma transform (t8 = 2: chosen per macroblock) --------
+  // The residual's cost under each size, on the scale of a SAD: 4x4 blocks
+  // (sum |H4 R H4|) / 2 - quads of warps 0-1, row r of block b, the column
+  // pass across the quad by shuffles - and 8x8 blocks (sum |H8 R H8| + 2) / 4
+  // - warp 2, eight lanes per block, transposed through s.t8. H4 and H8 are
+  // unnormalised Walsh-Hadamard matrices; any row order gives the same sums.
+  bool use8 = t8 == 1;
+  if (t8 == 2) {
+    if (tid < 64) {
+      const int bb = tid >> 2, rr = tid & 3;
+      int h[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) h[i] = s.res[bb][4 * rr + i];
+      const int a0 = h[0] + h[1], a1 = h[0] - h[1], a2 = h[2] + h[3], a3 = h[2] - h[3];
+      h[0] = a0 + a2;
+      h[1] = a1 + a3;
+      h[2] = a0 - a2;
+      h[3] = a1 - a3;
+      int sum = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int o1 = __shfl_xor_sync(0xffffffffu, h[i], 1);
+        const int u = (rr & 1) ? o1 - h[i] : h[i] + o1;
+        const int o2 = __shfl_xor_sync(0xffffffffu, u, 2);
+        const int w = (rr & 2) ? o2 - u : u + o2;
+        sum += abs(w);
+      }
+      sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+      sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+      int c = rr == 0 ? sum >> 1 : 0;
+#pragma unroll
+      for (int o = 4; o < 32; o <<= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+      if ((tid & 31) == 0) s.cost[tid >> 5] = c;
+    } else {
+      const int ln = tid - 64, qq = ln >> 3, kk = ln & 7, ox = 8 * (qq & 1), oy = 8 * (qq >> 1);
+      int v[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int xx = ox + c, yy = oy + kk;
+        v[c] = s.res[(yy >> 2) * 4 + (xx >> 2)][(yy & 3) * 4 + (xx & 3)];
+      }
+      had8(v);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) s.t8[qq][8 * kk + c] = v[c];
+      __syncwarp();
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = s.t8[qq][8 * i + kk];
+      had8(v);
+      int sum = 0;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) sum += abs(v[i]);
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      int c = kk == 0 ? (sum + 2) >> 2 : 0;
+      c += __shfl_xor_sync(0xffffffffu, c, 8);
+      c += __shfl_xor_sync(0xffffffffu, c, 16);
+      if (ln == 0) s.cost[2] = c;
+    }
+    __syncthreads();
+    use8 = s.cost[2] < s.cost[0] + s.cost[1];
+  }
+
   // ---- forward + quant: quad (b, r) owns row r of block b ---------------
   // (with the 8x8 luma transform, warp 0 codes the four 8x8 luma blocks
   // instead and warp 1 has no luma block; chroma is the same)
   const int b = tid >> 2, r = tid & 3;
   const bool luma = b < 16;
-  const bool quad = !(t8 && luma);
+  const bool quad = !(use8 && luma);
   const QP q = make_qp(luma ? qp : chroma_qp(qp), false);
   int x[4];
   if (quad) {
@@ -262,7 +325,7 @@ __global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict_
   // block: 8x8 scan positions i, i + 4, ... (7.3.5.3.2).
   const int q8 = tid >> 3, k8 = tid & 7, qx = 8 * (q8 & 1), qy = 8 * (q8 >> 1);
   const int per8 = qp / 6, rem8 = qp - 6 * per8;
-  if (t8 && tid < 32) {
+  if (use8 && tid < 32) {
     auto res_at = [&](int xx, int yy) { return (int)s.res[(yy >> 2) * 4 + (xx >> 2)][(yy & 3) * 4 + (xx & 3)]; };
     int v[8];
 #pragma unroll
@@ -317,7 +380,7 @@ __global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict_
   __syncwarp();
 
   // ---- dequant + inverse + recon ----------------------------------------
-  if (t8 && tid < 32) {  // 8x8 luma: scaling + inverse (8.5.13) onto the prediction
+  if (use8 && tid < 32) {  // 8x8 luma: scaling + inverse (8.5.13) onto the prediction
     const int16_t* lev8 = &s.lev[0][0] + 64 * q8;
     int v[8];
 #pragma unroll
@@ -386,6 +449,7 @@ __global__ void __launch_bounds__(384, 4) p_mb_kernel(const uint8_t* __restrict_
     }
   } else if (tid == 72) {
     pred_mode[mb] = 2u;  // residual_predict.comp:422
+    if (t8_flags) t8_flags[mb] = use8 ? 1u : 0u;
   }
 }
 
@@ -396,20 +460,23 @@ using namespace b200enc;
 extern "C" int b200enc_p_frame_t8(const uint8_t* cur_y, const uint8_t* cur_uv, int cur_pitch, const uint8_t* ref_y,
                                   const uint8_t* ref_uv, int ref_pitch, int W, int H, int RW, int RH, int qp,
                                   const void* mv, int16_t* levels, int32_t* dc, uint32_t* nz, uint32_t* pred_mode,
-                                  uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch, int t8, void* stream);
+                                  uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch, int t8, uint8_t* t8_flags,
+                                  void* stream);
 
 extern "C" int b200enc_p_frame(const uint8_t* cur_y, const uint8_t* cur_uv, int cur_pitch, const uint8_t* ref_y,
                                const uint8_t* ref_uv, int ref_pitch, int W, int H, int RW, int RH, int qp,
                                const void* mv, int16_t* levels, int32_t* dc, uint32_t* nz, uint32_t* pred_mode,
                                uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch, void* stream) {
   return b200enc_p_frame_t8(cur_y, cur_uv, cur_pitch, ref_y, ref_uv, ref_pitch, W, H, RW, RH, qp, mv, levels, dc,
-                            nz, pred_mode, rec_y, rec_uv, rec_pitch, 0, stream);
+                            nz, pred_mode, rec_y, rec_uv, rec_pitch, 0, nullptr, stream);
 }
 
 extern "C" int b200enc_p_frame_t8(const uint8_t* cur_y, const uint8_t* cur_uv, int cur_pitch, const uint8_t* ref_y,
                                   const uint8_t* ref_uv, int ref_pitch, int W, int H, int RW, int RH, int qp,
                                   const void* mv, int16_t* levels, int32_t* dc, uint32_t* nz, uint32_t* pred_mode,
-                                  uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch, int t8, void* stream) {
+                                  uint8_t* rec_y, uint8_t* rec_uv, int rec_pitch, int t8, uint8_t* t8_flags,
+                                  void* stream) {
+  if (t8 < 0 || t8 > 2) return -1;
   if (!cur_y || !cur_uv || !ref_y || !ref_uv || !mv || !levels || !dc || !nz || !pred_mode || !rec_y || !rec_uv)
     return -1;
   if (qp < 0 || qp > 51 || W <= 0 || H <= 0 || RW <= 1 || RH <= 1) return -1;
@@ -420,7 +487,7 @@ extern "C" int b200enc_p_frame_t8(const uint8_t* cur_y, const uint8_t* cur_uv, i
   const int T = b200enc_tuned(B200ENC_TUNE_PCHAIN_MBS_PER_CTA) > 0 ? b200enc_tuned(B200ENC_TUNE_PCHAIN_MBS_PER_CTA) : 1;
   p_mb_kernel<false><<<dim3((g.mbw + T - 1) / T, g.mbh), dim3(96, T), T * sizeof(PShared), (cudaStream_t)stream>>>(
       cur_y, cur_uv, cur_pitch, ref_y, ref_uv, ref_pitch, g, qp, (const MV*)mv, levels, dc, nz, pred_mode, rec_y,
-      rec_uv, rec_pitch, BatchTab{}, t8 ? 1 : 0);
+      rec_uv, rec_pitch, BatchTab{}, t8, t8_flags);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -42,6 +42,21 @@ __device__ __forceinline__ void fwd8(int (&s)[8]) {
   s[5] = b6 - (b5 >> 2);
 }
 
+// Unnormalised 8-point Walsh-Hadamard transform (butterflies, natural order
+// of the butterfly network; a cost measure only).
+__device__ __forceinline__ void had8(int (&v)[8]) {
+#pragma unroll
+  for (int h = 1; h < 8; h <<= 1)
+#pragma unroll
+    for (int i = 0; i < 8; i += 2 * h)
+#pragma unroll
+      for (int j = i; j < i + h; ++j) {
+        const int a = v[j], b = v[j + h];
+        v[j] = a + b;
+        v[j + h] = a - b;
+      }
+}
+
 // Inverse 1-D transform of eight values (8.5.13.2).
 __device__ __forceinline__ void inv8(int (&d)[8]) {
   const int a0 = d[0] + d[4], a2 = d[0] - d[4];

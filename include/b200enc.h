@@ -492,9 +492,14 @@ int b200enc_hevc_deblock(const b200enc_hevc_deblock_t *p, void *stream);
  * incomplete and must not be used), -1 = the read failed. */
 int b200enc_wavefront_status(const void *scratch, void *stream);
 
-/* b200enc_p_frame with t8 != 0: the luma of every macroblock through the 8x8
- * transform (High profile, transform_size_8x8_flag) instead of sixteen 4x4
- * ones; chroma unchanged. Levels: the four 8x8 luma blocks in raster order
+/* b200enc_p_frame with the 8x8 luma transform (High profile,
+ * transform_size_8x8_flag): t8 = 0 is b200enc_p_frame, 1 codes the luma of
+ * every macroblock as four 8x8 blocks instead of sixteen 4x4 ones, 2 chooses
+ * per macroblock - the 8x8 transform when the residual's 8x8 Hadamard cost,
+ * sum over the four 8x8 blocks of (sum |H8 R H8| + 2) >> 2, is below its 4x4
+ * one, sum over the sixteen 4x4 blocks of (sum |H4 R H4|) >> 1. t8_flags
+ * (device [mbs], may be NULL) gets each macroblock's choice, the input of
+ * b200enc_deblock_tiles_t8 and b200enc_cavlc_t.t8_flags. Chroma unchanged. Levels: the four 8x8 luma blocks in raster order
  * at levels[mb][0..255] (block q at 64 q, raster within), chroma at
  * [256..383] as before; the nz word of 4x4 block 4q + i (spec order) holds
  * the nonzero mask of the 16 levels CAVLC codes as that block (8x8 scan
@@ -505,7 +510,8 @@ int b200enc_p_frame_t8(const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitc
                        const uint8_t *ref_y, const uint8_t *ref_uv, int ref_pitch,
                        int W, int H, int RW, int RH, int qp, const void *mv,
                        int16_t *levels, int32_t *dc, uint32_t *nz, uint32_t *pred_mode,
-                       uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch, int t8, void *stream);
+                       uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch, int t8, uint8_t *t8_flags,
+                       void *stream);
 
 /* H.264 High-profile 8x8 luma transform (transform_size_8x8_flag). No
  * counterpart in the reference's encoder, which codes 4x4 transforms only;
@@ -564,8 +570,11 @@ typedef struct {
                                     only each slice's bytes cross the bus */
     void *scratch;               /* device, 256-byte aligned */
     size_t scratch_bytes;        /* >= b200enc_cavlc_scratch_bytes(mbw, mbh) */
-    int transform8x8;            /* P slices: the luma of coded macroblocks uses the 8x8 transform (levels and nz
-                                    words as b200enc_p_frame_t8 leaves them; transform_size_8x8_flag is written) */
+    int transform8x8;            /* P slices of a picture parameter set with transform_8x8_mode_flag: every
+                                    macroblock with coded luma carries transform_size_8x8_flag, and its luma uses
+                                    the 8x8 transform (levels and nz words as b200enc_p_frame_t8 leaves them) */
+    const uint8_t *t8_flags;     /* NULL, or device [mbs]: with transform8x8, the per-macroblock choice of
+                                    b200enc_p_frame_t8 (t8 = 2); 0 marks a 4x4 macroblock */
 } b200enc_cavlc_t;
 size_t b200enc_cavlc_scratch_bytes(int mbw, int mbh);
 int b200enc_cavlc_slices(const b200enc_cavlc_t *p, void *stream);

@@ -504,11 +504,76 @@ static void chroma_recon(const orc_frame_t *f, int qpc, const int coef[24][16], 
     for (int sub = 0; sub < 4; sub++) store_rec_chroma(f, rec_uv, rp, Xc, Yc, sub, rec[0][sub], rec[1][sub]);
 }
 
+/* H.264 8x8 frame zig-zag scan (Table 8-13): scan position -> raster 8y+x,
+ * built by walking the anti-diagonals, up-right on even ones and down-left
+ * on odd ones. */
+static void zigzag8(int zz[64])
+{
+    int n = 0;
+    for (int d = 0; d < 15; d++) {
+        const int lo = d > 7 ? d - 7 : 0, hi = d < 7 ? d : 7;
+        for (int k = hi; k >= lo; k--) {
+            const int x = (d & 1) ? k : d - k, y = d - x;
+            zz[n++] = 8 * y + x;
+        }
+    }
+}
+
+/* Sum of |coefficients| of the 2-D Walsh-Hadamard transform of an n x n
+ * block (n = 4 or 8), raster int. */
+static int hadamard_abs(const int *blk, int n)
+{
+    int t[64];
+    for (int i = 0; i < n * n; i++) t[i] = blk[i];
+    for (int pass = 0; pass < 2; pass++)
+        for (int line = 0; line < n; line++)
+            for (int h = 1; h < n; h <<= 1)
+                for (int i = 0; i < n; i += 2 * h)
+                    for (int j = i; j < i + h; j++) {
+                        int *a = pass ? &t[j * n + line] : &t[line * n + j];
+                        int *b = pass ? &t[(j + h) * n + line] : &t[line * n + j + h];
+                        const int u = *a, v = *b;
+                        *a = u + v;
+                        *b = u - v;
+                    }
+    int s = 0;
+    for (int i = 0; i < n * n; i++) s += abs(t[i]);
+    return s;
+}
+
+int orc_t8_choose(const int res[256])
+{
+    /* The luma residual's cost under each transform size, both on the scale
+     * of a sum of absolute differences: 4x4 blocks (sum |H4 R H4|) / 2,
+     * 8x8 blocks (sum |H8 R H8| + 2) / 4 (H4, H8 unnormalised Walsh-Hadamard
+     * matrices); the 8x8 transform when its cost is lower. */
+    int c4 = 0, c8 = 0, b[64];
+    for (int by = 0; by < 4; by++)
+        for (int bx = 0; bx < 4; bx++) {
+            for (int i = 0; i < 16; i++) b[i] = res[(4 * by + (i >> 2)) * 16 + 4 * bx + (i & 3)];
+            c4 += hadamard_abs(b, 4) >> 1;
+        }
+    for (int q = 0; q < 4; q++) {
+        for (int i = 0; i < 64; i++) b[i] = res[(8 * (q >> 1) + (i >> 3)) * 16 + 8 * (q & 1) + (i & 7)];
+        c8 += (hadamard_abs(b, 8) + 2) >> 2;
+    }
+    return c8 < c4;
+}
+
 void orc_p_frame(const orc_frame_t *f,
                  const uint8_t *cur_y, const uint8_t *cur_uv, int cp,
                  const uint8_t *ref_y, const uint8_t *ref_uv, int rfp,
                  const orc_mv_t *mv, orc_out_t *out,
                  uint8_t *rec_y, uint8_t *rec_uv, int rp)
+{
+    orc_p_frame_t8(f, cur_y, cur_uv, cp, ref_y, ref_uv, rfp, mv, out, rec_y, rec_uv, rp, 0, NULL);
+}
+
+void orc_p_frame_t8(const orc_frame_t *f,
+                    const uint8_t *cur_y, const uint8_t *cur_uv, int cp,
+                    const uint8_t *ref_y, const uint8_t *ref_uv, int rfp,
+                    const orc_mv_t *mv, orc_out_t *out,
+                    uint8_t *rec_y, uint8_t *rec_uv, int rp, int t8, uint8_t *t8_flags)
 {
     /* A1/shaders/residual_predict.comp:417-434 (luma MC), :576-635 (chroma
      * MC), dct_transform.comp:75-98, quantize.comp:189-225 (inter f = 1/6),
@@ -538,7 +603,51 @@ void orc_p_frame(const orc_frame_t *f,
                         pred[blk][pos] = pv;
                         res[blk][pos] = srcC(f, cur_uv, cp, pl, Xc + xo, Yc + yo) - pv;
                     }
-            for (int b = 0; b < 24; b++) {
+            /* 8x8 luma (High profile, clause 8.5.13; no counterpart in the
+             * reference's encoder): t8 = 1 always, 2 by orc_t8_choose. */
+            int use8 = t8 == 1;
+            if (t8 == 2) {
+                int r16[256];
+                for (int p = 0; p < 256; p++)
+                    r16[p] = res[((p >> 6) << 2) + ((p & 15) >> 2)][(((p >> 4) & 3) << 2) + (p & 3)];
+                use8 = orc_t8_choose(r16);
+            }
+            if (t8_flags) t8_flags[mb] = (uint8_t)use8;
+            if (use8) {
+                int zz[64];
+                zigzag8(zz);
+                for (int q8 = 0; q8 < 4; q8++) {
+                    const int qx = 8 * (q8 & 1), qy = 8 * (q8 >> 1);
+                    int16_t r8[64], l8[64];
+                    uint8_t p8[64];
+                    for (int i = 0; i < 64; i++) {
+                        const int xx = qx + (i & 7), yy = qy + (i >> 3);
+                        const int blk = (yy >> 2) * 4 + (xx >> 2), pos = (yy & 3) * 4 + (xx & 3);
+                        r8[i] = (int16_t)res[blk][pos];
+                        p8[i] = (uint8_t)pred[blk][pos];
+                    }
+                    orc_fwd_quant8(r8, l8, qp, 0);
+                    /* raster levels over the quadrant's four 16-level slots */
+                    for (int i = 0; i < 64; i++) out->levels[(size_t)mb * 384 + 64 * q8 + i] = l8[i];
+                    /* CAVLC codes the 8x8 block as four 4x4 blocks: block i
+                     * of the quadrant (spec order) holds scan positions
+                     * i, i + 4, ... (7.3.5.3.2); its nz word is their mask */
+                    for (int i = 0; i < 4; i++) {
+                        uint32_t m = 0;
+                        for (int j = 0; j < 16; j++)
+                            if (l8[zz[4 * j + i]]) m |= 1u << j;
+                        const int rb = (qy / 4 + (i >> 1)) * 4 + qx / 4 + (i & 1);
+                        out->nz[(size_t)mb * 24 + rb] = m;
+                        out->dc[(size_t)mb * 24 + rb] = 0;
+                    }
+                    orc_dequant_idct8_add(l8, p8, 8, qp);
+                    for (int i = 0; i < 64; i++) {
+                        const int xx = qx + (i & 7), yy = qy + (i >> 3);
+                        if (X + xx < f->RW && Y + yy < f->RH) rec_y[(size_t)(Y + yy) * rp + X + xx] = p8[i];
+                    }
+                }
+            }
+            for (int b = use8 ? 16 : 0; b < 24; b++) {
                 int q = b < 16 ? qp : qpc;
                 uint32_t nz = 0;
                 orc_forward_4x4(res[b], coef[b]);
@@ -551,7 +660,7 @@ void orc_p_frame(const orc_frame_t *f,
                 out->dc[(size_t)mb * 24 + b] = coef[b][0];
             }
             out->pred_mode[mb] = 2; /* residual_predict.comp:422 */
-            for (int b = 0; b < 16; b++) {
+            for (int b = 0; b < (use8 ? 0 : 16); b++) {
                 int d[16], r[16], v[16];
                 for (int p = 0; p < 16; p++) d[p] = orc_dequant_ac(lev[b][p], p, qp);
                 orc_inverse_4x4(d, r);

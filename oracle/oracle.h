@@ -164,6 +164,21 @@ void orc_set_threads(int n);
  * inverse transform and the add onto a prediction (clause 8.5.13, the
  * decoder side, pinned to the reference decoder's h264d_idct8_add).
  * Coefficients and levels in raster order. */
+/* The P chain with the 8x8 luma transform (High profile; no counterpart in
+ * the reference's encoder): t8 = 0 is orc_p_frame, 1 codes every
+ * macroblock's luma as four 8x8 blocks, 2 chooses per macroblock
+ * (orc_t8_choose). An 8x8 block's levels are raster over the four 16-level
+ * slots of its quadrant; the nz word of each of its 4x4 blocks is the mask of
+ * the 16 levels CAVLC codes as that block; t8_flags (may be NULL) gets each
+ * macroblock's choice. */
+void orc_p_frame_t8(const orc_frame_t *f,
+                    const uint8_t *cur_y, const uint8_t *cur_uv, int cur_pitch,
+                    const uint8_t *ref_y, const uint8_t *ref_uv, int ref_pitch,
+                    const orc_mv_t *mv, orc_out_t *out,
+                    uint8_t *rec_y, uint8_t *rec_uv, int rec_pitch, int t8, uint8_t *t8_flags);
+/* 1 when a macroblock's luma residual (int [16][16] raster) costs less under
+ * the 8x8 transform than under the 4x4 one. */
+int orc_t8_choose(const int res[256]);
 void orc_fwd_quant8(const int16_t res[64], int16_t lev[64], int qp, int intra);
 void orc_dequant_idct8_add(const int16_t lev[64], uint8_t *dst, int stride, int qp);
 

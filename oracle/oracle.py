@@ -150,6 +150,25 @@ def p_frame(f, cur_y, cur_uv, ref_y, ref_uv, mv, rec_y, rec_uv):
     return o
 
 
+def p_frame_t8(f, cur_y, cur_uv, ref_y, ref_uv, mv, rec_y, rec_uv, t8):
+    """The P chain with the 8x8 luma transform (t8 1: every macroblock, 2:
+    chosen per macroblock); returns the outputs and the per-macroblock flags."""
+    o = alloc_outputs(f.mbw * f.mbh)
+    o["mv"][:] = mv
+    flags = np.zeros(f.mbw * f.mbh, np.uint8)
+    lib().orc_p_frame_t8(ctypes.byref(f), _p(cur_y), _p(cur_uv), cur_y.shape[1], _p(ref_y), _p(ref_uv),
+                         ref_y.shape[1], _p(o["mv"]), ctypes.byref(_out_struct(o)), _p(rec_y), _p(rec_uv),
+                         rec_y.shape[1], int(t8), _p(flags))
+    return o, flags
+
+
+def t8_choose(res):
+    """1 when a macroblock's luma residual (int [16][16]) costs less under
+    the 8x8 transform."""
+    r = np.ascontiguousarray(res, np.int32).reshape(256)
+    return int(lib().orc_t8_choose(_p(r)))
+
+
 def i_frame(f, cur_y, cur_uv, rec_y, rec_uv):
     o = alloc_outputs(f.mbw * f.mbh)
     lib().orc_i_frame(ctypes.byref(f), _p(cur_y), _p(cur_uv), cur_y.shape[1], ctypes.byref(_out_struct(o)),

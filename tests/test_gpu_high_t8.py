@@ -2,7 +2,8 @@
 decoded by the reference's decoder.
 
 Every stage runs on the GPU through the C-ABI: full search, the P chain with
-the 8x8 luma transform (b200enc_p_frame_t8), the I16x16 wavefront, tile
+the 8x8 luma transform (b200enc_p_frame_t8; for every macroblock, or chosen
+per macroblock with the flags passed on), the I16x16 wavefront, tile
 deblocking with 8x8-transform macroblocks, and CAVLC slices with
 transform_size_8x8_flag and the four interleaved 4x4 blocks of each 8x8
 block (b200enc_cavlc_slices, transform8x8). The parameter sets (High profile,
@@ -137,7 +138,8 @@ def _i420(nv12_y, nv12_uv, W, H):
 
 @pytest.mark.skipif(not os.path.exists(DEC), reason="oracle/_ref/h264dec not built")
 @pytest.mark.parametrize("W,H,qp,ns,n", [(640, 352, 26, 2, 6), (1280, 720, 33, 4, 5), (320, 192, 18, 1, 5)])
-def test_high_profile_8x8_stream_decodes_to_the_gpu_reconstruction(gpu, tmp_path, W, H, qp, ns, n):
+@pytest.mark.parametrize("t8", [1, 2])
+def test_high_profile_8x8_stream_decodes_to_the_gpu_reconstruction(gpu, tmp_path, W, H, qp, ns, n, t8):
     import torch
     from b200enc import synth
     L = gpu.lib()
@@ -146,8 +148,8 @@ def test_high_profile_8x8_stream_decodes_to_the_gpu_reconstruction(gpu, tmp_path
     seq = synth.Sequence(W, H, seed=qp, pan=True)
     vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
     stream = [_sps(mbw, mbh), _pps(qp)]
-    recons, ref, used8 = [], None, 0
-    ones = torch.ones(mbs, dtype=torch.uint8, device="cuda")
+    recons, ref, used8, n8, n4 = [], None, 0, 0, 0
+    flags = torch.ones(mbs, dtype=torch.uint8, device="cuda")
     for t in range(n):
         cur = gpu.NV12.from_host(*seq.frame(t))
         out = gpu.Outputs(W, H)
@@ -158,26 +160,34 @@ def test_high_profile_8x8_stream_decodes_to_the_gpu_reconstruction(gpu, tmp_path
             gpu.i_frame(cur, W, H, W, H, qp, ns, out, rec, scr)
         else:
             gpu.me_full_search(cur, ref, W, H, W, H, 16, 5, 512, out.mv)
-            assert L.b200enc_p_frame_t8(cur.yp(), cur.uvp(), cur.pitch, ref.yp(), ref.uvp(), ref.pitch, W, H, W, H,
-                                        qp, vp(out.mv), vp(out.levels), vp(out.dc), vp(out.nz), vp(out.pred_mode),
-                                        rec.yp(), rec.uvp(), rec.pitch, 1, None) == 0
+            flags.fill_(7)
+            gpu.p_frame_t8(cur, ref, W, H, W, H, qp, out.mv, out, rec, t8, flags)
         recd = gpu.NV12(W, H)
         st = torch.zeros(4, dtype=torch.int32, device="cuda")
-        assert L.b200enc_deblock_tiles_t8(mbw, mbh, qp, int(idr), vp(out.nz), None if idr else vp(ones),
+        assert L.b200enc_deblock_tiles_t8(mbw, mbh, qp, int(idr), vp(out.nz), None if idr else vp(flags),
                                           vp(out.mv), rec.yp(), rec.uvp(), recd.yp(), recd.uvp(), rec.pitch,
                                           vp(st), None) == 0
         heads = [_slice_header(s * mbs // ns, idr, t) for s in range(ns)]
         slices = gpu.cavlc_slices(mbw, mbh, qp, int(idr), ns, out.levels.data_ptr(), out.dc.data_ptr(),
                                   out.nz.data_ptr(), out.pred_mode.data_ptr(), out.mv.data_ptr(), headers=heads,
-                                  transform8x8=0 if idr else 1)
+                                  transform8x8=0 if idr else 1, t8_flags=None if idr else flags.data_ptr())
         stream += [_nal(3 if idr else 2, 5 if idr else 1, s) for s in slices]
         torch.cuda.synchronize()
         assert st.cpu().tolist()[:2] == [0, 0]
         if not idr:
-            used8 += int((out.nz[:, :16].cpu().numpy() != 0).any(axis=1).sum())
+            f8 = flags.cpu().numpy()
+            assert set(np.unique(f8)) <= {0, 1}
+            coded = (out.nz[:, :16].cpu().numpy() != 0).any(axis=1)
+            used8 += int((coded & (f8 == 1)).sum())
+            n8 += int((f8 == 1).sum())
+            n4 += int((f8 == 0).sum())
         recons.append(_i420(recd.y.cpu().numpy(), recd.uv.cpu().numpy(), W, H))
         ref = recd
     assert used8 > 0  # the P frames did code 8x8 luma blocks
+    if t8 == 1:
+        assert n4 == 0
+    else:  # the per-macroblock choice took both sizes
+        assert n8 > 0 and n4 > 0, (n8, n4)
     path = os.path.join(str(tmp_path), "high8x8.264")
     with open(path, "wb") as f:
         f.write(b"".join(stream))
