@@ -86,7 +86,7 @@ def _sps(mbw, mbh):
     return _nal(3, 7, b.rbsp())
 
 
-def _pps(qp):
+def _pps(qp, t8=True):
     b = _Bits()
     b.ue(0)
     b.ue(0)
@@ -103,7 +103,7 @@ def _pps(qp):
     b.u(1, 1)            # deblocking_filter_control_present
     b.u(1, 0)
     b.u(1, 0)
-    b.u(1, 1)            # transform_8x8_mode_flag
+    b.u(1, int(t8))      # transform_8x8_mode_flag
     b.u(1, 0)
     b.se(0)
     return _nal(3, 8, b.rbsp())
@@ -136,19 +136,20 @@ def _i420(nv12_y, nv12_uv, W, H):
     return nv12_y[:H, :W], nv12_uv[:H // 2, 0:W:2], nv12_uv[:H // 2, 1:W:2]
 
 
-@pytest.mark.skipif(not os.path.exists(DEC), reason="oracle/_ref/h264dec not built")
-@pytest.mark.parametrize("W,H,qp,ns,n", [(640, 352, 26, 2, 6), (1280, 720, 33, 4, 5), (320, 192, 18, 1, 5)])
-@pytest.mark.parametrize("t8", [1, 2])
-def test_high_profile_8x8_stream_decodes_to_the_gpu_reconstruction(gpu, tmp_path, W, H, qp, ns, n, t8):
+def encode_high(gpu, seq, W, H, qp, ns, n, t8):
+    """Encodes n frames of `seq` (IDR, then P frames) on the GPU with the 8x8
+    luma transform mode t8 (0: 4x4 only and no transform_8x8_mode_flag, 1:
+    every macroblock, 2: chosen per macroblock). Returns the Annex B NAL units
+    (SPS, PPS, then each frame's slices), the deblocked reconstructions (I420
+    planes at W x H) and per-P-frame counts (coded 8x8, 8x8, 4x4
+    macroblocks)."""
     import torch
-    from b200enc import synth
     L = gpu.lib()
     mbw, mbh = W // 16, H // 16
     mbs = mbw * mbh
-    seq = synth.Sequence(W, H, seed=qp, pan=True)
     vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
-    stream = [_sps(mbw, mbh), _pps(qp)]
-    recons, ref, used8, n8, n4 = [], None, 0, 0, 0
+    nals = [_sps(mbw, mbh), _pps(qp, t8 != 0)]
+    recons, ref, counts = [], None, []
     flags = torch.ones(mbs, dtype=torch.uint8, device="cuda")
     for t in range(n):
         cur = gpu.NV12.from_host(*seq.frame(t))
@@ -170,37 +171,48 @@ def test_high_profile_8x8_stream_decodes_to_the_gpu_reconstruction(gpu, tmp_path
         heads = [_slice_header(s * mbs // ns, idr, t) for s in range(ns)]
         slices = gpu.cavlc_slices(mbw, mbh, qp, int(idr), ns, out.levels.data_ptr(), out.dc.data_ptr(),
                                   out.nz.data_ptr(), out.pred_mode.data_ptr(), out.mv.data_ptr(), headers=heads,
-                                  transform8x8=0 if idr else 1, t8_flags=None if idr else flags.data_ptr())
-        stream += [_nal(3 if idr else 2, 5 if idr else 1, s) for s in slices]
+                                  transform8x8=0 if idr or t8 == 0 else 1,
+                                  t8_flags=None if idr or t8 == 0 else flags.data_ptr())
+        nals += [_nal(3 if idr else 2, 5 if idr else 1, s) for s in slices]
         torch.cuda.synchronize()
         assert st.cpu().tolist()[:2] == [0, 0]
         if not idr:
             f8 = flags.cpu().numpy()
             assert set(np.unique(f8)) <= {0, 1}
             coded = (out.nz[:, :16].cpu().numpy() != 0).any(axis=1)
-            used8 += int((coded & (f8 == 1)).sum())
-            n8 += int((f8 == 1).sum())
-            n4 += int((f8 == 0).sum())
+            counts.append((int((coded & (f8 == 1)).sum()), int((f8 == 1).sum()), int((f8 == 0).sum())))
         recons.append(_i420(recd.y.cpu().numpy(), recd.uv.cpu().numpy(), W, H))
         ref = recd
-    assert used8 > 0  # the P frames did code 8x8 luma blocks
-    if t8 == 1:
-        assert n4 == 0
-    else:  # the per-macroblock choice took both sizes
-        assert n8 > 0 and n4 > 0, (n8, n4)
-    path = os.path.join(str(tmp_path), "high8x8.264")
-    with open(path, "wb") as f:
-        f.write(b"".join(stream))
+    return nals, recons, counts
+
+
+def decode(path, W, H, n):
     yuv = path + ".yuv"
     r = subprocess.run([DEC, path, yuv], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     data = np.fromfile(yuv, np.uint8)
     fs = W * H * 3 // 2
     assert data.size == n * fs, (data.size, n * fs)
-    for t in range(n):
-        f = data[t * fs:(t + 1) * fs]
-        y, u, v = f[:W * H].reshape(H, W), f[W * H:W * H * 5 // 4].reshape(H // 2, W // 2), f[W * H * 5 // 4:].reshape(H // 2, W // 2)
-        gy, gu, gv = recons[t]
-        np.testing.assert_array_equal(y, gy, err_msg=f"frame {t} luma")
-        np.testing.assert_array_equal(u, gu, err_msg=f"frame {t} Cb")
-        np.testing.assert_array_equal(v, gv, err_msg=f"frame {t} Cr")
+    return [(f[:W * H].reshape(H, W), f[W * H:W * H * 5 // 4].reshape(H // 2, W // 2),
+             f[W * H * 5 // 4:].reshape(H // 2, W // 2)) for f in (data[t * fs:(t + 1) * fs] for t in range(n))]
+
+
+@pytest.mark.skipif(not os.path.exists(DEC), reason="oracle/_ref/h264dec not built")
+@pytest.mark.parametrize("W,H,qp,ns,n", [(640, 352, 26, 2, 6), (1280, 720, 33, 4, 5), (320, 192, 18, 1, 5)])
+@pytest.mark.parametrize("t8", [1, 2])
+def test_high_profile_8x8_stream_decodes_to_the_gpu_reconstruction(gpu, tmp_path, W, H, qp, ns, n, t8):
+    from b200enc import synth
+    seq = synth.Sequence(W, H, seed=qp, pan=True)
+    nals, recons, counts = encode_high(gpu, seq, W, H, qp, ns, n, t8)
+    assert sum(c[0] for c in counts) > 0  # the P frames did code 8x8 luma blocks
+    n8, n4 = sum(c[1] for c in counts), sum(c[2] for c in counts)
+    if t8 == 1:
+        assert n4 == 0
+    else:  # the per-macroblock choice took both sizes
+        assert n8 > 0 and n4 > 0, (n8, n4)
+    path = os.path.join(str(tmp_path), "high8x8.264")
+    with open(path, "wb") as f:
+        f.write(b"".join(nals))
+    for t, (got, want) in enumerate(zip(decode(path, W, H, n), recons)):
+        for plane, a, b in zip("YUV", got, want):
+            np.testing.assert_array_equal(a, b, err_msg=f"frame {t} {plane}")
