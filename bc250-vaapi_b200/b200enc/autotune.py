@@ -58,6 +58,8 @@ def throughput_candidates(name, mbh):
         return [3, 4, 5, 6]
     if name in ("rescore_ctas_per_sm", "fallback_ctas_per_sm"):
         return [4, 8, 12, 16]
+    if name == "deblock_tile_w":  # wider tiles: less margin work per frame, longer chains
+        return [6, 8, 12, 16]
     return candidates(name, mbh)
 
 

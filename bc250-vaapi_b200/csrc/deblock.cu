@@ -670,7 +670,8 @@ __global__ void deblock_kernel(int mbw_, int mbh_, int R, int qp_, int is_intra_
 // instead of one wavefront of mbw + mbh - 1 steps. `dst` must not overlap
 // `src` (neighbouring tiles read each other's samples as their margin).
 // ---------------------------------------------------------------------------
-constexpr int kDbTileMax = 8;  // TW, TH <= 8
+constexpr int kDbTileMax = 8;    // TH <= 8 (a luma and a chroma warp per region row)
+constexpr int kDbTileMaxW = 16;  // TW <= 16 (the width sets shared memory only: 78 KB at 16 x 8)
 
 struct DbTilePlan {
   int sp;  // shared-memory row stride: 16 * (TW + 2) + 4 bytes, an odd word count
@@ -920,7 +921,7 @@ extern "C" int b200enc_deblock(int mbw, int mbh, int qp, int is_intra, const uin
 // autotuner chose otherwise.
 static void db_tile_shape(int* tw, int* th) {
   const int w = b200enc_tuned(B200ENC_TUNE_DEBLOCK_TILE_W), h = b200enc_tuned(B200ENC_TUNE_DEBLOCK_TILE_H);
-  *tw = w > 0 ? std::min(w, kDbTileMax) : 8;
+  *tw = w > 0 ? std::min(w, kDbTileMaxW) : 8;
   *th = h > 0 ? std::min(h, kDbTileMax) : 8;
 }
 
@@ -956,7 +957,7 @@ int b200enc_deblock_tile_count(int mbw, int mbh, int* tw, int* th) {
 int b200enc_deblock_tiles_batch_launch(const BatchTab& bt, int tiles, uint32_t max_wait, cudaStream_t st) {
   if (tiles <= 0) return 0;
   const int TW = bt.db_cols, TH = bt.db_rows;
-  if (TW < 1 || TH < 1 || TW > kDbTileMax || TH > kDbTileMax) return -1;
+  if (TW < 1 || TH < 1 || TW > kDbTileMaxW || TH > kDbTileMax) return -1;
   const DbTilePlan P = db_tile_plan(TW, TH);
   if (cudaFuncSetAttribute(deblock_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.bytes) !=
       cudaSuccess)

@@ -34,7 +34,7 @@ constexpr Knob kKnobs[B200ENC_TUNE_COUNT] = {
     {"fallback_ctas_per_sm", 1, 16},  // persistent fallback full-search grid, CTAs per SM
     {"intra_ctas", 1, 1 << 16},       // CTAs of the intra wavefront (rows in flight)
     {"me_stage", 1, 2},               // full-search window staging: 1 word loads, 2 TMA
-    {"deblock_tile_w", 1, 8},         // tile deblocking: tile width in macroblocks
+    {"deblock_tile_w", 1, 16},        // tile deblocking: tile width in macroblocks
     {"deblock_tile_h", 1, 8},         // tile deblocking: tile height in macroblocks
 };
 

@@ -644,14 +644,23 @@ def run_gpu(args):
         return vals
 
     k1 = max(K, 2 * GOP)
+
+    def one_stream(mode, vals):
+        """The single-stream arm: the tuned values but the built-in deblocking
+        tile (8 x 8, the latency choice; the throughput choice is wider)."""
+        autotune.apply(dict(vals, deblock_tile_w=0, deblock_tile_h=0))
+        r = arm(mode, 1, k1, Wm, perf=True)
+        autotune.apply(vals)
+        return r
+
     vals_l = tune_arm(LEARNED)
     ms_l, launches, _, clk = arm(LEARNED, S, K, Wm, clocks=True)
     ms_b, _, _, _ = arm(1, S, K, Wm)  # the learned form with the network's inference in BF16
-    ms_l1, _, perf_l1, _ = arm(LEARNED, 1, k1, Wm, perf=True)
+    ms_l1, _, perf_l1, _ = one_stream(LEARNED, vals_l)
     me_counts = ctxs[0].me_stats()  # the learned form's last P frame
-    tune_arm(0)
+    vals_p = tune_arm(0)
     ms_p, _, _, _ = arm(0, S, K, Wm)
-    ms_p1, _, perf_p1, _ = arm(0, 1, k1, Wm, perf=True)
+    ms_p1, _, perf_p1, _ = one_stream(0, vals_p)
     mvf = ctxs[0].mv_field()  # the plain form's last P frame: early-outs are MV 0 with SAD <= 512
     autotune.apply(vals_l)  # e2e and the full encode run the learned form
     searched = int(MBS - np.count_nonzero((mvf[:, 0] == 0) & (mvf[:, 1] == 0) & (mvf[:, 2].view(np.uint32) <= 512)))
@@ -759,7 +768,9 @@ def run_gpu(args):
                               "learned_stage_ms_per_p_frame": {k2: round(v, 4) for k2, v in stage_ms.items()},
                               "plain_stage_ms_per_p_frame": {k2: round(v, 4) for k2, v in plain_stage_ms.items()},
                               "stage_ms_per_i_frame": {k2: round(v, 4) for k2, v in intra_ms.items()},
-                              "last_p_frame_mbs": dict(zip(("learned", "fallback", "early"), me_counts))},
+                              "last_p_frame_mbs": dict(zip(("learned", "fallback", "early"), me_counts)),
+                              "deblock_tile": "8 x 8 macroblocks (the latency choice); the 8-stream arms use the "
+                                              "tuned shape in `tune`"},
             "me_int": {"value": round(me_abs / (plain_stage_ms["me"] / 1000.0), 1), "unit": "abs-diff/s",
                        "searched_mbs": searched,
                        "note": f"plain full search, one stream: ({2 * RANGE + 1}^2 + 16) x 256 abs-diffs per searched "

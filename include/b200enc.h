@@ -240,7 +240,7 @@ int b200enc_batch_graph_stats(void *b, long *instantiations, long *updates);
 #define B200ENC_TUNE_FALLBACK_CTAS_PER_SM 3 /* fallback full-search grid, CTAs per SM, 1..16 (default 8) */
 #define B200ENC_TUNE_INTRA_CTAS 4           /* intra wavefront CTAs (rows in flight), >= 1 (default: one per row) */
 #define B200ENC_TUNE_ME_STAGE 5             /* full-search window staging: 1 word loads, 2 TMA (default TMA) */
-#define B200ENC_TUNE_DEBLOCK_TILE_W 6       /* tile deblocking: tile width in macroblocks, 1..8 (default 8) */
+#define B200ENC_TUNE_DEBLOCK_TILE_W 6       /* tile deblocking: tile width in macroblocks, 1..16 (default 8) */
 #define B200ENC_TUNE_DEBLOCK_TILE_H 7       /* tile deblocking: tile height in macroblocks, 1..8 (default 8) */
 #define B200ENC_TUNE_COUNT 8
 /* Sets a knob (0 restores the default); -1 for an unknown key or a value

@@ -64,7 +64,8 @@ def test_deblock_tiles_default_shape(gpu, oracle_mod, mbw, mbh, qp, intra):
     _run(gpu, oracle_mod, mbw, mbh, qp, intra)
 
 
-@pytest.mark.parametrize("tw,th", [(1, 1), (2, 3), (3, 5), (8, 4), (4, 8), (5, 8), (8, 1), (7, 7)])
+@pytest.mark.parametrize("tw,th", [(1, 1), (2, 3), (3, 5), (8, 4), (4, 8), (5, 8), (8, 1), (7, 7), (12, 8), (16, 8),
+                                   (16, 1), (11, 6)])
 @pytest.mark.parametrize("mbw,mbh", [(13, 9), (120, 68)])
 @pytest.mark.parametrize("intra", [0, 1])
 def test_deblock_tiles_every_shape(gpu, oracle_mod, tile_shape, tw, th, mbw, mbh, intra):
