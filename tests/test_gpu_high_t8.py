@@ -61,7 +61,7 @@ def _nal(ref_idc, kind, rbsp):
     return b"\x00\x00\x00\x01" + bytes([(ref_idc << 5) | kind]) + bytes(out)
 
 
-def _sps(mbw, mbh):
+def _sps(mbw, mbh, crop_bottom=0):
     b = _Bits()
     b.u(8, 100)          # profile_idc: High
     b.u(8, 0)
@@ -81,7 +81,12 @@ def _sps(mbw, mbh):
     b.ue(mbh - 1)
     b.u(1, 1)            # frame_mbs_only
     b.u(1, 1)            # direct_8x8_inference
-    b.u(1, 0)
+    b.u(1, int(crop_bottom > 0))
+    if crop_bottom:      # frame cropping, in units of two luma rows (4:2:0 frames)
+        b.ue(0)
+        b.ue(0)
+        b.ue(0)
+        b.ue(crop_bottom // 2)
     b.u(1, 0)
     return _nal(3, 7, b.rbsp())
 
@@ -136,7 +141,7 @@ def _i420(nv12_y, nv12_uv, W, H):
     return nv12_y[:H, :W], nv12_uv[:H // 2, 0:W:2], nv12_uv[:H // 2, 1:W:2]
 
 
-def encode_high(gpu, seq, W, H, qp, ns, n, t8):
+def encode_high(gpu, seq, W, H, qp, ns, n, t8, rng=16):
     """Encodes n frames of `seq` (IDR, then P frames) on the GPU with the 8x8
     luma transform mode t8 (0: 4x4 only and no transform_8x8_mode_flag, 1:
     every macroblock, 2: chosen per macroblock). Returns the Annex B NAL units
@@ -145,10 +150,11 @@ def encode_high(gpu, seq, W, H, qp, ns, n, t8):
     macroblocks)."""
     import torch
     L = gpu.lib()
-    mbw, mbh = W // 16, H // 16
+    CW, CH = gpu.coded(W, H)
+    mbw, mbh = CW // 16, CH // 16
     mbs = mbw * mbh
     vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
-    nals = [_sps(mbw, mbh), _pps(qp, t8 != 0)]
+    nals = [_sps(mbw, mbh, CH - H), _pps(qp, t8 != 0)]
     recons, ref, counts = [], None, []
     flags = torch.ones(mbs, dtype=torch.uint8, device="cuda")
     for t in range(n):
@@ -158,11 +164,11 @@ def encode_high(gpu, seq, W, H, qp, ns, n, t8):
         idr = t == 0
         if idr:
             scr = gpu.scratch(mbh)
-            gpu.i_frame(cur, W, H, W, H, qp, ns, out, rec, scr)
+            gpu.i_frame(cur, W, H, CW, CH, qp, ns, out, rec, scr)
         else:
-            gpu.me_full_search(cur, ref, W, H, W, H, 16, 5, 512, out.mv)
+            gpu.me_full_search(cur, ref, W, H, CW, CH, rng, 5, 512, out.mv)
             flags.fill_(7)
-            gpu.p_frame_t8(cur, ref, W, H, W, H, qp, out.mv, out, rec, t8, flags)
+            gpu.p_frame_t8(cur, ref, W, H, CW, CH, qp, out.mv, out, rec, t8, flags)
         recd = gpu.NV12(W, H)
         st = torch.zeros(4, dtype=torch.int32, device="cuda")
         assert L.b200enc_deblock_tiles_t8(mbw, mbh, qp, int(idr), vp(out.nz), None if idr else vp(flags),
@@ -211,6 +217,26 @@ def test_high_profile_8x8_stream_decodes_to_the_gpu_reconstruction(gpu, tmp_path
     else:  # the per-macroblock choice took both sizes
         assert n8 > 0 and n4 > 0, (n8, n4)
     path = os.path.join(str(tmp_path), "high8x8.264")
+    with open(path, "wb") as f:
+        f.write(b"".join(nals))
+    for t, (got, want) in enumerate(zip(decode(path, W, H, n), recons)):
+        for plane, a, b in zip("YUV", got, want):
+            np.testing.assert_array_equal(a, b, err_msg=f"frame {t} {plane}")
+
+
+@pytest.mark.skipif(not os.path.exists(DEC), reason="oracle/_ref/h264dec not built")
+@pytest.mark.parametrize("qp", [22, 27, 32, 37])
+def test_high_profile_1080p_r32_qp_sweep(gpu, tmp_path, qp):
+    """The High configuration: 1920x1080 IPPP, full search +-32, 4x4 and 8x8
+    transforms chosen per macroblock, deblocking, on the seeded 1080p
+    generator (pan, noise patch); the reference decoder reconstructs every
+    frame exactly as the GPU did."""
+    from b200enc import synth
+    W, H, n = 1920, 1080, 6
+    seq = synth.workload("h264_1080p", seed=0, stream=qp)
+    nals, recons, counts = encode_high(gpu, seq, W, H, qp, 1, n, 2, rng=32)
+    assert sum(c[1] for c in counts) > 0 and sum(c[2] for c in counts) > 0
+    path = os.path.join(str(tmp_path), "high1080.264")
     with open(path, "wb") as f:
         f.write(b"".join(nals))
     for t, (got, want) in enumerate(zip(decode(path, W, H, n), recons)):
