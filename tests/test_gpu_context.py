@@ -202,3 +202,53 @@ def test_registered_host_buffers_upload_without_staging(gpu, oracle_mod):
     torch.cuda.synchronize()
     ctx.destroy_image(img, mem)
     ctx.close()
+
+
+@pytest.mark.parametrize("surfaces", [1, 2])
+def test_uploads_ahead_of_the_encode(gpu, oracle_mod, surfaces):
+    """Frame t+1 is uploaded from page-locked host memory (the call does not
+    wait for the copy) and dispatched before frame t's staged outputs are
+    read - into the other of two surfaces, or into the one surface frame t
+    reads - and every frame's outputs still equal the oracle's sequence: an
+    upload is ordered after the dispatch before it that reads the surface."""
+    import ctypes
+    import torch
+    from b200enc import synth
+    W, H, qp, n = 640, 480, 27, 6
+    seq = synth.workload("h264_640x480", seed=0, stream=21)
+    frames = [seq.frame(t) for t in range(n)]
+    pinned = [(torch.from_numpy(np.ascontiguousarray(y)).pin_memory(),
+               torch.from_numpy(np.ascontiguousarray(uv)).pin_memory()) for y, uv in frames]
+    ctx = gpu.Context()
+    ctx.configure(search_range=16, coded_clamp=True, deblock=1)
+    imgs = [ctx.create_image(W, H) for _ in range(surfaces)]
+    c = ctypes.byref(ctx.ctx)
+    CW, CH = gpu.coded(W, H)
+    f = oracle_mod.frame(W, H, qp)
+
+    def submit(t):
+        img, mem = imgs[t % surfaces]
+        py, puv = pinned[t]
+        assert ctx.L.gpu_compute_upload_nv12(c, ctypes.byref(img), mem, ctypes.c_void_p(py.data_ptr()), W,
+                                             ctypes.c_void_p(puv.data_ptr()), W, W, H) == 0
+        return ctx.encode(img, W, H, qp, t == 0)
+
+    ref_y = ref_uv = None
+    slot = submit(0)
+    for t in range(n):
+        nxt = submit(t + 1) if t + 1 < n else None
+        assert ctx.sync(slot) == 0
+        got = ctx.staging(slot)
+        y, uv = frames[t]
+        rec_y = np.zeros((CH, CW), np.uint8)
+        rec_uv = np.zeros((CH // 2, CW), np.uint8)
+        if ref_y is None:
+            ref_y, ref_uv = _pad(y, CH, CW), _pad(uv, CH // 2, CW)
+        want = oracle_mod.encode_frame(f, 16, 5, 512, t == 0, 1, y, uv, ref_y, ref_uv, rec_y, rec_uv)
+        for k in ("levels", "dc", "nz", "pred_mode", "mv"):
+            np.testing.assert_array_equal(got[k], want[k], err_msg=f"frame {t} {k}")
+        ref_y, ref_uv = rec_y, rec_uv
+        slot = nxt
+    for img, mem in imgs:
+        ctx.destroy_image(img, mem)
+    ctx.close()
