@@ -176,7 +176,7 @@ __device__ __forceinline__ uint32_t qpel_refine(RefineShared& rf, G8F G8, const 
 // which vavgu4 forms for 4 pels at once, and vabsdiff4 accumulates the SAD.
 // Results are identical to qpel_refine.
 struct RefineSimd {
-  int16_t hr[23][18];  // 6-tap sums of 8-bit samples: -2550 .. 10710
+  alignas(4) int16_t hr[23][18];  // 6-tap sums of 8-bit samples: -2550 .. 10710
   alignas(4) uint8_t pl[3][18][20];  // b, h, j at [ry+1][rx+1], ry, rx in -1..16
 };
 
@@ -207,10 +207,29 @@ __device__ __forceinline__ uint32_t qpel_refine_warp_simd(RefineSimd& rf, const 
                                                           int* qx_out, int* qy_out) {
   const int lane = threadIdx.x & 31;
   auto G8 = [&](int rx, int ry) -> int { return g[(g_r0 + ry) * gstride + g_c0 + rx]; };
-  for (int i = lane; i < 23 * 18; i += 32) {
-    const int ry = i / 18 - 3, rx = i % 18 - 1;
-    rf.hr[ry + 3][rx + 1] = G8(rx - 2, ry) - 5 * G8(rx - 1, ry) + 20 * G8(rx, ry) + 20 * G8(rx + 1, ry) -
-                             5 * G8(rx + 2, ry) + G8(rx + 3, ry);
+  // horizontal sums, four columns (rx .. rx+3) per lane and pass: the nine
+  // bytes rx-2 .. rx+6 of the row come from three word loads; the pairs of
+  // 16-bit sums are stored as words (hr rows are 36 bytes, rx+1 is 0 mod 4)
+  for (int i = lane; i < 23 * 5; i += 32) {
+    const int q = i / 5, ry = q - 3, rx = (i - 5 * q) * 4 - 1;
+    const int bo = g_c0 + rx - 2;
+    const uint32_t* wp = reinterpret_cast<const uint32_t*>(g + (g_r0 + ry) * gstride) + (bo >> 2);
+    const int sh = (bo & 3) * 8;
+    const uint32_t a0 = wp[0], a1 = wp[1], a2 = wp[2];
+    const uint32_t lo = __funnelshift_r(a0, a1, sh), hi = __funnelshift_r(a1, a2, sh);
+    int e[9];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      e[k] = (int)((lo >> (8 * k)) & 0xffu);
+      e[k + 4] = (int)((hi >> (8 * k)) & 0xffu);
+    }
+    e[8] = (int)((a2 >> sh) & 0xffu);
+    int v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v[j] = e[j] - 5 * e[j + 1] + 20 * e[j + 2] + 20 * e[j + 3] - 5 * e[j + 4] + e[j + 5];
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&rf.hr[ry + 3][rx + 1]);
+    dst[0] = (uint32_t)(uint16_t)v[0] | ((uint32_t)(uint16_t)v[1] << 16);
+    if (rx + 3 < 17) dst[1] = (uint32_t)(uint16_t)v[2] | ((uint32_t)(uint16_t)v[3] << 16);
   }
   __syncwarp();
   for (int i = lane; i < 18 * 18; i += 32) {
@@ -234,7 +253,7 @@ __device__ __forceinline__ uint32_t qpel_refine_warp_simd(RefineSimd& rf, const 
     if (p == 0) row8(g + (g_r0 + ry) * gstride, g_c0 + rx, w0, w1);
     else row8(&rf.pl[p - 1][ry + 1][0], rx + 1, w0, w1);
   };
-  auto score = [&](int ox, int oy) -> uint32_t {  // SAD at quarter-pel offset (ox, oy) from the winner
+  auto part = [&](int ox, int oy) -> uint32_t {  // the lane's share of the SAD at quarter-pel (ox, oy)
     const int dx = ox >> 2, dy = oy >> 2, ph = (oy & 3) * 4 + (ox & 3);
     uint32_t a0, a1;
     operand(kQpelOp[ph][0], dx, dy, kQpelOp[ph][1], kQpelOp[ph][2], a0, a1);
@@ -244,22 +263,45 @@ __device__ __forceinline__ uint32_t qpel_refine_warp_simd(RefineSimd& rf, const 
       a0 = __vavgu4(a0, b0);
       a1 = __vavgu4(a1, b1);
     }
-    uint32_t sad = sad4_acc(a0, c0, 0u);
-    sad = sad4_acc(a1, c1, sad);
+    return sad4_acc(a1, c1, sad4_acc(a0, c0, 0u));
+  };
+  // The 8 positions (bx, by) + off[c] summed over the warp together: the
+  // exchanges at distances 16, 8 and 4 each hand half of the lane's partial
+  // sums to its partner, so that lane L is left with position (L >> 2) & 7,
+  // and two more finish its sum. Returns min over c of (SAD_c << 3 | c): the
+  // smallest SAD, the earliest position among equal ones.
+  auto best8 = [&](const int8_t(*off)[2], int bx, int by) -> uint32_t {
+    uint32_t v[8];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sad += __shfl_xor_sync(0xffffffffu, sad, o);
-    return sad;
+    for (int c = 0; c < 8; ++c) v[c] = part(bx + off[c][0], by + off[c][1]);
+    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+    uint32_t w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      w[i] = (h16 ? v[i + 4] : v[i]) + __shfl_xor_sync(0xffffffffu, h16 ? v[i] : v[i + 4], 16);
+    uint32_t x[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+      x[i] = (h8 ? w[i + 2] : w[i]) + __shfl_xor_sync(0xffffffffu, h8 ? w[i] : w[i + 2], 8);
+    uint32_t t = (h4 ? x[1] : x[0]) + __shfl_xor_sync(0xffffffffu, h4 ? x[0] : x[1], 4);
+    t += __shfl_xor_sync(0xffffffffu, t, 2);
+    t += __shfl_xor_sync(0xffffffffu, t, 1);
+    return __reduce_min_sync(0xffffffffu, (t << 3) | (uint32_t)((lane >> 2) & 7));
   };
   uint32_t bsad = int_sad;
   int hx = 0, hy = 0;
-  for (int c = 0; c < 8; ++c) {
-    const uint32_t v = score(kHalfOff[c][0], kHalfOff[c][1]);
-    if (v < bsad) { bsad = v; hx = kHalfOff[c][0]; hy = kHalfOff[c][1]; }
+  const uint32_t mh = best8(kHalfOff, 0, 0);
+  if ((mh >> 3) < bsad) {
+    bsad = mh >> 3;
+    hx = kHalfOff[mh & 7][0];
+    hy = kHalfOff[mh & 7][1];
   }
   int qx = 0, qy = 0;
-  for (int c = 0; c < 8; ++c) {
-    const uint32_t v = score(hx + kQtrOff[c][0], hy + kQtrOff[c][1]);
-    if (v < bsad) { bsad = v; qx = kQtrOff[c][0]; qy = kQtrOff[c][1]; }
+  const uint32_t mq = best8(kQtrOff, hx, hy);
+  if ((mq >> 3) < bsad) {
+    bsad = mq >> 3;
+    qx = kQtrOff[mq & 7][0];
+    qy = kQtrOff[mq & 7][1];
   }
   *qx_out = hx + qx;
   *qy_out = hy + qy;

@@ -266,17 +266,22 @@ __global__ void lp_select_kernel(int mbs, LpBuf b, int mode, float param, int la
 // ---------------------------------------------------------------------------
 // One warp per MB, four independent warps per block; every warp walks the
 // learned list on its own and synchronises only itself.
-// Candidate k's patch covers rows cy-5 .. cy+21 and 32 bytes from
-// xa = (X+cx-5) & ~3: the +-2 search window plus the refine's -3..+19 reach
-// around any winner inside that window, so the refine reads no global memory.
-// Rows are kPatchStride = 9 words apart (8 used) and candidates 244 words
-// (20 mod 32): the 25 offsets of two candidates that a warp scores at once
-// then read 32 different banks, where 8-word rows put offsets 0 and 4 rows
-// apart, and the next candidate, on the same banks.
-constexpr int kPatchRows = 27, kPatchStride = 9;  // 8 words used per row
+// Candidate k's patch covers rows cy-5 .. cy+21 and 32 bytes starting
+// exactly at byte X+cx-5 (the staging shifts each row into place): the +-2
+// search window plus the refine's -3..+19 reach around any winner inside
+// that window, so the refine reads no global memory. With the row starting
+// at that byte, integer offset ox of the window begins at byte 3+ox of every
+// patch row whatever the candidate, so the search's byte shifts are
+// compile-time constants. One lane scores a whole row of the window (the 5
+// offsets at one oy) from three 64-bit loads of the patch row and one
+// 128-bit load of the current row per macroblock row. Rows are kPatchStride
+// = 10 words apart (8 used) and candidates kCandWords = 274 words: the 20
+// lanes' 64-bit loads of one instruction then fall on distinct banks in
+// each half-warp phase.
+constexpr int kPatchRows = 27, kPatchStride = 10, kCandWords = 274;  // 8 words used per row
 struct RescoreWarp {
-  uint32_t patch[4][kPatchRows * kPatchStride + 1];
-  uint32_t cur[64];
+  alignas(16) uint32_t patch[4 * kCandWords];
+  alignas(16) uint32_t cur[64];
   int ccx[4], ccy[4];
   RefineSimd rf;
 };
@@ -343,65 +348,93 @@ __global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restri
       }
       sh.cur[i] = v;
     }
-    // one patch row (8 words from xa = (X+cx-5) & ~3) per lane and pass:
-    // three 16-byte loads from xa & ~15 where the 48 bytes lie inside the
-    // row of a 16-byte aligned plane, else the clamped word loads
+    // one patch row (8 words from s = X+cx-5) per lane and pass: three
+    // 16-byte loads from s & ~15 where the 48 bytes lie inside the row of a
+    // 16-byte aligned plane, else the clamped word loads from s & ~3; the
+    // words are then shifted by (s & 3) bytes into place
     for (int t = lane; t < nk * kPatchRows; t += 32) {
       const int k = t / kPatchRows, r = t - k * kPatchRows;
-      const int xa = (X + sh.ccx[k] - 5) & ~3, xa16 = xa & ~15, off = (xa - xa16) >> 2;
+      const int s0 = X + sh.ccx[k] - 5, xa16 = s0 & ~15, sft = (s0 & 3) * 8;
       const uint8_t* rp = ref + (size_t)clampi(Y + sh.ccy[k] - 5 + r, 0, g.RH - 1) * ref_pitch;
-      uint32_t* dst = sh.patch[k] + r * kPatchStride;
+      uint32_t* dst = sh.patch + k * kCandWords + r * kPatchStride;
+      uint32_t v[9];
       if (ref_vec && xa16 >= 0 && xa16 + 48 <= g.RW) {
         const uint4 a = __ldg(reinterpret_cast<const uint4*>(rp + xa16));
         const uint4 b2 = __ldg(reinterpret_cast<const uint4*>(rp + xa16 + 16));
         const uint4 c = __ldg(reinterpret_cast<const uint4*>(rp + xa16 + 32));
         const uint32_t u[12] = {a.x, a.y, a.z, a.w, b2.x, b2.y, b2.z, b2.w, c.x, c.y, c.z, c.w};
-        switch (off) {  // word w of the patch row is u[off + w]
+        switch ((s0 - xa16) >> 2) {  // word w of the aligned row is u[q + w]
           case 0:
 #pragma unroll
-            for (int w = 0; w < 8; ++w) dst[w] = u[w];
+            for (int w = 0; w < 9; ++w) v[w] = u[w];
             break;
           case 1:
 #pragma unroll
-            for (int w = 0; w < 8; ++w) dst[w] = u[w + 1];
+            for (int w = 0; w < 9; ++w) v[w] = u[w + 1];
             break;
           case 2:
 #pragma unroll
-            for (int w = 0; w < 8; ++w) dst[w] = u[w + 2];
+            for (int w = 0; w < 9; ++w) v[w] = u[w + 2];
             break;
           default:
 #pragma unroll
-            for (int w = 0; w < 8; ++w) dst[w] = u[w + 3];
+            for (int w = 0; w < 9; ++w) v[w] = u[w + 3];
             break;
         }
       } else {
 #pragma unroll
-        for (int w = 0; w < 8; ++w) dst[w] = load_word_clamped(rp, xa + 4 * w, g.RW);
+        for (int w = 0; w < 9; ++w) v[w] = load_word_clamped(rp, (s0 & ~3) + 4 * w, g.RW);
       }
+#pragma unroll
+      for (int w = 0; w < 8; w += 2)
+        *reinterpret_cast<uint2*>(dst + w) =
+            make_uint2(__funnelshift_r(v[w], v[w + 1], sft), __funnelshift_r(v[w + 1], v[w + 2], sft));
     }
     __syncwarp();
 
-    // 25 integer offsets per candidate, up to 100 positions over 32 lanes
+    // the 25 integer offsets of each candidate: lane k*5+oy scores the row
+    // of offsets (ox = 0..4, oy) of candidate k
     uint32_t best = 0xffffffffu;
-    for (int pos = lane; pos < nk * 25; pos += 32) {
-      const int k = pos / 25, o = pos - k * 25, oy = o / 5, ox = o - oy * 5;
-      const int cx = sh.ccx[k], cy = sh.ccy[k];
-      const int dx = cx - 2 + ox, dy = cy - 2 + oy;
-      const int xa = (X + cx - 5) & ~3;
-      const int byte0 = (X + dx) - xa;  // 3..10
-      const int w0 = byte0 >> 2, shft = (byte0 & 3) * 8;
-      uint32_t sad = 0;
+    if (lane < nk * 5) {
+      const int k = lane / 5, oy = lane - 5 * k;
+      const uint32_t* prow = sh.patch + k * kCandWords + (oy + 3) * kPatchStride;
+      uint32_t s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
 #pragma unroll 4
       for (int r = 0; r < 16; ++r) {
-        const uint32_t* rw = sh.patch[k] + (oy + 3 + r) * kPatchStride + w0;
-        const uint32_t a0 = rw[0], a1 = rw[1], a2 = rw[2], a3 = rw[3], a4 = rw[4];
-        sad = sad4_acc(__funnelshift_r(a0, a1, shft), sh.cur[r * 4 + 0], sad);
-        sad = sad4_acc(__funnelshift_r(a1, a2, shft), sh.cur[r * 4 + 1], sad);
-        sad = sad4_acc(__funnelshift_r(a2, a3, shft), sh.cur[r * 4 + 2], sad);
-        sad = sad4_acc(__funnelshift_r(a3, a4, shft), sh.cur[r * 4 + 3], sad);
+        const uint2 p0 = *reinterpret_cast<const uint2*>(prow + r * kPatchStride);
+        const uint2 p1 = *reinterpret_cast<const uint2*>(prow + r * kPatchStride + 2);
+        const uint2 p2 = *reinterpret_cast<const uint2*>(prow + r * kPatchStride + 4);
+        const uint4 c = *reinterpret_cast<const uint4*>(sh.cur + 4 * r);
+        const uint32_t u0 = p0.x, u1 = p0.y, u2 = p1.x, u3 = p1.y, u4 = p2.x, u5 = p2.y;
+        s0 = sad4_acc(__funnelshift_r(u0, u1, 24), c.x, s0);  // ox 0: bytes 3..18
+        s0 = sad4_acc(__funnelshift_r(u1, u2, 24), c.y, s0);
+        s0 = sad4_acc(__funnelshift_r(u2, u3, 24), c.z, s0);
+        s0 = sad4_acc(__funnelshift_r(u3, u4, 24), c.w, s0);
+        s1 = sad4_acc(u1, c.x, s1);  // ox 1: bytes 4..19
+        s1 = sad4_acc(u2, c.y, s1);
+        s1 = sad4_acc(u3, c.z, s1);
+        s1 = sad4_acc(u4, c.w, s1);
+        s2 = sad4_acc(__funnelshift_r(u1, u2, 8), c.x, s2);  // ox 2: bytes 5..20
+        s2 = sad4_acc(__funnelshift_r(u2, u3, 8), c.y, s2);
+        s2 = sad4_acc(__funnelshift_r(u3, u4, 8), c.z, s2);
+        s2 = sad4_acc(__funnelshift_r(u4, u5, 8), c.w, s2);
+        s3 = sad4_acc(__funnelshift_r(u1, u2, 16), c.x, s3);  // ox 3: bytes 6..21
+        s3 = sad4_acc(__funnelshift_r(u2, u3, 16), c.y, s3);
+        s3 = sad4_acc(__funnelshift_r(u3, u4, 16), c.z, s3);
+        s3 = sad4_acc(__funnelshift_r(u4, u5, 16), c.w, s3);
+        s4 = sad4_acc(__funnelshift_r(u1, u2, 24), c.x, s4);  // ox 4: bytes 7..22
+        s4 = sad4_acc(__funnelshift_r(u2, u3, 24), c.y, s4);
+        s4 = sad4_acc(__funnelshift_r(u3, u4, 24), c.z, s4);
+        s4 = sad4_acc(__funnelshift_r(u4, u5, 24), c.w, s4);
       }
-      const uint32_t cost = sad + (uint32_t)lambda * (uint32_t)(abs(dx) + abs(dy));
-      best = min(best, (cost << 14) | (uint32_t)((dy + R) * SIDE + (dx + R)));
+      const int dy = sh.ccy[k] - 2 + oy, dx0 = sh.ccx[k] - 2;
+      const uint32_t sads[5] = {s0, s1, s2, s3, s4};
+#pragma unroll
+      for (int ox = 0; ox < 5; ++ox) {
+        const int dx = dx0 + ox;
+        const uint32_t cost = sads[ox] + (uint32_t)lambda * (uint32_t)(abs(dx) + abs(dy));
+        best = min(best, (cost << 14) | (uint32_t)((dy + R) * SIDE + (dx + R)));
+      }
     }
     best = __reduce_min_sync(0xffffffffu, best);
     const int idx = (int)(best & 0x3fffu);
@@ -413,8 +446,8 @@ __global__ void __launch_bounds__(128) lp_rescore_kernel(const uint8_t* __restri
     int kw = 0;
     for (int k = nk - 1; k >= 0; --k)
       if (abs(mx - sh.ccx[k]) <= 2 && abs(my - sh.ccy[k]) <= 2) kw = k;
-    const uint8_t* pb8 = reinterpret_cast<const uint8_t*>(&sh.patch[kw][0]);
-    const int row0 = my - (sh.ccy[kw] - 5), col0 = (X + mx) - ((X + sh.ccx[kw] - 5) & ~3);
+    const uint8_t* pb8 = reinterpret_cast<const uint8_t*>(sh.patch + kw * kCandWords);
+    const int row0 = my - (sh.ccy[kw] - 5), col0 = mx - sh.ccx[kw] + 5;
     int qx, qy;
     const uint32_t bsad =
         qpel_refine_warp_simd(sh.rf, pb8, kPatchStride * 4, row0, col0, sh.cur, int_sad, &qx, &qy);
