@@ -270,10 +270,26 @@ __device__ __forceinline__ uint32_t qpel_refine_warp_simd(RefineSimd& rf, const 
   // sums to its partner, so that lane L is left with position (L >> 2) & 7,
   // and two more finish its sum. Returns min over c of (SAD_c << 3 | c): the
   // smallest SAD, the earliest position among equal ones.
+  // Half-pel positions (kHalfOff order) each read one plane: b at (2,0) and
+  // (-2,0), h at (0,2) and (0,-2), j at the diagonals; the integer offset is
+  // -1 where the quarter-pel offset is -2. Plane and offsets are constants.
+  auto half_part = [&](int c) -> uint32_t {
+    const int p = c < 2 ? 1 : (c < 4 ? 2 : 3);
+    const int dx = (c == 1 || c == 6 || c == 7) ? -1 : 0;
+    const int dy = (c == 3 || c == 5 || c == 7) ? -1 : 0;
+    uint32_t a0, a1;
+    operand(p, dx, dy, 0, 0, a0, a1);
+    return sad4_acc(a1, c1, sad4_acc(a0, c0, 0u));
+  };
   auto best8 = [&](const int8_t(*off)[2], int bx, int by) -> uint32_t {
     uint32_t v[8];
+    if (off == nullptr) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) v[c] = part(bx + off[c][0], by + off[c][1]);
+      for (int c = 0; c < 8; ++c) v[c] = half_part(c);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) v[c] = part(bx + off[c][0], by + off[c][1]);
+    }
     const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
     uint32_t w[4];
 #pragma unroll
@@ -290,7 +306,7 @@ __device__ __forceinline__ uint32_t qpel_refine_warp_simd(RefineSimd& rf, const 
   };
   uint32_t bsad = int_sad;
   int hx = 0, hy = 0;
-  const uint32_t mh = best8(kHalfOff, 0, 0);
+  const uint32_t mh = best8(nullptr, 0, 0);  // the half-pel positions, kHalfOff order
   if ((mh >> 3) < bsad) {
     bsad = mh >> 3;
     hx = kHalfOff[mh & 7][0];
